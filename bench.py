@@ -1,0 +1,335 @@
+"""Benchmark: Fock-build seconds per SCF iteration on one B200 (mixed tensor-core form vs FP64).
+
+One step = one direct-form RCS Fock build (Coulomb + exchange r12 contractions, Fock assembly and
+energy) for the workload's density on its radial x Lebedev grid.  `value` is device time per step
+with every input resident in HBM; `e2e` is the same through the public C ABI from host buffers
+(grid upload, device basis evaluation, Fock build, G/Fock/energy back to the host).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload kr|ne|he]
+                  [--precision bf16x3|fp64|tf32]
+
+Under torchrun (N > 1) every rank runs an independent replica (the Fock build does not shard in
+this design); rank 0 prints the whole-job line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}
+
+
+def load_peaks() -> tuple[dict, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return json.loads(p.read_text()), "measured"
+    return PEAKS_FALLBACK, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while the timed region runs."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def scf_guess_density(basis, Z: int, nocc: int):
+    """Core-Hamiltonian guess (the reference's first iteration: zero density -> F = h), solved with
+    canonical orthogonalisation so that the ill-conditioned even-tempered overlap is handled."""
+    from tcscf_b200 import api
+
+    S, h = api.overlap_core(basis, Z)
+    s, U = np.linalg.eigh(S)
+    keep = s > 1e-10 * s.max()
+    X = U[:, keep] / np.sqrt(s[keep])
+    e, Cp = np.linalg.eigh(X.T @ h @ X)
+    C = X @ Cp[:, :nocc]
+    return (C @ C.T).astype(np.complex128), h
+
+
+def workload(name: str):
+    from tcscf_b200 import basis as wl
+
+    return {"kr": wl.kr, "ne": wl.ne, "he": wl.he}[name]()
+
+
+def cpu_reference(w, grid, D, h, budget_s: float, threads: int | None = None) -> dict:
+    """The reference algorithm (precomputeIntegrand + computeF, then calculateIaa / calculateFai /
+    assembly) timed on the host cores through the oracle port on a sample of r1 rows with the full
+    r2 grid, extrapolated linearly to all rows (rows are independent and of equal cost)."""
+    import oracle
+
+    if threads:
+        oracle.set_threads(threads)
+    cores = oracle.threads()
+    vals2 = oracle.basis_values(grid.points, w.basis)
+    rng = np.random.default_rng(0)
+    # calibrate with one row per thread, then size the sample to the budget
+    rows = cores
+    t_row = None
+    sample_rows = rows
+    for _ in range(2):
+        idx = np.sort(rng.choice(grid.n, sample_rows, replace=False))
+        p1 = np.ascontiguousarray(grid.points[:, idx])
+        t0 = time.perf_counter()
+        F = oracle.compute_F(p1, grid.points, grid.weights, vals2, w.nb)
+        t_pre = time.perf_counter() - t0
+        vals1 = np.ascontiguousarray(vals2[idx])
+        t0 = time.perf_counter()
+        oracle.fock_build(F, vals1, np.ascontiguousarray(grid.weights[idx]), D, h)
+        t_it = time.perf_counter() - t0
+        t_row = (t_pre + t_it) / sample_rows
+        want = int(max(cores, min(grid.n, budget_s / max(t_row, 1e-9))))
+        want = (want // cores) * cores or cores
+        if want <= sample_rows * 1.2:
+            break
+        sample_rows = want
+    scale = grid.n / sample_rows
+    return {"s_per_iter": (t_pre + t_it) * scale, "precompute_s": t_pre * scale, "iteration_s": t_it * scale,
+            "cores": cores, "rows": sample_rows, "sample": f"{sample_rows} of {grid.n} r1 rows x all {grid.n} r2 points, "
+            "precompute form (computeF + Fock iteration), extrapolated linearly to all rows"}
+
+
+def run_reference(args, rank: int) -> None:
+    from tcscf_b200 import grids
+
+    if rank != 0:
+        return
+    w = workload(args.workload)
+    g = grids.product_grid(w.nrad, w.order)
+    D, h = scf_guess_density(w.basis, w.Z, w.n_up)
+    vals = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_reference(w, g, D, h, budget_s=args.ref_seconds)
+        if i >= args.warmup:
+            vals.append(r["s_per_iter"])
+    v = statistics.median(vals)
+    line = {"metric": METRIC, "value": v, "unit": "s/iter", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": f"{w.name} RCS Fock build", "n_points": g.n, "n_basis": w.nb, "n_occ": w.n_up},
+            "cpu_baseline": {"value": v, "unit": "s/iter", "cores": r["cores"], "kind": "port", "sample": r["sample"]},
+            "e2e": {"value": v, "unit": "s/iter", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+METRIC = "Fock-build s/iter, mixed vs FP64 GPU at |dE|<=1 uEh; % of roofline"
+
+
+def run_ours(args, rank: int, world: int) -> None:
+    import torch
+
+    from tcscf_b200 import api, ffi, grids
+
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    prec = {"fp64": ffi.PREC_FP64, "bf16x3": ffi.PREC_BF16X3, "tf32": ffi.PREC_TF32}[args.precision]
+    w = workload(args.workload)
+    g = grids.product_grid(w.nrad, w.order)
+    D, h = scf_guess_density(w.basis, w.Z, w.n_up)
+    peaks, peak_kind = load_peaks()
+
+    ctx = api.Context(local)
+    G = api.QMCGrid(ctx, g)
+    G.setBasisFunctions(w.basis)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
+    dD = torch.from_numpy(D[None].view(np.float64).copy()).to(dev)
+    dH = torch.from_numpy(h).to(dev)
+    dE = torch.zeros(1, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)  # > 126 MB L2
+
+    def step(precision: int) -> None:
+        ffi.check(ffi.lib().tcscf_fock_build_device(ctx.handle, G.id, G.id, 1, dD.data_ptr(), dH.data_ptr(), 1, precision,
+                                                    None, None, dE.data_ptr()), ctx.handle)
+
+    def timed(precision: int, steps: int, warmup: int):
+        for _ in range(warmup):
+            step(precision)
+        torch.cuda.synchronize()
+        ms, contraction, launches = [], [], 0
+        for _ in range(steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            if world > 1:
+                torch.distributed.barrier()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step(precision)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms.append(e0.elapsed_time(e1))
+            c, _, n = ctx.last_timing()
+            contraction.append(c)
+            launches += n
+        return ms, contraction, launches, float(dE.item())
+
+    with ClockSampler(local) as clk:
+        ms, cms, launches, E = timed(prec, args.steps, args.warmup)
+    total_ms = sum(ms)
+    if world > 1:
+        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    s_per_iter = total_ms / 1e3 / (args.steps * world)
+
+    # FP64 comparison (the plain FP64 GPU form) at the same density
+    fp64 = None
+    if prec != ffi.PREC_FP64 and not args.skip_fp64:
+        fsteps = max(1, min(args.steps, args.fp64_steps))
+        fms, fcms, _, E64 = timed(ffi.PREC_FP64, fsteps, 1)
+        fp64 = {"s_per_iter": statistics.median(fms) / 1e3, "energy": E64, "dE_mixed_vs_fp64": E - E64,
+                "contraction_ms": statistics.median(fcms)}
+
+    # end-to-end through the public C ABI from pinned host buffers
+    e2e = None
+    if not args.skip_e2e:
+        pts = torch.from_numpy(g.points).pin_memory().numpy()
+        wts = torch.from_numpy(g.weights).pin_memory().numpy()
+        Dh = torch.from_numpy(D[None].view(np.float64).copy()).pin_memory().numpy().view(np.complex128)
+        e_times = []
+        for i in range(max(1, args.e2e_steps) + 1):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            Gg = api.QMCGrid(ctx, grids.QuadratureGrid(pts, wts))
+            Gg.setBasisFunctions(w.basis)
+            Gm, Fm, Em = api.fock_build(Gg, Gg, Dh, h, precision=prec)
+            Gg.close()
+            torch.cuda.synchronize()
+            if i > 0:
+                e_times.append(time.perf_counter() - t0)
+        nb = w.nb
+        e2e = {"value": statistics.median(e_times), "unit": "s/iter",
+               "h2d_bytes_per_step": int(pts.nbytes + wts.nbytes + Dh.nbytes + h.nbytes),
+               "d2h_bytes_per_step": int(2 * 16 * nb * nb + 8)}
+
+    if rank != 0:
+        return
+    n = g.n
+    flops = 2.0 * n * n * (w.n_up + w.nb + 1)   # rho GEMM (nocc) + exchange GEMM (nb) + Coulomb, per Fock build
+    c_ms = statistics.median(cms)
+    achieved = flops / (c_ms / 1e3) / 1e12
+    if prec == ffi.PREC_FP64:
+        roof = {"bound": "fp64", "achieved": achieved, "peak": args.fp64_peak, "unit": "TFLOP/s", "frac": achieved / args.fp64_peak,
+                "traffic": None, "peak_source": "measured FP64 matmul (DESIGN.md)"}
+    else:
+        peak = peaks["bf16_tflops"]
+        roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                "peak_source": f"bf16 dense burst, {peak_kind}",
+                "issued_tensor_tflops": achieved * 3.0, "issued_frac": achieved * 3.0 / peak}
+    cpu = None
+    if not args.skip_cpu:
+        r = cpu_reference(w, g, D, h, budget_s=args.cpu_seconds)
+        cpu = {"value": r["s_per_iter"], "unit": "s/iter", "cores": r["cores"], "kind": "port", "sample": r["sample"],
+               "precompute_s": r["precompute_s"], "iteration_s": r["iteration_s"]}
+    line = {"metric": METRIC, "value": s_per_iter, "unit": "s/iter", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": total_ms / args.steps, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": {"fp64": "f64", "bf16x3": "bf16x3 (fp32 accumulate, fp64 flush)", "tf32": "tf32"}[args.precision],
+            "data": "synthetic",
+            "config": {"workload": f"{w.name} RCS Fock build (direct form)", "Z": w.Z, "n_points": n, "n_basis": w.nb,
+                       "n_occ": w.n_up, "grid": f"{w.nrad} radial (Gauss-Chebyshev, r=(1+x)/(1-x)) x Lebedev order {w.order}",
+                       "precision": args.precision, "l2": "flushed (256 MB write) between timed steps",
+                       "density": "core-Hamiltonian guess (canonical orthogonalisation)"},
+            "energy": E, "contraction_ms": c_ms, "gpu_launches": launches, "roofline": roof, "fp64": fp64,
+            "speedup_vs_fp64": (fp64["s_per_iter"] / s_per_iter) if fp64 else None,
+            "e2e": e2e, "cpu_baseline": cpu, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="kr", choices=["kr", "ne", "he"])
+    ap.add_argument("--precision", default="bf16x3", choices=["bf16x3", "fp64", "tf32"])
+    ap.add_argument("--fp64-steps", type=int, default=2)
+    ap.add_argument("--fp64-peak", type=float, default=float(os.environ.get("TCSCF_FP64_PEAK_TFLOPS", "37.0")))
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--ref-seconds", type=float, default=10.0)
+    ap.add_argument("--skip-fp64", action="store_true")
+    ap.add_argument("--skip-e2e", action="store_true")
+    ap.add_argument("--skip-cpu", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank)
+        else:
+            run_ours(args, rank, world)
+    finally:
+        if world > 1:
+            import torch
+
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

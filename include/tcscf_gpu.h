@@ -1,0 +1,181 @@
+/*
+ * tcscf_gpu.h — C ABI of libtcscf_gpu.so, the B200 (sm_100a) grid-quadrature Fock build.
+ *
+ * Drop-in boundary for corbett5/tcscf's integral routines (src/integration/integrateAll.hpp,
+ * src/HartreeFock.hpp:23-229) and the per-iteration Fock build / SCF drivers of
+ * src/HartreeFock.cpp.  Plain pointers and sizes only; complex numbers are interleaved
+ * (re, im) doubles exactly like std::complex<double> (src/RAJAInterface.hpp:98-103 relies on that
+ * layout too).  Every entry point returns a tcscf_status; the message of the last failure on a
+ * context is available from tcscf_last_error().
+ *
+ * Layouts (reference index orders, last index contiguous):
+ *   points      [ndim][N]            (integration::QuadratureGrid::points, quadrature.hpp:25-35)
+ *   weights     [N]
+ *   basis vals  [N][nb]              (QMCGrid::basisValues, integrateAll.hpp:139-141); complex for
+ *                                    3-D grids, real for 2-D grids
+ *   basis grads [N][nb][3] complex   (QMCGrid::basisGradients)
+ *   Fji         [N1][nb][nb]         (computeF, HartreeFock.hpp:88-180); complex for a 3-D r2 grid,
+ *                                    real (with the 2*pi of HartreeFock.hpp:123) for a 2-D r2 grid
+ *   Vji         [N1][nb][nb][3] complex (computeV, HartreeFock.hpp:185-229)
+ *   density, G, Fock [nspin][nb][nb] complex, element (j,i) at [s][j][i] (row-major; the reference's
+ *                                    fockOperator is PERM_IKJ, i.e. its transpose per spin)
+ *   S, H        [nb][nb] real row-major
+ *
+ * Threading: one context per host thread; calls on a context are not reentrant.  All device work
+ * of a context runs on its own CUDA stream (tcscf_ctx_stream).
+ */
+#ifndef TCSCF_GPU_H
+#define TCSCF_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum tcscf_status {
+  TCSCF_OK = 0,
+  TCSCF_ERR_INVALID_ARGUMENT = 1, /* LVARRAY_ERROR_IF_NE / CHECK_BOUNDS_* in the reference */
+  TCSCF_ERR_CUDA = 2,
+  TCSCF_ERR_TIMEOUT = 3,          /* a bounded device wait gave up */
+  TCSCF_ERR_NONFINITE = 4,        /* NaN/Inf in an energy or Fock matrix */
+  TCSCF_ERR_NOT_CONVERGED = 5,    /* tcscf::ConvergenceError (HartreeFock.hpp:13-19) */
+  TCSCF_ERR_LINALG = 6,           /* LvArray::dense::Error (eigen-solve failure) */
+  TCSCF_ERR_UNSUPPORTED = 7,      /* shape or feature outside what this build implements */
+  TCSCF_ERR_NO_DEVICE = 8
+} tcscf_status;
+
+/* Slater-type orbital (SlaterTypeOrbital.hpp:27-37): alpha = orbital exponent zeta. */
+typedef struct tcscf_sto {
+  double alpha;
+  int32_t n, l, m, pad;
+} tcscf_sto;
+
+/* Ochi / Boys-Handy Jastrow factor (jastrowFunctions.hpp:9-115):
+ * u = sum_k c[k][same] * (r12/(r12+a12))^S[k][0] * (r1/(r1+a))^S[k][1] * (r2/(r2+a))^S[k][2];
+ * c[k][0] is the opposite-spin and c[k][1] the same-spin coefficient. */
+typedef struct tcscf_ochi {
+  double a, a12;
+  int32_t nterms, pad;
+  int32_t S[8][3];
+  double c[8][2];
+} tcscf_ochi;
+
+/* r12 kernels: the lambdas of src/unitTests/HartreeFockTest.cpp:248-253 (1/r12), :276-296
+ * (TC scalar 2/r12 - |grad_1 u(r1,r2)|^2 - |grad_1 u(r2,r1)|^2) and :300-318 (grad_1 u). An exactly
+ * coincident pair r1 == r2 contributes 0 in every kernel. */
+typedef enum tcscf_kernel {
+  TCSCF_K_INV_R12 = 0,
+  TCSCF_K_TC_SCALAR_SAME = 1,
+  TCSCF_K_TC_SCALAR_OPPO = 2,
+  TCSCF_K_GRAD_U_SAME = 3,
+  TCSCF_K_GRAD_U_OPPO = 4
+} tcscf_kernel;
+
+/* Precision of the r12 contraction.  FP64: CUDA-core FP64 throughout.  BF16X3: tcgen05 tensor
+ * cores with hi+lo BF16 operand pairs (3 products), FP32 accumulation in TMEM, flushed into FP64.
+ * TF32: tcgen05 kind::tf32, one product, FP32 accumulation flushed into FP64. */
+typedef enum tcscf_precision {
+  TCSCF_PREC_FP64 = 0,
+  TCSCF_PREC_BF16X3 = 1,
+  TCSCF_PREC_TF32 = 2
+} tcscf_precision;
+
+/* radial changes of variables (changeOfVariables.hpp:8-232); TCSCF_MAP_ONE_PLUS_X is
+ * r = (1+x)/(1-x) (jacobian 2/(1-x)^2), which the reference does not have. */
+typedef enum tcscf_map {
+  TCSCF_MAP_NONE = 0,
+  TCSCF_MAP_LINEAR = 1,             /* p0 = scale */
+  TCSCF_MAP_X_OVER_1MX = 2,
+  TCSCF_MAP_TREUTLER_AHLRICHS_M4 = 3, /* p0 = a, p1 = epsilon */
+  TCSCF_MAP_ONE_PLUS_X = 4
+} tcscf_map;
+
+typedef struct tcscf_ctx tcscf_ctx;
+
+/* ---- context -------------------------------------------------------------------------------- */
+int tcscf_ctx_create(int device, tcscf_ctx ** ctx);
+int tcscf_ctx_destroy(tcscf_ctx * ctx);
+const char * tcscf_last_error(tcscf_ctx * ctx);
+/* the context's cudaStream_t, for callers that time or order work around it */
+int tcscf_ctx_stream(tcscf_ctx * ctx, void ** stream);
+int tcscf_synchronize(tcscf_ctx * ctx);
+/* device time in ms of the dominant r12 contraction kernel(s) of the most recent Fock build /
+ * computeF call, measured with CUDA events on the context stream; launches = kernels launched */
+int tcscf_last_timing(tcscf_ctx * ctx, double * contraction_ms, double * total_ms, int * launches);
+/* accumulation window of the tensor-core paths: r2 blocks of 64 accumulated in FP32 in TMEM before
+ * being flushed into FP64 (default 4); 1 flushes every block */
+int tcscf_set_flush_window(tcscf_ctx * ctx, int blocks);
+
+/* ---- host-side grid generation (replaces ChebyshevGauss/changeOfVariables/createGrid,
+ *      TreutlerAhlrichsLebedev and QMCGrid's point mapping) ---------------------------------- */
+/* createGrid(ChebyshevGauss(n), map) (quadrature.hpp:75-102): abscissae u[n], weights w[n] */
+int tcscf_grid_radial(int n, int map, double p0, double p1, double * u, double * w);
+/* radial x angular product grid, index ir*nang + ia; ang = nang x {theta, phi, weight} (the
+ * reference's Lebedev table layout, src/integration/data/LebedevData_*.hpp); weight r^2 w_r w_ang
+ * (TreutlerAhlrichsLebedev.hpp:46-74 with the caller's r^2). pts [3][N], w [N]. */
+int tcscf_grid_product(int nrad, const double * r, const double * wr, int nang, const double * ang, double * pts, double * w);
+/* QMCGrid<REAL,NDIM> point mapping (integrateAll.hpp:21-65, qmcWrapper.hpp:128-136) of unit-cube
+ * points u [ndim][N]: TA-M4(a=0, eps=0.9) radius, theta = acos(1-2u), phi = 2 pi u, weight
+ * jacobian * r^2 sin(theta) / N.  ndim 2 gives (x, z) rows. */
+int tcscf_grid_qmc(int ndim, int64_t n, const double * u, double * pts, double * w);
+/* seeded scrambled Sobol points in [0,1)^ndim (ndim <= 3), layout [ndim][n]; replaces the
+ * un-vendored mppmu/qmc lattice generator (qmcWrapper.hpp:94-141). */
+int tcscf_sobol(int ndim, int64_t n, uint64_t seed, double * u);
+
+/* ---- analytic one-electron matrices (SlaterTypeOrbital.hpp:134-181) -------------------------- */
+int tcscf_overlap_core_analytic(const tcscf_sto * basis, int nb, int Z, double * S, double * H);
+
+/* ---- device-resident grids (QMCGrid, integrateAll.hpp:12-142) ------------------------------- */
+/* copies points [ndim][n] and weights [n] from host memory; ndim 2 or 3 */
+int tcscf_grid_create(tcscf_ctx * ctx, const double * points, const double * weights, int64_t n, int ndim, int * grid);
+int tcscf_grid_destroy(tcscf_ctx * ctx, int grid);
+/* QMCGrid::setBasisFunctions (integrateAll.hpp:88-137): evaluates the STOs (and gradients) on the
+ * device.  The basis must contain the -m partner of every m != 0 function. */
+int tcscf_grid_set_basis(tcscf_ctx * ctx, int grid, const tcscf_sto * basis, int nb, int gradients);
+/* copies QMCGrid::basisValues / basisGradients to host buffers (either may be NULL) */
+int tcscf_grid_basis_values(tcscf_ctx * ctx, int grid, double * values, double * gradients);
+
+/* quadrature S_ij = sum_g w phi_i^* phi_j and H_ij = sum_g w (1/2 grad phi_i^* . grad phi_j - Z phi_i^* phi_j / r)
+ * on a 3-D grid with gradients; S, H complex [nb][nb] */
+int tcscf_overlap_core_quadrature(tcscf_ctx * ctx, int grid, int Z, double * S, double * H);
+
+/* ---- r12 kernel contractions (precompute form) --------------------------------------------- */
+/* precomputeIntegrand + computeF (HartreeFock.hpp:23-180): F written to host memory in the Fji
+ * layout (complex for a 3-D r2 grid, real x 2 pi for a 2-D r2 grid).  When keep != 0 the result also
+ * stays on the device as handle *fji for tcscf_fock_build_precomputed. */
+int tcscf_compute_F(tcscf_ctx * ctx, int r1, int r2, int kernel, const tcscf_ochi * jastrow, double * F, int keep, int * fji);
+/* precomputeIntegrand + computeV (HartreeFock.hpp:55-83, :185-229), vector kernels only */
+int tcscf_compute_V(tcscf_ctx * ctx, int r1, int r2, int kernel, const tcscf_ochi * jastrow, double * V, int keep, int * vji);
+int tcscf_tensor_destroy(tcscf_ctx * ctx, int handle);
+
+/* ---- per-iteration Fock build ---------------------------------------------------------------- */
+/* Direct form: G from the density without any stored Fji.  Same result as calculateIaa /
+ * calculateFai / assembly (HartreeFock.cpp:817-843 RCS, :925-956 UOS) on Fji = computeF(r1, r2,
+ * 1/r12), followed by enforceOneElectronSymmetry (when respect_symmetry) and constructSCFOperator
+ * (HartreeFock.cpp:48-98).  nspin 1 (RCS, energy x2) or 2 (UOS).  h real [nb][nb].
+ * Outputs (any may be NULL): G, Fock [nspin][nb][nb] complex, energy. */
+int tcscf_fock_build(tcscf_ctx * ctx, int r1, int r2, int nspin, const double * density, const double * h,
+                     int respect_symmetry, int precision, double * G, double * fock, double * energy);
+/* Same as tcscf_fock_build with density, h, G, fock and energy in device memory (G / fock may be
+ * NULL); the work is ordered on the context stream, which is synchronised before returning. */
+int tcscf_fock_build_device(tcscf_ctx * ctx, int r1, int r2, int nspin, const double * density, const double * h,
+                            int respect_symmetry, int precision, double * G, double * fock, double * energy);
+/* Same, from a device-resident Fji handle (the reference's precompute form). */
+int tcscf_fock_build_precomputed(tcscf_ctx * ctx, int r1, int fji, int nspin, const double * density, const double * h,
+                                 int respect_symmetry, double * G, double * fock, double * energy);
+
+/* ---- SCF drivers (RCSHartreeFock/UOSHartreeFock::compute, HartreeFock.cpp:785-1003) ---------- */
+/* Zero initial density, Fock build (direct form at `precision`), FP64 generalized Hermitian
+ * eigen-solve on the device (upper triangle, as LAPACK zhegvd in the reference), new density,
+ * until |dE| < tol or max_iter.  S real [nb][nb].  Outputs: energy, iterations, density, eigenvalues
+ * [nspin][nb].  Returns TCSCF_ERR_NOT_CONVERGED after max_iter. */
+int tcscf_scf(tcscf_ctx * ctx, int r1, int r2, int nspin, int n_up, int n_down, const double * S, const double * h,
+              int respect_symmetry, int precision, double tol, int max_iter, double * energy, int * iterations,
+              double * density, double * eigenvalues);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TCSCF_GPU_H */

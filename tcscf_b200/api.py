@@ -1,0 +1,276 @@
+"""Host-side mirror of tcscf's integral / SCF interface, driving libtcscf_gpu.so.
+
+Names follow the reference: QMCGrid.setBasisFunctions (src/integration/integrateAll.hpp:88-137),
+computeF / computeV (src/HartreeFock.hpp:88-229), RCSHartreeFock / UOSHartreeFock::compute
+(src/HartreeFock.hpp:233-349), overlap / coreMatrixElement (src/SlaterTypeOrbital.hpp:134-181).
+Errors are raised as ffi.TcscfError carrying the C status; ConvergenceError mirrors
+tcscf::ConvergenceError (src/HartreeFock.hpp:13-19).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import ffi
+from .grids import QuadratureGrid
+
+
+class ConvergenceError(ffi.TcscfError):
+    pass
+
+
+class LinearAlgebraError(ffi.TcscfError):
+    pass
+
+
+def _raise(code: int, ctx) -> None:
+    if code == ffi.OK:
+        return
+    msg = ffi.lib().tcscf_last_error(ctx).decode()
+    if code == ffi.ERR_NOT_CONVERGED:
+        raise ConvergenceError(code, msg)
+    if code == ffi.ERR_LINALG:
+        raise LinearAlgebraError(code, msg)
+    raise ffi.TcscfError(code, msg)
+
+
+class Context:
+    """One tcscf_ctx (device, stream, cuSOLVER handle, device-resident grids)."""
+
+    def __init__(self, device: int = 0):
+        self._h = C.c_void_p()
+        code = ffi.lib().tcscf_ctx_create(device, C.byref(self._h))
+        if code != ffi.OK:
+            raise ffi.TcscfError(code, "tcscf_ctx_create failed (a B200 / sm_100 device is required)")
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self) -> None:
+        if self._h:
+            ffi.lib().tcscf_ctx_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def stream(self) -> int:
+        s = C.c_void_p()
+        _raise(ffi.lib().tcscf_ctx_stream(self._h, C.byref(s)), self._h)
+        return s.value or 0
+
+    def synchronize(self) -> None:
+        _raise(ffi.lib().tcscf_synchronize(self._h), self._h)
+
+    def last_timing(self) -> tuple[float, float, int]:
+        a, b, n = C.c_double(), C.c_double(), C.c_int()
+        _raise(ffi.lib().tcscf_last_timing(self._h, C.byref(a), C.byref(b), C.byref(n)), self._h)
+        return a.value, b.value, n.value
+
+    def set_flush_window(self, blocks: int) -> None:
+        _raise(ffi.lib().tcscf_set_flush_window(self._h, blocks), self._h)
+
+
+class QMCGrid:
+    """Device-resident integration::QMCGrid built from a host QuadratureGrid (points already Cartesian)."""
+
+    def __init__(self, ctx: Context, grid: QuadratureGrid):
+        self.ctx = ctx
+        self.quadratureGrid = grid
+        self._id = C.c_int()
+        pts = np.ascontiguousarray(grid.points, dtype=np.float64)
+        w = np.ascontiguousarray(grid.weights, dtype=np.float64)
+        _raise(ffi.lib().tcscf_grid_create(ctx.handle, ffi.dptr(pts), ffi.dptr(w), grid.n, grid.ndim, C.byref(self._id)), ctx.handle)
+        self.basis: list = []
+        self.gradients = False
+
+    @property
+    def id(self) -> int:
+        return self._id.value
+
+    def nGrid(self) -> int:
+        return self.quadratureGrid.n
+
+    def nBasis(self) -> int:
+        return len(self.basis)
+
+    def setBasisFunctions(self, basis, storeGradients: bool = False) -> None:
+        arr = ffi.sto_array(basis)
+        _raise(ffi.lib().tcscf_grid_set_basis(self.ctx.handle, self.id, arr, len(basis), int(storeGradients)), self.ctx.handle)
+        self.basis = list(basis)
+        self.gradients = bool(storeGradients)
+
+    @property
+    def basisValues(self) -> np.ndarray:
+        n, nb = self.nGrid(), self.nBasis()
+        out = np.empty((n, nb), dtype=np.complex128 if self.quadratureGrid.ndim == 3 else np.float64)
+        _raise(ffi.lib().tcscf_grid_basis_values(self.ctx.handle, self.id, ffi.dptr(out), None), self.ctx.handle)
+        return out
+
+    @property
+    def basisGradients(self) -> np.ndarray:
+        n, nb = self.nGrid(), self.nBasis()
+        out = np.empty((n, nb, 3), dtype=np.complex128)
+        _raise(ffi.lib().tcscf_grid_basis_values(self.ctx.handle, self.id, None, ffi.dptr(out)), self.ctx.handle)
+        return out
+
+    def close(self) -> None:
+        if self._id.value:
+            ffi.lib().tcscf_grid_destroy(self.ctx.handle, self.id)
+            self._id = C.c_int()
+
+
+def overlap_core(basis, Z: int) -> tuple[np.ndarray, np.ndarray]:
+    """Analytic overlap and core-Hamiltonian matrices (SlaterTypeOrbital.hpp:134-181)."""
+    nb = len(basis)
+    S = np.empty((nb, nb))
+    H = np.empty((nb, nb))
+    ffi.check(ffi.lib().tcscf_overlap_core_analytic(ffi.sto_array(basis), nb, Z, ffi.dptr(S), ffi.dptr(H)))
+    return S, H
+
+
+def overlap_core_quadrature(grid: QMCGrid, Z: int) -> tuple[np.ndarray, np.ndarray | None]:
+    nb = grid.nBasis()
+    S = np.empty((nb, nb), dtype=np.complex128)
+    H = np.empty((nb, nb), dtype=np.complex128) if grid.gradients else None
+    _raise(ffi.lib().tcscf_overlap_core_quadrature(grid.ctx.handle, grid.id, Z, ffi.dptr(S), ffi.dptr(H)), grid.ctx.handle)
+    return S, H
+
+
+class DeviceTensor:
+    def __init__(self, ctx: Context, handle: int):
+        self.ctx, self.handle = ctx, handle
+
+    def close(self) -> None:
+        if self.handle:
+            ffi.lib().tcscf_tensor_destroy(self.ctx.handle, self.handle)
+            self.handle = 0
+
+
+def computeF(r1Grid: QMCGrid, r2Grid: QMCGrid, kernel: int = ffi.K_INV_R12, jastrow: ffi.Ochi | None = None,
+             keep: bool = False, copy: bool = True):
+    """precomputeIntegrand + computeF: Fji [N1][nb][nb] (complex for a 3-D r2 grid, real x 2 pi for 2-D)."""
+    ctx = r1Grid.ctx
+    n1, nb = r1Grid.nGrid(), r1Grid.nBasis()
+    F = None
+    if copy:
+        F = np.empty((n1, nb, nb), dtype=np.complex128 if r2Grid.quadratureGrid.ndim == 3 else np.float64)
+    h = C.c_int()
+    _raise(ffi.lib().tcscf_compute_F(ctx.handle, r1Grid.id, r2Grid.id, kernel, C.byref(jastrow) if jastrow else None,
+                                     ffi.dptr(F), int(keep), C.byref(h)), ctx.handle)
+    return (F, DeviceTensor(ctx, h.value)) if keep else F
+
+
+def computeV(r1Grid: QMCGrid, r2Grid: QMCGrid, kernel: int, jastrow: ffi.Ochi, keep: bool = False, copy: bool = True):
+    """precomputeIntegrand + computeV: Vji [N1][nb][nb][3] complex."""
+    ctx = r1Grid.ctx
+    n1, nb = r1Grid.nGrid(), r1Grid.nBasis()
+    V = np.empty((n1, nb, nb, 3), dtype=np.complex128) if copy else None
+    h = C.c_int()
+    _raise(ffi.lib().tcscf_compute_V(ctx.handle, r1Grid.id, r2Grid.id, kernel, C.byref(jastrow), ffi.dptr(V), int(keep),
+                                     C.byref(h)), ctx.handle)
+    return (V, DeviceTensor(ctx, h.value)) if keep else V
+
+
+def _check_shapes(D: np.ndarray, h: np.ndarray, nb: int) -> None:
+    """CHECK_BOUNDS_3(density, nSpin, nBasis, nBasis) / CHECK_BOUNDS_2(oneElectronTerms, nBasis, nBasis)."""
+    if D.ndim != 3 or D.shape[0] not in (1, 2) or D.shape[1:] != (nb, nb) or h.shape != (nb, nb):
+        raise ffi.TcscfError(ffi.ERR_INVALID_ARGUMENT, f"density {D.shape} / h {h.shape} do not match nBasis {nb}")
+
+
+def fock_build(r1Grid: QMCGrid, r2Grid: QMCGrid, density: np.ndarray, h: np.ndarray, respect_symmetry: bool = True,
+               precision: int = ffi.PREC_FP64):
+    """Direct-form Fock build: density [nspin][nb][nb] complex -> (G, Fock, energy)."""
+    ctx = r1Grid.ctx
+    D = np.ascontiguousarray(density, dtype=np.complex128)
+    if D.ndim == 2:
+        D = D[None]
+    nspin, nb = D.shape[0], r1Grid.nBasis()
+    hh = np.ascontiguousarray(h, dtype=np.float64)
+    _check_shapes(D, hh, nb)
+    G = np.empty((nspin, nb, nb), dtype=np.complex128)
+    F = np.empty((nspin, nb, nb), dtype=np.complex128)
+    e = C.c_double()
+    _raise(ffi.lib().tcscf_fock_build(ctx.handle, r1Grid.id, r2Grid.id, nspin, ffi.dptr(D), ffi.dptr(hh), int(respect_symmetry),
+                                      precision, ffi.dptr(G), ffi.dptr(F), C.byref(e)), ctx.handle)
+    return G, F, e.value
+
+
+def fock_build_precomputed(r1Grid: QMCGrid, Fji: DeviceTensor, density: np.ndarray, h: np.ndarray, respect_symmetry: bool = True):
+    ctx = r1Grid.ctx
+    D = np.ascontiguousarray(density, dtype=np.complex128)
+    if D.ndim == 2:
+        D = D[None]
+    nspin, nb = D.shape[0], r1Grid.nBasis()
+    hh = np.ascontiguousarray(h, dtype=np.float64)
+    _check_shapes(D, hh, nb)
+    G = np.empty((nspin, nb, nb), dtype=np.complex128)
+    F = np.empty((nspin, nb, nb), dtype=np.complex128)
+    e = C.c_double()
+    _raise(ffi.lib().tcscf_fock_build_precomputed(ctx.handle, r1Grid.id, Fji.handle, nspin, ffi.dptr(D), ffi.dptr(hh),
+                                                  int(respect_symmetry), ffi.dptr(G), ffi.dptr(F), C.byref(e)), ctx.handle)
+    return G, F, e.value
+
+
+class _SCF:
+    nspin = 1
+
+    def __init__(self, numSpinUp: int, numSpinDown: int, numBasisFunctions: int):
+        self.nElectrons = (numSpinUp, numSpinDown)
+        self.basisSize = numBasisFunctions
+        self.density = np.zeros((self.nspin, numBasisFunctions, numBasisFunctions), dtype=np.complex128)
+        self.eigenvalues = np.zeros((self.nspin, numBasisFunctions))
+        self._iter = 0
+
+    def numberOfConvergenceLoops(self) -> int:
+        return self._iter
+
+    def compute(self, overlap: np.ndarray, oneElectronTerms: np.ndarray, r1Grid: QMCGrid, r2Grid: QMCGrid,
+                respectOneElectronSymmetry: bool = True, precision: int = ffi.PREC_FP64, tol: float = 1e-5,
+                max_iter: int | None = None) -> float:
+        ctx = r1Grid.ctx
+        S = np.ascontiguousarray(np.real(overlap), dtype=np.float64)
+        hh = np.ascontiguousarray(oneElectronTerms, dtype=np.float64)
+        nb = r1Grid.nBasis()
+        if S.shape != (nb, nb) or hh.shape != (nb, nb) or nb != self.basisSize:
+            raise ffi.TcscfError(ffi.ERR_INVALID_ARGUMENT, "overlap / oneElectronTerms do not match nBasis")
+        e = C.c_double()
+        it = C.c_int()
+        code = ffi.lib().tcscf_scf(ctx.handle, r1Grid.id, r2Grid.id, self.nspin, self.nElectrons[0], self.nElectrons[1],
+                                   ffi.dptr(S), ffi.dptr(hh), int(respectOneElectronSymmetry), precision, tol,
+                                   max_iter or self.max_iter, C.byref(e), C.byref(it), ffi.dptr(self.density),
+                                   ffi.dptr(self.eigenvalues))
+        self._iter = it.value
+        _raise(code, ctx.handle)
+        return e.value
+
+
+class RCSHartreeFock(_SCF):
+    """RCSHartreeFock (HartreeFock.hpp:233-293): restricted closed shell, at most 50 iterations."""
+
+    nspin = 1
+    max_iter = 50
+
+    def highestOccupiedOrbitalEnergy(self) -> float:
+        return float(self.eigenvalues[0, sum(self.nElectrons) // 2 - 1])
+
+
+class UOSHartreeFock(_SCF):
+    """UOSHartreeFock (HartreeFock.hpp:297-349): unrestricted open shell, at most 100 iterations."""
+
+    nspin = 2
+    max_iter = 100
+
+    def highestOccupiedOrbitalEnergy(self) -> float:
+        return float(max(self.eigenvalues[0, self.nElectrons[0] - 1], self.eigenvalues[1, self.nElectrons[1] - 1]))

@@ -1,0 +1,142 @@
+// Shared declarations of libtcscf_gpu.so: the context, device-resident grids and tensors, error
+// plumbing and small device helpers.  Everything here is product code for sm_100a.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cusolverDn.h>
+#include <cstdint>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/tcscf_gpu.h"
+
+namespace tcscf {
+
+constexpr int kMaxL = 12;            // highest angular momentum the device basis evaluator accepts
+constexpr double kPi = 3.141592653589793238462643383279502884;
+
+// Per basis function data the device evaluators read (SlaterTypeOrbital.hpp:27-37 fields plus the
+// real-harmonic type used by the tensor paths).
+struct DevSto {
+  double alpha, norm;
+  int n, l, m;
+  int rtype;    // 0: m == 0, 1: cos-type (m > 0), 2: sin-type (m < 0)
+  int partner;  // index of the -m function (-1 for m == 0)
+  int pad;
+};
+
+struct MixedOperands;  // tensor-core operand cache of a grid (flash_tc.cu)
+
+struct Grid {
+  int64_t n = 0;
+  int ndim = 3;
+  double * pts = nullptr;   // [3][n] Cartesian (y row zero for 2-D grids)
+  double * w = nullptr;     // [n]
+  // basis
+  int nb = 0;
+  int hasGrad = 0;
+  std::vector<tcscf_sto> basis;
+  DevSto * dsto = nullptr;  // [nb]
+  double * phiR = nullptr;  // real-harmonic basis values [n][nb]
+  double * vals = nullptr;  // reference-basis values [n][nb] (complex for ndim 3, real for ndim 2)
+  double * grads = nullptr; // [n][nb][3] complex
+  MixedOperands * mixed = nullptr;
+};
+
+struct Tensor {
+  double * d = nullptr;
+  int64_t n1 = 0;
+  int nb = 0;
+  int isComplex = 1;
+  int vec = 0;  // 3 components (Vji)
+};
+
+struct Scratch {
+  void * p = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace tcscf
+
+struct tcscf_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cusolverDnHandle_t solver = nullptr;
+  std::string err;
+  std::map<int, tcscf::Grid> grids;
+  std::map<int, tcscf::Tensor> tensors;
+  int nextId = 1;
+  int flushWindow = 4;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  double lastContractionMs = 0, lastTotalMs = 0;
+  int lastLaunches = 0;
+  int launchCount = 0;
+  std::map<std::string, tcscf::Scratch> scratch;
+};
+
+namespace tcscf {
+
+int fail(tcscf_ctx * ctx, int code, std::string const & msg);
+
+#define TCSCF_CUDA(ctx, call)                                                                 \
+  do {                                                                                        \
+    cudaError_t e_ = (call);                                                                  \
+    if (e_ != cudaSuccess)                                                                    \
+      return ::tcscf::fail((ctx), TCSCF_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+#define TCSCF_LAUNCH(ctx)                                                                     \
+  do {                                                                                        \
+    (ctx)->launchCount++;                                                                     \
+    cudaError_t e_ = cudaGetLastError();                                                      \
+    if (e_ != cudaSuccess)                                                                    \
+      return ::tcscf::fail((ctx), TCSCF_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e_)); \
+  } while (0)
+
+#define TCSCF_CHECK(ctx, cond, code, msg)                                                     \
+  do {                                                                                        \
+    if (!(cond)) return ::tcscf::fail((ctx), (code), (msg));                                  \
+  } while (0)
+
+#define TCSCF_TRY(expr)                                                                       \
+  do {                                                                                        \
+    int s_ = (expr);                                                                          \
+    if (s_ != TCSCF_OK) return s_;                                                            \
+  } while (0)
+
+// context-owned scratch buffer, grown on demand and kept until the context is destroyed
+int scratch(tcscf_ctx * ctx, char const * name, size_t bytes, void ** out);
+
+Grid * findGrid(tcscf_ctx * ctx, int id);
+
+inline unsigned gridBlocks(int64_t n, int threads)
+{
+  int64_t b = (n + threads - 1) / threads;
+  return unsigned(b < 1 ? 1 : (b > 1048576 ? 1048576 : b));
+}
+
+// ---- kernels shared between translation units -------------------------------------------------
+// r12 kernel evaluation in FP64 (scalar kernels); returns 0 for an exactly coincident pair.
+struct OchiDev {
+  double a, a12;
+  int nterms;
+  int S[8][3];
+  double c[8][2];
+};
+
+__device__ __forceinline__ double rsqrt_fp64(double x)
+{
+  // 1/sqrt(x) by two Newton-Raphson steps y <- y (3 - x y^2) / 2 from the FP32 hardware estimate
+  // (quadratic convergence: ~2^-22 -> 2^-44 -> below FP64 rounding).
+  double y = double(rsqrtf(float(x)));
+  double h = x * y;
+  y = y * fma(-0.5 * h, y, 1.5);
+  h = x * y;
+  y = y * fma(-0.5 * h, y, 1.5);
+  // final correction step
+  double const r = fma(-x * y, y, 1.0);
+  return fma(0.5 * y, r, y);
+}
+
+}  // namespace tcscf

@@ -1,0 +1,449 @@
+// FP64 CUDA-core r12 contractions and Fock-matrix reductions.
+//
+// The r12 contraction is written flash-style: for a tile of r1 points the kernel streams r2 in
+// blocks, generates g(r1,r2) from the point coordinates (never stored), forms the density-matrix
+// kernel rho(r1,r2) from the occupied-orbital factors, and accumulates  T += (g .* rho) V  in
+// registers.  This reassociates the reference's stored-kernel contraction
+//   Fai(r1,i) = sum_j (sum_k D(k,j) phi_k(r1)) Fji(r1,j,i),  Fji = computeF(1/r12)
+// (HartreeFock.cpp:144-179, HartreeFock.hpp:136-180) into
+//   Fai(r1,i) = sum_r2 g(r1,r2) w2 rho(r1,r2) phi_i(r2),  rho(r1,r2) = sum_kj D(k,j) phi_k(r1) phi_j(r2)^*
+// and computes the Coulomb potential Faa(r1) (calculateIaa, HartreeFock.cpp:183-213) in the same
+// pass.  With R == 0 (rho == 1) and V = weighted basis-pair products the same kernel is the FP64
+// precompute form computeF / computeV.
+#include "kernels.cuh"
+
+namespace tcscf {
+namespace {
+
+constexpr int BM = 64;    // r1 rows per block
+constexpr int BK = 32;    // r2 points per block step
+constexpr int BN = 128;   // columns per block
+constexpr int NT = 256;
+
+struct KArgs {
+  int64_t n1, n2, r2PerSplit;
+  int R, ncol, ldpsi, ldv, ldt, component, same;
+  const double * p1;
+  const double * p2;
+  const double * psi1;
+  const double * psi2;
+  const double * coul;
+  const double * V;
+  double * T;
+  double * VH;
+  int64_t tStrideSplit;   // elements between split partials of T (0 when not split)
+  int64_t vhStrideSplit;
+  OchiDev u;
+};
+
+__device__ __forceinline__ double ipow(double x, int k)
+{
+  double r = 1;
+  for (int i = 0; i < k; ++i) r *= x;
+  return r;
+}
+
+// jastrowFunctions.hpp:72-108 (Ochi::gradient) for points p (first argument) and q.
+__device__ __forceinline__ void ochiGrad(OchiDev const & u, double px, double py, double pz, double qx, double qy, double qz,
+                                         int same, double & gx, double & gy, double & gz)
+{
+  double const dx = px - qx, dy = py - qy, dz = pz - qz;
+  double const r1 = sqrt(px * px + py * py + pz * pz);
+  double const r2 = sqrt(qx * qx + qy * qy + qz * qz);
+  double const r12 = sqrt(dx * dx + dy * dy + dz * dz);
+  double const r1T = r1 / (r1 + u.a), r2T = r2 / (r2 + u.a), r12T = r12 / (r12 + u.a12);
+  double const r1Scale = u.a / (r1 * r1 * (r1 + u.a));
+  double const r12Scale = u.a12 / (r12 * r12 * (r12 + u.a12));
+  double r1L = 0, r12L = 0;
+  for (int k = 0; k < u.nterms; ++k) {
+    int const i = u.S[k][0], j = u.S[k][1], kk = u.S[k][2];
+    double const f = u.c[k][same] * ipow(r12T, i) * ipow(r1T, j) * ipow(r2T, kk);
+    r1L += f * j * r1Scale;
+    r12L += f * i * r12Scale;
+  }
+  gx = r12L * dx + r1L * px;
+  gy = r12L * dy + r1L * py;
+  gz = r12L * dz + r1L * pz;
+}
+
+// g(r1, r2): KIND 0 = 1/r12, 1 = TC scalar, 2 = one component of grad_1 u.  0 for r1 == r2.
+template <int KIND>
+__device__ __forceinline__ double r12Kernel(KArgs const & a, double x1, double y1, double z1, double x2, double y2, double z2)
+{
+  double const dx = x1 - x2, dy = y1 - y2, dz = z1 - z2;
+  double const rr = fma(dx, dx, fma(dy, dy, dz * dz));
+  if (rr == 0.0) return 0.0;
+  if (KIND == 0) return rsqrt_fp64(rr);
+  if (KIND == 1) {
+    double ax, ay, az, bx, by, bz;
+    ochiGrad(a.u, x1, y1, z1, x2, y2, z2, a.same, ax, ay, az);
+    ochiGrad(a.u, x2, y2, z2, x1, y1, z1, a.same, bx, by, bz);
+    return 2.0 / sqrt(rr) - (ax * ax + ay * ay + az * az) - (bx * bx + by * by + bz * bz);
+  }
+  double gx, gy, gz;
+  ochiGrad(a.u, x1, y1, z1, x2, y2, z2, a.same, gx, gy, gz);
+  return a.component == 0 ? gx : (a.component == 1 ? gy : gz);
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(NT, 2) kContractFp64(KArgs a)
+{
+  extern __shared__ double sm[];
+  int const R = a.R;
+  double * sP1 = sm;                        // [R][BM]
+  double * sC1 = sP1 + R * BM;              // [3][BM]
+  double * sP2 = sC1 + 3 * BM;              // [R][BK]
+  double * sC2 = sP2 + R * BK;              // [4][BK] x, y, z, coul
+  double * sV = sC2 + 4 * BK;               // [BK][BN]
+  double * sX = sV + BK * BN;               // [BK][BM]
+
+  int const tid = threadIdx.x;
+  int64_t const r1base = int64_t(blockIdx.x) * BM;
+  int const cg = blockIdx.z;
+  int64_t const r2begin = int64_t(blockIdx.y) * a.r2PerSplit;
+  int64_t const r2end = min(a.n2, r2begin + a.r2PerSplit);
+
+  for (int idx = tid; idx < R * BM; idx += NT) {
+    int const r = idx / R, b = idx % R;
+    int64_t const g = r1base + r;
+    sP1[b * BM + r] = g < a.n1 ? a.psi1[g * a.ldpsi + b] : 0.0;
+  }
+  for (int idx = tid; idx < 3 * BM; idx += NT) {
+    int const d = idx / BM, r = idx % BM;
+    int64_t const g = r1base + r;
+    sC1[idx] = g < a.n1 ? a.p1[d * a.n1 + g] : 1.0e6;
+  }
+  __syncthreads();
+
+  int const rB = tid >> 2;         // phase-B row
+  int const cB = (tid & 3) * 8;    // phase-B first column
+  double const x1 = sC1[rB], y1 = sC1[BM + rB], z1 = sC1[2 * BM + rB];
+  int const tr = tid >> 4, tc = tid & 15;
+  double acc[4][8];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
+  double vh = 0.0;
+  bool const doCoul = a.coul != nullptr && cg == 0;
+
+  for (int64_t k0 = r2begin; k0 < r2end; k0 += BK) {
+    int const kn = int(min(int64_t(BK), r2end - k0));
+    __syncthreads();
+    for (int idx = tid; idx < BK * BN; idx += NT) {
+      int const k = idx / BN, c = idx % BN;
+      int const col = cg * BN + c;
+      sV[idx] = (k < kn && col < a.ncol) ? a.V[(k0 + k) * a.ldv + col] : 0.0;
+    }
+    for (int idx = tid; idx < R * BK; idx += NT) {
+      int const k = idx / R, b = idx % R;
+      sP2[b * BK + k] = k < kn ? a.psi2[(k0 + k) * a.ldpsi + b] : 0.0;
+    }
+    if (tid < BK) {
+      int const k = tid;
+      bool const ok = k < kn;
+      sC2[k] = ok ? a.p2[k0 + k] : 0.0;
+      sC2[BK + k] = ok ? a.p2[a.n2 + k0 + k] : 0.0;
+      sC2[2 * BK + k] = ok ? a.p2[2 * a.n2 + k0 + k] : 0.0;
+      sC2[3 * BK + k] = (ok && doCoul) ? a.coul[k0 + k] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      int const c = cB + j;
+      double rho = 1.0;
+      if (R > 0) {
+        rho = 0.0;
+        for (int b = 0; b < R; ++b) rho = fma(sP1[b * BM + rB], sP2[b * BK + c], rho);
+      }
+      double g = r12Kernel<KIND>(a, x1, y1, z1, sC2[c], sC2[BK + c], sC2[2 * BK + c]);
+      g = c < kn ? g : 0.0;
+      vh = fma(g, sC2[3 * BK + c], vh);
+      sX[c * BM + rB] = g * rho;
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int k = 0; k < BK; ++k) {
+      double2 const a01 = *reinterpret_cast<double2 const *>(&sX[k * BM + tr * 4]);
+      double2 const a23 = *reinterpret_cast<double2 const *>(&sX[k * BM + tr * 4 + 2]);
+      double av[4] = {a01.x, a01.y, a23.x, a23.y};
+      double bv[8];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        double2 const bb = *reinterpret_cast<double2 const *>(&sV[k * BN + tc * 8 + 2 * q]);
+        bv[2 * q] = bb.x;
+        bv[2 * q + 1] = bb.y;
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+    }
+  }
+
+  double * T = a.T + blockIdx.y * a.tStrideSplit;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    int64_t const g = r1base + tr * 4 + i;
+    if (g >= a.n1) continue;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      int const col = cg * BN + tc * 8 + j;
+      if (col < a.ncol) T[g * a.ldt + col] = acc[i][j];
+    }
+  }
+  if (doCoul) {
+    vh += __shfl_xor_sync(0xffffffffu, vh, 1);
+    vh += __shfl_xor_sync(0xffffffffu, vh, 2);
+    int64_t const g = r1base + rB;
+    if ((tid & 3) == 0 && g < a.n1) a.VH[blockIdx.y * a.vhStrideSplit + g] = vh;
+  }
+}
+
+// deterministic sum of split partials: out[i] = sum_s part[s*stride + i]
+__global__ void kSumSplits(int64_t n, int nsplit, int64_t stride, const double * part, double * out, int64_t rows, int cols, int ldOut, int ldPart)
+{
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
+    int64_t const r = i / cols;
+    int const c = int(i % cols);
+    double s = 0.0;
+    for (int k = 0; k < nsplit; ++k) s += part[k * stride + r * ldPart + c];
+    out[r * ldOut + c] = s;
+  }
+  (void)rows;
+}
+
+// ---- real Fock reduction:  out[k][l] = sum_r w[r] phi[r][k] (cJ phi[r][l] VH[r] - sgnT T[r][l]) ----
+constexpr int RB = 16;      // rows per step
+constexpr int RCH = 1024;   // rows per block
+
+__global__ void __launch_bounds__(NT) kReduceReal(int64_t n1, int nb, const double * phi, const double * w, const double * VH,
+                                                  double cJ, const double * T, int ldt, double sgnT, double * part)
+{
+  __shared__ __align__(16) double sA[RB][BN];
+  __shared__ __align__(16) double sY[RB][BN];
+  int const tid = threadIdx.x;
+  int const kg = blockIdx.y * BN, lg = blockIdx.z * BN;
+  int64_t const rbeg = int64_t(blockIdx.x) * RCH, rend = min(n1, rbeg + RCH);
+  int const tk = tid >> 4, tl = tid & 15;
+  double acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
+  for (int64_t r0 = rbeg; r0 < rend; r0 += RB) {
+    __syncthreads();
+    for (int idx = tid; idx < RB * BN; idx += NT) {
+      int const rr = idx / BN, c = idx % BN;
+      int64_t const r = r0 + rr;
+      double av = 0.0, yv = 0.0;
+      if (r < rend) {
+        int const k = kg + c, l = lg + c;
+        if (k < nb) av = w[r] * phi[r * nb + k];
+        if (l < nb) {
+          double y = 0.0;
+          if (VH) y = cJ * phi[r * nb + l] * VH[r];
+          if (T) y -= sgnT * T[r * ldt + l];
+          yv = y;
+        }
+      }
+      sA[rr][c] = av;
+      sY[rr][c] = yv;
+    }
+    __syncthreads();
+#pragma unroll 2
+    for (int rr = 0; rr < RB; ++rr) {
+      double av[8], bv[8];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        double2 const x = *reinterpret_cast<double2 const *>(&sA[rr][tk * 8 + 2 * q]);
+        double2 const y = *reinterpret_cast<double2 const *>(&sY[rr][tl * 8 + 2 * q]);
+        av[2 * q] = x.x; av[2 * q + 1] = x.y;
+        bv[2 * q] = y.x; bv[2 * q + 1] = y.y;
+      }
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+    }
+  }
+  double * out = part + int64_t(blockIdx.x) * nb * nb;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    int const k = kg + tk * 8 + i;
+    if (k >= nb) continue;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      int const l = lg + tl * 8 + j;
+      if (l < nb) out[k * nb + l] = acc[i][j];
+    }
+  }
+}
+
+__global__ void kSumChunks(int n, int nchunk, const double * part, double * out)
+{
+  int const i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double s = 0.0;
+  for (int k = 0; k < nchunk; ++k) s += part[int64_t(k) * n + i];
+  out[i] += s;
+}
+
+// ---- complex Fock reduction (precompute form): out(j,i) += sum_r w conj(A[r][j]) (cJ A[r][i] Faa[r] - Fai[r][i])
+constexpr int CRB = 16;
+__global__ void __launch_bounds__(NT) kReduceComplex(int64_t n1, int nb, const double2 * A, const double * w, const double2 * Faa,
+                                                     double cJ, const double2 * Fai, double2 * part)
+{
+  extern __shared__ double2 csm[];
+  double2 * sA = csm;              // [CRB][nb]
+  double2 * sY = csm + CRB * nb;   // [CRB][nb]
+  int const tid = threadIdx.x;
+  int64_t const rbeg = int64_t(blockIdx.x) * RCH, rend = min(n1, rbeg + RCH);
+  int const nn = nb * nb;
+  int const per = (nn + NT - 1) / NT;
+  double2 acc[16];
+  for (int q = 0; q < 16; ++q) acc[q] = make_double2(0, 0);
+  for (int64_t r0 = rbeg; r0 < rend; r0 += CRB) {
+    __syncthreads();
+    for (int idx = tid; idx < CRB * nb; idx += NT) {
+      int const rr = idx / nb, c = idx % nb;
+      int64_t const r = r0 + rr;
+      double2 av = make_double2(0, 0), yv = make_double2(0, 0);
+      if (r < rend) {
+        double2 const x = A[r * nb + c];
+        av = make_double2(w[r] * x.x, -w[r] * x.y);   // w conj(A)
+        double2 const f = Faa[r];
+        double2 const t = Fai[r * nb + c];
+        yv.x = cJ * (x.x * f.x - x.y * f.y) - t.x;
+        yv.y = cJ * (x.x * f.y + x.y * f.x) - t.y;
+      }
+      sA[idx] = av;
+      sY[idx] = yv;
+    }
+    __syncthreads();
+    for (int rr = 0; rr < CRB; ++rr)
+      for (int q = 0; q < per && q < 16; ++q) {
+        int const e = tid + q * NT;
+        if (e >= nn) break;
+        int const j = e / nb, i = e % nb;
+        double2 const x = sA[rr * nb + j], y = sY[rr * nb + i];
+        acc[q].x = fma(x.x, y.x, fma(-x.y, y.y, acc[q].x));
+        acc[q].y = fma(x.x, y.y, fma(x.y, y.x, acc[q].y));
+      }
+  }
+  double2 * out = part + int64_t(blockIdx.x) * nn;
+  for (int q = 0; q < per && q < 16; ++q) {
+    int const e = tid + q * NT;
+    if (e < nn) out[e] = acc[q];
+  }
+}
+
+}  // namespace
+
+int contractFp64(tcscf_ctx * ctx, Contraction const & c)
+{
+  TCSCF_CHECK(ctx, c.R >= 0 && c.R <= 128, TCSCF_ERR_UNSUPPORTED, "contraction rank must be <= 128");
+  TCSCF_CHECK(ctx, c.ncol > 0 && c.n1 > 0 && c.n2 > 0, TCSCF_ERR_INVALID_ARGUMENT, "empty contraction");
+  int64_t const tiles = (c.n1 + BM - 1) / BM;
+  int const cgroups = (c.ncol + BN - 1) / BN;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  // split r2 so that small r1 sets still fill the machine (partials are summed deterministically)
+  int64_t const want = int64_t(sms) * 4;
+  int64_t nsplit = (want + tiles * cgroups - 1) / (tiles * cgroups);
+  nsplit = std::max<int64_t>(1, std::min<int64_t>(nsplit, (c.n2 + 4 * BK - 1) / (4 * BK)));
+  nsplit = std::min<int64_t>(nsplit, 65535);
+  int64_t perSplit = (c.n2 + nsplit - 1) / nsplit;
+  perSplit = ((perSplit + BK - 1) / BK) * BK;
+  nsplit = (c.n2 + perSplit - 1) / perSplit;
+
+  KArgs a{};
+  a.n1 = c.n1; a.n2 = c.n2; a.r2PerSplit = perSplit;
+  a.R = c.R; a.ncol = c.ncol; a.ldpsi = c.ldpsi; a.ldv = c.ldv; a.ldt = c.ldt;
+  a.component = c.component; a.same = (c.kernel == TCSCF_K_TC_SCALAR_SAME || c.kernel == TCSCF_K_GRAD_U_SAME) ? 1 : 0;
+  a.p1 = c.p1; a.p2 = c.p2; a.psi1 = c.psi1; a.psi2 = c.psi2; a.coul = c.coul; a.V = c.V;
+  if (c.jastrow) {
+    a.u.a = c.jastrow->a; a.u.a12 = c.jastrow->a12; a.u.nterms = c.jastrow->nterms;
+    for (int k = 0; k < 8; ++k) {
+      for (int d = 0; d < 3; ++d) a.u.S[k][d] = c.jastrow->S[k][d];
+      a.u.c[k][0] = c.jastrow->c[k][0]; a.u.c[k][1] = c.jastrow->c[k][1];
+    }
+  }
+  double * Tpart = c.T;
+  double * VHpart = c.VH;
+  if (nsplit > 1) {
+    void * p = nullptr;
+    size_t const tb = size_t(nsplit) * c.n1 * c.ldt * sizeof(double);
+    size_t const vb = c.coul ? size_t(nsplit) * c.n1 * sizeof(double) : 0;
+    TCSCF_TRY(scratch(ctx, "contract_split", tb + vb, &p));
+    Tpart = static_cast<double *>(p);
+    VHpart = c.coul ? Tpart + size_t(nsplit) * c.n1 * c.ldt : nullptr;
+    a.tStrideSplit = c.n1 * c.ldt;
+    a.vhStrideSplit = c.n1;
+  }
+  a.T = Tpart;
+  a.VH = VHpart;
+  size_t const smem = sizeof(double) * (size_t(c.R) * BM + 3 * BM + size_t(c.R) * BK + 4 * BK + BK * BN + BK * BM);
+  dim3 grid{unsigned(tiles), unsigned(nsplit), unsigned(cgroups)};
+  int const kind = c.kernel == TCSCF_K_INV_R12 ? 0 : (c.kernel <= TCSCF_K_TC_SCALAR_OPPO ? 1 : 2);
+  if (kind == 0) {
+    TCSCF_CUDA(ctx, cudaFuncSetAttribute(kContractFp64<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    kContractFp64<0><<<grid, NT, smem, ctx->stream>>>(a);
+  } else if (kind == 1) {
+    TCSCF_CUDA(ctx, cudaFuncSetAttribute(kContractFp64<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    kContractFp64<1><<<grid, NT, smem, ctx->stream>>>(a);
+  } else {
+    TCSCF_CUDA(ctx, cudaFuncSetAttribute(kContractFp64<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+    kContractFp64<2><<<grid, NT, smem, ctx->stream>>>(a);
+  }
+  TCSCF_LAUNCH(ctx);
+  if (nsplit > 1) {
+    int64_t const n = c.n1 * c.ncol;
+    kSumSplits<<<gridBlocks(n, 256), 256, 0, ctx->stream>>>(n, int(nsplit), c.n1 * c.ldt, Tpart, c.T, c.n1, c.ncol, c.ldt, c.ldt);
+    TCSCF_LAUNCH(ctx);
+    if (c.coul) {
+      kSumSplits<<<gridBlocks(c.n1, 256), 256, 0, ctx->stream>>>(c.n1, int(nsplit), c.n1, VHpart, c.VH, c.n1, 1, 1, 1);
+      TCSCF_LAUNCH(ctx);
+    }
+  }
+  return TCSCF_OK;
+}
+
+int reduceFockReal(tcscf_ctx * ctx, int64_t n1, int nb, const double * phi, const double * w1, const double * VH, double cJ,
+                   const double * T, int ldt, double sgnT, double * out)
+{
+  int const g = (nb + BN - 1) / BN;
+  int64_t const chunks = (n1 + RCH - 1) / RCH;
+  void * p = nullptr;
+  TCSCF_TRY(scratch(ctx, "reduce_real", size_t(chunks) * nb * nb * sizeof(double), &p));
+  double * part = static_cast<double *>(p);
+  dim3 grid{unsigned(chunks), unsigned(g), unsigned(g)};
+  kReduceReal<<<grid, NT, 0, ctx->stream>>>(n1, nb, phi, w1, VH, cJ, T, ldt, sgnT, part);
+  TCSCF_LAUNCH(ctx);
+  int const n = nb * nb;
+  kSumChunks<<<(n + 255) / 256, 256, 0, ctx->stream>>>(n, int(chunks), part, out);
+  TCSCF_LAUNCH(ctx);
+  return TCSCF_OK;
+}
+
+int reduceFockComplex(tcscf_ctx * ctx, int64_t n1, int nb, const double * A, const double * w, const double * Faa, double cJ,
+                      const double * Fai, double * out)
+{
+  TCSCF_CHECK(ctx, nb * nb <= 16 * NT, TCSCF_ERR_UNSUPPORTED, "precompute-form Fock reduction supports nb <= 64");
+  int64_t const chunks = (n1 + RCH - 1) / RCH;
+  void * p = nullptr;
+  TCSCF_TRY(scratch(ctx, "reduce_complex", size_t(chunks) * nb * nb * 2 * sizeof(double), &p));
+  size_t const smem = size_t(2) * CRB * nb * sizeof(double2);
+  kReduceComplex<<<unsigned(chunks), NT, smem, ctx->stream>>>(n1, nb, reinterpret_cast<const double2 *>(A), w,
+                                                              reinterpret_cast<const double2 *>(Faa), cJ,
+                                                              reinterpret_cast<const double2 *>(Fai), static_cast<double2 *>(p));
+  TCSCF_LAUNCH(ctx);
+  int const n = 2 * nb * nb;
+  kSumChunks<<<(n + 255) / 256, 256, 0, ctx->stream>>>(n, int(chunks), static_cast<double *>(p), out);
+  TCSCF_LAUNCH(ctx);
+  return TCSCF_OK;
+}
+
+}  // namespace tcscf

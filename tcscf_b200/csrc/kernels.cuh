@@ -1,0 +1,45 @@
+// Internal launcher interfaces shared by the translation units of libtcscf_gpu.so.
+#pragma once
+
+#include "common.cuh"
+
+namespace tcscf {
+
+// One r12 contraction  T[r1][c] = sum_r2 g(r1,r2) * rho(r1,r2) * V[r2][c]  (+ Coulomb potential
+// VH[r1] = sum_r2 g(r1,r2) * coul[r2]) with rho(r1,r2) = sum_b psi1[r1][b] psi2[r2][b].
+// With R == 0 rho is 1 (precompute form: V holds weighted basis-pair products).
+struct Contraction {
+  int64_t n1 = 0, n2 = 0;
+  int R = 0;                       // rank of rho (columns of psi1 / psi2)
+  int ncol = 0;                    // columns of V / T
+  const double * p1 = nullptr;     // [3][n1]
+  const double * p2 = nullptr;     // [3][n2]
+  const double * psi1 = nullptr;   // [n1][ldpsi]
+  const double * psi2 = nullptr;   // [n2][ldpsi]
+  int ldpsi = 0;
+  const double * coul = nullptr;   // [n2] or null
+  const double * V = nullptr;      // [n2][ldv]
+  int ldv = 0;
+  double * T = nullptr;            // [n1][ldt]
+  int ldt = 0;
+  double * VH = nullptr;           // [n1] (required when coul != null)
+  int kernel = TCSCF_K_INV_R12;    // r12 kernel g (vector kernels use `component`)
+  int component = 0;
+  const tcscf_ochi * jastrow = nullptr;
+};
+
+int contractFp64(tcscf_ctx * ctx, Contraction const & c);
+
+// tensor-core (tcgen05) contraction of the same quantity for g = 1/r12 (flash_tc.cu)
+int contractTensor(tcscf_ctx * ctx, Contraction const & c, int precision);
+bool tensorPathAvailable(Contraction const & c, int precision, std::string * why);
+
+// G_s[k][l] (+)= sum_r1 w1 phi[r1][k] * (cJ * phi[r1][l] * VH[r1] - sgnT * T[r1][l]); real, out [nb][nb]
+int reduceFockReal(tcscf_ctx * ctx, int64_t n1, int nb, const double * phi, const double * w1, const double * VH, double cJ,
+                   const double * T, int ldt, double sgnT, double * out);
+
+// complex reduction G(j,i) = sum_r w[r] conj(A[r][j]) Y[r][i] with Y = cJ * A[r][i] * Faa[r] - Fai[r][i]
+int reduceFockComplex(tcscf_ctx * ctx, int64_t n1, int nb, const double * A, const double * w, const double * Faa, double cJ,
+                      const double * Fai, double * out);
+
+}  // namespace tcscf

@@ -1,0 +1,1267 @@
+// libtcscf_gpu.so: context, device grids and basis evaluation, one-electron quadrature, density
+// factorisation, the Fock-build pipeline (direct and precompute forms) and the SCF driver.
+#include <cmath>
+#include <cstring>
+#include <limits>
+#include <algorithm>
+#include <vector>
+
+#include "kernels.cuh"
+
+namespace tcscf {
+
+int fail(tcscf_ctx * ctx, int code, std::string const & msg)
+{
+  if (ctx) ctx->err = msg;
+  return code;
+}
+
+int scratch(tcscf_ctx * ctx, char const * name, size_t bytes, void ** out)
+{
+  Scratch & s = ctx->scratch[name];
+  if (s.bytes < bytes || !s.p) {
+    if (s.p) { cudaStreamSynchronize(ctx->stream); cudaFree(s.p); s.p = nullptr; s.bytes = 0; }
+    size_t const want = std::max<size_t>(bytes, 256);
+    cudaError_t const e = cudaMalloc(&s.p, want);
+    if (e != cudaSuccess) return fail(ctx, TCSCF_ERR_CUDA, std::string("cudaMalloc(scratch ") + name + "): " + cudaGetErrorString(e));
+    s.bytes = want;
+  }
+  *out = s.p;
+  return TCSCF_OK;
+}
+
+Grid * findGrid(tcscf_ctx * ctx, int id)
+{
+  auto it = ctx->grids.find(id);
+  return it == ctx->grids.end() ? nullptr : &it->second;
+}
+
+namespace {
+
+__device__ __forceinline__ double ipow(double x, int k)
+{
+  double r = 1;
+  for (int i = 0; i < k; ++i) r *= x;
+  return r;
+}
+
+// Fully normalised associated Legendre function with the Condon-Shortley phase,
+// P(l, m, cos t) = (-1)^m sqrt((2l+1)/(4 pi) (l-m)!/(l+m)!) P_l^m(cos t), i.e. Y_l^m(t, 0), evaluated
+// with the standard three-term recurrences in l at fixed m (x = cos t, s = sin t).
+__device__ double sphLegendre(int l, int m, double x, double s)
+{
+  if (m > l || m < 0) return 0.0;
+  double pmm = 1.0;
+  for (int k = 1; k <= m; ++k) pmm *= -s * sqrt((2.0 * k - 1.0) / (2.0 * k));
+  pmm *= sqrt((2.0 * m + 1.0) / (4.0 * kPi));
+  if (l == m) return pmm;
+  double pm1 = x * sqrt(2.0 * m + 3.0) * pmm;
+  if (l == m + 1) return pm1;
+  double pll = 0.0;
+  for (int ll = m + 2; ll <= l; ++ll) {
+    double const a = sqrt((4.0 * ll * ll - 1.0) / (double(ll) * ll - double(m) * m));
+    double const b = sqrt((double(ll - 1) * (ll - 1) - double(m) * m) / (4.0 * (ll - 1) * (ll - 1) - 1.0));
+    pll = a * (x * pm1 - b * pmm);
+    pmm = pm1;
+    pm1 = pll;
+  }
+  return pll;
+}
+
+// QMCGrid::setBasisFunctions (integrateAll.hpp:88-137) with SlaterTypeOrbital::operator() and
+// ::gradient (SlaterTypeOrbital.hpp:51-106).  One thread per (point, function), function index
+// fastest, so every store is coalesced.  Also writes the real-harmonic values phiR used by the
+// contraction kernels: cos-type sqrt2 R P cos(|m| phi) for m > 0, sin-type sqrt2 R P sin(|m| phi)
+// for m < 0, R P for m == 0.
+__global__ void kBasis(int64_t n, int nb, int ndim, const double * __restrict__ pts, const DevSto * __restrict__ sto,
+                       double * __restrict__ phiR, double * __restrict__ vals, double * __restrict__ grads)
+{
+  int64_t const total = n * nb;
+  for (int64_t idx = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; idx < total; idx += int64_t(gridDim.x) * blockDim.x) {
+    int64_t const i = idx / nb;
+    int const b = int(idx % nb);
+    double const x = pts[i], y = pts[n + i], z = pts[2 * n + i];
+    double const r = norm3d(x, y, z);
+    double const ct = z / r;
+    double const st = sqrt(x * x + y * y) / r;
+    double const ph = atan2(y, x);
+    DevSto const s = sto[b];
+    double const R = s.norm * ipow(r, s.n - 1) * exp(-s.alpha * r);
+    int const am = s.m < 0 ? -s.m : s.m;
+    double const P = sphLegendre(s.l, am, ct, st);
+    double sn, cs;
+    sincos(double(s.m) * ph, &sn, &cs);
+    double const rp = R * P;
+    double pr;
+    if (s.rtype == 0) pr = rp;
+    else if (s.rtype == 1) pr = 1.4142135623730950488 * rp * cs;
+    else pr = -1.4142135623730950488 * rp * sn;
+    phiR[idx] = pr;
+    if (vals) {
+      if (ndim == 3) { vals[2 * idx] = rp * cs; vals[2 * idx + 1] = rp * sn; }
+      else vals[idx] = rp * cs;
+    }
+    if (grads) {
+      // SlaterTypeOrbital.hpp:63-106, arithmetic kept (including its m < 0 and pole behaviour)
+      double const th = acos(ct);
+      double const l = s.l, m = s.m;
+      double const dRadialPart = ((s.n - 1) / r - s.alpha) * R;
+      double const ylmRe = P * cs, ylmIm = P * sn;
+      double const c1 = (s.l != s.m) ? sqrt((l - m) * (l + m + 1)) : 0.0;
+      int const m1 = s.m + 1;
+      double const P1 = sphLegendre(s.l, m1 < 0 ? -m1 : m1, ct, st);
+      double sn1, cs1, snm, csm;
+      sincos(double(m1) * ph, &sn1, &cs1);
+      sincos(-ph, &snm, &csm);
+      // cExp(-phi) * Y_l^{m+1}
+      double const y1Re = P1 * cs1, y1Im = P1 * sn1;
+      double const ylmp1Re = c1 * (csm * y1Re - snm * y1Im);
+      double const ylmp1Im = c1 * (csm * y1Im + snm * y1Re);
+      double const rHatRe = dRadialPart * ylmRe, rHatIm = dRadialPart * ylmIm;
+      double const tnt = tan(th), sth = sin(th), cth = cos(th);
+      double const thRe = (m * ylmRe / tnt + ylmp1Re) * R / r;
+      double const thIm = (m * ylmIm / tnt + ylmp1Im) * R / r;
+      // i m Ylm R / (r sin t)
+      double const phRe = -m * ylmIm * R / (r * sth);
+      double const phIm = m * ylmRe * R / (r * sth);
+      double sp, cp;
+      sincos(ph, &sp, &cp);
+      double const rx = cp * sth, ry = sp * sth, rz = cth;
+      double const tx = cp * cth, ty = sp * cth, tz = -sth;
+      double const px = -sp, py = cp;
+      double * g = grads + 6 * idx;
+      g[0] = rHatRe * rx + thRe * tx + phRe * px;
+      g[1] = rHatIm * rx + thIm * tx + phIm * px;
+      g[2] = rHatRe * ry + thRe * ty + phRe * py;
+      g[3] = rHatIm * ry + thIm * ty + phIm * py;
+      g[4] = rHatRe * rz + thRe * tz;
+      g[5] = rHatIm * rz + thIm * tz;
+    }
+  }
+}
+
+// ---- compensated block reduction helpers -------------------------------------------------------
+__device__ __forceinline__ void twoSum(double a, double b, double & s, double & e)
+{
+  s = a + b;
+  double const bb = s - a;
+  e = (a - (s - bb)) + (b - bb);
+}
+
+// S_ij / H_ij quadrature, one block per (i, j); complex reference-basis values and gradients.
+__global__ void kQuadOverlapCore(int64_t n, int nb, int Z, const double * pts, const double * w, const double2 * vals,
+                                 const double2 * grads, double2 * S, double2 * H)
+{
+  int const i = blockIdx.x / nb, j = blockIdx.x % nb;
+  double sRe = 0, sIm = 0, hRe = 0, hIm = 0;
+  for (int64_t p = threadIdx.x; p < n; p += blockDim.x) {
+    double2 const a = vals[p * nb + i], b = vals[p * nb + j];
+    double const ovRe = a.x * b.x + a.y * b.y, ovIm = a.x * b.y - a.y * b.x;  // conj(a) b
+    sRe += w[p] * ovRe;
+    sIm += w[p] * ovIm;
+    if (grads) {
+      double const r = norm3d(pts[p], pts[n + p], pts[2 * n + p]);
+      double kRe = 0, kIm = 0;
+      for (int d = 0; d < 3; ++d) {
+        double2 const ga = grads[(p * nb + i) * 3 + d], gb = grads[(p * nb + j) * 3 + d];
+        kRe += ga.x * gb.x + ga.y * gb.y;
+        kIm += ga.x * gb.y - ga.y * gb.x;
+      }
+      hRe += w[p] * (0.5 * kRe - Z * ovRe / r);
+      hIm += w[p] * (0.5 * kIm - Z * ovIm / r);
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    sRe += __shfl_xor_sync(0xffffffffu, sRe, o);
+    sIm += __shfl_xor_sync(0xffffffffu, sIm, o);
+    hRe += __shfl_xor_sync(0xffffffffu, hRe, o);
+    hIm += __shfl_xor_sync(0xffffffffu, hIm, o);
+  }
+  __shared__ double red[4][32];
+  int const wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) { red[0][wid] = sRe; red[1][wid] = sIm; red[2][wid] = hRe; red[3][wid] = hIm; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a[4] = {0, 0, 0, 0};
+    for (int k = 0; k < int(blockDim.x >> 5); ++k)
+      for (int q = 0; q < 4; ++q) a[q] += red[q][k];
+    S[blockIdx.x] = make_double2(a[0], a[1]);
+    if (H) H[blockIdx.x] = make_double2(a[2], a[3]);
+  }
+}
+
+// U coefficient U[k][i] of the unitary complex -> real-harmonic map phiR_k = sum_i U[k][i] phi_i
+__device__ __forceinline__ double2 urow(const DevSto * s, int k, int i)
+{
+  double const h = 0.70710678118654752440;
+  int const t = s[k].rtype;
+  if (i == k) return t == 0 ? make_double2(1, 0) : (t == 1 ? make_double2(h, 0) : make_double2(0, h));
+  return t == 1 ? make_double2(h, 0) : make_double2(0, -h);
+}
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+__device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+
+// DR = conj(U) D U^T for each spin; D complex [nspin][nb][nb] (reference basis)
+__global__ void kDensityToReal(int nspin, int nb, const DevSto * s, const double2 * D, double2 * DR)
+{
+  int const total = nspin * nb * nb;
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
+    int const sp = idx / (nb * nb), k = (idx / nb) % nb, l = idx % nb;
+    int const ik[2] = {k, s[k].partner};
+    int const jl[2] = {l, s[l].partner};
+    double2 acc = make_double2(0, 0);
+    for (int a = 0; a < 2; ++a) {
+      int const i = ik[a];
+      if (i < 0) continue;
+      double2 const u1 = cconj(urow(s, k, i));
+      for (int b = 0; b < 2; ++b) {
+        int const j = jl[b];
+        if (j < 0) continue;
+        double2 const t = cmul(cmul(u1, D[sp * nb * nb + i * nb + j]), urow(s, l, j));
+        acc.x += t.x;
+        acc.y += t.y;
+      }
+    }
+    DR[idx] = acc;
+  }
+}
+
+// symmetric real part (column-major == row-major) and the imaginary magnitude, per spin
+__global__ void kSplitDensity(int nb, const double2 * DR, double * A, double * maxAbs)
+{
+  __shared__ double sre[256], sim[256];
+  double mr = 0, mi = 0;
+  for (int idx = threadIdx.x; idx < nb * nb; idx += blockDim.x) {
+    int const k = idx / nb, l = idx % nb;
+    double2 const a = DR[k * nb + l], b = DR[l * nb + k];
+    A[idx] = 0.5 * (a.x + b.x);
+    mr = fmax(mr, fabs(a.x));
+    mi = fmax(mi, fabs(a.y));
+  }
+  sre[threadIdx.x] = mr;
+  sim[threadIdx.x] = mi;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) { sre[threadIdx.x] = fmax(sre[threadIdx.x], sre[threadIdx.x + o]); sim[threadIdx.x] = fmax(sim[threadIdx.x], sim[threadIdx.x + o]); }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) { maxAbs[0] = sre[0]; maxAbs[1] = sim[0]; }
+}
+
+// Hermitian (conj-symmetrised) copy of DR, column-major, for the complex factorisation
+__global__ void kHermitianCopy(int nb, const double2 * DR, double2 * Z)
+{
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < nb * nb; idx += gridDim.x * blockDim.x) {
+    int const row = idx % nb, col = idx / nb;   // column-major element (row, col)
+    double2 const a = DR[row * nb + col], b = DR[col * nb + row];
+    Z[idx] = make_double2(0.5 * (a.x + b.x), 0.5 * (a.y - b.y));
+  }
+}
+
+// factor matrices X1, X2 [nb][ldx] from the kept eigenpairs (real case): X2 = v sqrt|l|, X1 = sign(l) X2
+__global__ void kRealFactors(int nb, int nkeep, const int * keep, const double * W, const double * V, int ldx, double * X1, double * X2)
+{
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < nb * nkeep; idx += gridDim.x * blockDim.x) {
+    int const k = idx / nkeep, b = idx % nkeep;
+    int const e = keep[b];
+    double const lam = W[e];
+    double const sq = sqrt(fabs(lam));
+    double const v = V[e * nb + k] * sq;
+    X2[k * ldx + b] = v;
+    X1[k * ldx + b] = lam < 0 ? -v : v;
+  }
+}
+
+// complex case: X2 = [Re z | Im z], X1re = [l Re z | l Im z], X1im = [l Im z | -l Re z]
+__global__ void kComplexFactors(int nb, int nkeep, const int * keep, const double * W, const double2 * Z, int ldx, double * X1re,
+                                double * X1im, double * X2)
+{
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < nb * nkeep; idx += gridDim.x * blockDim.x) {
+    int const k = idx / nkeep, b = idx % nkeep;
+    int const e = keep[b];
+    double const lam = W[e];
+    double2 const z = Z[e * nb + k];
+    X2[k * ldx + b] = z.x;
+    X2[k * ldx + nkeep + b] = z.y;
+    X1re[k * ldx + b] = lam * z.x;
+    X1re[k * ldx + nkeep + b] = lam * z.y;
+    X1im[k * ldx + b] = lam * z.y;
+    X1im[k * ldx + nkeep + b] = -lam * z.x;
+  }
+}
+
+// psi[r][b] = sum_k phi[r][k] X[k][b]  (FP64), b < R, row stride ld
+__global__ void kOrbitals(int64_t n, int nb, int R, const double * __restrict__ phi, const double * __restrict__ X, int ldx,
+                          double * __restrict__ psi, int ld)
+{
+  extern __shared__ double sXo[];
+  for (int i = threadIdx.x; i < nb * R; i += blockDim.x) sXo[i] = X[(i / R) * ldx + (i % R)];
+  __syncthreads();
+  int64_t const total = n * R;
+  for (int64_t idx = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; idx < total; idx += int64_t(gridDim.x) * blockDim.x) {
+    int64_t const r = idx / R;
+    int const b = int(idx % R);
+    double s = 0;
+    const double * pr = phi + r * nb;
+    for (int k = 0; k < nb; ++k) s = fma(pr[k], sXo[k * R + b], s);
+    psi[r * ld + b] = s;
+  }
+}
+
+// coul[r] = scale w[r] sum_b psiA[r][b] psiB[r][b]
+__global__ void kCoulombSource(int64_t n, int R, const double * psiA, const double * psiB, int ld, const double * w, double scale, double * coul)
+{
+  for (int64_t r = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; r < n; r += int64_t(gridDim.x) * blockDim.x) {
+    double s = 0;
+    for (int b = 0; b < R; ++b) s = fma(psiA[r * ld + b], psiB[r * ld + b], s);
+    coul[r] = scale * w[r] * s;
+  }
+}
+
+// V[r][l] = scale w[r] phi[r][l]
+__global__ void kWeightedBasis(int64_t n, int nb, const double * phi, const double * w, double scale, double * V)
+{
+  for (int64_t idx = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; idx < n * nb; idx += int64_t(gridDim.x) * blockDim.x)
+    V[idx] = scale * w[idx / nb] * phi[idx];
+}
+
+// V[r][p(k,l)] = scale w[r] phi[r][k] phi[r][l], k <= l, pair index p = k*nb - k(k-1)/2 + (l-k)
+__global__ void kPairProducts(int64_t n, int nb, const double * phi, const double * w, double scale, double * V)
+{
+  int const np = nb * (nb + 1) / 2;
+  for (int64_t idx = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; idx < n * np; idx += int64_t(gridDim.x) * blockDim.x) {
+    int64_t const r = idx / np;
+    int p = int(idx % np);
+    int k = 0;
+    while (p >= nb - k) { p -= nb - k; ++k; }
+    int const l = k + p;
+    V[idx] = scale * w[r] * phi[r * nb + k] * phi[r * nb + l];
+  }
+}
+
+__device__ __forceinline__ int pairIndex(int nb, int k, int l)
+{
+  if (k > l) { int t = k; k = l; l = t; }
+  return k * nb - k * (k - 1) / 2 + (l - k);
+}
+
+// F(j,i) = sum_{k,l} U[k][j] FR(k,l) conj(U[l][i]) per r1 row; FR packed symmetric [n1][np] (component c of ncomp)
+// out complex [n1][nb][nb](*ncomp) or real (x 1) when realOut
+__global__ void kPairsToReference(int64_t n1, int nb, const DevSto * s, const double * FR, int ncomp, int comp, int realOut, double * out)
+{
+  int const np = nb * (nb + 1) / 2;
+  int64_t const total = n1 * nb * nb;
+  for (int64_t idx = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; idx < total; idx += int64_t(gridDim.x) * blockDim.x) {
+    int64_t const r = idx / (nb * nb);
+    int const j = int((idx / nb) % nb), i = int(idx % nb);
+    int const kj[2] = {j, s[j].partner};
+    int const li[2] = {i, s[i].partner};
+    double2 acc = make_double2(0, 0);
+    for (int a = 0; a < 2; ++a) {
+      int const k = kj[a];
+      if (k < 0) continue;
+      double2 const uk = urow(s, k, j);
+      for (int b = 0; b < 2; ++b) {
+        int const l = li[b];
+        if (l < 0) continue;
+        double const f = FR[r * np + pairIndex(nb, k, l)];
+        double2 const t = cmul(uk, cconj(urow(s, l, i)));
+        acc.x += f * t.x;
+        acc.y += f * t.y;
+      }
+    }
+    if (realOut) out[idx] = acc.x;
+    else {
+      out[2 * (idx * ncomp + comp)] = acc.x;
+      out[2 * (idx * ncomp + comp) + 1] = acc.y;
+    }
+  }
+}
+
+// G(j,i) = sum_{k,l} U[k][j] GR(k,l) conj(U[l][i]); GR complex [nspin][nb][nb] given as re/im planes
+__global__ void kRealToReference(int nspin, int nb, const DevSto * s, const double * GRre, const double * GRim, double2 * G)
+{
+  int const total = nspin * nb * nb;
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
+    int const sp = idx / (nb * nb), j = (idx / nb) % nb, i = idx % nb;
+    int const kj[2] = {j, s[j].partner};
+    int const li[2] = {i, s[i].partner};
+    double2 acc = make_double2(0, 0);
+    for (int a = 0; a < 2; ++a) {
+      int const k = kj[a];
+      if (k < 0) continue;
+      double2 const uk = urow(s, k, j);
+      for (int b = 0; b < 2; ++b) {
+        int const l = li[b];
+        if (l < 0) continue;
+        int64_t const o = int64_t(sp) * nb * nb + k * nb + l;
+        double2 const g = make_double2(GRre[o], GRim ? GRim[o] : 0.0);
+        double2 const t = cmul(cmul(uk, g), cconj(urow(s, l, i)));
+        acc.x += t.x;
+        acc.y += t.y;
+      }
+    }
+    G[idx] = acc;
+  }
+}
+
+// enforceOneElectronSymmetry (HartreeFock.cpp:758-780) and constructSCFOperator (:48-98) with a
+// compensated FP64 energy sum.  One block.  energy = factor * Re sum D(i,j) (h(j,i) + G(j,i)/2 - G3(j,i)/3)
+__global__ void kFinalize(int nspin, int nb, const double * h, double2 * G, const double2 * G3, const double2 * D, int respectSym,
+                          double factor, double2 * fock, double * energy)
+{
+  __shared__ double ss[512], se[512];
+  double s = 0, c = 0;
+  int const nn = nb * nb;
+  for (int idx = threadIdx.x; idx < nspin * nn; idx += blockDim.x) {
+    int const sp = idx / nn, ji = idx % nn, j = ji / nb, i = ji % nb;
+    double2 g = G[idx];
+    double2 g3 = G3 ? G3[idx] : make_double2(0, 0);
+    if (respectSym && !(fabs(h[ji]) > 0)) { g = make_double2(0, 0); g3 = make_double2(0, 0); }
+    G[idx] = g;
+    double2 f = make_double2(h[ji] + g.x - g3.x, g.y - g3.y);
+    if (fock) fock[idx] = f;
+    double2 const e = make_double2(h[ji] + g.x / 2 - g3.x / 3, g.y / 2 - g3.y / 3);
+    double2 const d = D[int64_t(sp) * nn + i * nb + j];
+    double const term = d.x * e.x - d.y * e.y;
+    double t, err;
+    twoSum(s, term, t, err);
+    s = t;
+    c += err;
+  }
+  ss[threadIdx.x] = s;
+  se[threadIdx.x] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double tot = 0, comp = 0;
+    for (int k = 0; k < int(blockDim.x); ++k) {
+      double t, err;
+      twoSum(tot, ss[k], t, err);
+      tot = t;
+      comp += err + se[k];
+    }
+    energy[0] = factor * (tot + comp);
+  }
+}
+
+// Faa(r) (+)= sum_ji F(r,j,i) D(i,j) ; Fai(r,i) (+)= sum_j (sum_k D(k,j) vals(r,k)) F(r,j,i)
+// (calculateIaa / calculateFai, HartreeFock.cpp:144-213) for one spin density; one block per row.
+template <bool CX>
+__global__ void kFaaFai(int64_t n1, int nb, const double * F, const double2 * vals, const double2 * D, double2 * Faa, double2 * Fai)
+{
+  extern __shared__ double2 sk[];
+  int64_t const r = blockIdx.x;
+  int const tid = threadIdx.x;
+  for (int j = tid; j < nb; j += blockDim.x) {
+    double2 a = make_double2(0, 0);
+    for (int k = 0; k < nb; ++k) {
+      double2 const t = cmul(D[k * nb + j], vals[r * nb + k]);
+      a.x += t.x; a.y += t.y;
+    }
+    sk[j] = a;
+  }
+  __syncthreads();
+  int64_t const base = r * nb * nb;
+  auto fval = [&](int j, int i) -> double2 {
+    if (CX) return reinterpret_cast<const double2 *>(F)[base + j * nb + i];
+    return make_double2(F[base + j * nb + i], 0.0);
+  };
+  for (int i = tid; i < nb; i += blockDim.x) {
+    double2 a = make_double2(0, 0);
+    for (int j = 0; j < nb; ++j) {
+      double2 const t = cmul(sk[j], fval(j, i));
+      a.x += t.x; a.y += t.y;
+    }
+    Fai[r * nb + i].x += a.x;
+    Fai[r * nb + i].y += a.y;
+  }
+  double sr = 0, si = 0;
+  for (int e = tid; e < nb * nb; e += blockDim.x) {
+    int const j = e / nb, i = e % nb;
+    double2 const t = cmul(fval(j, i), D[i * nb + j]);
+    sr += t.x; si += t.y;
+  }
+  for (int o = 16; o > 0; o >>= 1) { sr += __shfl_xor_sync(0xffffffffu, sr, o); si += __shfl_xor_sync(0xffffffffu, si, o); }
+  __shared__ double red[2][32];
+  if ((tid & 31) == 0) { red[0][tid >> 5] = sr; red[1][tid >> 5] = si; }
+  __syncthreads();
+  if (tid == 0) {
+    double a = 0, b = 0;
+    for (int k = 0; k < int(blockDim.x >> 5); ++k) { a += red[0][k]; b += red[1][k]; }
+    Faa[r].x += a;
+    Faa[r].y += b;
+  }
+}
+
+__global__ void kAddInto(int64_t n, const double * a, double * out)
+{
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) out[i] += a[i];
+}
+
+// column-major complex copy of the row-major (j,i) Fock matrix, and of a real row-major S
+__global__ void kToColumnMajor(int nb, const double2 * fockRow, const double * S, double2 * A, double2 * B)
+{
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < nb * nb; idx += gridDim.x * blockDim.x) {
+    int const row = idx % nb, col = idx / nb;
+    A[idx] = fockRow[row * nb + col];
+    B[idx] = make_double2(S[row * nb + col], 0.0);
+  }
+}
+
+// getNewDensity (HartreeFock.cpp:20-44): D(u,v) = sum_a C(u,a) conj(C(v,a)); C column-major
+__global__ void kDensityFromOrbitals(int nb, int nocc, const double2 * C, double2 * D)
+{
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < nb * nb; idx += gridDim.x * blockDim.x) {
+    int const u = idx / nb, v = idx % nb;
+    double2 t = make_double2(0, 0);
+    for (int a = 0; a < nocc; ++a) {
+      double2 const x = cmul(C[a * nb + u], cconj(C[a * nb + v]));
+      t.x += x.x; t.y += x.y;
+    }
+    D[idx] = t;
+  }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------------------
+// Fock-build pipeline
+// ------------------------------------------------------------------------------------------------
+namespace {
+
+struct Factor {
+  int R = 0;          // columns of the factor matrices
+  bool complex = false;
+  double * X1 = nullptr, * X1im = nullptr, * X2 = nullptr;   // device [nb][ldx]
+  int ldx = 0;
+};
+
+// Factor the spin density's real-harmonic form DR = X1 X2^T (real) or, for a density that is not
+// real in the real-harmonic basis, into the real/imaginary pair described in kComplexFactors.
+int factorDensity(tcscf_ctx * ctx, Grid & g, const double2 * dD, int spin, Factor & f)
+{
+  int const nb = g.nb;
+  size_t const nn = size_t(nb) * nb;
+  void * p = nullptr;
+  TCSCF_TRY(scratch(ctx, spin ? "fac1" : "fac0", nn * sizeof(double2) * 3 + nn * sizeof(double) * 8 + 64 * sizeof(double) + nb * sizeof(int) + 4096, &p));
+  char * base = static_cast<char *>(p);
+  double2 * DR = reinterpret_cast<double2 *>(base); base += nn * sizeof(double2);
+  double2 * Z = reinterpret_cast<double2 *>(base); base += nn * sizeof(double2) * 2;
+  double * A = reinterpret_cast<double *>(base); base += nn * sizeof(double);
+  double * W = reinterpret_cast<double *>(base); base += nn * sizeof(double);
+  f.X1 = reinterpret_cast<double *>(base); base += nn * sizeof(double) * 2;
+  f.X1im = reinterpret_cast<double *>(base); base += nn * sizeof(double) * 2;
+  f.X2 = reinterpret_cast<double *>(base); base += nn * sizeof(double) * 2;
+  double * maxAbs = reinterpret_cast<double *>(base); base += 64 * sizeof(double);
+  int * keep = reinterpret_cast<int *>(base);
+  f.ldx = 2 * nb;
+
+  kDensityToReal<<<gridBlocks(nn, 256), 256, 0, ctx->stream>>>(1, nb, g.dsto, dD, DR);
+  TCSCF_LAUNCH(ctx);
+  kSplitDensity<<<1, 256, 0, ctx->stream>>>(nb, DR, A, maxAbs);
+  TCSCF_LAUNCH(ctx);
+  double hmax[2];
+  TCSCF_CUDA(ctx, cudaMemcpyAsync(hmax, maxAbs, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (!(hmax[0] == hmax[0]) || !(hmax[1] == hmax[1])) return fail(ctx, TCSCF_ERR_NONFINITE, "non-finite density");
+  f.complex = hmax[1] > 1e-13 * std::max(hmax[0], 1e-300);
+  if (hmax[0] == 0 && hmax[1] == 0) { f.R = 0; return TCSCF_OK; }
+
+  int * devInfo = reinterpret_cast<int *>(maxAbs + 8);
+  int lwork = 0;
+  std::vector<double> hW(nb);
+  if (!f.complex) {
+    if (cusolverDnDsyevd_bufferSize(ctx->solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, nb, A, nb, W, &lwork) != CUSOLVER_STATUS_SUCCESS)
+      return fail(ctx, TCSCF_ERR_LINALG, "cusolverDnDsyevd_bufferSize failed");
+    void * wk = nullptr;
+    TCSCF_TRY(scratch(ctx, "syevd_work", size_t(lwork) * sizeof(double) + 64, &wk));
+    if (cusolverDnDsyevd(ctx->solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, nb, A, nb, W, static_cast<double *>(wk), lwork, devInfo) != CUSOLVER_STATUS_SUCCESS)
+      return fail(ctx, TCSCF_ERR_LINALG, "cusolverDnDsyevd failed");
+  } else {
+    kHermitianCopy<<<gridBlocks(nn, 256), 256, 0, ctx->stream>>>(nb, DR, Z);
+    TCSCF_LAUNCH(ctx);
+    if (cusolverDnZheevd_bufferSize(ctx->solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, nb, reinterpret_cast<cuDoubleComplex *>(Z), nb, W, &lwork) != CUSOLVER_STATUS_SUCCESS)
+      return fail(ctx, TCSCF_ERR_LINALG, "cusolverDnZheevd_bufferSize failed");
+    void * wk = nullptr;
+    TCSCF_TRY(scratch(ctx, "heevd_work", size_t(lwork) * sizeof(double2) + 64, &wk));
+    if (cusolverDnZheevd(ctx->solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, nb, reinterpret_cast<cuDoubleComplex *>(Z), nb, W,
+                         static_cast<cuDoubleComplex *>(wk), lwork, devInfo) != CUSOLVER_STATUS_SUCCESS)
+      return fail(ctx, TCSCF_ERR_LINALG, "cusolverDnZheevd failed");
+  }
+  int info = 0;
+  TCSCF_CUDA(ctx, cudaMemcpyAsync(hW.data(), W, nb * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  TCSCF_CUDA(ctx, cudaMemcpyAsync(&info, devInfo, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (info != 0) return fail(ctx, TCSCF_ERR_LINALG, "density eigen-decomposition failed");
+  double lmax = 0;
+  for (double v : hW) lmax = std::max(lmax, std::fabs(v));
+  std::vector<int> hk;
+  for (int e = nb - 1; e >= 0; --e)
+    if (std::fabs(hW[e]) > 1e-12 * lmax) hk.push_back(e);
+  int const nk = int(hk.size());
+  if (nk == 0) { f.R = 0; return TCSCF_OK; }
+  TCSCF_CUDA(ctx, cudaMemcpyAsync(keep, hk.data(), nk * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+  if (!f.complex) {
+    kRealFactors<<<gridBlocks(int64_t(nb) * nk, 256), 256, 0, ctx->stream>>>(nb, nk, keep, W, A, f.ldx, f.X1, f.X2);
+    f.R = nk;
+  } else {
+    kComplexFactors<<<gridBlocks(int64_t(nb) * nk, 256), 256, 0, ctx->stream>>>(nb, nk, keep, W, Z, f.ldx, f.X1, f.X1im, f.X2);
+    f.R = 2 * nk;
+  }
+  TCSCF_LAUNCH(ctx);
+  // host vectors go out of scope only after the stream has consumed `keep`
+  TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return TCSCF_OK;
+}
+
+int checkBasisPair(tcscf_ctx * ctx, Grid * g1, Grid * g2)
+{
+  TCSCF_CHECK(ctx, g1 && g2, TCSCF_ERR_INVALID_ARGUMENT, "unknown grid handle");
+  TCSCF_CHECK(ctx, g1->nb > 0 && g2->nb > 0, TCSCF_ERR_INVALID_ARGUMENT, "setBasisFunctions has not been called on the grid");
+  TCSCF_CHECK(ctx, g1->nb == g2->nb, TCSCF_ERR_INVALID_ARGUMENT, "r1Grid.nBasis() != r2Grid.nBasis()");
+  TCSCF_CHECK(ctx, g1->ndim == 3, TCSCF_ERR_INVALID_ARGUMENT, "the r1 grid must be three dimensional");
+  for (int b = 0; b < g1->nb; ++b) {
+    tcscf_sto const & a = g1->basis[b];
+    tcscf_sto const & c = g2->basis[b];
+    TCSCF_CHECK(ctx, a.alpha == c.alpha && a.n == c.n && a.l == c.l && a.m == c.m, TCSCF_ERR_INVALID_ARGUMENT,
+                "r1 and r2 grids carry different basis sets");
+  }
+  return TCSCF_OK;
+}
+
+// Direct-form Fock build with device-resident densities dD [nspin][nb][nb] complex.
+// Leaves G (masked), Fock (row-major) and the energy on the device.
+int fockBuildDevice(tcscf_ctx * ctx, Grid & g1, Grid & g2, int nspin, const double2 * dD, const double * dH, int respectSym,
+                    int precision, double2 * dG, double2 * dFock, double * dE)
+{
+  int const nb = g1.nb;
+  int64_t const n1 = g1.n, n2 = g2.n;
+  double const scale = g2.ndim == 2 ? 2 * kPi : 1.0;
+  int const ldt = nb;
+  int const ldpsi = 2 * nb;
+  size_t const bytes = sizeof(double) * (size_t(n2) * nb                 // V
+                                         + size_t(n1) * ldpsi + 2 * size_t(n2) * ldpsi  // psi1, psi2, psi1 on r2
+                                         + size_t(n2)                              // coul
+                                         + size_t(nspin) * n1 * ldt                // T re
+                                         + size_t(nspin) * n1 * ldt                // T im
+                                         + size_t(nspin) * n1 + n1                 // VH per spin + total
+                                         + size_t(nspin) * nb * nb * 2);           // GR re/im
+  void * p = nullptr;
+  TCSCF_TRY(scratch(ctx, "fock", bytes, &p));
+  double * V = static_cast<double *>(p);
+  double * psi1 = V + size_t(n2) * nb;
+  double * psi2 = psi1 + size_t(n1) * ldpsi;
+  double * psi1at2 = psi2 + size_t(n2) * ldpsi;
+  double * coul = psi1at2 + size_t(n2) * ldpsi;
+  double * Tre = coul + n2;
+  double * Tim = Tre + size_t(nspin) * n1 * ldt;
+  double * VH = Tim + size_t(nspin) * n1 * ldt;
+  double * VHtot = VH + size_t(nspin) * n1;
+  double * GRre = VHtot + n1;
+  double * GRim = GRre + size_t(nspin) * nb * nb;
+
+  cudaEventRecord(ctx->ev[0], ctx->stream);
+  int const launch0 = ctx->launchCount;
+  kWeightedBasis<<<gridBlocks(n2 * nb, 256), 256, 0, ctx->stream>>>(n2, nb, g2.phiR, g2.w, scale, V);
+  TCSCF_LAUNCH(ctx);
+  TCSCF_CUDA(ctx, cudaMemsetAsync(VH, 0, sizeof(double) * (size_t(nspin) * n1 + n1), ctx->stream));
+  TCSCF_CUDA(ctx, cudaMemsetAsync(GRre, 0, sizeof(double) * size_t(nspin) * nb * nb * 2, ctx->stream));
+  bool anyComplex = false;
+  double contractionMs = 0;
+  for (int s = 0; s < nspin; ++s) {
+    Factor f;
+    TCSCF_TRY(factorDensity(ctx, g1, dD + size_t(s) * nb * nb, s, f));
+    double * Ts = Tre + size_t(s) * n1 * ldt;
+    double * Ti = Tim + size_t(s) * n1 * ldt;
+    if (f.R == 0) {
+      TCSCF_CUDA(ctx, cudaMemsetAsync(Ts, 0, sizeof(double) * n1 * ldt, ctx->stream));
+      continue;
+    }
+    int const R = f.R;
+    for (int part = 0; part < (f.complex ? 2 : 1); ++part) {
+      double const * X1 = part == 0 ? f.X1 : f.X1im;
+      size_t const sm = sizeof(double) * size_t(nb) * R;
+      kOrbitals<<<gridBlocks(n1 * R, 256), 256, sm, ctx->stream>>>(n1, nb, R, g1.phiR, X1, f.ldx, psi1, ldpsi);
+      TCSCF_LAUNCH(ctx);
+      if (part == 0) {
+        kOrbitals<<<gridBlocks(n2 * R, 256), 256, sm, ctx->stream>>>(n2, nb, R, g2.phiR, f.X2, f.ldx, psi2, ldpsi);
+        TCSCF_LAUNCH(ctx);
+        // rho(r2, r2) needs the r1-side factor evaluated on the r2 points
+        kOrbitals<<<gridBlocks(n2 * R, 256), 256, sm, ctx->stream>>>(n2, nb, R, g2.phiR, f.X1, f.ldx, psi1at2, ldpsi);
+        TCSCF_LAUNCH(ctx);
+      }
+      Contraction c;
+      c.n1 = n1; c.n2 = n2; c.R = R; c.ncol = nb;
+      c.p1 = g1.pts; c.p2 = g2.pts; c.psi1 = psi1; c.psi2 = psi2; c.ldpsi = ldpsi;
+      c.V = V; c.ldv = nb; c.T = part == 0 ? Ts : Ti; c.ldt = ldt;
+      if (part == 0) {
+        kCoulombSource<<<gridBlocks(n2, 256), 256, 0, ctx->stream>>>(n2, R, psi1at2, psi2, ldpsi, g2.w, scale, coul);
+        TCSCF_LAUNCH(ctx);
+        c.coul = coul;
+        c.VH = VH + size_t(s) * n1;
+      }
+      cudaEventRecord(ctx->ev[2], ctx->stream);
+      if (precision == TCSCF_PREC_FP64) TCSCF_TRY(contractFp64(ctx, c));
+      else TCSCF_TRY(contractTensor(ctx, c, precision));
+      cudaEventRecord(ctx->ev[3], ctx->stream);
+      TCSCF_CUDA(ctx, cudaEventSynchronize(ctx->ev[3]));
+      float ms = 0;
+      cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]);
+      contractionMs += ms;
+    }
+    if (f.complex) anyComplex = true;
+    else TCSCF_CUDA(ctx, cudaMemsetAsync(Ti, 0, sizeof(double) * n1 * ldt, ctx->stream));
+  }
+  for (int s = 0; s < nspin; ++s) {
+    kAddInto<<<gridBlocks(n1, 256), 256, 0, ctx->stream>>>(n1, VH + size_t(s) * n1, VHtot);
+    TCSCF_LAUNCH(ctx);
+  }
+  double const cJ = nspin == 1 ? 2.0 : 1.0;
+  for (int s = 0; s < nspin; ++s) {
+    TCSCF_TRY(reduceFockReal(ctx, n1, nb, g1.phiR, g1.w, VHtot, cJ, Tre + size_t(s) * n1 * ldt, ldt, 1.0, GRre + size_t(s) * nb * nb));
+    if (anyComplex)
+      TCSCF_TRY(reduceFockReal(ctx, n1, nb, g1.phiR, g1.w, nullptr, 0.0, Tim + size_t(s) * n1 * ldt, ldt, 1.0, GRim + size_t(s) * nb * nb));
+  }
+  kRealToReference<<<gridBlocks(int64_t(nspin) * nb * nb, 256), 256, 0, ctx->stream>>>(nspin, nb, g1.dsto, GRre, anyComplex ? GRim : nullptr, dG);
+  TCSCF_LAUNCH(ctx);
+  kFinalize<<<1, 512, 0, ctx->stream>>>(nspin, nb, dH, dG, nullptr, dD, respectSym, nspin == 1 ? 2.0 : 1.0, dFock, dE);
+  TCSCF_LAUNCH(ctx);
+  cudaEventRecord(ctx->ev[1], ctx->stream);
+  TCSCF_CUDA(ctx, cudaEventSynchronize(ctx->ev[1]));
+  float tot = 0;
+  cudaEventElapsedTime(&tot, ctx->ev[0], ctx->ev[1]);
+  ctx->lastTotalMs = tot;
+  ctx->lastContractionMs = contractionMs;
+  ctx->lastLaunches = ctx->launchCount - launch0;
+  return TCSCF_OK;
+}
+
+int validateBasis(tcscf_ctx * ctx, const tcscf_sto * basis, int nb, std::vector<DevSto> & out)
+{
+  TCSCF_CHECK(ctx, basis && nb > 0, TCSCF_ERR_INVALID_ARGUMENT, "empty basis");
+  out.resize(nb);
+  auto fact = [](int k) { double r = 1; for (int i = 2; i <= k; ++i) r *= i; return r; };
+  for (int b = 0; b < nb; ++b) {
+    tcscf_sto const & s = basis[b];
+    // SlaterTypeOrbital.hpp:34-36
+    TCSCF_CHECK(ctx, s.n >= 1 && s.n >= s.l && s.l >= std::abs(s.m), TCSCF_ERR_INVALID_ARGUMENT, "invalid STO quantum numbers");
+    TCSCF_CHECK(ctx, s.l <= kMaxL, TCSCF_ERR_UNSUPPORTED, "angular momentum above 12");
+    TCSCF_CHECK(ctx, s.alpha > 0, TCSCF_ERR_INVALID_ARGUMENT, "non-positive STO exponent");
+    DevSto d{};
+    d.alpha = s.alpha;
+    d.norm = std::pow(2 * s.alpha, s.n) * std::sqrt(2 * s.alpha / fact(2 * s.n));
+    d.n = s.n; d.l = s.l; d.m = s.m;
+    d.rtype = s.m == 0 ? 0 : (s.m > 0 ? 1 : 2);
+    d.partner = -1;
+    if (s.m != 0) {
+      for (int c = 0; c < nb; ++c)
+        if (basis[c].alpha == s.alpha && basis[c].n == s.n && basis[c].l == s.l && basis[c].m == -s.m) { d.partner = c; break; }
+      TCSCF_CHECK(ctx, d.partner >= 0, TCSCF_ERR_UNSUPPORTED, "basis lacks the -m partner of an m != 0 function");
+    }
+    out[b] = d;
+  }
+  return TCSCF_OK;
+}
+
+}  // namespace
+}  // namespace tcscf
+
+using namespace tcscf;
+
+extern "C" {
+
+int tcscf_ctx_create(int device, tcscf_ctx ** out)
+{
+  if (!out) return TCSCF_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return TCSCF_ERR_NO_DEVICE;
+  if (device < 0 || device >= count) return TCSCF_ERR_INVALID_ARGUMENT;
+  if (cudaSetDevice(device) != cudaSuccess) return TCSCF_ERR_CUDA;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return TCSCF_ERR_CUDA;
+  if (prop.major != 10) return TCSCF_ERR_UNSUPPORTED;  // built for sm_100a only
+  tcscf_ctx * ctx = new tcscf_ctx();
+  ctx->device = device;
+  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) { delete ctx; return TCSCF_ERR_CUDA; }
+  for (auto & e : ctx->ev) cudaEventCreate(&e);
+  if (cusolverDnCreate(&ctx->solver) != CUSOLVER_STATUS_SUCCESS) { delete ctx; return TCSCF_ERR_CUDA; }
+  cusolverDnSetStream(ctx->solver, ctx->stream);
+  *out = ctx;
+  return TCSCF_OK;
+}
+
+int tcscf_ctx_destroy(tcscf_ctx * ctx)
+{
+  if (!ctx) return TCSCF_OK;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  for (auto & kv : ctx->grids) {
+    Grid & g = kv.second;
+    cudaFree(g.pts); cudaFree(g.w); cudaFree(g.dsto); cudaFree(g.phiR); cudaFree(g.vals); cudaFree(g.grads);
+  }
+  for (auto & kv : ctx->tensors) cudaFree(kv.second.d);
+  for (auto & kv : ctx->scratch) cudaFree(kv.second.p);
+  for (auto & e : ctx->ev) cudaEventDestroy(e);
+  if (ctx->solver) cusolverDnDestroy(ctx->solver);
+  cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return TCSCF_OK;
+}
+
+const char * tcscf_last_error(tcscf_ctx * ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int tcscf_ctx_stream(tcscf_ctx * ctx, void ** stream)
+{
+  if (!ctx || !stream) return TCSCF_ERR_INVALID_ARGUMENT;
+  *stream = ctx->stream;
+  return TCSCF_OK;
+}
+
+int tcscf_synchronize(tcscf_ctx * ctx)
+{
+  if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
+  TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return TCSCF_OK;
+}
+
+int tcscf_last_timing(tcscf_ctx * ctx, double * contraction_ms, double * total_ms, int * launches)
+{
+  if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
+  if (contraction_ms) *contraction_ms = ctx->lastContractionMs;
+  if (total_ms) *total_ms = ctx->lastTotalMs;
+  if (launches) *launches = ctx->lastLaunches;
+  return TCSCF_OK;
+}
+
+int tcscf_set_flush_window(tcscf_ctx * ctx, int blocks)
+{
+  if (!ctx || blocks < 1 || blocks > 4096) return TCSCF_ERR_INVALID_ARGUMENT;
+  ctx->flushWindow = blocks;
+  return TCSCF_OK;
+}
+
+int tcscf_grid_create(tcscf_ctx * ctx, const double * points, const double * weights, int64_t n, int ndim, int * grid)
+{
+  if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
+  TCSCF_CHECK(ctx, points && weights && grid && n > 0 && (ndim == 2 || ndim == 3), TCSCF_ERR_INVALID_ARGUMENT, "invalid grid arguments");
+  cudaSetDevice(ctx->device);
+  Grid g;
+  g.n = n;
+  g.ndim = ndim;
+  TCSCF_CUDA(ctx, cudaMalloc(&g.pts, sizeof(double) * 3 * n));
+  TCSCF_CUDA(ctx, cudaMalloc(&g.w, sizeof(double) * n));
+  if (ndim == 3) TCSCF_CUDA(ctx, cudaMemcpyAsync(g.pts, points, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, ctx->stream));
+  else {
+    TCSCF_CUDA(ctx, cudaMemcpyAsync(g.pts, points, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
+    TCSCF_CUDA(ctx, cudaMemsetAsync(g.pts + n, 0, sizeof(double) * n, ctx->stream));
+    TCSCF_CUDA(ctx, cudaMemcpyAsync(g.pts + 2 * n, points + n, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
+  }
+  TCSCF_CUDA(ctx, cudaMemcpyAsync(g.w, weights, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
+  TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  int const id = ctx->nextId++;
+  ctx->grids[id] = g;
+  *grid = id;
+  return TCSCF_OK;
+}
+
+int tcscf_grid_destroy(tcscf_ctx * ctx, int grid)
+{
+  if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
+  Grid * g = findGrid(ctx, grid);
+  TCSCF_CHECK(ctx, g, TCSCF_ERR_INVALID_ARGUMENT, "unknown grid handle");
+  cudaStreamSynchronize(ctx->stream);
+  cudaFree(g->pts); cudaFree(g->w); cudaFree(g->dsto); cudaFree(g->phiR); cudaFree(g->vals); cudaFree(g->grads);
+  ctx->grids.erase(grid);
+  return TCSCF_OK;
+}
+
+int tcscf_grid_set_basis(tcscf_ctx * ctx, int grid, const tcscf_sto * basis, int nb, int gradients)
+{
+  if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
+  Grid * g = findGrid(ctx, grid);
+  TCSCF_CHECK(ctx, g, TCSCF_ERR_INVALID_ARGUMENT, "unknown grid handle");
+  std::vector<DevSto> ds;
+  TCSCF_TRY(validateBasis(ctx, basis, nb, ds));
+  cudaStreamSynchronize(ctx->stream);
+  cudaFree(g->dsto); cudaFree(g->phiR); cudaFree(g->vals); cudaFree(g->grads);
+  g->dsto = nullptr; g->phiR = g->vals = g->grads = nullptr;
+  g->nb = 0;
+  TCSCF_CUDA(ctx, cudaMalloc(&g->dsto, sizeof(DevSto) * nb));
+  TCSCF_CUDA(ctx, cudaMalloc(&g->phiR, sizeof(double) * g->n * nb));
+  TCSCF_CUDA(ctx, cudaMalloc(&g->vals, sizeof(double) * g->n * nb * (g->ndim == 3 ? 2 : 1)));
+  if (gradients) TCSCF_CUDA(ctx, cudaMalloc(&g->grads, sizeof(double) * g->n * nb * 6));
+  TCSCF_CUDA(ctx, cudaMemcpyAsync(g->dsto, ds.data(), sizeof(DevSto) * nb, cudaMemcpyHostToDevice, ctx->stream));
+  kBasis<<<gridBlocks(g->n * nb, 256), 256, 0, ctx->stream>>>(g->n, nb, g->ndim, g->pts, g->dsto, g->phiR, g->vals, g->grads);
+  TCSCF_LAUNCH(ctx);
+  TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  g->nb = nb;
+  g->hasGrad = gradients ? 1 : 0;
+  g->basis.assign(basis, basis + nb);
+  return TCSCF_OK;
+}
+
+int tcscf_grid_basis_values(tcscf_ctx * ctx, int grid, double * values, double * gradients)
+{
+  if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
+  Grid * g = findGrid(ctx, grid);
+  TCSCF_CHECK(ctx, g && g->nb > 0, TCSCF_ERR_INVALID_ARGUMENT, "grid has no basis");
+  if (values)
+    TCSCF_CUDA(ctx, cudaMemcpyAsync(values, g->vals, sizeof(double) * g->n * g->nb * (g->ndim == 3 ? 2 : 1), cudaMemcpyDeviceToHost, ctx->stream));
+  if (gradients) {
+    TCSCF_CHECK(ctx, g->grads, TCSCF_ERR_INVALID_ARGUMENT, "gradients were not stored");
+    TCSCF_CUDA(ctx, cudaMemcpyAsync(gradients, g->grads, sizeof(double) * g->n * g->nb * 6, cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return TCSCF_OK;
+}
+
+int tcscf_overlap_core_quadrature(tcscf_ctx * ctx, int grid, int Z, double * S, double * H)
+{
+  if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
+  Grid * g = findGrid(ctx, grid);
+  TCSCF_CHECK(ctx, g && g->nb > 0 && g->ndim == 3, TCSCF_ERR_INVALID_ARGUMENT, "needs a 3-D grid with a basis");
+  TCSCF_CHECK(ctx, S, TCSCF_ERR_INVALID_ARGUMENT, "S is required");
+  TCSCF_CHECK(ctx, !H || g->grads, TCSCF_ERR_INVALID_ARGUMENT, "H needs stored gradients");
+  int const nb = g->nb;
+  void * p = nullptr;
+  TCSCF_TRY(scratch(ctx, "quad_sh", sizeof(double2) * nb * nb * 2, &p));
+  double2 * dS = static_cast<double2 *>(p);
+  double2 * dH = dS + nb * nb;
+  kQuadOverlapCore<<<nb * nb, 256, 0, ctx->stream>>>(g->n, nb, Z, g->pts, g->w, reinterpret_cast<double2 *>(g->vals),
+                                                      H ? reinterpret_cast<double2 *>(g->grads) : nullptr, dS, H ? dH : nullptr);
+  TCSCF_LAUNCH(ctx);
+  TCSCF_CUDA(ctx, cudaMemcpyAsync(S, dS, sizeof(double2) * nb * nb, cudaMemcpyDeviceToHost, ctx->stream));
+  if (H) TCSCF_CUDA(ctx, cudaMemcpyAsync(H, dH, sizeof(double2) * nb * nb, cudaMemcpyDeviceToHost, ctx->stream));
+  TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return TCSCF_OK;
+}
+
+int tcscf_fock_build(tcscf_ctx * ctx, int r1, int r2, int nspin, const double * density, const double * h, int respect_symmetry,
+                     int precision, double * G, double * fock, double * energy)
+{
+  if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  Grid * g1 = findGrid(ctx, r1);
+  Grid * g2 = findGrid(ctx, r2);
+  TCSCF_TRY(checkBasisPair(ctx, g1, g2));
+  TCSCF_CHECK(ctx, nspin == 1 || nspin == 2, TCSCF_ERR_INVALID_ARGUMENT, "nspin must be 1 or 2");
+  TCSCF_CHECK(ctx, density && h, TCSCF_ERR_INVALID_ARGUMENT, "density and h are required");
+  TCSCF_CHECK(ctx, precision >= TCSCF_PREC_FP64 && precision <= TCSCF_PREC_TF32, TCSCF_ERR_INVALID_ARGUMENT, "unknown precision");
+  int const nb = g1->nb;
+  size_t const nn = size_t(nb) * nb;
+  void * p = nullptr;
+  TCSCF_TRY(scratch(ctx, "fock_io", sizeof(double2) * nn * nspin * 3 + sizeof(double) * nn + 64, &p));
+  double2 * dD = static_cast<double2 *>(p);
+  double2 * dG = dD + nn * nspin;
+  double2 * dF = dG + nn * nspin;
+  double * dH = reinterpret_cast<double *>(dF + nn * nspin);
+  double * dE = dH + nn;
+  TCSCF_CUDA(ctx, cudaMemcpyAsync(dD, density, sizeof(double2) * nn * nspin, cudaMemcpyHostToDevice, ctx->stream));
+  TCSCF_CUDA(ctx, cudaMemcpyAsync(dH, h, sizeof(double) * nn, cudaMemcpyHostToDevice, ctx->stream));
+  TCSCF_TRY(fockBuildDevice(ctx, *g1, *g2, nspin, dD, dH, respect_symmetry, precision, dG, dF, dE));
+  if (G) TCSCF_CUDA(ctx, cudaMemcpyAsync(G, dG, sizeof(double2) * nn * nspin, cudaMemcpyDeviceToHost, ctx->stream));
+  if (fock) TCSCF_CUDA(ctx, cudaMemcpyAsync(fock, dF, sizeof(double2) * nn * nspin, cudaMemcpyDeviceToHost, ctx->stream));
+  double e = 0;
+  TCSCF_CUDA(ctx, cudaMemcpyAsync(&e, dE, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (energy) *energy = e;
+  if (!(e == e) || std::isinf(e)) return fail(ctx, TCSCF_ERR_NONFINITE, "non-finite energy");
+  return TCSCF_OK;
+}
+
+int tcscf_fock_build_device(tcscf_ctx * ctx, int r1, int r2, int nspin, const double * density, const double * h, int respect_symmetry,
+                            int precision, double * G, double * fock, double * energy)
+{
+  if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  Grid * g1 = findGrid(ctx, r1);
+  Grid * g2 = findGrid(ctx, r2);
+  TCSCF_TRY(checkBasisPair(ctx, g1, g2));
+  TCSCF_CHECK(ctx, nspin == 1 || nspin == 2, TCSCF_ERR_INVALID_ARGUMENT, "nspin must be 1 or 2");
+  TCSCF_CHECK(ctx, density && h && energy, TCSCF_ERR_INVALID_ARGUMENT, "density, h and energy are required");
+  TCSCF_CHECK(ctx, precision >= TCSCF_PREC_FP64 && precision <= TCSCF_PREC_TF32, TCSCF_ERR_INVALID_ARGUMENT, "unknown precision");
+  size_t const nn = size_t(g1->nb) * g1->nb;
+  void * p = nullptr;
+  TCSCF_TRY(scratch(ctx, "fock_dev_io", sizeof(double2) * nn * nspin * 2, &p));
+  double2 * dG = G ? reinterpret_cast<double2 *>(G) : static_cast<double2 *>(p);
+  double2 * dF = fock ? reinterpret_cast<double2 *>(fock) : static_cast<double2 *>(p) + nn * nspin;
+  TCSCF_TRY(fockBuildDevice(ctx, *g1, *g2, nspin, reinterpret_cast<const double2 *>(density), h, respect_symmetry, precision, dG, dF, energy));
+  TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return TCSCF_OK;
+}
+
+int tcscf_compute_F(tcscf_ctx * ctx, int r1, int r2, int kernel, const tcscf_ochi * jastrow, double * F, int keep, int * fji)
+{
+  if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  Grid * g1 = findGrid(ctx, r1);
+  Grid * g2 = findGrid(ctx, r2);
+  TCSCF_TRY(checkBasisPair(ctx, g1, g2));
+  TCSCF_CHECK(ctx, kernel >= TCSCF_K_INV_R12 && kernel <= TCSCF_K_TC_SCALAR_OPPO, TCSCF_ERR_INVALID_ARGUMENT, "computeF takes a scalar kernel");
+  TCSCF_CHECK(ctx, kernel == TCSCF_K_INV_R12 || jastrow, TCSCF_ERR_INVALID_ARGUMENT, "TC kernels need the Jastrow parameters");
+  TCSCF_CHECK(ctx, !jastrow || (jastrow->nterms >= 0 && jastrow->nterms <= 8), TCSCF_ERR_INVALID_ARGUMENT, "at most 8 Jastrow terms");
+  TCSCF_CHECK(ctx, F || keep, TCSCF_ERR_INVALID_ARGUMENT, "nothing to do");
+  int const nb = g1->nb;
+  int const np = nb * (nb + 1) / 2;
+  int64_t const n1 = g1->n, n2 = g2->n;
+  bool const realOut = g2->ndim == 2;
+  double const scale = realOut ? 2 * kPi : 1.0;
+  void * p = nullptr;
+  TCSCF_TRY(scratch(ctx, "computeF", sizeof(double) * (size_t(n2) * np + size_t(n1) * np), &p));
+  double * pairs = static_cast<double *>(p);
+  double * FR = pairs + size_t(n2) * np;
+  size_t const outElems = size_t(n1) * nb * nb * (realOut ? 1 : 2);
+  double * dOut = nullptr;
+  TCSCF_CUDA(ctx, cudaMalloc(&dOut, sizeof(double) * outElems));
+  cudaEventRecord(ctx->ev[0], ctx->stream);
+  int const launch0 = ctx->launchCount;
+  kPairProducts<<<gridBlocks(n2 * np, 256), 256, 0, ctx->stream>>>(n2, nb, g2->phiR, g2->w, scale, pairs);
+  TCSCF_LAUNCH(ctx);
+  Contraction c;
+  c.n1 = n1; c.n2 = n2; c.R = 0; c.ncol = np; c.p1 = g1->pts; c.p2 = g2->pts; c.V = pairs; c.ldv = np; c.T = FR; c.ldt = np;
+  c.kernel = kernel; c.jastrow = jastrow;
+  cudaEventRecord(ctx->ev[2], ctx->stream);
+  int st = contractFp64(ctx, c);
+  cudaEventRecord(ctx->ev[3], ctx->stream);
+  if (st == TCSCF_OK) {
+    kPairsToReference<<<gridBlocks(n1 * nb * nb, 256), 256, 0, ctx->stream>>>(n1, nb, g1->dsto, FR, 1, 0, realOut ? 1 : 0, dOut);
+    cudaError_t const e = cudaGetLastError();
+    if (e != cudaSuccess) st = fail(ctx, TCSCF_ERR_CUDA, cudaGetErrorString(e));
+    ctx->launchCount++;
+  }
+  if (st == TCSCF_OK && F) {
+    cudaError_t const e = cudaMemcpyAsync(F, dOut, sizeof(double) * outElems, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e != cudaSuccess) st = fail(ctx, TCSCF_ERR_CUDA, cudaGetErrorString(e));
+  }
+  cudaEventRecord(ctx->ev[1], ctx->stream);
+  cudaStreamSynchronize(ctx->stream);
+  float a = 0, b = 0;
+  cudaEventElapsedTime(&a, ctx->ev[2], ctx->ev[3]);
+  cudaEventElapsedTime(&b, ctx->ev[0], ctx->ev[1]);
+  ctx->lastContractionMs = a;
+  ctx->lastTotalMs = b;
+  ctx->lastLaunches = ctx->launchCount - launch0;
+  if (st != TCSCF_OK || !keep) { cudaFree(dOut); return st; }
+  Tensor t;
+  t.d = dOut; t.n1 = n1; t.nb = nb; t.isComplex = realOut ? 0 : 1; t.vec = 0;
+  int const id = ctx->nextId++;
+  ctx->tensors[id] = t;
+  if (fji) *fji = id;
+  return TCSCF_OK;
+}
+
+int tcscf_compute_V(tcscf_ctx * ctx, int r1, int r2, int kernel, const tcscf_ochi * jastrow, double * V, int keep, int * vji)
+{
+  if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  Grid * g1 = findGrid(ctx, r1);
+  Grid * g2 = findGrid(ctx, r2);
+  TCSCF_TRY(checkBasisPair(ctx, g1, g2));
+  TCSCF_CHECK(ctx, g2->ndim == 3, TCSCF_ERR_INVALID_ARGUMENT, "computeV needs a 3-D r2 grid");
+  TCSCF_CHECK(ctx, kernel == TCSCF_K_GRAD_U_SAME || kernel == TCSCF_K_GRAD_U_OPPO, TCSCF_ERR_INVALID_ARGUMENT, "computeV takes a vector kernel");
+  TCSCF_CHECK(ctx, jastrow && jastrow->nterms >= 0 && jastrow->nterms <= 8, TCSCF_ERR_INVALID_ARGUMENT, "Jastrow parameters required");
+  TCSCF_CHECK(ctx, V || keep, TCSCF_ERR_INVALID_ARGUMENT, "nothing to do");
+  int const nb = g1->nb;
+  int const np = nb * (nb + 1) / 2;
+  int64_t const n1 = g1->n, n2 = g2->n;
+  void * p = nullptr;
+  TCSCF_TRY(scratch(ctx, "computeF", sizeof(double) * (size_t(n2) * np + size_t(n1) * np), &p));
+  double * pairs = static_cast<double *>(p);
+  double * FR = pairs + size_t(n2) * np;
+  size_t const outElems = size_t(n1) * nb * nb * 3 * 2;
+  double * dOut = nullptr;
+  TCSCF_CUDA(ctx, cudaMalloc(&dOut, sizeof(double) * outElems));
+  cudaEventRecord(ctx->ev[0], ctx->stream);
+  int const launch0 = ctx->launchCount;
+  kPairProducts<<<gridBlocks(n2 * np, 256), 256, 0, ctx->stream>>>(n2, nb, g2->phiR, g2->w, 1.0, pairs);
+  TCSCF_LAUNCH(ctx);
+  int st = TCSCF_OK;
+  float contraction = 0;
+  for (int comp = 0; comp < 3 && st == TCSCF_OK; ++comp) {
+    Contraction c;
+    c.n1 = n1; c.n2 = n2; c.R = 0; c.ncol = np; c.p1 = g1->pts; c.p2 = g2->pts; c.V = pairs; c.ldv = np; c.T = FR; c.ldt = np;
+    c.kernel = kernel; c.component = comp; c.jastrow = jastrow;
+    cudaEventRecord(ctx->ev[2], ctx->stream);
+    st = contractFp64(ctx, c);
+    cudaEventRecord(ctx->ev[3], ctx->stream);
+    if (st == TCSCF_OK) {
+      kPairsToReference<<<gridBlocks(n1 * nb * nb, 256), 256, 0, ctx->stream>>>(n1, nb, g1->dsto, FR, 3, comp, 0, dOut);
+      ctx->launchCount++;
+      cudaError_t const e = cudaGetLastError();
+      if (e != cudaSuccess) st = fail(ctx, TCSCF_ERR_CUDA, cudaGetErrorString(e));
+    }
+    cudaStreamSynchronize(ctx->stream);
+    float a = 0;
+    cudaEventElapsedTime(&a, ctx->ev[2], ctx->ev[3]);
+    contraction += a;
+  }
+  if (st == TCSCF_OK && V) {
+    cudaError_t const e = cudaMemcpyAsync(V, dOut, sizeof(double) * outElems, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e != cudaSuccess) st = fail(ctx, TCSCF_ERR_CUDA, cudaGetErrorString(e));
+  }
+  cudaEventRecord(ctx->ev[1], ctx->stream);
+  cudaStreamSynchronize(ctx->stream);
+  float b = 0;
+  cudaEventElapsedTime(&b, ctx->ev[0], ctx->ev[1]);
+  ctx->lastContractionMs = contraction;
+  ctx->lastTotalMs = b;
+  ctx->lastLaunches = ctx->launchCount - launch0;
+  if (st != TCSCF_OK || !keep) { cudaFree(dOut); return st; }
+  Tensor t;
+  t.d = dOut; t.n1 = n1; t.nb = nb; t.isComplex = 1; t.vec = 1;
+  int const id = ctx->nextId++;
+  ctx->tensors[id] = t;
+  if (vji) *vji = id;
+  return TCSCF_OK;
+}
+
+int tcscf_tensor_destroy(tcscf_ctx * ctx, int handle)
+{
+  if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
+  auto it = ctx->tensors.find(handle);
+  TCSCF_CHECK(ctx, it != ctx->tensors.end(), TCSCF_ERR_INVALID_ARGUMENT, "unknown tensor handle");
+  cudaStreamSynchronize(ctx->stream);
+  cudaFree(it->second.d);
+  ctx->tensors.erase(it);
+  return TCSCF_OK;
+}
+
+int tcscf_fock_build_precomputed(tcscf_ctx * ctx, int r1, int fji, int nspin, const double * density, const double * h,
+                                 int respect_symmetry, double * G, double * fock, double * energy)
+{
+  if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  Grid * g1 = findGrid(ctx, r1);
+  TCSCF_CHECK(ctx, g1 && g1->nb > 0 && g1->ndim == 3, TCSCF_ERR_INVALID_ARGUMENT, "r1 grid needs a basis");
+  auto it = ctx->tensors.find(fji);
+  TCSCF_CHECK(ctx, it != ctx->tensors.end() && !it->second.vec, TCSCF_ERR_INVALID_ARGUMENT, "unknown Fji handle");
+  Tensor const & t = it->second;
+  TCSCF_CHECK(ctx, t.n1 == g1->n && t.nb == g1->nb, TCSCF_ERR_INVALID_ARGUMENT, "Fji does not match the r1 grid");
+  TCSCF_CHECK(ctx, nspin == 1 || nspin == 2, TCSCF_ERR_INVALID_ARGUMENT, "nspin must be 1 or 2");
+  TCSCF_CHECK(ctx, density && h, TCSCF_ERR_INVALID_ARGUMENT, "density and h are required");
+  int const nb = g1->nb;
+  int64_t const n1 = g1->n;
+  size_t const nn = size_t(nb) * nb;
+  void * p = nullptr;
+  TCSCF_TRY(scratch(ctx, "fock_pre", sizeof(double2) * (nn * nspin * 3 + size_t(nspin) * n1 * (nb + 1) + n1) + sizeof(double) * (nn + 8), &p));
+  double2 * dD = static_cast<double2 *>(p);
+  double2 * dG = dD + nn * nspin;
+  double2 * dF = dG + nn * nspin;
+  double2 * Faa = dF + nn * nspin;
+  double2 * FaaTot = Faa + size_t(nspin) * n1;
+  double2 * Fai = FaaTot + n1;
+  double * dH = reinterpret_cast<double *>(Fai + size_t(nspin) * n1 * nb);
+  double * dE = dH + nn;
+  TCSCF_CUDA(ctx, cudaMemcpyAsync(dD, density, sizeof(double2) * nn * nspin, cudaMemcpyHostToDevice, ctx->stream));
+  TCSCF_CUDA(ctx, cudaMemcpyAsync(dH, h, sizeof(double) * nn, cudaMemcpyHostToDevice, ctx->stream));
+  TCSCF_CUDA(ctx, cudaMemsetAsync(Faa, 0, sizeof(double2) * (size_t(nspin) * n1 * (nb + 1) + n1), ctx->stream));
+  TCSCF_CUDA(ctx, cudaMemsetAsync(dG, 0, sizeof(double2) * nn * nspin, ctx->stream));
+  cudaEventRecord(ctx->ev[0], ctx->stream);
+  int const launch0 = ctx->launchCount;
+  for (int s = 0; s < nspin; ++s) {
+    size_t const sm = sizeof(double2) * nb;
+    if (t.isComplex)
+      kFaaFai<true><<<unsigned(n1), 128, sm, ctx->stream>>>(n1, nb, t.d, reinterpret_cast<double2 *>(g1->vals), dD + s * nn, Faa + s * n1, Fai + s * n1 * nb);
+    else
+      kFaaFai<false><<<unsigned(n1), 128, sm, ctx->stream>>>(n1, nb, t.d, reinterpret_cast<double2 *>(g1->vals), dD + s * nn, Faa + s * n1, Fai + s * n1 * nb);
+    TCSCF_LAUNCH(ctx);
+    kAddInto<<<gridBlocks(2 * n1, 256), 256, 0, ctx->stream>>>(2 * n1, reinterpret_cast<double *>(Faa + s * n1), reinterpret_cast<double *>(FaaTot));
+    TCSCF_LAUNCH(ctx);
+  }
+  double const cJ = nspin == 1 ? 2.0 : 1.0;
+  for (int s = 0; s < nspin; ++s)
+    TCSCF_TRY(reduceFockComplex(ctx, n1, nb, g1->vals, g1->w, reinterpret_cast<double *>(FaaTot), cJ,
+                                reinterpret_cast<double *>(Fai + s * n1 * nb), reinterpret_cast<double *>(dG + s * nn)));
+  kFinalize<<<1, 512, 0, ctx->stream>>>(nspin, nb, dH, dG, nullptr, dD, respect_symmetry, nspin == 1 ? 2.0 : 1.0, dF, dE);
+  TCSCF_LAUNCH(ctx);
+  cudaEventRecord(ctx->ev[1], ctx->stream);
+  if (G) TCSCF_CUDA(ctx, cudaMemcpyAsync(G, dG, sizeof(double2) * nn * nspin, cudaMemcpyDeviceToHost, ctx->stream));
+  if (fock) TCSCF_CUDA(ctx, cudaMemcpyAsync(fock, dF, sizeof(double2) * nn * nspin, cudaMemcpyDeviceToHost, ctx->stream));
+  double e = 0;
+  TCSCF_CUDA(ctx, cudaMemcpyAsync(&e, dE, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+  TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  float ms = 0;
+  cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
+  ctx->lastTotalMs = ms;
+  ctx->lastContractionMs = ms;
+  ctx->lastLaunches = ctx->launchCount - launch0;
+  if (energy) *energy = e;
+  if (!(e == e) || std::isinf(e)) return fail(ctx, TCSCF_ERR_NONFINITE, "non-finite energy");
+  return TCSCF_OK;
+}
+
+int tcscf_scf(tcscf_ctx * ctx, int r1, int r2, int nspin, int n_up, int n_down, const double * S, const double * h, int respect_symmetry,
+              int precision, double tol, int max_iter, double * energy, int * iterations, double * density, double * eigenvalues)
+{
+  if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  Grid * g1 = findGrid(ctx, r1);
+  Grid * g2 = findGrid(ctx, r2);
+  TCSCF_TRY(checkBasisPair(ctx, g1, g2));
+  TCSCF_CHECK(ctx, nspin == 1 || nspin == 2, TCSCF_ERR_INVALID_ARGUMENT, "nspin must be 1 or 2");
+  TCSCF_CHECK(ctx, S && h && max_iter > 0, TCSCF_ERR_INVALID_ARGUMENT, "S, h and max_iter are required");
+  // RCSHartreeFock requires an even electron count (HartreeFock.hpp:248)
+  TCSCF_CHECK(ctx, nspin == 2 || (n_up + n_down) % 2 == 0, TCSCF_ERR_INVALID_ARGUMENT, "RCS needs an even electron count");
+  int const nb = g1->nb;
+  int const nocc[2] = {nspin == 1 ? (n_up + n_down) / 2 : n_up, n_down};
+  TCSCF_CHECK(ctx, nocc[0] <= nb && nocc[1] <= nb && nocc[0] >= 0 && nocc[1] >= 0, TCSCF_ERR_INVALID_ARGUMENT, "more electrons than basis functions");
+  size_t const nn = size_t(nb) * nb;
+  void * p = nullptr;
+  TCSCF_TRY(scratch(ctx, "scf", sizeof(double2) * (nn * nspin * 3 + nn * 2) + sizeof(double) * (nn * 2 + nb * nspin + 16), &p));
+  double2 * dD = static_cast<double2 *>(p);
+  double2 * dG = dD + nn * nspin;
+  double2 * dF = dG + nn * nspin;
+  double2 * A = dF + nn * nspin;
+  double2 * B = A + nn;
+  double * dH = reinterpret_cast<double *>(B + nn);
+  double * dS = dH + nn;
+  double * W = dS + nn;
+  double * dE = W + nb * nspin;
+  int * devInfo = reinterpret_cast<int *>(dE + 8);
+  TCSCF_CUDA(ctx, cudaMemsetAsync(dD, 0, sizeof(double2) * nn * nspin, ctx->stream));
+  TCSCF_CUDA(ctx, cudaMemcpyAsync(dH, h, sizeof(double) * nn, cudaMemcpyHostToDevice, ctx->stream));
+  TCSCF_CUDA(ctx, cudaMemcpyAsync(dS, S, sizeof(double) * nn, cudaMemcpyHostToDevice, ctx->stream));
+  int lwork = 0;
+  if (cusolverDnZhegvd_bufferSize(ctx->solver, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, nb,
+                                  reinterpret_cast<cuDoubleComplex *>(A), nb, reinterpret_cast<cuDoubleComplex *>(B), nb, W, &lwork) != CUSOLVER_STATUS_SUCCESS)
+    return fail(ctx, TCSCF_ERR_LINALG, "cusolverDnZhegvd_bufferSize failed");
+  void * wk = nullptr;
+  TCSCF_TRY(scratch(ctx, "hegvd_work", sizeof(double2) * size_t(lwork) + 64, &wk));
+  double e = std::numeric_limits<double>::max();
+  for (int it = 0; it < max_iter; ++it) {
+    TCSCF_TRY(fockBuildDevice(ctx, *g1, *g2, nspin, dD, dH, respect_symmetry, precision, dG, dF, dE));
+    double ne = 0;
+    TCSCF_CUDA(ctx, cudaMemcpyAsync(&ne, dE, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (!(ne == ne) || std::isinf(ne)) return fail(ctx, TCSCF_ERR_NONFINITE, "non-finite energy");
+    if (iterations) *iterations = it + 1;
+    if (std::fabs(ne - e) < tol) {
+      if (energy) *energy = ne;
+      if (density) TCSCF_CUDA(ctx, cudaMemcpy(density, dD, sizeof(double2) * nn * nspin, cudaMemcpyDeviceToHost));
+      if (eigenvalues) TCSCF_CUDA(ctx, cudaMemcpy(eigenvalues, W, sizeof(double) * nb * nspin, cudaMemcpyDeviceToHost));
+      return TCSCF_OK;
+    }
+    e = ne;
+    for (int s = 0; s < nspin; ++s) {
+      kToColumnMajor<<<gridBlocks(nn, 256), 256, 0, ctx->stream>>>(nb, dF + s * nn, dS, A, B);
+      TCSCF_LAUNCH(ctx);
+      if (cusolverDnZhegvd(ctx->solver, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, nb,
+                           reinterpret_cast<cuDoubleComplex *>(A), nb, reinterpret_cast<cuDoubleComplex *>(B), nb, W + s * nb,
+                           static_cast<cuDoubleComplex *>(wk), lwork, devInfo) != CUSOLVER_STATUS_SUCCESS)
+        return fail(ctx, TCSCF_ERR_LINALG, "cusolverDnZhegvd failed");
+      int info = 0;
+      TCSCF_CUDA(ctx, cudaMemcpyAsync(&info, devInfo, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+      TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+      if (info != 0) return fail(ctx, TCSCF_ERR_LINALG, "generalized eigen-solve failed (info " + std::to_string(info) + ")");
+      kDensityFromOrbitals<<<gridBlocks(nn, 256), 256, 0, ctx->stream>>>(nb, nocc[s], A, dD + s * nn);
+      TCSCF_LAUNCH(ctx);
+    }
+  }
+  if (energy) *energy = e;
+  if (density) TCSCF_CUDA(ctx, cudaMemcpy(density, dD, sizeof(double2) * nn * nspin, cudaMemcpyDeviceToHost));
+  if (eigenvalues) TCSCF_CUDA(ctx, cudaMemcpy(eigenvalues, W, sizeof(double) * nb * nspin, cudaMemcpyDeviceToHost));
+  return fail(ctx, TCSCF_ERR_NOT_CONVERGED, "Did not converge.");
+}
+
+}  // extern "C"

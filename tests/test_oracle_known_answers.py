@@ -1,0 +1,136 @@
+"""Pins the CPU oracle (and the host grid generators) against the reference's own known answers.
+
+Each constant comes from tests/golden/known_answers.json, which cites the reference test it is
+taken from (generated by tests/golden/make_golden.py).
+"""
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oracle
+from tcscf_b200 import ffi, grids
+
+KA = json.loads((Path(__file__).parent / "golden" / "known_answers.json").read_text())
+MAP_NONE, MAP_TA = 0, 3
+
+
+def _cg(n, map_=MAP_NONE, p0=0.0, p1=0.0):
+    return oracle.radial_grid(n, map_, p0, p1)
+
+
+def test_chebyshev_gauss_polynomials():
+    # IntegrationTest.cpp:19-57
+    for key, f in (("chebyshev_linear", lambda x: x), ("chebyshev_quadratic", lambda x: x * x),
+                   ("chebyshev_cubic", lambda x: x ** 3 + 3 * x ** 2 - 4 * x)):
+        ka = KA[key]
+        x, w = _cg(ka["n"])
+        assert abs(np.sum(f(x) * w) - ka["value"]) < ka["tol"], key
+
+
+def test_radial_maps_exponential_integrals():
+    # IntegrationTest.cpp:76-139 with the reference's current Treutler-Ahlrichs M4 map (a = 1, eps = 1),
+    # the map TreutlerAhlrichsLebedev builds (TreutlerAhlrichsLebedev.hpp:28-31)
+    ka = KA["radial_exponential"]
+    r, w = _cg(ka["n"], MAP_TA, 1.0, 1.0)
+    assert abs(np.sum(np.exp(-r) * w) - ka["value"]) < ka["tol"]
+    ka = KA["radial_exp_polynomial"]
+    assert abs(np.sum((r ** 2 - 3 * r) * np.exp(-1.5 * r) * w) - ka["value"]) < ka["tol"]
+
+
+def test_library_radial_grid_matches_oracle():
+    for map_, p0, p1 in ((0, 0, 0), (1, 2.5, 0), (2, 0, 0), (3, 1.0, 0.9), (3, 0.0, 0.9), (4, 0, 0)):
+        u1, w1 = oracle.radial_grid(37, map_, p0, p1)
+        u2, w2 = grids.radial_grid(37, map_, p0, p1)
+        np.testing.assert_allclose(u2, u1, rtol=1e-15, atol=0)
+        np.testing.assert_allclose(w2, w1, rtol=1e-15, atol=0)
+
+
+def test_lebedev_constant():
+    ka = KA["lebedev_constant"]
+    ang = grids.lebedev_table(ka["order"])
+    assert abs(ang[:, 2].sum() - ka["value"]) < ka["tol"]
+
+
+ORDERS = [3, 5, 7, 9, 11, 13, 15, 17, 19, 21, 23, 25, 27, 29, 31, 35, 41, 47, 53, 59, 65, 71, 77, 83, 89, 95, 101,
+          107, 113, 119, 125, 131]
+
+
+@pytest.mark.parametrize("order", ORDERS)
+def test_lebedev_spherical_harmonics_orthonormal(order):
+    # IntegrationTest.cpp:157-197: 10 m = l samples and 50 random (l, m) pairs per order
+    tol_unit = KA["lebedev_ylm_tol_per_degree"]["value"]
+    ang = grids.lebedev_table(order)
+    rng = np.random.default_rng(order)
+    for i in range(60):
+        l1 = int(rng.integers(0, order + 1))
+        l2 = int(rng.integers(0, order - l1 + 1))
+        m1, m2 = l1, l2
+        if i >= 10:
+            m1 = int(rng.integers(-l1, l1 + 1))
+            m2 = int(rng.integers(-l2, l2 + 1))
+        if max(l1, l2) > 40:  # keep the pure-Python loop short; the high-l pairs still cover every order
+            continue
+        val = 0.0
+        for th, ph, w in ang:
+            val += w * np.conj(oracle.sph_harmonic(l1, m1, th, ph)) * oracle.sph_harmonic(l2, m2, th, ph)
+        delta = 1.0 if (l1 == l2 and m1 == m2) else 0.0
+        assert abs(val - delta) < (l1 + l2 + order) * tol_unit, (order, l1, m1, l2, m2, val)
+
+
+def test_sto_quadrature_overlap_equals_analytic():
+    # SlaterTypeOrbitalTest.cpp:14-47: radial(1000, TA-M4(1, eps=1)) x Lebedev(11), all n < 5, n' <= n
+    ka = KA["sto_overlap"]
+    r, wr = oracle.radial_grid(ka["radial"], MAP_TA, 1.0, ka["epsilon"])
+    pts, w = oracle.product_grid(r, wr, grids.lebedev_table(ka["order"]))
+    basis = []
+    pairs = []
+    for n in range(1, ka["order"] // 2):
+        for npr in range(1, n + 1):
+            for l in range(0, npr + 1):
+                for m in range(-l, l + 1):
+                    pairs.append((len(basis), len(basis) + 1))
+                    basis += [(ka["alpha1"], n, l, m), (ka["alpha2"], npr, l, m)]
+    vals = oracle.basis_values(pts, basis)
+    S_an, _ = oracle.overlap_core(basis, 1)
+    for i, j in pairs:
+        q = np.sum(w * np.conj(vals[:, i]) * vals[:, j])
+        assert abs(q.real - S_an[i, j]) < ka["tol"] and abs(q.imag) < ka["tol"], (basis[i], basis[j], q, S_an[i, j])
+
+
+def test_ochi_gradient_matches_finite_difference():
+    # gradientsTest.cpp:59-93 (positive c, opposite spin)
+    ka = KA["ochi_gradient"]
+    u = oracle.ochi(ka["a"], ka["a"], [((1, 0, 0), ka["c_oppo"], ka["c_same"])])
+    rng = np.random.default_rng(0)
+    h = ka["h"]
+    r1 = np.array(ka["r1"], dtype=float)
+    for _ in range(ka["samples"]):
+        r2 = rng.uniform(*ka["range"], size=3)
+
+        def f(p):
+            return oracle.ochi_value(u, np.linalg.norm(p), np.linalg.norm(r2), np.linalg.norm(p - r2), False)
+
+        fd = np.array([(f(r1 + h * e) - f(r1 - h * e)) / (2 * h) for e in np.eye(3)])
+        g = oracle.ochi_gradient(u, r1, r2, False)
+        np.testing.assert_allclose(g, fd, atol=ka["tol"], rtol=0)
+
+
+def test_modified_gram_schmidt_orthonormal():
+    # orthogonalizationTest.cpp:48-62
+    rng = np.random.default_rng(1)
+    v = rng.normal(size=(6, 10)) + 1j * rng.normal(size=(6, 10))
+    q = oracle.mgs(v)
+    np.testing.assert_allclose(q.conj() @ q.T, np.eye(6), atol=1e-12)
+
+
+def test_sto_normalization_and_overlap_diagonal_is_one():
+    basis = [(0.7, 1, 0, 0), (1.3, 2, 1, -1), (2.1, 3, 2, 1), (0.4, 4, 3, 3)]
+    S, _ = oracle.overlap_core(basis, 2)
+    np.testing.assert_allclose(np.diag(S), 1.0, rtol=1e-13)
+    S2, H2 = np.empty((4, 4)), np.empty((4, 4))
+    ffi.check(ffi.lib().tcscf_overlap_core_analytic(ffi.sto_array(basis), 4, 2, ffi.dptr(S2), ffi.dptr(H2)))
+    S1, H1 = oracle.overlap_core(basis, 2)
+    np.testing.assert_allclose(S2, S1, rtol=1e-15, atol=0)
+    np.testing.assert_allclose(H2, H1, rtol=1e-15, atol=0)
