@@ -85,23 +85,66 @@ __device__ __forceinline__ double r12Kernel(KArgs const & a, double x1, double y
   return a.component == 0 ? gx : (a.component == 1 ? gy : gz);
 }
 
-template <int KIND>
+__device__ __forceinline__ void cpAsync8(double * dst, const double * src, bool valid)
+{
+  unsigned const d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  int const n = valid ? 8 : 0;   // src-size 0 zero-fills the destination
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cpAsyncWait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+// Block: BM r1 rows x BN columns, 256 threads.  r2 streamed in BK blocks through a two-stage
+// cp.async pipeline (coordinates, Coulomb source, psi2 and V of block i+1 load while block i
+// computes).  Phase B: each thread generates 8 kernel values g(r1,r2) (and rho) of one row;
+// phase C: register-tiled FP64 GEMM, each thread 4 rows x BN/16 columns, columns interleaved in
+// pairs so that a half-warp reads 16 consecutive 16-byte chunks (conflict-free).
+template <int KIND, int BN>
 __global__ void __launch_bounds__(NT, 2) kContractFp64(KArgs a)
 {
-  extern __shared__ double sm[];
+  constexpr int CPT = BN / 16;            // columns per thread
+  extern __shared__ __align__(16) double sm[];
   int const R = a.R;
-  double * sP1 = sm;                        // [R][BM]
-  double * sC1 = sP1 + R * BM;              // [3][BM]
-  double * sP2 = sC1 + 3 * BM;              // [R][BK]
-  double * sC2 = sP2 + R * BK;              // [4][BK] x, y, z, coul
-  double * sV = sC2 + 4 * BK;               // [BK][BN]
-  double * sX = sV + BK * BN;               // [BK][BM]
+  double * sP1 = sm;                              // [R][BM]
+  double * sC1 = sP1 + R * BM;                    // [3][BM]
+  double * sX = sC1 + 3 * BM;                     // [BK][BM]
+  double * stage0 = sX + BK * BM;                 // per stage: sV [BK][BN], sC2 [4][BK], sP2 [R][BK]
+  int const stageSize = BK * BN + 4 * BK + R * BK;
 
   int const tid = threadIdx.x;
   int64_t const r1base = int64_t(blockIdx.x) * BM;
   int const cg = blockIdx.z;
   int64_t const r2begin = int64_t(blockIdx.y) * a.r2PerSplit;
   int64_t const r2end = min(a.n2, r2begin + a.r2PerSplit);
+  bool const doCoul = a.coul != nullptr && cg == 0;
+
+  auto issue = [&](int64_t k0, int st) {
+    double * sV = stage0 + st * stageSize;
+    double * sC2 = sV + BK * BN;
+    double * sP2 = sC2 + 4 * BK;
+    int const kn = int(min(int64_t(BK), r2end - k0));
+    for (int idx = tid; idx < BK * BN; idx += NT) {
+      int const k = idx / BN, c = idx % BN;
+      int const col = cg * BN + c;
+      bool const ok = k < kn && col < a.ncol;
+      cpAsync8(&sV[idx], ok ? &a.V[(k0 + k) * a.ldv + col] : a.V, ok);
+    }
+    for (int idx = tid; idx < R * BK; idx += NT) {
+      int const k = idx / R, b = idx % R;
+      bool const ok = k < kn;
+      cpAsync8(&sP2[b * BK + k], ok ? &a.psi2[(k0 + k) * a.ldpsi + b] : a.psi2, ok);
+    }
+    if (tid < 4 * BK) {
+      int const d = tid / BK, k = tid % BK;
+      bool const ok = k < kn && (d < 3 || doCoul);
+      const double * src = d < 3 ? &a.p2[d * a.n2 + k0 + k] : (doCoul ? &a.coul[k0 + k] : a.p2);
+      cpAsync8(&sC2[d * BK + k], ok ? src : a.p2, ok);
+    }
+  };
+
+  int64_t const nsteps = (r2end - r2begin + BK - 1) / BK;
+  if (nsteps > 0) issue(r2begin, 0);
+  cpAsyncCommit();
 
   for (int idx = tid; idx < R * BM; idx += NT) {
     int const r = idx / R, b = idx % R;
@@ -119,35 +162,25 @@ __global__ void __launch_bounds__(NT, 2) kContractFp64(KArgs a)
   int const cB = (tid & 3) * 8;    // phase-B first column
   double const x1 = sC1[rB], y1 = sC1[BM + rB], z1 = sC1[2 * BM + rB];
   int const tr = tid >> 4, tc = tid & 15;
-  double acc[4][8];
+  double acc[4][CPT];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
+    for (int j = 0; j < CPT; ++j) acc[i][j] = 0.0;
   double vh = 0.0;
-  bool const doCoul = a.coul != nullptr && cg == 0;
 
-  for (int64_t k0 = r2begin; k0 < r2end; k0 += BK) {
+  for (int64_t step = 0; step < nsteps; ++step) {
+    int64_t const k0 = r2begin + step * BK;
+    int const st = int(step & 1);
+    __syncthreads();   // every thread is done with the stage the next issue overwrites
+    if (step + 1 < nsteps) issue(k0 + BK, st ^ 1);
+    cpAsyncCommit();
+    cpAsyncWait1();
+    __syncthreads();
+    double const * sV = stage0 + st * stageSize;
+    double const * sC2 = sV + BK * BN;
+    double const * sP2 = sC2 + 4 * BK;
     int const kn = int(min(int64_t(BK), r2end - k0));
-    __syncthreads();
-    for (int idx = tid; idx < BK * BN; idx += NT) {
-      int const k = idx / BN, c = idx % BN;
-      int const col = cg * BN + c;
-      sV[idx] = (k < kn && col < a.ncol) ? a.V[(k0 + k) * a.ldv + col] : 0.0;
-    }
-    for (int idx = tid; idx < R * BK; idx += NT) {
-      int const k = idx / R, b = idx % R;
-      sP2[b * BK + k] = k < kn ? a.psi2[(k0 + k) * a.ldpsi + b] : 0.0;
-    }
-    if (tid < BK) {
-      int const k = tid;
-      bool const ok = k < kn;
-      sC2[k] = ok ? a.p2[k0 + k] : 0.0;
-      sC2[BK + k] = ok ? a.p2[a.n2 + k0 + k] : 0.0;
-      sC2[2 * BK + k] = ok ? a.p2[2 * a.n2 + k0 + k] : 0.0;
-      sC2[3 * BK + k] = (ok && doCoul) ? a.coul[k0 + k] : 0.0;
-    }
-    __syncthreads();
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
       int const c = cB + j;
@@ -166,18 +199,18 @@ __global__ void __launch_bounds__(NT, 2) kContractFp64(KArgs a)
     for (int k = 0; k < BK; ++k) {
       double2 const a01 = *reinterpret_cast<double2 const *>(&sX[k * BM + tr * 4]);
       double2 const a23 = *reinterpret_cast<double2 const *>(&sX[k * BM + tr * 4 + 2]);
-      double av[4] = {a01.x, a01.y, a23.x, a23.y};
-      double bv[8];
+      double const av[4] = {a01.x, a01.y, a23.x, a23.y};
+      double bv[CPT];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        double2 const bb = *reinterpret_cast<double2 const *>(&sV[k * BN + tc * 8 + 2 * q]);
+      for (int q = 0; q < CPT / 2; ++q) {
+        double2 const bb = *reinterpret_cast<double2 const *>(&sV[k * BN + 32 * q + 2 * tc]);
         bv[2 * q] = bb.x;
         bv[2 * q + 1] = bb.y;
       }
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 8; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+        for (int j = 0; j < CPT; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
     }
   }
 
@@ -187,8 +220,8 @@ __global__ void __launch_bounds__(NT, 2) kContractFp64(KArgs a)
     int64_t const g = r1base + tr * 4 + i;
     if (g >= a.n1) continue;
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      int const col = cg * BN + tc * 8 + j;
+    for (int j = 0; j < CPT; ++j) {
+      int const col = cg * BN + 32 * (j / 2) + 2 * tc + (j & 1);
       if (col < a.ncol) T[g * a.ldt + col] = acc[i][j];
     }
   }
@@ -338,6 +371,34 @@ __global__ void __launch_bounds__(NT) kReduceComplex(int64_t n1, int nb, const d
   }
 }
 
+template <int KIND, int BNV>
+int launchOne(tcscf_ctx * ctx, KArgs const & a, dim3 grid, size_t smem)
+{
+  TCSCF_CUDA(ctx, cudaFuncSetAttribute(kContractFp64<KIND, BNV>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  kContractFp64<KIND, BNV><<<grid, NT, smem, ctx->stream>>>(a);
+  TCSCF_LAUNCH(ctx);
+  return TCSCF_OK;
+}
+
+int launchContract(tcscf_ctx * ctx, int kind, int bn, KArgs const & a, unsigned tiles, unsigned nsplit, size_t smem)
+{
+  unsigned const cgroups = a.ncol <= 128 ? 1u : unsigned((a.ncol + BN - 1) / BN);
+  dim3 const grid{tiles, nsplit, cgroups};
+  if (kind == 0) {
+    if (bn == 32) return launchOne<0, 32>(ctx, a, grid, smem);
+    if (bn == 64) return launchOne<0, 64>(ctx, a, grid, smem);
+    return launchOne<0, 128>(ctx, a, grid, smem);
+  }
+  if (kind == 1) {
+    if (bn == 32) return launchOne<1, 32>(ctx, a, grid, smem);
+    if (bn == 64) return launchOne<1, 64>(ctx, a, grid, smem);
+    return launchOne<1, 128>(ctx, a, grid, smem);
+  }
+  if (bn == 32) return launchOne<2, 32>(ctx, a, grid, smem);
+  if (bn == 64) return launchOne<2, 64>(ctx, a, grid, smem);
+  return launchOne<2, 128>(ctx, a, grid, smem);
+}
+
 }  // namespace
 
 int contractFp64(tcscf_ctx * ctx, Contraction const & c)
@@ -345,7 +406,7 @@ int contractFp64(tcscf_ctx * ctx, Contraction const & c)
   TCSCF_CHECK(ctx, c.R >= 0 && c.R <= 128, TCSCF_ERR_UNSUPPORTED, "contraction rank must be <= 128");
   TCSCF_CHECK(ctx, c.ncol > 0 && c.n1 > 0 && c.n2 > 0, TCSCF_ERR_INVALID_ARGUMENT, "empty contraction");
   int64_t const tiles = (c.n1 + BM - 1) / BM;
-  int const cgroups = (c.ncol + BN - 1) / BN;
+  int const cgroups = c.ncol <= 128 ? 1 : (c.ncol + BN - 1) / BN;
   int dev = 0;
   cudaGetDevice(&dev);
   int sms = 148;
@@ -385,20 +446,10 @@ int contractFp64(tcscf_ctx * ctx, Contraction const & c)
   }
   a.T = Tpart;
   a.VH = VHpart;
-  size_t const smem = sizeof(double) * (size_t(c.R) * BM + 3 * BM + size_t(c.R) * BK + 4 * BK + BK * BN + BK * BM);
-  dim3 grid{unsigned(tiles), unsigned(nsplit), unsigned(cgroups)};
+  int const bn = c.ncol <= 32 ? 32 : (c.ncol <= 64 ? 64 : 128);
+  size_t const smem = sizeof(double) * (size_t(c.R) * BM + 3 * BM + BK * BM + 2 * (size_t(BK) * bn + 4 * BK + size_t(c.R) * BK));
   int const kind = c.kernel == TCSCF_K_INV_R12 ? 0 : (c.kernel <= TCSCF_K_TC_SCALAR_OPPO ? 1 : 2);
-  if (kind == 0) {
-    TCSCF_CUDA(ctx, cudaFuncSetAttribute(kContractFp64<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    kContractFp64<0><<<grid, NT, smem, ctx->stream>>>(a);
-  } else if (kind == 1) {
-    TCSCF_CUDA(ctx, cudaFuncSetAttribute(kContractFp64<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    kContractFp64<1><<<grid, NT, smem, ctx->stream>>>(a);
-  } else {
-    TCSCF_CUDA(ctx, cudaFuncSetAttribute(kContractFp64<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-    kContractFp64<2><<<grid, NT, smem, ctx->stream>>>(a);
-  }
-  TCSCF_LAUNCH(ctx);
+  TCSCF_TRY(launchContract(ctx, kind, bn, a, unsigned(tiles), unsigned(nsplit), smem));
   if (nsplit > 1) {
     int64_t const n = c.n1 * c.ncol;
     kSumSplits<<<gridBlocks(n, 256), 256, 0, ctx->stream>>>(n, int(nsplit), c.n1 * c.ldt, Tpart, c.T, c.n1, c.ncol, c.ldt, c.ldt);
