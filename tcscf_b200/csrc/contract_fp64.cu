@@ -181,18 +181,26 @@ __global__ void __launch_bounds__(NT, 2) kContractFp64(KArgs a)
     double const * sC2 = sV + BK * BN;
     double const * sP2 = sC2 + 4 * BK;
     int const kn = int(min(int64_t(BK), r2end - k0));
+    double rho[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) rho[j] = R > 0 ? 0.0 : 1.0;
+    for (int b = 0; b < R; ++b) {
+      // one psi1 value against 8 psi2 values: 5 shared loads for 8 FMAs
+      double const p = sP1[b * BM + rB];
+#pragma unroll
+      for (int j = 0; j < 8; j += 2) {
+        double2 const q = *reinterpret_cast<double2 const *>(&sP2[b * BK + cB + j]);
+        rho[j] = fma(p, q.x, rho[j]);
+        rho[j + 1] = fma(p, q.y, rho[j + 1]);
+      }
+    }
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
       int const c = cB + j;
-      double rho = 1.0;
-      if (R > 0) {
-        rho = 0.0;
-        for (int b = 0; b < R; ++b) rho = fma(sP1[b * BM + rB], sP2[b * BK + c], rho);
-      }
       double g = r12Kernel<KIND>(a, x1, y1, z1, sC2[c], sC2[BK + c], sC2[2 * BK + c]);
       g = c < kn ? g : 0.0;
       vh = fma(g, sC2[3 * BK + c], vh);
-      sX[c * BM + rB] = g * rho;
+      sX[c * BM + rB] = g * rho[j];
     }
     __syncthreads();
 #pragma unroll 4
@@ -375,6 +383,7 @@ template <int KIND, int BNV>
 int launchOne(tcscf_ctx * ctx, KArgs const & a, dim3 grid, size_t smem)
 {
   TCSCF_CUDA(ctx, cudaFuncSetAttribute(kContractFp64<KIND, BNV>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  TCSCF_CUDA(ctx, cudaFuncSetAttribute(kContractFp64<KIND, BNV>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
   kContractFp64<KIND, BNV><<<grid, NT, smem, ctx->stream>>>(a);
   TCSCF_LAUNCH(ctx);
   return TCSCF_OK;
@@ -459,6 +468,14 @@ int contractFp64(tcscf_ctx * ctx, Contraction const & c)
       TCSCF_LAUNCH(ctx);
     }
   }
+  return TCSCF_OK;
+}
+
+int sumSplitsLaunch(tcscf_ctx * ctx, int64_t n, int nsplit, int64_t stride, const double * part, double * out, int64_t rows, int cols,
+                    int ldOut, int ldPart)
+{
+  kSumSplits<<<gridBlocks(n, 256), 256, 0, ctx->stream>>>(n, nsplit, stride, part, out, rows, cols, ldOut, ldPart);
+  TCSCF_LAUNCH(ctx);
   return TCSCF_OK;
 }
 

@@ -34,6 +34,10 @@ int contractFp64(tcscf_ctx * ctx, Contraction const & c);
 int contractTensor(tcscf_ctx * ctx, Contraction const & c, int precision);
 bool tensorPathAvailable(Contraction const & c, int precision, std::string * why);
 
+// out[r][c] = sum_s part[s*stride + r*ldPart + c] for r < rows, c < cols (deterministic split sum)
+int sumSplitsLaunch(tcscf_ctx * ctx, int64_t n, int nsplit, int64_t stride, const double * part, double * out, int64_t rows, int cols,
+                    int ldOut, int ldPart);
+
 // G_s[k][l] (+)= sum_r1 w1 phi[r1][k] * (cJ * phi[r1][l] * VH[r1] - sgnT * T[r1][l]); real, out [nb][nb]
 int reduceFockReal(tcscf_ctx * ctx, int64_t n1, int nb, const double * phi, const double * w1, const double * VH, double cJ,
                    const double * T, int ldt, double sgnT, double * out);
