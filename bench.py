@@ -90,17 +90,24 @@ class ClockSampler:
 
 
 def scf_guess_density(basis, Z: int, nocc: int):
-    """Core-Hamiltonian guess (the reference's first iteration: zero density -> F = h), solved with
-    canonical orthogonalisation so that the ill-conditioned even-tempered overlap is handled."""
+    """Core-Hamiltonian guess (the reference's first iteration: zero density -> F = h), solved in the
+    real-harmonic basis with canonical orthogonalisation (the even-tempered overlap is
+    ill-conditioned), so the closed-shell density is real there; returned in the reference basis."""
     from tcscf_b200 import api
+    from tcscf_b200.basis import real_harmonic_unitary
 
     S, h = api.overlap_core(basis, Z)
-    s, U = np.linalg.eigh(S)
+    U = real_harmonic_unitary(basis)
+    SR = np.real(U.conj() @ S @ U.T)
+    hR = np.real(U.conj() @ h @ U.T)
+    s, V = np.linalg.eigh(SR)
     keep = s > 1e-10 * s.max()
-    X = U[:, keep] / np.sqrt(s[keep])
-    e, Cp = np.linalg.eigh(X.T @ h @ X)
-    C = X @ Cp[:, :nocc]
-    return (C @ C.T).astype(np.complex128), h
+    X = V[:, keep] / np.sqrt(s[keep])
+    e, Cp = np.linalg.eigh(X.T @ hR @ X)
+    CR = X @ Cp[:, :nocc]
+    DR = CR @ CR.T
+    D = U.T @ DR @ U.conj()
+    return np.ascontiguousarray(D.astype(np.complex128)), h
 
 
 def workload(name: str):

@@ -103,8 +103,11 @@ int tcscf_synchronize(tcscf_ctx * ctx);
 /* device time in ms of the dominant r12 contraction kernel(s) of the most recent Fock build /
  * computeF call, measured with CUDA events on the context stream; launches = kernels launched */
 int tcscf_last_timing(tcscf_ctx * ctx, double * contraction_ms, double * total_ms, int * launches);
+/* diagnostics: the Coulomb potential VH[N1] (both spins) and the first spin's exchange potential
+ * T[N1][nb] (real-harmonic basis) of the most recent direct Fock build on this context */
+int tcscf_last_potentials(tcscf_ctx * ctx, double * VH, double * T);
 /* accumulation window of the tensor-core paths: r2 blocks of 64 accumulated in FP32 in TMEM before
- * being flushed into FP64 (default 4); 1 flushes every block */
+ * being flushed into FP64 (default 1: every block, the most accurate setting) */
 int tcscf_set_flush_window(tcscf_ctx * ctx, int blocks);
 
 /* ---- host-side grid generation (replaces ChebyshevGauss/changeOfVariables/createGrid,

@@ -78,6 +78,13 @@ class Context:
         _raise(ffi.lib().tcscf_last_timing(self._h, C.byref(a), C.byref(b), C.byref(n)), self._h)
         return a.value, b.value, n.value
 
+    def last_potentials(self, n1: int, nb: int):
+        """(VH [n1], T [n1][nb]) of the most recent direct Fock build (diagnostics)."""
+        VH = np.empty(n1)
+        T = np.empty((n1, nb))
+        _raise(ffi.lib().tcscf_last_potentials(self._h, ffi.dptr(VH), ffi.dptr(T)), self._h)
+        return VH, T
+
     def set_flush_window(self, blocks: int) -> None:
         _raise(ffi.lib().tcscf_set_flush_window(self._h, blocks), self._h)
 

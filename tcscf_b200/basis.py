@@ -31,6 +31,25 @@ def budget_counts(budget: int, total: int, lmax: int = 3) -> dict[int, int]:
     return counts
 
 
+def real_harmonic_unitary(basis: Basis) -> np.ndarray:
+    """U with phi^R = U phi: m > 0 -> (phi_m + phi_-m)/sqrt2, m < 0 -> (phi_|m| - phi_-|m|)/(i sqrt2)
+    (the reference's Y_l^m = P_l^|m| e^{i m phi} convention, mathFunctions.hpp:126-139)."""
+    nb = len(basis)
+    idx = {tuple(b): i for i, b in enumerate(basis)}
+    U = np.zeros((nb, nb), dtype=complex)
+    h = 1 / np.sqrt(2)
+    for k, (a, n, l, m) in enumerate(basis):
+        if m == 0:
+            U[k, k] = 1
+            continue
+        p = idx[(a, n, l, -m)]
+        if m > 0:
+            U[k, k], U[k, p] = h, h
+        else:
+            U[k, p], U[k, k] = -1j * h, 1j * h
+    return U
+
+
 @dataclass
 class Workload:
     name: str

@@ -26,8 +26,6 @@ struct DevSto {
   int pad;
 };
 
-struct MixedOperands;  // tensor-core operand cache of a grid (flash_tc.cu)
-
 struct Grid {
   int64_t n = 0;
   int ndim = 3;
@@ -41,7 +39,12 @@ struct Grid {
   double * phiR = nullptr;  // real-harmonic basis values [n][nb]
   double * vals = nullptr;  // reference-basis values [n][nb] (complex for ndim 3, real for ndim 2)
   double * grads = nullptr; // [n][nb][3] complex
-  MixedOperands * mixed = nullptr;
+  // tensor-path cache of the transposed, BF16-split weighted basis values (depends only on the
+  // grid and basis, so it is packed once per grid)
+  void * vtCache = nullptr;
+  int vtNB = 0;
+  int64_t vtN2pad = 0;
+  double vtScale = 0;
 };
 
 struct Tensor {
@@ -67,12 +70,17 @@ struct tcscf_ctx {
   std::map<int, tcscf::Grid> grids;
   std::map<int, tcscf::Tensor> tensors;
   int nextId = 1;
-  int flushWindow = 4;
+  int flushWindow = 1;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   double lastContractionMs = 0, lastTotalMs = 0;
   int lastLaunches = 0;
   int launchCount = 0;
   std::map<std::string, tcscf::Scratch> scratch;
+  // device buffers of the most recent direct Fock build (for tcscf_last_potentials)
+  const double * lastVH = nullptr;
+  const double * lastT = nullptr;
+  int64_t lastN1 = 0;
+  int lastNb = 0;
 };
 
 namespace tcscf {

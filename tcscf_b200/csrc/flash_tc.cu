@@ -9,11 +9,12 @@
 // accumulator is double-buffered so the MMA never waits for a flush).  The kernel matrix g is
 // generated in registers and only ever exists as the BF16 X tile in shared memory.
 //
-// Warp roles (320 threads, one CTA per SM, persistent over (r1 tile, r2 split) work items):
+// Warp roles (384 threads, one CTA per SM, persistent over (r1 tile, r2 split) work items):
 //   warp 0      TMA producer: psi1 tile (once per work item), psi2 / Vt blocks (TMA, no multicast),
 //               r2 coordinates + Coulomb source (1-D bulk copy)
 //   warp 1      MMA issuer (one elected thread) and TMEM allocator
-//   warps 2-9   compute: warp w owns TMEM lanes 32*(w%4).. (r1 rows), column half (w-2)/4
+//   warps 2-3   idle (they complete warpgroup 0, whose registers setmaxnreg hands to the compute warps)
+//   warps 4-11  compute: warp w owns TMEM lanes 32*(w%4).. (r1 rows), column half (w-4)/4
 // Every mbarrier wait is bounded by a wall-clock limit; on expiry the kernel records the failure in
 // a device status word, drains its own TMA / MMA work with bounded waits, frees TMEM and returns.
 #include <cuda.h>
@@ -26,18 +27,23 @@ namespace tc {
 
 constexpr int BM = 128;        // r1 rows per tile
 constexpr int BK = 64;         // r2 points per block
-constexpr int RP = 32;         // padded rank of rho (GEMM1 K)
-constexpr int NSTAGE = 2;      // TMA stages
+// TMA stages: three when the rank padding leaves room in shared memory
+__host__ __device__ constexpr int stagesFor(int RP) { return RP == 32 ? 3 : 2; }
 constexpr int NCW = 8;         // compute warps
-constexpr int NTHREADS = 32 * (2 + NCW);
+constexpr int NTHREADS = 384;  // warpgroup 0: TMA, MMA, 2 idle warps; warpgroups 1-2: compute
+// register split: 384 threads x 168 at launch = 64512 = 128 x 56 (producer warpgroup) + 256 x 224
+constexpr int kRegsLaunch = 168, kRegsProducer = 56, kRegsCompute = 224;
+static_assert(128 * kRegsProducer + 256 * kRegsCompute <= NTHREADS * kRegsLaunch, "register split exceeds the launch allocation");
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s per wait
 
-template <int NB>
+// RP: padded rank of rho (GEMM1 K): 32 (64-byte rows, 64B swizzle) or 64 (128-byte rows, 128B swizzle)
+template <int NB, int RP>
 struct __align__(1024) Smem {
+  static constexpr int NSTAGE = stagesFor(RP);
   uint8_t v[NSTAGE][2][NB * BK * 2];       // Vt block hi/lo: SW128 K-major [NB rows][64]
   uint8_t x[2][2][BM * BK * 2];            // X tile hi/lo:   SW128 K-major [128 rows][64]
-  uint8_t psi2[NSTAGE][2][BK * RP * 2];    // psi2 block hi/lo: SW64 K-major [64 rows][32]
-  uint8_t psi1[2][BM * RP * 2];            // psi1 tile hi/lo:  SW64 K-major [128 rows][32]
+  uint8_t psi2[NSTAGE][2][BK * RP * 2];    // psi2 block hi/lo: K-major [64 rows][RP]
+  uint8_t psi1[2][BM * RP * 2];            // psi1 tile hi/lo:  K-major [128 rows][RP]
   float4 coords[NSTAGE][BK];               // x, y, z, coul of the r2 block
   uint64_t full[NSTAGE], empty[NSTAGE];
   uint64_t sfull[2], sfree[2], xfull[2], xfree[2], tfull[2], tfree[2];
@@ -214,14 +220,15 @@ __device__ __forceinline__ bool flushWindow(SmemT & S, uint32_t taddr, uint32_t 
 }
 
 // ---- the kernel ------------------------------------------------------------------------------------
-template <int NB>
+template <int NB, int RP>
 __global__ void __launch_bounds__(NTHREADS, 1)
     kFlashTc(const __grid_constant__ CUtensorMap mapPsi1Hi, const __grid_constant__ CUtensorMap mapPsi1Lo,
              const __grid_constant__ CUtensorMap mapPsi2Hi, const __grid_constant__ CUtensorMap mapPsi2Lo,
              const __grid_constant__ CUtensorMap mapVHi, const __grid_constant__ CUtensorMap mapVLo, Params P)
 {
   extern __shared__ uint8_t smemRaw[];
-  Smem<NB> & S = *reinterpret_cast<Smem<NB> *>((reinterpret_cast<uintptr_t>(smemRaw) + 1023) & ~uintptr_t(1023));
+  Smem<NB, RP> & S = *reinterpret_cast<Smem<NB, RP> *>((reinterpret_cast<uintptr_t>(smemRaw) + 1023) & ~uintptr_t(1023));
+  constexpr int NSTAGE = stagesFor(RP);
   int const warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   volatile int * abortFlag = &S.abort;
 
@@ -251,10 +258,12 @@ __global__ void __launch_bounds__(NTHREADS, 1)
 
   int const nItems = P.nTiles * P.nSplit;
 
+  if (warp < 4) {
+    asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(kRegsProducer));
   if (warp == 0) {
     // ---------------------------------------------------------------- TMA producer
     if (lane == 0) {
-      uint32_t stageUse[NSTAGE] = {0, 0};
+      uint32_t stageUse[NSTAGE] = {};
       uint32_t issuedLoads = 0;
       uint32_t p1Use = 0;
       bool ok = true;
@@ -297,7 +306,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       constexpr uint32_t idesc1 = instrDescBf16(BM, BK);
       constexpr uint32_t idesc2 = instrDescBf16(BM, NB);
       uint32_t const aPsi1[2] = {smemAddr(S.psi1[0]), smemAddr(S.psi1[1])};
-      uint32_t fullUse[NSTAGE] = {0, 0};
+      uint32_t fullUse[NSTAGE] = {};
       uint32_t sfreeUse[2] = {0, 0}, xfullUse[2] = {0, 0}, tfreeUse[2] = {0, 0};
       uint32_t blockCount = 0;   // global block counter: selects stage, S/X buffers
       uint32_t windowCount = 0;  // global window counter: selects the T buffer
@@ -324,14 +333,18 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           fenceAfterSync();
           uint32_t const d = tmem + b * BK;
           uint32_t const bPsi2[2] = {smemAddr(S.psi2[s][0]), smemAddr(S.psi2[s][1])};
+          // the two small cross products accumulate first, the hi*hi product last, so that only
+          // the final steps round the full-magnitude accumulator
+          constexpr uint32_t sbo = RP == 64 ? 1024 : 512, swz = RP == 64 ? 2 : 4;
           uint32_t acc = 0;
 #pragma unroll
           for (int k = 0; k < RP / 16; ++k) {
-            // hi*hi, hi*lo, lo*hi
-            mmaBf16(d, smemDesc(aPsi1[0] + 32 * k, 512, 4), smemDesc(bPsi2[0] + 32 * k, 512, 4), idesc1, acc); acc = 1;
-            mmaBf16(d, smemDesc(aPsi1[0] + 32 * k, 512, 4), smemDesc(bPsi2[1] + 32 * k, 512, 4), idesc1, 1);
-            mmaBf16(d, smemDesc(aPsi1[1] + 32 * k, 512, 4), smemDesc(bPsi2[0] + 32 * k, 512, 4), idesc1, 1);
+            mmaBf16(d, smemDesc(aPsi1[0] + 32 * k, sbo, swz), smemDesc(bPsi2[1] + 32 * k, sbo, swz), idesc1, acc); acc = 1;
+            mmaBf16(d, smemDesc(aPsi1[1] + 32 * k, sbo, swz), smemDesc(bPsi2[0] + 32 * k, sbo, swz), idesc1, 1);
           }
+#pragma unroll
+          for (int k = 0; k < RP / 16; ++k)
+            mmaBf16(d, smemDesc(aPsi1[0] + 32 * k, sbo, swz), smemDesc(bPsi2[0] + 32 * k, sbo, swz), idesc1, 1);
           mmaCommit(&S.sfull[b]);
           return true;
         };
@@ -356,10 +369,12 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           uint32_t acc = inWin == 0 ? 0u : 1u;
 #pragma unroll
           for (int k = 0; k < BK / 16; ++k) {
-            mmaBf16(d, smemDesc(aX[0] + 32 * k, 1024, 2), smemDesc(bV[0] + 32 * k, 1024, 2), idesc2, acc); acc = 1;
-            mmaBf16(d, smemDesc(aX[0] + 32 * k, 1024, 2), smemDesc(bV[1] + 32 * k, 1024, 2), idesc2, 1);
+            mmaBf16(d, smemDesc(aX[0] + 32 * k, 1024, 2), smemDesc(bV[1] + 32 * k, 1024, 2), idesc2, acc); acc = 1;
             mmaBf16(d, smemDesc(aX[1] + 32 * k, 1024, 2), smemDesc(bV[0] + 32 * k, 1024, 2), idesc2, 1);
           }
+#pragma unroll
+          for (int k = 0; k < BK / 16; ++k)
+            mmaBf16(d, smemDesc(aX[0] + 32 * k, 1024, 2), smemDesc(bV[0] + 32 * k, 1024, 2), idesc2, 1);
           mmaCommit(&S.xfree[b]);
           mmaCommit(&S.empty[s]);
           if (lastInWin) { mmaCommit(&S.tfull[t]); ++windowCount; }
@@ -369,14 +384,26 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       }
       mmaCommit(&S.done);
     }
+  }
+    // teardown of warpgroup 0: every MMA this CTA issued completes before TMEM is released (bounded)
+    fenceBeforeSync();
+    __syncthreads();
+    if (warp == 1) {
+      unsigned long long const t0 = globalTimer();
+      while (!mbarTryWait(&S.done, 0) && globalTimer() - t0 < kWaitLimitNs) {}
+      fenceAfterSync();
+      __syncwarp();
+      asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem) : "memory");
+    }
   } else {
+    asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;" ::"n"(kRegsCompute));
     // ---------------------------------------------------------------- compute warps
-    int const cw = warp - 2;
+    int const cw = warp - 4;
     int const quarter = warp & 3;
     int const half = cw >> 2;
     int const row = quarter * 32 + lane;
     uint32_t const laneBase = uint32_t(quarter * 32) << 16;
-    uint32_t fullUse[NSTAGE] = {0, 0};
+    uint32_t fullUse[NSTAGE] = {};
     uint32_t sfullUse[2] = {0, 0}, xfreeUse[2] = {0, 0}, tfullUse[2] = {0, 0};
     uint32_t blockCount = 0, windowCount = 0;
     bool ok = true;
@@ -400,49 +427,59 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         if (!(ok = waitBar(&S.sfull[b], sfullUse[b] & 1, abortFlag, P.status, 33))) break;
         ++sfullUse[b];
         fenceAfterSync();
-        float rho[32];
+        float rho[16];
         tmemLoad16(tmem + laneBase + b * BK + half * 32, rho);
-        tmemLoad16(tmem + laneBase + b * BK + half * 32 + 16, rho + 16);
         tmemWaitLoad();
-        fenceBeforeSync();
-        __syncwarp();
-        if (lane == 0) mbarArrive(&S.sfree[b]);
         if (g >= 2) {
           if (!(ok = waitBar(&S.xfree[b], xfreeUse[b] & 1, abortFlag, P.status, 34))) break;
           ++xfreeUse[b];
         }
-        float4 const * cc = S.coords[s] + half * 32;
+            float4 const * cc = S.coords[s] + half * 32;
         uint8_t * xhi = S.x[b][0];
         uint8_t * xlo = S.x[b][1];
-        float vsum = 0.f;
-#pragma unroll
-        for (int ch = 0; ch < 4; ++ch) {
-          uint32_t hi[4], lo[4];
-#pragma unroll
-          for (int e = 0; e < 8; e += 2) {
-            float xv[2];
-#pragma unroll
-            for (int u = 0; u < 2; ++u) {
-              float4 const q = cc[ch * 8 + e + u];
-              float const dx = p1.x - q.x, dy = p1.y - q.y, dz = p1.z - q.z;
-              float const r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-              float y = rsqrtf(r2);
-              float const h = r2 * y;
-              float const ee = fmaf(-h, y, 1.0f);
-              y = fmaf(0.5f * y, ee, y);           // one Newton step on the hardware estimate
-              y = r2 > 0.0f ? y : 0.0f;            // coincident pair contributes 0
-              vsum = fmaf(y, q.w, vsum);
-              xv[u] = y * rho[ch * 8 + e + u];
-            }
-            uint32_t const h2 = packBf16(xv[0], xv[1]);
-            float const h0 = __uint_as_float(h2 << 16), h1 = __uint_as_float(h2 & 0xFFFF0000u);
-            hi[e >> 1] = h2;
-            lo[e >> 1] = packBf16(xv[0] - h0, xv[1] - h1);
+        float vsum0 = 0.f, vsum1 = 0.f;
+#pragma unroll 1
+        for (int hh = 0; hh < 2; ++hh) {
+          if (hh == 1) {
+            // second half of this warp's 32 rho columns; the S buffer is then free for the next GEMM1
+            tmemLoad16(tmem + laneBase + b * BK + half * 32 + 16, rho);
+            tmemWaitLoad();
+            fenceBeforeSync();
+            __syncwarp();
+            if (lane == 0) mbarArrive(&S.sfree[b]);
           }
-          uint32_t const off = sw128(row, half * 4 + ch);
-          *reinterpret_cast<uint4 *>(xhi + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-          *reinterpret_cast<uint4 *>(xlo + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+#pragma unroll
+          for (int c2 = 0; c2 < 2; ++c2) {
+            int const ch = hh * 2 + c2;
+            uint32_t hi[4], lo[4];
+#pragma unroll
+            for (int e = 0; e < 8; e += 2) {
+              float xv[2];
+#pragma unroll
+              for (int u = 0; u < 2; ++u) {
+                float4 const q = cc[ch * 8 + e + u];
+                float const dx = p1.x - q.x, dy = p1.y - q.y, dz = p1.z - q.z;
+                float const r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                float y = rsqrtf(r2);
+                float const h = r2 * y;
+                float const ee = fmaf(-h, y, 1.0f);
+                y = fmaf(0.5f * y, ee, y);           // one Newton step on the hardware estimate
+                y = r2 > 0.0f ? y : 0.0f;            // coincident pair contributes 0
+                if (u == 0) vsum0 = fmaf(y, q.w, vsum0);
+                else vsum1 = fmaf(y, q.w, vsum1);
+                xv[u] = y * rho[c2 * 8 + e + u];
+              }
+              // hi = X with the low 16 mantissa bits cleared (exact), lo = BF16(X - hi)
+              uint32_t const b0 = __float_as_uint(xv[0]) & 0xFFFF0000u, b1 = __float_as_uint(xv[1]) & 0xFFFF0000u;
+              hi[e >> 1] = __byte_perm(b0, b1, 0x7632);
+              lo[e >> 1] = packBf16(xv[0] - __uint_as_float(b0), xv[1] - __uint_as_float(b1));
+            }
+            uint32_t const off = sw128(row, half * 4 + ch);
+            *reinterpret_cast<uint4 *>(xhi + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+            *reinterpret_cast<uint4 *>(xlo + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+          }
         }
+        float const vsum = vsum0 + vsum1;
         vh += double(vsum);
         fenceProxyAsync();
         __syncwarp();
@@ -472,24 +509,14 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       // the two column-half warps of a row each summed half of the r2 points of every block
       if (r1 < P.n1) atomicAdd(&P.VH[int64_t(split) * P.vhStride + r1], vh);
     }
-  }
-
-  // ------------------------------------------------------------------- teardown
-  fenceBeforeSync();
-  __syncthreads();
-  if (warp == 1) {
-    // every MMA this CTA issued has completed before TMEM is released (bounded)
-    unsigned long long const t0 = globalTimer();
-    while (!mbarTryWait(&S.done, 0) && globalTimer() - t0 < kWaitLimitNs) {}
-    fenceAfterSync();
-    __syncwarp();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem) : "memory");
+    fenceBeforeSync();
+    __syncthreads();
   }
 }
 
 // ---- operand packing ---------------------------------------------------------------------------------
-// psi [n][ldpsi] FP64 (R columns) -> hi/lo BF16 [npad][32], zero padded
-__global__ void kPackPsi(int64_t n, int64_t npad, int R, const double * psi, int ldpsi, __nv_bfloat16 * hi, __nv_bfloat16 * lo)
+// psi [n][ldpsi] FP64 (R columns) -> hi/lo BF16 [npad][RP], zero padded
+__global__ void kPackPsi(int64_t n, int64_t npad, int R, int RP, const double * psi, int ldpsi, __nv_bfloat16 * hi, __nv_bfloat16 * lo)
 {
   for (int64_t idx = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; idx < npad * RP; idx += int64_t(gridDim.x) * blockDim.x) {
     int64_t const r = idx / RP;
@@ -571,23 +598,47 @@ bool makeMap(CUtensorMap * m, void * base, uint64_t inner, uint64_t outer, uint3
             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-template <int NB>
+template <int NB, int RP>
 int launchFlash(tcscf_ctx * ctx, CUtensorMap const * maps, tc::Params const & P, int grid)
 {
-  size_t const smem = sizeof(tc::Smem<NB>) + 1024;
-  TCSCF_CUDA(ctx, cudaFuncSetAttribute(tc::kFlashTc<NB>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-  tc::kFlashTc<NB><<<grid, tc::NTHREADS, smem, ctx->stream>>>(maps[0], maps[1], maps[2], maps[3], maps[4], maps[5], P);
+  size_t const smem = sizeof(tc::Smem<NB, RP>) + 1024;
+  TCSCF_CUDA(ctx, cudaFuncSetAttribute(tc::kFlashTc<NB, RP>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  tc::kFlashTc<NB, RP><<<grid, tc::NTHREADS, smem, ctx->stream>>>(maps[0], maps[1], maps[2], maps[3], maps[4], maps[5], P);
   TCSCF_LAUNCH(ctx);
   return TCSCF_OK;
 }
 
 }  // namespace
 
+int tensorPackedV(tcscf_ctx * ctx, Grid & g2, const double * V, double scale, const void ** hi, const void ** lo)
+{
+  int const NB = g2.nb <= 64 ? 64 : 128;
+  int64_t const n2pad = (g2.n + tc::BK - 1) / tc::BK * tc::BK;
+  if (!g2.vtCache || g2.vtNB != NB || g2.vtN2pad != n2pad || g2.vtScale != scale) {
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(g2.vtCache);
+    g2.vtCache = nullptr;
+    TCSCF_CUDA(ctx, cudaMalloc(&g2.vtCache, size_t(2) * NB * n2pad * sizeof(__nv_bfloat16)));
+    auto * vh = static_cast<__nv_bfloat16 *>(g2.vtCache);
+    dim3 const tb{32, 8, 1};
+    dim3 const tg{unsigned((n2pad + 31) / 32), unsigned((NB + 31) / 32), 1};
+    tc::kPackVt<<<tg, tb, 0, ctx->stream>>>(g2.n, n2pad, g2.nb, NB, V, g2.nb, vh, vh + size_t(NB) * n2pad);
+    TCSCF_LAUNCH(ctx);
+    g2.vtNB = NB;
+    g2.vtN2pad = n2pad;
+    g2.vtScale = scale;
+  }
+  auto * vh = static_cast<__nv_bfloat16 *>(g2.vtCache);
+  *hi = vh;
+  *lo = vh + size_t(NB) * n2pad;
+  return TCSCF_OK;
+}
+
 bool tensorPathAvailable(Contraction const & c, int precision, std::string * why)
 {
   if (precision != TCSCF_PREC_BF16X3) { if (why) *why = "only the bf16x3 tensor path is built"; return false; }
   if (c.kernel != TCSCF_K_INV_R12) { if (why) *why = "tensor path implements the 1/r12 kernel"; return false; }
-  if (c.R < 1 || c.R > tc::RP) { if (why) *why = "density rank must be 1..32 for the tensor path"; return false; }
+  if (c.R < 1 || c.R > 64) { if (why) *why = "density factor rank must be 1..64 for the tensor path"; return false; }
   if (c.ncol > 128) { if (why) *why = "tensor path supports nb <= 128"; return false; }
   if (!encodeTiled()) { if (why) *why = "cuTensorMapEncodeTiled unavailable"; return false; }
   return true;
@@ -598,6 +649,7 @@ int contractTensor(tcscf_ctx * ctx, Contraction const & c, int precision)
   std::string why;
   if (!tensorPathAvailable(c, precision, &why)) return fail(ctx, TCSCF_ERR_UNSUPPORTED, why);
   int const NB = c.ncol <= 64 ? 64 : 128;
+  int const RP = c.R <= 32 ? 32 : 64;
   int64_t const n1pad = (c.n1 + tc::BM - 1) / tc::BM * tc::BM;
   int64_t const n2pad = (c.n2 + tc::BK - 1) / tc::BK * tc::BK;
   int const nTiles = int(n1pad / tc::BM);
@@ -611,42 +663,49 @@ int contractTensor(tcscf_ctx * ctx, Contraction const & c, int precision)
   nSplit = (nBlocks + perSplit - 1) / perSplit;
 
   size_t const bf = sizeof(__nv_bfloat16);
-  size_t bytes = 2 * size_t(n1pad) * tc::RP * bf + 2 * size_t(n2pad) * tc::RP * bf + 2 * size_t(NB) * n2pad * bf
+  size_t bytes = 2 * size_t(n1pad) * RP * bf + 2 * size_t(n2pad) * RP * bf + 2 * size_t(NB) * n2pad * bf
                  + size_t(n1pad) * sizeof(float4) + size_t(n2pad) * sizeof(float4) + 64;
   void * p = nullptr;
   TCSCF_TRY(scratch(ctx, "flash_tc_ops", bytes, &p));
   char * q = static_cast<char *>(p);
   auto take = [&](size_t n) { char * r = q; q += (n + 255) & ~size_t(255); return r; };
-  auto * psi1hi = reinterpret_cast<__nv_bfloat16 *>(take(size_t(n1pad) * tc::RP * bf));
-  auto * psi1lo = reinterpret_cast<__nv_bfloat16 *>(take(size_t(n1pad) * tc::RP * bf));
-  auto * psi2hi = reinterpret_cast<__nv_bfloat16 *>(take(size_t(n2pad) * tc::RP * bf));
-  auto * psi2lo = reinterpret_cast<__nv_bfloat16 *>(take(size_t(n2pad) * tc::RP * bf));
+  auto * psi1hi = reinterpret_cast<__nv_bfloat16 *>(take(size_t(n1pad) * RP * bf));
+  auto * psi1lo = reinterpret_cast<__nv_bfloat16 *>(take(size_t(n1pad) * RP * bf));
+  auto * psi2hi = reinterpret_cast<__nv_bfloat16 *>(take(size_t(n2pad) * RP * bf));
+  auto * psi2lo = reinterpret_cast<__nv_bfloat16 *>(take(size_t(n2pad) * RP * bf));
   auto * vthi = reinterpret_cast<__nv_bfloat16 *>(take(size_t(NB) * n2pad * bf));
   auto * vtlo = reinterpret_cast<__nv_bfloat16 *>(take(size_t(NB) * n2pad * bf));
   auto * r1c = reinterpret_cast<float4 *>(take(size_t(n1pad) * sizeof(float4)));
   auto * r2c = reinterpret_cast<float4 *>(take(size_t(n2pad) * sizeof(float4)));
   int * status = reinterpret_cast<int *>(take(64));
+  bool const haveVt = c.vtHi && c.vtLo;
   TCSCF_CHECK(ctx, size_t(q - static_cast<char *>(p)) <= bytes + 16 * 256, TCSCF_ERR_INVALID_ARGUMENT, "internal: scratch layout");
 
   // operand preparation (BF16 hi/lo split, transposes, FP32 coordinates)
-  tc::kPackPsi<<<gridBlocks(n1pad * tc::RP, 256), 256, 0, ctx->stream>>>(c.n1, n1pad, c.R, c.psi1, c.ldpsi, psi1hi, psi1lo);
+  tc::kPackPsi<<<gridBlocks(n1pad * RP, 256), 256, 0, ctx->stream>>>(c.n1, n1pad, c.R, RP, c.psi1, c.ldpsi, psi1hi, psi1lo);
   TCSCF_LAUNCH(ctx);
-  tc::kPackPsi<<<gridBlocks(n2pad * tc::RP, 256), 256, 0, ctx->stream>>>(c.n2, n2pad, c.R, c.psi2, c.ldpsi, psi2hi, psi2lo);
+  tc::kPackPsi<<<gridBlocks(n2pad * RP, 256), 256, 0, ctx->stream>>>(c.n2, n2pad, c.R, RP, c.psi2, c.ldpsi, psi2hi, psi2lo);
   TCSCF_LAUNCH(ctx);
   dim3 const tb{32, 8, 1};
   dim3 const tg{unsigned((n2pad + 31) / 32), unsigned((NB + 31) / 32), 1};
-  tc::kPackVt<<<tg, tb, 0, ctx->stream>>>(c.n2, n2pad, c.ncol, NB, c.V, c.ldv, vthi, vtlo);
-  TCSCF_LAUNCH(ctx);
+  if (haveVt) {
+    vthi = static_cast<__nv_bfloat16 *>(const_cast<void *>(c.vtHi));
+    vtlo = static_cast<__nv_bfloat16 *>(const_cast<void *>(c.vtLo));
+  } else {
+    tc::kPackVt<<<tg, tb, 0, ctx->stream>>>(c.n2, n2pad, c.ncol, NB, c.V, c.ldv, vthi, vtlo);
+    TCSCF_LAUNCH(ctx);
+  }
   tc::kPackCoords<<<gridBlocks(n1pad, 256), 256, 0, ctx->stream>>>(c.n1, n1pad, c.p1, nullptr, r1c);
   TCSCF_LAUNCH(ctx);
   tc::kPackCoords<<<gridBlocks(n2pad, 256), 256, 0, ctx->stream>>>(c.n2, n2pad, c.p2, c.coul, r2c);
   TCSCF_LAUNCH(ctx);
 
   CUtensorMap maps[6];
-  bool okm = makeMap(&maps[0], psi1hi, tc::RP, n1pad, tc::RP, tc::BM, CU_TENSOR_MAP_SWIZZLE_64B)
-             && makeMap(&maps[1], psi1lo, tc::RP, n1pad, tc::RP, tc::BM, CU_TENSOR_MAP_SWIZZLE_64B)
-             && makeMap(&maps[2], psi2hi, tc::RP, n2pad, tc::RP, tc::BK, CU_TENSOR_MAP_SWIZZLE_64B)
-             && makeMap(&maps[3], psi2lo, tc::RP, n2pad, tc::RP, tc::BK, CU_TENSOR_MAP_SWIZZLE_64B)
+  CUtensorMapSwizzle const psw = RP == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B;
+  bool okm = makeMap(&maps[0], psi1hi, RP, n1pad, RP, tc::BM, psw)
+             && makeMap(&maps[1], psi1lo, RP, n1pad, RP, tc::BM, psw)
+             && makeMap(&maps[2], psi2hi, RP, n2pad, RP, tc::BK, psw)
+             && makeMap(&maps[3], psi2lo, RP, n2pad, RP, tc::BK, psw)
              && makeMap(&maps[4], vthi, n2pad, NB, tc::BK, NB, CU_TENSOR_MAP_SWIZZLE_128B)
              && makeMap(&maps[5], vtlo, n2pad, NB, tc::BK, NB, CU_TENSOR_MAP_SWIZZLE_128B);
   TCSCF_CHECK(ctx, okm, TCSCF_ERR_CUDA, "cuTensorMapEncodeTiled failed");
@@ -669,8 +728,10 @@ int contractTensor(tcscf_ctx * ctx, Contraction const & c, int precision)
   P.r1xyz = r1c; P.r2xyzc = r2c; P.T = Tout; P.VH = VHout; P.ldt = c.ldt;
   P.tStride = int64_t(c.n1) * c.ldt; P.vhStride = c.n1; P.status = status;
   int const grid = std::min(nTiles * nSplit, sms);
-  if (NB == 64) TCSCF_TRY(launchFlash<64>(ctx, maps, P, grid));
-  else TCSCF_TRY(launchFlash<128>(ctx, maps, P, grid));
+  if (NB == 64 && RP == 32) TCSCF_TRY((launchFlash<64, 32>(ctx, maps, P, grid)));
+  else if (NB == 64) TCSCF_TRY((launchFlash<64, 64>(ctx, maps, P, grid)));
+  else if (RP == 32) TCSCF_TRY((launchFlash<128, 32>(ctx, maps, P, grid)));
+  else TCSCF_TRY((launchFlash<128, 64>(ctx, maps, P, grid)));
 
   int st = 0;
   TCSCF_CUDA(ctx, cudaMemcpyAsync(&st, status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));

@@ -668,6 +668,9 @@ int fockBuildDevice(tcscf_ctx * ctx, Grid & g1, Grid & g2, int nspin, const doub
   TCSCF_CUDA(ctx, cudaMemsetAsync(GRre, 0, sizeof(double) * size_t(nspin) * nb * nb * 2, ctx->stream));
   bool anyComplex = false;
   double contractionMs = 0;
+  const void * vtHi = nullptr;
+  const void * vtLo = nullptr;
+  if (precision != TCSCF_PREC_FP64) TCSCF_TRY(tensorPackedV(ctx, g2, V, scale, &vtHi, &vtLo));
   for (int s = 0; s < nspin; ++s) {
     Factor f;
     TCSCF_TRY(factorDensity(ctx, g1, dD + size_t(s) * nb * nb, s, f));
@@ -694,6 +697,7 @@ int fockBuildDevice(tcscf_ctx * ctx, Grid & g1, Grid & g2, int nspin, const doub
       c.n1 = n1; c.n2 = n2; c.R = R; c.ncol = nb;
       c.p1 = g1.pts; c.p2 = g2.pts; c.psi1 = psi1; c.psi2 = psi2; c.ldpsi = ldpsi;
       c.V = V; c.ldv = nb; c.T = part == 0 ? Ts : Ti; c.ldt = ldt;
+      c.vtHi = vtHi; c.vtLo = vtLo;
       if (part == 0) {
         kCoulombSource<<<gridBlocks(n2, 256), 256, 0, ctx->stream>>>(n2, R, psi1at2, psi2, ldpsi, g2.w, scale, coul);
         TCSCF_LAUNCH(ctx);
@@ -722,6 +726,10 @@ int fockBuildDevice(tcscf_ctx * ctx, Grid & g1, Grid & g2, int nspin, const doub
     if (anyComplex)
       TCSCF_TRY(reduceFockReal(ctx, n1, nb, g1.phiR, g1.w, nullptr, 0.0, Tim + size_t(s) * n1 * ldt, ldt, 1.0, GRim + size_t(s) * nb * nb));
   }
+  ctx->lastVH = VHtot;
+  ctx->lastT = Tre;
+  ctx->lastN1 = n1;
+  ctx->lastNb = nb;
   kRealToReference<<<gridBlocks(int64_t(nspin) * nb * nb, 256), 256, 0, ctx->stream>>>(nspin, nb, g1.dsto, GRre, anyComplex ? GRim : nullptr, dG);
   TCSCF_LAUNCH(ctx);
   kFinalize<<<1, 512, 0, ctx->stream>>>(nspin, nb, dH, dG, nullptr, dD, respectSym, nspin == 1 ? 2.0 : 1.0, dFock, dE);
@@ -798,7 +806,7 @@ int tcscf_ctx_destroy(tcscf_ctx * ctx)
   cudaStreamSynchronize(ctx->stream);
   for (auto & kv : ctx->grids) {
     Grid & g = kv.second;
-    cudaFree(g.pts); cudaFree(g.w); cudaFree(g.dsto); cudaFree(g.phiR); cudaFree(g.vals); cudaFree(g.grads);
+    cudaFree(g.pts); cudaFree(g.w); cudaFree(g.dsto); cudaFree(g.phiR); cudaFree(g.vals); cudaFree(g.grads); cudaFree(g.vtCache);
   }
   for (auto & kv : ctx->tensors) cudaFree(kv.second.d);
   for (auto & kv : ctx->scratch) cudaFree(kv.second.p);
@@ -831,6 +839,16 @@ int tcscf_last_timing(tcscf_ctx * ctx, double * contraction_ms, double * total_m
   if (contraction_ms) *contraction_ms = ctx->lastContractionMs;
   if (total_ms) *total_ms = ctx->lastTotalMs;
   if (launches) *launches = ctx->lastLaunches;
+  return TCSCF_OK;
+}
+
+int tcscf_last_potentials(tcscf_ctx * ctx, double * VH, double * T)
+{
+  if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
+  TCSCF_CHECK(ctx, ctx->lastVH && ctx->lastT, TCSCF_ERR_INVALID_ARGUMENT, "no direct Fock build has run on this context");
+  if (VH) TCSCF_CUDA(ctx, cudaMemcpyAsync(VH, ctx->lastVH, sizeof(double) * ctx->lastN1, cudaMemcpyDeviceToHost, ctx->stream));
+  if (T) TCSCF_CUDA(ctx, cudaMemcpyAsync(T, ctx->lastT, sizeof(double) * ctx->lastN1 * ctx->lastNb, cudaMemcpyDeviceToHost, ctx->stream));
+  TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return TCSCF_OK;
 }
 
@@ -871,7 +889,7 @@ int tcscf_grid_destroy(tcscf_ctx * ctx, int grid)
   Grid * g = findGrid(ctx, grid);
   TCSCF_CHECK(ctx, g, TCSCF_ERR_INVALID_ARGUMENT, "unknown grid handle");
   cudaStreamSynchronize(ctx->stream);
-  cudaFree(g->pts); cudaFree(g->w); cudaFree(g->dsto); cudaFree(g->phiR); cudaFree(g->vals); cudaFree(g->grads);
+  cudaFree(g->pts); cudaFree(g->w); cudaFree(g->dsto); cudaFree(g->phiR); cudaFree(g->vals); cudaFree(g->grads); cudaFree(g->vtCache);
   ctx->grids.erase(grid);
   return TCSCF_OK;
 }
@@ -884,8 +902,10 @@ int tcscf_grid_set_basis(tcscf_ctx * ctx, int grid, const tcscf_sto * basis, int
   std::vector<DevSto> ds;
   TCSCF_TRY(validateBasis(ctx, basis, nb, ds));
   cudaStreamSynchronize(ctx->stream);
-  cudaFree(g->dsto); cudaFree(g->phiR); cudaFree(g->vals); cudaFree(g->grads);
+  cudaFree(g->dsto); cudaFree(g->phiR); cudaFree(g->vals); cudaFree(g->grads); cudaFree(g->vtCache);
   g->dsto = nullptr; g->phiR = g->vals = g->grads = nullptr;
+  g->vtCache = nullptr;
+  g->vtNB = 0;
   g->nb = 0;
   TCSCF_CUDA(ctx, cudaMalloc(&g->dsto, sizeof(DevSto) * nb));
   TCSCF_CUDA(ctx, cudaMalloc(&g->phiR, sizeof(double) * g->n * nb));
