@@ -35,6 +35,9 @@ constexpr int NTHREADS = 384;  // warpgroup 0: TMA, MMA, 2 idle warps; warpgroup
 constexpr int kRegsLaunch = 168, kRegsProducer = 56, kRegsCompute = 224;
 static_assert(128 * kRegsProducer + 256 * kRegsCompute <= NTHREADS * kRegsLaunch, "register split exceeds the launch allocation");
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s per wait
+// a waiting thread sleeps in mbarrier.try_wait (woken when the phase completes) instead of spinning
+// on the issue slots the compute warps need
+constexpr uint32_t kSuspendHintNs = 1000000;
 
 // RP: padded rank of rho (GEMM1 K): 32 (64-byte rows, 64B swizzle) or 64 (128-byte rows, 128B swizzle)
 template <int NB, int RP>
@@ -44,7 +47,7 @@ struct __align__(1024) Smem {
   uint8_t x[2][2][BM * BK * 2];            // X tile hi/lo:   SW128 K-major [128 rows][64]
   uint8_t psi2[NSTAGE][2][BK * RP * 2];    // psi2 block hi/lo: K-major [64 rows][RP]
   uint8_t psi1[2][BM * RP * 2];            // psi1 tile hi/lo:  K-major [128 rows][RP]
-  float4 coords[NSTAGE][BK];               // x, y, z, coul of the r2 block
+  float4 coords[NSTAGE][BK];               // r2 block as 32 pairs {x0,x1,y0,y1}{z0,z1,c0,c1}
   uint64_t full[NSTAGE], empty[NSTAGE];
   uint64_t sfull[2], sfree[2], xfull[2], xfree[2], tfull[2], tfree[2];
   uint64_t p1full, p1free, done;
@@ -93,10 +96,10 @@ __device__ __forceinline__ bool mbarTryWait(uint64_t * b, uint32_t parity)
   uint32_t ok;
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
       "selp.u32 %0, 1, 0, p;\n\t}"
       : "=r"(ok)
-      : "r"(smemAddr(b)), "r"(parity)
+      : "r"(smemAddr(b)), "r"(parity), "r"(kSuspendHintNs)
       : "memory");
   return ok != 0;
 }
@@ -184,6 +187,39 @@ __device__ __forceinline__ void tmemLoad16(uint32_t taddr, float * v)
 }
 __device__ __forceinline__ void tmemWaitLoad() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
+// ---- packed FP32 pairs (sm_100 f32x2 arithmetic on 64-bit register pairs) ---------------------
+__device__ __forceinline__ uint64_t f2pack(float a, float b)
+{
+  uint64_t d;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(d) : "f"(a), "f"(b));
+  return d;
+}
+__device__ __forceinline__ void f2unpack(uint64_t v, float & a, float & b) { asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v)); }
+__device__ __forceinline__ uint64_t f2sub(uint64_t a, uint64_t b)
+{
+  uint64_t d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ uint64_t f2mul(uint64_t a, uint64_t b)
+{
+  uint64_t d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ uint64_t f2fma(uint64_t a, uint64_t b, uint64_t c)
+{
+  uint64_t d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+__device__ __forceinline__ float rsqrtApprox(float x)
+{
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 // byte offset of element (row, k) in a K-major SW128 tile of 64 BF16 columns
 __device__ __forceinline__ uint32_t sw128(int row, int chunk)
 {
@@ -199,11 +235,11 @@ __device__ __forceinline__ uint32_t packBf16(float a, float b)
 // Adds one finished FP32 TMEM accumulation window (64 of the NB columns of this thread's row) into
 // the FP64 accumulators and hands the TMEM buffer back to the MMA issuer.
 template <int NB, class SmemT>
-__device__ __forceinline__ bool flushWindow(SmemT & S, uint32_t taddr, uint32_t t, uint32_t (&tfullUse)[2], double (&acc)[64], int lane,
+__device__ __forceinline__ bool flushWindow(SmemT & S, uint32_t taddr, uint32_t window, double (&acc)[64], int lane,
                                             volatile int * abortFlag, int * status)
 {
-  if (!waitBar(&S.tfull[t], tfullUse[t] & 1, abortFlag, status, 31)) return false;
-  ++tfullUse[t];
+  uint32_t const t = window & 1;
+  if (!waitBar(&S.tfull[t], (window >> 1) & 1, abortFlag, status, 31)) return false;
   fenceAfterSync();
 #pragma unroll
   for (int q = 0; q < (NB >= 128 ? 4 : 2); ++q) {
@@ -263,7 +299,6 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   if (warp == 0) {
     // ---------------------------------------------------------------- TMA producer
     if (lane == 0) {
-      uint32_t stageUse[NSTAGE] = {};
       uint32_t issuedLoads = 0;
       uint32_t p1Use = 0;
       bool ok = true;
@@ -279,22 +314,21 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         for (int j = jb; j < je; ++j) {
           uint32_t const q = issuedLoads++;
           int const s = q % NSTAGE;
-          if (stageUse[s] > 0 && !(ok = waitBar(&S.empty[s], (stageUse[s] - 1) & 1, abortFlag, P.status, 12))) break;
+          // use u = q / NSTAGE of stage s needs consumption u - 1 of it
+          if (q >= uint32_t(NSTAGE) && !(ok = waitBar(&S.empty[s], ((q / NSTAGE) - 1) & 1, abortFlag, P.status, 12))) break;
           mbarArriveTx(&S.full[s], kStageBytes);
           tmaLoad2d(S.psi2[s][0], &mapPsi2Hi, 0, j * BK, &S.full[s]);
           tmaLoad2d(S.psi2[s][1], &mapPsi2Lo, 0, j * BK, &S.full[s]);
           tmaLoad2d(S.v[s][0], &mapVHi, j * BK, 0, &S.full[s]);
           tmaLoad2d(S.v[s][1], &mapVLo, j * BK, 0, &S.full[s]);
           bulkLoad(S.coords[s], P.r2xyzc + int64_t(j) * BK, BK * sizeof(float4), &S.full[s]);
-          ++stageUse[s];
         }
       }
       // drain: every issued load lands before the CTA can exit (bounded)
-      for (int s = 0; s < NSTAGE; ++s)
-        if (stageUse[s] > 0) {
-          unsigned long long const t0 = globalTimer();
-          while (!mbarTryWait(&S.full[s], (stageUse[s] - 1) & 1) && globalTimer() - t0 < kWaitLimitNs) {}
-        }
+      for (uint32_t q = issuedLoads > uint32_t(NSTAGE) ? issuedLoads - NSTAGE : 0; q < issuedLoads; ++q) {
+        unsigned long long const t0 = globalTimer();
+        while (!mbarTryWait(&S.full[q % NSTAGE], (q / NSTAGE) & 1) && globalTimer() - t0 < kWaitLimitNs) {}
+      }
       if (p1Use > 0) {
         unsigned long long const t0 = globalTimer();
         while (!mbarTryWait(&S.p1full, (p1Use - 1) & 1) && globalTimer() - t0 < kWaitLimitNs) {}
@@ -306,8 +340,6 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       constexpr uint32_t idesc1 = instrDescBf16(BM, BK);
       constexpr uint32_t idesc2 = instrDescBf16(BM, NB);
       uint32_t const aPsi1[2] = {smemAddr(S.psi1[0]), smemAddr(S.psi1[1])};
-      uint32_t fullUse[NSTAGE] = {};
-      uint32_t sfreeUse[2] = {0, 0}, xfullUse[2] = {0, 0}, tfreeUse[2] = {0, 0};
       uint32_t blockCount = 0;   // global block counter: selects stage, S/X buffers
       uint32_t windowCount = 0;  // global window counter: selects the T buffer
       uint32_t p1Use = 0;
@@ -324,12 +356,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         auto gemm1 = [&](int jj) -> bool {
           uint32_t const g = base + jj;
           int const s = g % NSTAGE, b = g & 1;
-          if (!waitBar(&S.full[s], fullUse[s] & 1, abortFlag, P.status, 22)) return false;
-          ++fullUse[s];
-          if (g >= 2) {
-            if (!waitBar(&S.sfree[b], sfreeUse[b] & 1, abortFlag, P.status, 23)) return false;
-            ++sfreeUse[b];
-          }
+          if (!waitBar(&S.full[s], (g / NSTAGE) & 1, abortFlag, P.status, 22)) return false;
+          if (g >= 2 && !waitBar(&S.sfree[b], ((g >> 1) - 1) & 1, abortFlag, P.status, 23)) return false;
           fenceAfterSync();
           uint32_t const d = tmem + b * BK;
           uint32_t const bPsi2[2] = {smemAddr(S.psi2[s][0]), smemAddr(S.psi2[s][1])};
@@ -356,12 +384,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           int const inWin = jj % P.window;
           bool const lastInWin = (inWin == P.window - 1) || (jj == nblk - 1);
           uint32_t const t = windowCount & 1;
-          if (inWin == 0 && windowCount >= 2) {
-            if (!(ok = waitBar(&S.tfree[t], tfreeUse[t] & 1, abortFlag, P.status, 24))) break;
-            ++tfreeUse[t];
-          }
-          if (!(ok = waitBar(&S.xfull[b], xfullUse[b] & 1, abortFlag, P.status, 25))) break;
-          ++xfullUse[b];
+          if (inWin == 0 && windowCount >= 2 && !(ok = waitBar(&S.tfree[t], ((windowCount >> 1) - 1) & 1, abortFlag, P.status, 24))) break;
+          if (!(ok = waitBar(&S.xfull[b], (g >> 1) & 1, abortFlag, P.status, 25))) break;
           fenceAfterSync();
           uint32_t const d = tmem + TCOL0 + t * NB;
           uint32_t const aX[2] = {smemAddr(S.x[b][0]), smemAddr(S.x[b][1])};
@@ -403,8 +427,6 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     int const half = cw >> 2;
     int const row = quarter * 32 + lane;
     uint32_t const laneBase = uint32_t(quarter * 32) << 16;
-    uint32_t fullUse[NSTAGE] = {};
-    uint32_t sfullUse[2] = {0, 0}, xfreeUse[2] = {0, 0}, tfullUse[2] = {0, 0};
     uint32_t blockCount = 0, windowCount = 0;
     bool ok = true;
     double acc[64];
@@ -418,26 +440,24 @@ __global__ void __launch_bounds__(NTHREADS, 1)
 #pragma unroll
       for (int c = 0; c < 64; ++c) acc[c] = 0.0;
       double vh = 0.0;
-      int pendingFlush = -1;   // T buffer whose flush is deferred by one block
+      int pendingFlush = -1;   // window whose flush is deferred by one block
       for (int jj = 0; jj < nblk && ok; ++jj) {
         uint32_t const g = blockCount + jj;
         int const s = g % NSTAGE, b = g & 1;
-        if (!(ok = waitBar(&S.full[s], fullUse[s] & 1, abortFlag, P.status, 32))) break;
-        ++fullUse[s];
-        if (!(ok = waitBar(&S.sfull[b], sfullUse[b] & 1, abortFlag, P.status, 33))) break;
-        ++sfullUse[b];
+        if (!(ok = waitBar(&S.full[s], (g / NSTAGE) & 1, abortFlag, P.status, 32))) break;
+        if (!(ok = waitBar(&S.sfull[b], (g >> 1) & 1, abortFlag, P.status, 33))) break;
         fenceAfterSync();
         float rho[16];
         tmemLoad16(tmem + laneBase + b * BK + half * 32, rho);
         tmemWaitLoad();
-        if (g >= 2) {
-          if (!(ok = waitBar(&S.xfree[b], xfreeUse[b] & 1, abortFlag, P.status, 34))) break;
-          ++xfreeUse[b];
-        }
-            float4 const * cc = S.coords[s] + half * 32;
+        if (g >= 2 && !(ok = waitBar(&S.xfree[b], ((g >> 1) - 1) & 1, abortFlag, P.status, 34))) break;
+        // this warp's 32 r2 points: 16 pairs of {x0,x1,y0,y1}{z0,z1,c0,c1}
+        float4 const * cc = S.coords[s] + half * 32;
         uint8_t * xhi = S.x[b][0];
         uint8_t * xlo = S.x[b][1];
-        float vsum0 = 0.f, vsum1 = 0.f;
+        uint64_t vsum2 = 0;
+        uint64_t const p1x = f2pack(p1.x, p1.x), p1y = f2pack(p1.y, p1.y), p1z = f2pack(p1.z, p1.z);
+        uint64_t const mOne = f2pack(-1.0f, -1.0f), mHalf = f2pack(-0.5f, -0.5f);
 #pragma unroll 1
         for (int hh = 0; hh < 2; ++hh) {
           if (hh == 1) {
@@ -453,49 +473,59 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             int const ch = hh * 2 + c2;
             uint32_t hi[4], lo[4];
 #pragma unroll
-            for (int e = 0; e < 8; e += 2) {
-              float xv[2];
-#pragma unroll
-              for (int u = 0; u < 2; ++u) {
-                float4 const q = cc[ch * 8 + e + u];
-                float const dx = p1.x - q.x, dy = p1.y - q.y, dz = p1.z - q.z;
-                float const r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                float y = rsqrtf(r2);
-                float const h = r2 * y;
-                float const ee = fmaf(-h, y, 1.0f);
-                y = fmaf(0.5f * y, ee, y);           // one Newton step on the hardware estimate
-                y = r2 > 0.0f ? y : 0.0f;            // coincident pair contributes 0
-                if (u == 0) vsum0 = fmaf(y, q.w, vsum0);
-                else vsum1 = fmaf(y, q.w, vsum1);
-                xv[u] = y * rho[c2 * 8 + e + u];
-              }
+            for (int e = 0; e < 4; ++e) {
+              int const pr = ch * 4 + e;                 // pair index within the warp's 16 pairs
+              float4 const qa = cc[2 * pr], qb = cc[2 * pr + 1];
+              uint64_t const dx = f2sub(p1x, f2pack(qa.x, qa.y));
+              uint64_t const dy = f2sub(p1y, f2pack(qa.z, qa.w));
+              uint64_t const dz = f2sub(p1z, f2pack(qb.x, qb.y));
+              uint64_t const r2 = f2fma(dx, dx, f2fma(dy, dy, f2mul(dz, dz)));
+              float r2a, r2b;
+              f2unpack(r2, r2a, r2b);
+              uint64_t y = f2pack(rsqrtApprox(r2a), rsqrtApprox(r2b));
+              // one Newton step on the hardware estimate: y += (-y/2) (r2 y^2 - 1)
+              uint64_t const em = f2fma(f2mul(r2, y), y, mOne);
+              y = f2fma(f2mul(y, mHalf), em, y);
+              float ya, yb;
+              f2unpack(y, ya, yb);
+              ya = r2a > 0.0f ? ya : 0.0f;                // coincident pair contributes 0
+              yb = r2b > 0.0f ? yb : 0.0f;
+              y = f2pack(ya, yb);
+              vsum2 = f2fma(y, f2pack(qb.z, qb.w), vsum2);
+              uint64_t const x = f2mul(y, f2pack(rho[c2 * 8 + 2 * e], rho[c2 * 8 + 2 * e + 1]));
+              float xa, xb;
+              f2unpack(x, xa, xb);
               // hi = X with the low 16 mantissa bits cleared (exact), lo = BF16(X - hi)
-              uint32_t const b0 = __float_as_uint(xv[0]) & 0xFFFF0000u, b1 = __float_as_uint(xv[1]) & 0xFFFF0000u;
-              hi[e >> 1] = __byte_perm(b0, b1, 0x7632);
-              lo[e >> 1] = packBf16(xv[0] - __uint_as_float(b0), xv[1] - __uint_as_float(b1));
+              uint32_t const b0 = __float_as_uint(xa) & 0xFFFF0000u, b1 = __float_as_uint(xb) & 0xFFFF0000u;
+              hi[e] = __byte_perm(b0, b1, 0x7632);
+              float la, lb;
+              f2unpack(f2sub(x, f2pack(__uint_as_float(b0), __uint_as_float(b1))), la, lb);
+              lo[e] = packBf16(la, lb);
             }
             uint32_t const off = sw128(row, half * 4 + ch);
             *reinterpret_cast<uint4 *>(xhi + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
             *reinterpret_cast<uint4 *>(xlo + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
           }
         }
-        float const vsum = vsum0 + vsum1;
+        float vs0, vs1;
+        f2unpack(vsum2, vs0, vs1);
+        float const vsum = vs0 + vs1;
         vh += double(vsum);
         fenceProxyAsync();
         __syncwarp();
         if (lane == 0) { mbarArrive(&S.xfull[b]); mbarArrive(&S.empty[s]); }
         if (pendingFlush >= 0) {
-          if (!(ok = flushWindow<NB>(S, tmem + laneBase + TCOL0 + uint32_t(pendingFlush) * NB + half * (NB / 2), uint32_t(pendingFlush), tfullUse,
-                                 acc, lane, abortFlag, P.status)))
+          if (!(ok = flushWindow<NB>(S, tmem + laneBase + TCOL0 + uint32_t(pendingFlush & 1) * NB + half * (NB / 2), uint32_t(pendingFlush),
+                                     acc, lane, abortFlag, P.status)))
             break;
           pendingFlush = -1;
         }
         int const inWin = jj % P.window;
-        if (inWin == P.window - 1 || jj == nblk - 1) { pendingFlush = int(windowCount & 1); ++windowCount; }
+        if (inWin == P.window - 1 || jj == nblk - 1) { pendingFlush = int(windowCount); ++windowCount; }
       }
       if (ok && pendingFlush >= 0)
-        ok = flushWindow<NB>(S, tmem + laneBase + TCOL0 + uint32_t(pendingFlush) * NB + half * (NB / 2), uint32_t(pendingFlush), tfullUse, acc, lane,
-                         abortFlag, P.status);
+        ok = flushWindow<NB>(S, tmem + laneBase + TCOL0 + uint32_t(pendingFlush & 1) * NB + half * (NB / 2), uint32_t(pendingFlush), acc, lane,
+                             abortFlag, P.status);
       blockCount += nblk;
       if (!ok) break;
       if (r1 < P.n1) {
@@ -559,6 +589,24 @@ __global__ void kPackCoords(int64_t n, int64_t npad, const double * pts, const d
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < npad; i += int64_t(gridDim.x) * blockDim.x) {
     if (i < n) out[i] = make_float4(float(pts[i]), float(pts[n + i]), float(pts[2 * n + i]), coul ? float(coul[i]) : 0.0f);
     else out[i] = make_float4(1.0e4f, 1.0e4f, 1.0e4f, 0.0f);
+  }
+}
+
+// same in pairs: point pair p -> {x_2p, x_2p+1, y_2p, y_2p+1}, {z_2p, z_2p+1, c_2p, c_2p+1} (npad even)
+__global__ void kPackCoordPairs(int64_t n, int64_t npad, const double * pts, const double * coul, float4 * out)
+{
+  for (int64_t p = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; p < npad / 2; p += int64_t(gridDim.x) * blockDim.x) {
+    float v[2][4];
+    for (int u = 0; u < 2; ++u) {
+      int64_t const i = 2 * p + u;
+      bool const in = i < n;
+      v[u][0] = in ? float(pts[i]) : 1.0e4f;
+      v[u][1] = in ? float(pts[n + i]) : 1.0e4f;
+      v[u][2] = in ? float(pts[2 * n + i]) : 1.0e4f;
+      v[u][3] = (in && coul) ? float(coul[i]) : 0.0f;
+    }
+    out[2 * p] = make_float4(v[0][0], v[1][0], v[0][1], v[1][1]);
+    out[2 * p + 1] = make_float4(v[0][2], v[1][2], v[0][3], v[1][3]);
   }
 }
 
@@ -697,7 +745,7 @@ int contractTensor(tcscf_ctx * ctx, Contraction const & c, int precision)
   }
   tc::kPackCoords<<<gridBlocks(n1pad, 256), 256, 0, ctx->stream>>>(c.n1, n1pad, c.p1, nullptr, r1c);
   TCSCF_LAUNCH(ctx);
-  tc::kPackCoords<<<gridBlocks(n2pad, 256), 256, 0, ctx->stream>>>(c.n2, n2pad, c.p2, c.coul, r2c);
+  tc::kPackCoordPairs<<<gridBlocks(n2pad / 2, 256), 256, 0, ctx->stream>>>(c.n2, n2pad, c.p2, c.coul, r2c);
   TCSCF_LAUNCH(ctx);
 
   CUtensorMap maps[6];
