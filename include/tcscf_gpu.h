@@ -142,6 +142,12 @@ int tcscf_grid_basis_values(tcscf_ctx * ctx, int grid, double * values, double *
 /* quadrature S_ij = sum_g w phi_i^* phi_j and H_ij = sum_g w (1/2 grad phi_i^* . grad phi_j - Z phi_i^* phi_j / r)
  * on a 3-D grid with gradients; S, H complex [nb][nb] */
 int tcscf_overlap_core_quadrature(tcscf_ctx * ctx, int grid, int Z, double * S, double * H);
+/* Same quadrature with no device allocation: the block results use a fixed 2 MiB device array
+ * (nb <= 256, else TCSCF_ERR_UNSUPPORTED), for callers that cannot allocate device memory at that
+ * point (device memory already handed to their own pool, or no device-wide synchronisation allowed).
+ * The first call on a device sets up the array's address and should come before any stream capture;
+ * overlapping calls on one device share the array and race.  No counterpart in the reference. */
+int tcscf_overlap_core_quadrature_static(tcscf_ctx * ctx, int grid, int Z, double * S, double * H);
 
 /* ---- r12 kernel contractions (precompute form) --------------------------------------------- */
 /* precomputeIntegrand + computeF (HartreeFock.hpp:23-180): F written to host memory in the Fji

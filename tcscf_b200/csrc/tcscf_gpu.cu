@@ -3,6 +3,8 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <mutex>
+#include <string>
 #include <algorithm>
 #include <vector>
 
@@ -188,6 +190,29 @@ __global__ void kQuadOverlapCore(int64_t n, int nb, int Z, const double * pts, c
     S[blockIdx.x] = make_double2(a[0], a[1]);
     if (H) H[blockIdx.x] = make_double2(a[2], a[3]);
   }
+}
+
+// Fixed scratch of tcscf_overlap_core_quadrature_static: S block results, then H (2 MiB).
+constexpr int kQuadStaticMaxNb = 256;
+static __device__ __align__(256) double2 gQuadStaticScratch[2 * kQuadStaticMaxNb * kQuadStaticMaxNb];
+
+// Device address of gQuadStaticScratch on the context's device, looked up once per device with that
+// device current (the caller has made it current).
+int quadStaticScratch(tcscf_ctx * ctx, double2 ** out)
+{
+  constexpr int kMaxDevices = 64;
+  static std::mutex lock;
+  static double2 * addr[kMaxDevices] = {};
+  TCSCF_CHECK(ctx, ctx->device >= 0 && ctx->device < kMaxDevices, TCSCF_ERR_INVALID_ARGUMENT, "device index out of range");
+  std::lock_guard<std::mutex> guard(lock);
+  if (!addr[ctx->device]) {
+    void * p = nullptr;
+    cudaError_t const e = cudaGetSymbolAddress(&p, gQuadStaticScratch);
+    if (e != cudaSuccess) return fail(ctx, TCSCF_ERR_CUDA, std::string("cudaGetSymbolAddress(gQuadStaticScratch): ") + cudaGetErrorString(e));
+    addr[ctx->device] = static_cast<double2 *>(p);
+  }
+  *out = addr[ctx->device];
+  return TCSCF_OK;
 }
 
 // U coefficient U[k][i] of the unitary complex -> real-harmonic map phiR_k = sum_i U[k][i] phi_i
@@ -948,6 +973,42 @@ int tcscf_overlap_core_quadrature(tcscf_ctx * ctx, int grid, int Z, double * S, 
   TCSCF_TRY(scratch(ctx, "quad_sh", sizeof(double2) * nb * nb * 2, &p));
   double2 * dS = static_cast<double2 *>(p);
   double2 * dH = dS + nb * nb;
+  kQuadOverlapCore<<<nb * nb, 256, 0, ctx->stream>>>(g->n, nb, Z, g->pts, g->w, reinterpret_cast<double2 *>(g->vals),
+                                                      H ? reinterpret_cast<double2 *>(g->grads) : nullptr, dS, H ? dH : nullptr);
+  TCSCF_LAUNCH(ctx);
+  TCSCF_CUDA(ctx, cudaMemcpyAsync(S, dS, sizeof(double2) * nb * nb, cudaMemcpyDeviceToHost, ctx->stream));
+  if (H) TCSCF_CUDA(ctx, cudaMemcpyAsync(H, dH, sizeof(double2) * nb * nb, cudaMemcpyDeviceToHost, ctx->stream));
+  TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return TCSCF_OK;
+}
+
+// Fixed-scratch form of the S/H quadrature: the block results go to a file-scope device array
+// instead of context scratch, so this entry point allocates nothing.  It serves callers that cannot
+// allocate device memory at this point: a host whose device memory is already handed out to its own
+// pool (grids and tensors sized to fill HBM), and a host that cannot accept the device-wide
+// synchronisation that cudaFree implies while its other streams are running.
+//   * Limit: nb <= kQuadStaticMaxNb (256), i.e. 2 x 256 x 256 complex doubles = 2 MiB per device;
+//     larger bases are rejected with TCSCF_ERR_UNSUPPORTED.
+//   * Set-up: the first call on a device looks up the array's device address with that device
+//     current (cudaGetSymbolAddress); make that first call before any stream capture.
+//   * Sharing: every call on a device uses the same array, so overlapping calls on one device (other
+//     streams or other contexts) race; callers serialise them.  Nothing in the array needs to start
+//     at zero: kQuadOverlapCore writes every element it returns (one block per (i, j)).
+int tcscf_overlap_core_quadrature_static(tcscf_ctx * ctx, int grid, int Z, double * S, double * H)
+{
+  if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
+  Grid * g = findGrid(ctx, grid);
+  TCSCF_CHECK(ctx, g && g->nb > 0 && g->ndim == 3, TCSCF_ERR_INVALID_ARGUMENT, "needs a 3-D grid with a basis");
+  TCSCF_CHECK(ctx, S, TCSCF_ERR_INVALID_ARGUMENT, "S is required");
+  TCSCF_CHECK(ctx, !H || g->grads, TCSCF_ERR_INVALID_ARGUMENT, "H needs stored gradients");
+  int const nb = g->nb;
+  TCSCF_CHECK(ctx, nb <= kQuadStaticMaxNb, TCSCF_ERR_UNSUPPORTED,
+              "nb = " + std::to_string(nb) + " exceeds the fixed scratch of tcscf_overlap_core_quadrature_static (nb <= " +
+                  std::to_string(kQuadStaticMaxNb) + "); use tcscf_overlap_core_quadrature");
+  TCSCF_CUDA(ctx, cudaSetDevice(ctx->device));
+  double2 * dS = nullptr;
+  TCSCF_TRY(quadStaticScratch(ctx, &dS));
+  double2 * dH = dS + kQuadStaticMaxNb * kQuadStaticMaxNb;
   kQuadOverlapCore<<<nb * nb, 256, 0, ctx->stream>>>(g->n, nb, Z, g->pts, g->w, reinterpret_cast<double2 *>(g->vals),
                                                       H ? reinterpret_cast<double2 *>(g->grads) : nullptr, dS, H ? dH : nullptr);
   TCSCF_LAUNCH(ctx);
