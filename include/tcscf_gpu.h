@@ -73,8 +73,9 @@ typedef enum tcscf_kernel {
 } tcscf_kernel;
 
 /* Precision of the r12 contraction.  FP64: CUDA-core FP64 throughout.  BF16X3: tcgen05 tensor
- * cores with hi+lo BF16 operand pairs (3 products), FP32 accumulation in TMEM, flushed into FP64.
- * TF32: tcgen05 kind::tf32, one product, FP32 accumulation flushed into FP64. */
+ * cores with hi+lo BF16 operand pairs (3 products) in fixed point (power-of-two scale per row /
+ * column / r2 block), so the FP32 accumulation in TMEM of each r2 block of 64 is exact; every block
+ * is added into FP64.  TF32: reserved (returns TCSCF_ERR_UNSUPPORTED). */
 typedef enum tcscf_precision {
   TCSCF_PREC_FP64 = 0,
   TCSCF_PREC_BF16X3 = 1,
@@ -106,9 +107,6 @@ int tcscf_last_timing(tcscf_ctx * ctx, double * contraction_ms, double * total_m
 /* diagnostics: the Coulomb potential VH[N1] (both spins) and the first spin's exchange potential
  * T[N1][nb] (real-harmonic basis) of the most recent direct Fock build on this context */
 int tcscf_last_potentials(tcscf_ctx * ctx, double * VH, double * T);
-/* accumulation window of the tensor-core paths: r2 blocks of 64 accumulated in FP32 in TMEM before
- * being flushed into FP64 (default 1: every block, the most accurate setting) */
-int tcscf_set_flush_window(tcscf_ctx * ctx, int blocks);
 
 /* ---- host-side grid generation (replaces ChebyshevGauss/changeOfVariables/createGrid,
  *      TreutlerAhlrichsLebedev and QMCGrid's point mapping) ---------------------------------- */

@@ -85,9 +85,6 @@ class Context:
         _raise(ffi.lib().tcscf_last_potentials(self._h, ffi.dptr(VH), ffi.dptr(T)), self._h)
         return VH, T
 
-    def set_flush_window(self, blocks: int) -> None:
-        _raise(ffi.lib().tcscf_set_flush_window(self._h, blocks), self._h)
-
 
 class QMCGrid:
     """Device-resident integration::QMCGrid built from a host QuadratureGrid (points already Cartesian)."""

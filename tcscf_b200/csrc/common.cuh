@@ -70,7 +70,6 @@ struct tcscf_ctx {
   std::map<int, tcscf::Grid> grids;
   std::map<int, tcscf::Tensor> tensors;
   int nextId = 1;
-  int flushWindow = 1;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   double lastContractionMs = 0, lastTotalMs = 0;
   int lastLaunches = 0;

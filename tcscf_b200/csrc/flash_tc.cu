@@ -1,20 +1,31 @@
-// tcgen05 (sm_100a) r12 contraction for the direct Fock build, split-BF16 ("bf16x3") precision.
+// tcgen05 (sm_100a) r12 contraction for the direct Fock build in split-BF16 precision with exact
+// tensor-core accumulation.
 //
 // For a tile of 128 r1 points (one TMEM lane each) the kernel streams r2 in blocks of 64:
-//   GEMM1 (tensor):  S[r1][r2]  = psi1[r1][:] . psi2[r2][:]        rho(r1,r2), K = 32 (padded rank)
+//   GEMM1 (tensor):  rho(r1,r2) = psi1[r1][:] . psi2[r2][:]            K = 32 or 64 (padded rank)
 //   CUDA cores:      g = 1/|r1 - r2| (FP32, Newton-refined), X = g * rho, VH(r1) += g * coul(r2)
-//   GEMM2 (tensor):  T[r1][i]  += X[r1][r2] . Vt[i][r2]            Vt = (w2 phi_i(r2))^T, N = NB
-// Every operand is a hi+lo BF16 pair and each GEMM issues hi*hi + hi*lo + lo*hi; accumulation is
-// FP32 in TMEM, flushed every `window` r2 blocks into per-thread FP64 accumulators (the TMEM
-// accumulator is double-buffered so the MMA never waits for a flush).  The kernel matrix g is
-// generated in registers and only ever exists as the BF16 X tile in shared memory.
+//   GEMM2 (tensor):  T[r1][i] += X[r1][r2] . Vt[i][r2]                 Vt = (w2 phi_i(r2))^T, N = NB
+//
+// Fixed-point BF16 slices.  Each row of psi1 / psi2, each (r1, block) row of X and each (block, i)
+// column of Vt carries a power-of-two scale s chosen from its largest entry.  The per-point factors
+// psi1, psi2 and Vt (whose rounding is shared by every pair a point takes part in) keep 24 bits:
+// u s in [2^23, 2^24) is written as 65536 h + 256 m + l with integers |h| <= 256, |m|, |l| <= 128
+// (round to nearest, each exact in BF16); X keeps 16 bits, u s = 256 h + l.  Per r2 block:
+//   A = sum h h'                      (integers below 2^16 each, a K <= 64 sum below 2^23: exact)
+//   B = sum h m' + m h' + (h l' + l h' + m m')/256   (the level 2^-8 below A; its own FP32 rounding
+//                                                     is scaled down by 2^-8 in the result)
+// and the product is 256 A + B in units of the block's scales (GEMM2 keeps h m', l h', h l'/256 of
+// its 16-bit X).  The hi*hi accumulation being exact, the tensor core's FP32 adder rounding cannot
+// bias the result; the products below 2^-24 of the largest term are dropped.  Each block's T is added into per-thread
+// FP64 accumulators with its scales as soon as the block completes.  The kernel matrix g exists
+// only as the BF16 X tile in shared memory.
 //
 // Warp roles (384 threads, one CTA per SM, persistent over (r1 tile, r2 split) work items):
 //   warp 0      TMA producer: psi1 tile (once per work item), psi2 / Vt blocks (TMA, no multicast),
-//               r2 coordinates + Coulomb source (1-D bulk copy)
+//               r2 coordinates + Coulomb source, psi2 row scales and Vt column scales (1-D bulk copies)
 //   warp 1      MMA issuer (one elected thread) and TMEM allocator
 //   warps 2-3   idle (they complete warpgroup 0, whose registers setmaxnreg hands to the compute warps)
-//   warps 4-11  compute: warp w owns TMEM lanes 32*(w%4).. (r1 rows), column half (w-4)/4
+//   warps 4-11  compute: warp w owns TMEM lanes 32*(w%4).. (r1 rows), r2 / column half (w-4)/4
 // Every mbarrier wait is bounded by a wall-clock limit; on expiry the kernel records the failure in
 // a device status word, drains its own TMA / MMA work with bounded waits, frees TMEM and returns.
 #include <cuda.h>
@@ -27,8 +38,8 @@ namespace tc {
 
 constexpr int BM = 128;        // r1 rows per tile
 constexpr int BK = 64;         // r2 points per block
-// TMA stages: three when the rank padding leaves room in shared memory
-__host__ __device__ constexpr int stagesFor(int RP) { return RP == 32 ? 3 : 2; }
+// TMA stages: three when the tile shapes leave room in shared memory
+__host__ __device__ constexpr int stagesFor(int NB, int RP) { return NB == 64 && RP == 32 ? 3 : 2; }
 constexpr int NCW = 8;         // compute warps
 constexpr int NTHREADS = 384;  // warpgroup 0: TMA, MMA, 2 idle warps; warpgroups 1-2: compute
 // register split: 384 threads x 168 at launch = 64512 = 128 x 56 (producer warpgroup) + 256 x 224
@@ -38,18 +49,34 @@ constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s per wait
 // a waiting thread sleeps in mbarrier.try_wait (woken when the phase completes) instead of spinning
 // on the issue slots the compute warps need
 constexpr uint32_t kSuspendHintNs = 1000000;
+// slicing: scale = 2^(k - floor(log2 max|u|)) puts the largest entry in [2^k, 2^(k+1)): k = 23 for
+// the three-slice factors, 15 for the two-slice X; entries of a row whose maximum is below
+// 2^kMinExp are sliced against 2^kMinExp
+constexpr int kFactorExp = 23;
+constexpr int kXExp = 15;
+constexpr int kMinExp = -100;
+
+// TMEM columns: rho buffers b = 0, 1 at 128 b (hi*hi) and 128 b + 64 (cross); T at TCOL0 (hi*hi) and
+// TCOL0 + NB (cross)
+constexpr uint32_t TCOL0 = 256;
 
 // RP: padded rank of rho (GEMM1 K): 32 (64-byte rows, 64B swizzle) or 64 (128-byte rows, 128B swizzle)
 template <int NB, int RP>
 struct __align__(1024) Smem {
-  static constexpr int NSTAGE = stagesFor(RP);
-  uint8_t v[NSTAGE][2][NB * BK * 2];       // Vt block hi/lo: SW128 K-major [NB rows][64]
-  uint8_t x[2][2][BM * BK * 2];            // X tile hi/lo:   SW128 K-major [128 rows][64]
-  uint8_t psi2[NSTAGE][2][BK * RP * 2];    // psi2 block hi/lo: K-major [64 rows][RP]
-  uint8_t psi1[2][BM * RP * 2];            // psi1 tile hi/lo:  K-major [128 rows][RP]
+  static constexpr int NSTAGE = stagesFor(NB, RP);
+  uint8_t v[NSTAGE][3][NB * BK * 2];       // Vt block h / m / l/256: SW128 K-major [NB rows][64]
+  uint8_t x[2][BM * BK * 2];               // X tile h / l:   SW128 K-major [128 rows][64]
+  uint8_t psi2[NSTAGE][3][BK * RP * 2];    // psi2 block h / m / l/256: K-major [64 rows][RP]
+  uint8_t psi1[4][BM * RP * 2];            // psi1 tile h / m / l/256 / m/256: K-major [128 rows][RP]
   float4 coords[NSTAGE][BK];               // r2 block as 32 pairs {x0,x1,y0,y1}{z0,z1,c0,c1}
+  float a2inv[NSTAGE][BK];                 // 1 / (psi2 row scale) of the block's r2 points
+  float cinv[NSTAGE][NB];                  // 1 / (Vt column scale) of the block
+  float cinvT[NCW][2][NB / 2];             // each compute warp's copy of its columns' cinv, by block parity
+  float rowmax[2][2][BM];                  // [block parity][r2 half][row] max |X'| of the half
   uint64_t full[NSTAGE], empty[NSTAGE];
-  uint64_t sfull[2], sfree[2], xfull[2], xfree[2], tfull[2], tfree[2];
+  uint64_t sfull[2], sfree[2], xfull, xfree;
+  uint64_t rmax[2][4];                     // [block parity][lane quarter]: both r2 halves posted their maxima
+  uint64_t tfull, tfree;
   uint64_t p1full, p1free, done;
   uint32_t tmemBase;
   int abort;
@@ -59,9 +86,11 @@ struct Params {
   int nTiles, nSplit, blocksPerSplit, nBlocks;   // r2 blocks in total, per split
   int n1;                                          // real r1 rows
   int nb;                                          // real columns of T
-  int window;                                      // r2 blocks per FP32 accumulation window
   const float4 * r1xyz;                            // [n1pad] x, y, z, 0
-  const float4 * r2xyzc;                           // [nBlocks*64] x, y, z, coul
+  const float4 * r2pairs;                          // [nBlocks*64] r2 points in pair layout
+  const float * a1inv;                             // [n1pad] 1 / psi1 row scale
+  const float * a2inv;                             // [nBlocks*64] 1 / psi2 row scale
+  const float * cinv;                              // [nBlocks][NB] 1 / Vt column scale
   double * T;                                      // [nSplit][n1][ldt]
   double * VH;                                     // [nSplit][n1]
   int ldt;
@@ -195,6 +224,12 @@ __device__ __forceinline__ uint64_t f2pack(float a, float b)
   return d;
 }
 __device__ __forceinline__ void f2unpack(uint64_t v, float & a, float & b) { asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v)); }
+__device__ __forceinline__ uint64_t f2add(uint64_t a, uint64_t b)
+{
+  uint64_t d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
 __device__ __forceinline__ uint64_t f2sub(uint64_t a, uint64_t b)
 {
   uint64_t d;
@@ -226,59 +261,75 @@ __device__ __forceinline__ uint32_t sw128(int row, int chunk)
   return uint32_t((row >> 3) * 1024 + (row & 7) * 128 + ((chunk ^ (row & 7)) << 4));
 }
 
-__device__ __forceinline__ uint32_t packBf16(float a, float b)
+// the BF16 pair {a, b} of two FP32 values whose low 16 mantissa bits are zero (exact truncation)
+__device__ __forceinline__ uint32_t bf16PairExact(uint64_t ab)
 {
-  __nv_bfloat162 const h = __floats2bfloat162_rn(a, b);
-  return *reinterpret_cast<uint32_t const *>(&h);
+  float a, b;
+  f2unpack(ab, a, b);
+  return __byte_perm(__float_as_uint(a), __float_as_uint(b), 0x7632);
 }
 
-// Adds one finished FP32 TMEM accumulation window (64 of the NB columns of this thread's row) into
-// the FP64 accumulators and hands the TMEM buffer back to the MMA issuer.
+// Adds the finished block f (this thread's row, NB/2 columns of T) into the FP64 accumulators with the
+// block's scales and hands the TMEM accumulators back to the MMA issuer.
 template <int NB, class SmemT>
-__device__ __forceinline__ bool flushWindow(SmemT & S, uint32_t taddr, uint32_t window, double (&acc)[64], int lane,
-                                            volatile int * abortFlag, int * status)
+__device__ __forceinline__ bool flushBlock(SmemT & S, uint32_t taddr, uint32_t f, int cw, double fac, double (&acc)[NB / 2], int lane,
+                                           volatile int * abortFlag, int * status)
 {
-  uint32_t const t = window & 1;
-  if (!waitBar(&S.tfull[t], (window >> 1) & 1, abortFlag, status, 31)) return false;
+  if (!waitBar(&S.tfull, f & 1, abortFlag, status, 31)) return false;
   fenceAfterSync();
+  float const * cs = S.cinvT[cw][f & 1];
+  uint64_t const k256 = f2pack(256.0f, 256.0f);
 #pragma unroll
-  for (int q = 0; q < (NB >= 128 ? 4 : 2); ++q) {
-    float v[16];
-    tmemLoad16(taddr + q * 16, v);
+  for (int q = 0; q < NB / 32; ++q) {
+    float hh[16], mm[16];
+    tmemLoad16(taddr + q * 16, hh);
+    tmemLoad16(taddr + NB + q * 16, mm);
     tmemWaitLoad();
 #pragma unroll
-    for (int i = 0; i < 16; ++i) acc[q * 16 + i] += double(v[i]);
+    for (int i = 0; i < 8; ++i) {
+      float2 const c2 = *reinterpret_cast<float2 const *>(cs + q * 16 + 2 * i);
+      // 256 hh + cross is the block's exact integer sum up to one FP32 rounding; cinv is a power of two
+      uint64_t const v = f2mul(f2fma(f2pack(hh[2 * i], hh[2 * i + 1]), k256, f2pack(mm[2 * i], mm[2 * i + 1])), f2pack(c2.x, c2.y));
+      float va, vb;
+      f2unpack(v, va, vb);
+      acc[q * 16 + 2 * i] = fma(double(va), fac, acc[q * 16 + 2 * i]);
+      acc[q * 16 + 2 * i + 1] = fma(double(vb), fac, acc[q * 16 + 2 * i + 1]);
+    }
   }
   fenceBeforeSync();
   __syncwarp();
-  if (lane == 0) mbarArrive(&S.tfree[t]);
+  if (lane == 0) mbarArrive(&S.tfree);
   return true;
 }
 
 // ---- the kernel ------------------------------------------------------------------------------------
 template <int NB, int RP>
 __global__ void __launch_bounds__(NTHREADS, 1)
-    kFlashTc(const __grid_constant__ CUtensorMap mapPsi1Hi, const __grid_constant__ CUtensorMap mapPsi1Lo,
-             const __grid_constant__ CUtensorMap mapPsi2Hi, const __grid_constant__ CUtensorMap mapPsi2Lo,
-             const __grid_constant__ CUtensorMap mapVHi, const __grid_constant__ CUtensorMap mapVLo, Params P)
+    kFlashTc(const __grid_constant__ CUtensorMap mapPsi1H, const __grid_constant__ CUtensorMap mapPsi1M,
+             const __grid_constant__ CUtensorMap mapPsi1L, const __grid_constant__ CUtensorMap mapPsi1Ms,
+             const __grid_constant__ CUtensorMap mapPsi2H,
+             const __grid_constant__ CUtensorMap mapPsi2M, const __grid_constant__ CUtensorMap mapPsi2L,
+             const __grid_constant__ CUtensorMap mapVH, const __grid_constant__ CUtensorMap mapVM,
+             const __grid_constant__ CUtensorMap mapVL, Params P)
 {
   extern __shared__ uint8_t smemRaw[];
   Smem<NB, RP> & S = *reinterpret_cast<Smem<NB, RP> *>((reinterpret_cast<uintptr_t>(smemRaw) + 1023) & ~uintptr_t(1023));
-  constexpr int NSTAGE = stagesFor(RP);
+  constexpr int NSTAGE = stagesFor(NB, RP);
   int const warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   volatile int * abortFlag = &S.abort;
 
-  constexpr uint32_t TCOL0 = 2 * BK;   // TMEM columns: S buffers [0, 128), T buffers [128, 128 + 2 NB)
-  constexpr uint32_t kStageBytes = 2 * NB * BK * 2 + 2 * BK * RP * 2 + BK * sizeof(float4);
-  constexpr uint32_t kPsi1Bytes = 2 * BM * RP * 2;
+  static_assert(TCOL0 + 2 * NB <= 512, "TMEM columns");
+  constexpr uint32_t kStageBytes = 3 * NB * BK * 2 + 3 * BK * RP * 2 + BK * sizeof(float4) + BK * sizeof(float) + NB * sizeof(float);
+  constexpr uint32_t kPsi1Bytes = 4 * BM * RP * 2;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < NSTAGE; ++s) { mbarInit(&S.full[s], 1); mbarInit(&S.empty[s], 1 + NCW); }
     for (int b = 0; b < 2; ++b) {
       mbarInit(&S.sfull[b], 1); mbarInit(&S.sfree[b], NCW);
-      mbarInit(&S.xfull[b], NCW); mbarInit(&S.xfree[b], 1);
-      mbarInit(&S.tfull[b], 1); mbarInit(&S.tfree[b], NCW);
+      for (int q = 0; q < 4; ++q) mbarInit(&S.rmax[b][q], 2);
     }
+    mbarInit(&S.xfull, NCW); mbarInit(&S.xfree, 1);
+    mbarInit(&S.tfull, 1); mbarInit(&S.tfree, NCW);
     mbarInit(&S.p1full, 1); mbarInit(&S.p1free, 1); mbarInit(&S.done, 1);
     S.abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -308,8 +359,10 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         int const je = min(P.nBlocks, jb + P.blocksPerSplit);
         if (p1Use > 0 && !(ok = waitBar(&S.p1free, (p1Use - 1) & 1, abortFlag, P.status, 11))) break;
         mbarArriveTx(&S.p1full, kPsi1Bytes);
-        tmaLoad2d(S.psi1[0], &mapPsi1Hi, 0, tile * BM, &S.p1full);
-        tmaLoad2d(S.psi1[1], &mapPsi1Lo, 0, tile * BM, &S.p1full);
+        tmaLoad2d(S.psi1[0], &mapPsi1H, 0, tile * BM, &S.p1full);
+        tmaLoad2d(S.psi1[1], &mapPsi1M, 0, tile * BM, &S.p1full);
+        tmaLoad2d(S.psi1[2], &mapPsi1L, 0, tile * BM, &S.p1full);
+        tmaLoad2d(S.psi1[3], &mapPsi1Ms, 0, tile * BM, &S.p1full);
         ++p1Use;
         for (int j = jb; j < je; ++j) {
           uint32_t const q = issuedLoads++;
@@ -317,11 +370,15 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           // use u = q / NSTAGE of stage s needs consumption u - 1 of it
           if (q >= uint32_t(NSTAGE) && !(ok = waitBar(&S.empty[s], ((q / NSTAGE) - 1) & 1, abortFlag, P.status, 12))) break;
           mbarArriveTx(&S.full[s], kStageBytes);
-          tmaLoad2d(S.psi2[s][0], &mapPsi2Hi, 0, j * BK, &S.full[s]);
-          tmaLoad2d(S.psi2[s][1], &mapPsi2Lo, 0, j * BK, &S.full[s]);
-          tmaLoad2d(S.v[s][0], &mapVHi, j * BK, 0, &S.full[s]);
-          tmaLoad2d(S.v[s][1], &mapVLo, j * BK, 0, &S.full[s]);
-          bulkLoad(S.coords[s], P.r2xyzc + int64_t(j) * BK, BK * sizeof(float4), &S.full[s]);
+          tmaLoad2d(S.psi2[s][0], &mapPsi2H, 0, j * BK, &S.full[s]);
+          tmaLoad2d(S.psi2[s][1], &mapPsi2M, 0, j * BK, &S.full[s]);
+          tmaLoad2d(S.psi2[s][2], &mapPsi2L, 0, j * BK, &S.full[s]);
+          tmaLoad2d(S.v[s][0], &mapVH, j * BK, 0, &S.full[s]);
+          tmaLoad2d(S.v[s][1], &mapVM, j * BK, 0, &S.full[s]);
+          tmaLoad2d(S.v[s][2], &mapVL, j * BK, 0, &S.full[s]);
+          bulkLoad(S.coords[s], P.r2pairs + int64_t(j) * BK, BK * sizeof(float4), &S.full[s]);
+          bulkLoad(S.a2inv[s], P.a2inv + int64_t(j) * BK, BK * sizeof(float), &S.full[s]);
+          bulkLoad(S.cinv[s], P.cinv + int64_t(j) * NB, NB * sizeof(float), &S.full[s]);
         }
       }
       // drain: every issued load lands before the CTA can exit (bounded)
@@ -339,9 +396,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     if (lane == 0) {
       constexpr uint32_t idesc1 = instrDescBf16(BM, BK);
       constexpr uint32_t idesc2 = instrDescBf16(BM, NB);
-      uint32_t const aPsi1[2] = {smemAddr(S.psi1[0]), smemAddr(S.psi1[1])};
-      uint32_t blockCount = 0;   // global block counter: selects stage, S/X buffers
-      uint32_t windowCount = 0;  // global window counter: selects the T buffer
+      uint32_t const aPsi1[4] = {smemAddr(S.psi1[0]), smemAddr(S.psi1[1]), smemAddr(S.psi1[2]), smemAddr(S.psi1[3])};
+      uint32_t blockCount = 0;   // global block counter: selects stage, rho / X buffers, T phase
       uint32_t p1Use = 0;
       bool ok = true;
       for (int item = blockIdx.x; item < nItems && ok; item += gridDim.x) {
@@ -359,20 +415,22 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           if (!waitBar(&S.full[s], (g / NSTAGE) & 1, abortFlag, P.status, 22)) return false;
           if (g >= 2 && !waitBar(&S.sfree[b], ((g >> 1) - 1) & 1, abortFlag, P.status, 23)) return false;
           fenceAfterSync();
-          uint32_t const d = tmem + b * BK;
-          uint32_t const bPsi2[2] = {smemAddr(S.psi2[s][0]), smemAddr(S.psi2[s][1])};
-          // the two small cross products accumulate first, the hi*hi product last, so that only
-          // the final steps round the full-magnitude accumulator
+          uint32_t const dHH = tmem + b * 2 * BK, dX = dHH + BK;
+          uint32_t const bPsi2[3] = {smemAddr(S.psi2[s][0]), smemAddr(S.psi2[s][1]), smemAddr(S.psi2[s][2])};
           constexpr uint32_t sbo = RP == 64 ? 1024 : 512, swz = RP == 64 ? 2 : 4;
-          uint32_t acc = 0;
+          auto da = [&](int sl, int k) { return smemDesc(aPsi1[sl] + 32 * k, sbo, swz); };
+          auto db = [&](int sl, int k) { return smemDesc(bPsi2[sl] + 32 * k, sbo, swz); };
 #pragma unroll
           for (int k = 0; k < RP / 16; ++k) {
-            mmaBf16(d, smemDesc(aPsi1[0] + 32 * k, sbo, swz), smemDesc(bPsi2[1] + 32 * k, sbo, swz), idesc1, acc); acc = 1;
-            mmaBf16(d, smemDesc(aPsi1[1] + 32 * k, sbo, swz), smemDesc(bPsi2[0] + 32 * k, sbo, swz), idesc1, 1);
+            uint32_t const acc = k > 0 ? 1u : 0u;
+            // B: h m' + m h' + h l'/256 + l/256 h' + m/256 m'; A: h h'
+            mmaBf16(dX, da(0, k), db(1, k), idesc1, acc);
+            mmaBf16(dX, da(1, k), db(0, k), idesc1, 1);
+            mmaBf16(dX, da(0, k), db(2, k), idesc1, 1);
+            mmaBf16(dX, da(2, k), db(0, k), idesc1, 1);
+            mmaBf16(dX, da(3, k), db(1, k), idesc1, 1);
+            mmaBf16(dHH, da(0, k), db(0, k), idesc1, acc);
           }
-#pragma unroll
-          for (int k = 0; k < RP / 16; ++k)
-            mmaBf16(d, smemDesc(aPsi1[0] + 32 * k, sbo, swz), smemDesc(bPsi2[0] + 32 * k, sbo, swz), idesc1, 1);
           mmaCommit(&S.sfull[b]);
           return true;
         };
@@ -381,27 +439,25 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           if (jj + 1 < nblk && !(ok = gemm1(jj + 1))) break;
           uint32_t const g = base + jj;
           int const s = g % NSTAGE, b = g & 1;
-          int const inWin = jj % P.window;
-          bool const lastInWin = (inWin == P.window - 1) || (jj == nblk - 1);
-          uint32_t const t = windowCount & 1;
-          if (inWin == 0 && windowCount >= 2 && !(ok = waitBar(&S.tfree[t], ((windowCount >> 1) - 1) & 1, abortFlag, P.status, 24))) break;
-          if (!(ok = waitBar(&S.xfull[b], (g >> 1) & 1, abortFlag, P.status, 25))) break;
+          // the T accumulators are free once the compute warps flushed block g - 1
+          if (g >= 1 && !(ok = waitBar(&S.tfree, (g - 1) & 1, abortFlag, P.status, 24))) break;
+          if (!(ok = waitBar(&S.xfull, g & 1, abortFlag, P.status, 25))) break;
           fenceAfterSync();
-          uint32_t const d = tmem + TCOL0 + t * NB;
-          uint32_t const aX[2] = {smemAddr(S.x[b][0]), smemAddr(S.x[b][1])};
-          uint32_t const bV[2] = {smemAddr(S.v[s][0]), smemAddr(S.v[s][1])};
-          uint32_t acc = inWin == 0 ? 0u : 1u;
+          uint32_t const dHH = tmem + TCOL0, dX = dHH + NB;
+          uint32_t const aX[2] = {smemAddr(S.x[0]), smemAddr(S.x[1])};
+          uint32_t const bV[3] = {smemAddr(S.v[s][0]), smemAddr(S.v[s][1]), smemAddr(S.v[s][2])};
 #pragma unroll
           for (int k = 0; k < BK / 16; ++k) {
-            mmaBf16(d, smemDesc(aX[0] + 32 * k, 1024, 2), smemDesc(bV[1] + 32 * k, 1024, 2), idesc2, acc); acc = 1;
-            mmaBf16(d, smemDesc(aX[1] + 32 * k, 1024, 2), smemDesc(bV[0] + 32 * k, 1024, 2), idesc2, 1);
+            uint32_t const acc = k > 0 ? 1u : 0u;
+            // B: hX mV + lX hV + hX lV/256; A: hX hV
+            mmaBf16(dX, smemDesc(aX[0] + 32 * k, 1024, 2), smemDesc(bV[1] + 32 * k, 1024, 2), idesc2, acc);
+            mmaBf16(dX, smemDesc(aX[1] + 32 * k, 1024, 2), smemDesc(bV[0] + 32 * k, 1024, 2), idesc2, 1);
+            mmaBf16(dX, smemDesc(aX[0] + 32 * k, 1024, 2), smemDesc(bV[2] + 32 * k, 1024, 2), idesc2, 1);
+            mmaBf16(dHH, smemDesc(aX[0] + 32 * k, 1024, 2), smemDesc(bV[0] + 32 * k, 1024, 2), idesc2, acc);
           }
-#pragma unroll
-          for (int k = 0; k < BK / 16; ++k)
-            mmaBf16(d, smemDesc(aX[0] + 32 * k, 1024, 2), smemDesc(bV[0] + 32 * k, 1024, 2), idesc2, 1);
-          mmaCommit(&S.xfree[b]);
+          mmaCommit(&S.xfree);
           mmaCommit(&S.empty[s]);
-          if (lastInWin) { mmaCommit(&S.tfull[t]); ++windowCount; }
+          mmaCommit(&S.tfull);
           if (jj == nblk - 1) mmaCommit(&S.p1free);
         }
         blockCount += nblk;
@@ -427,9 +483,13 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     int const half = cw >> 2;
     int const row = quarter * 32 + lane;
     uint32_t const laneBase = uint32_t(quarter * 32) << 16;
-    uint32_t blockCount = 0, windowCount = 0;
+    uint32_t const tAddr = tmem + laneBase + TCOL0 + uint32_t(half * (NB / 2));
+    uint32_t blockCount = 0;
     bool ok = true;
-    double acc[64];
+    double acc[NB / 2];
+    uint64_t const k256 = f2pack(256.0f, 256.0f), kInv256 = f2pack(1.0f / 256.0f, 1.0f / 256.0f), kM256 = f2pack(-256.0f, -256.0f);
+    uint64_t const kMagic = f2pack(12582912.0f, 12582912.0f);   // 1.5 * 2^23: adding it rounds |x| < 2^22 to an integer
+    uint64_t const mOne = f2pack(-1.0f, -1.0f), mHalf = f2pack(-0.5f, -0.5f);
     for (int item = blockIdx.x; item < nItems && ok; item += gridDim.x) {
       int const tile = item / P.nSplit, split = item % P.nSplit;
       int const jb = split * P.blocksPerSplit;
@@ -437,95 +497,116 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       int const nblk = je - jb;
       int const r1 = tile * BM + row;
       float4 const p1 = P.r1xyz[r1];
+      // rho = 2^24 a1inv a2inv (256 A + B), X' = g a2inv (256 A + B) = X / (2^24 a1inv), and a block's
+      // sum_r2 X' Vt = 2^16 (256 A + B) / (bs c): T += 2^40 a1inv / bs * cinv (256 A + B)
+      double const rowA = 1099511627776.0 * double(P.a1inv[r1]);
 #pragma unroll
-      for (int c = 0; c < 64; ++c) acc[c] = 0.0;
+      for (int c = 0; c < NB / 2; ++c) acc[c] = 0.0;
       double vh = 0.0;
-      int pendingFlush = -1;   // window whose flush is deferred by one block
+      double pendingFac = 0.0;
+      bool pending = false;   // block g - 1 still to be flushed
+      uint64_t const p1x = f2pack(p1.x, p1.x), p1y = f2pack(p1.y, p1.y), p1z = f2pack(p1.z, p1.z);
       for (int jj = 0; jj < nblk && ok; ++jj) {
         uint32_t const g = blockCount + jj;
         int const s = g % NSTAGE, b = g & 1;
         if (!(ok = waitBar(&S.full[s], (g / NSTAGE) & 1, abortFlag, P.status, 32))) break;
         if (!(ok = waitBar(&S.sfull[b], (g >> 1) & 1, abortFlag, P.status, 33))) break;
         fenceAfterSync();
-        float rho[16];
-        tmemLoad16(tmem + laneBase + b * BK + half * 32, rho);
-        tmemWaitLoad();
-        if (g >= 2 && !(ok = waitBar(&S.xfree[b], ((g >> 1) - 1) & 1, abortFlag, P.status, 34))) break;
-        // this warp's 32 r2 points: 16 pairs of {x0,x1,y0,y1}{z0,z1,c0,c1}
+        // this warp's Vt column scales, kept for the flush of block g after the stage is released
+        for (int c = lane; c < NB / 2; c += 32) S.cinvT[cw][b][c] = S.cinv[s][half * (NB / 2) + c];
+        // X' = g * a2inv * (256 rho_hh + rho_cross) for this warp's 32 r2 points (16 pairs)
         float4 const * cc = S.coords[s] + half * 32;
-        uint8_t * xhi = S.x[b][0];
-        uint8_t * xlo = S.x[b][1];
+        float2 const * sa = reinterpret_cast<float2 const *>(S.a2inv[s] + half * 32);
+        uint64_t xv[16];
         uint64_t vsum2 = 0;
-        uint64_t const p1x = f2pack(p1.x, p1.x), p1y = f2pack(p1.y, p1.y), p1z = f2pack(p1.z, p1.z);
-        uint64_t const mOne = f2pack(-1.0f, -1.0f), mHalf = f2pack(-0.5f, -0.5f);
-#pragma unroll 1
+        uint32_t const rhoAddr = tmem + laneBase + uint32_t(b * 2 * BK + half * 32);
+#pragma unroll
         for (int hh = 0; hh < 2; ++hh) {
+          float rh[16], rx[16];
+          tmemLoad16(rhoAddr + hh * 16, rh);
+          tmemLoad16(rhoAddr + BK + hh * 16, rx);
+          tmemWaitLoad();
           if (hh == 1) {
-            // second half of this warp's 32 rho columns; the S buffer is then free for the next GEMM1
-            tmemLoad16(tmem + laneBase + b * BK + half * 32 + 16, rho);
-            tmemWaitLoad();
+            // both rho accumulators of this warp's columns are read: the buffer is free for GEMM1
             fenceBeforeSync();
             __syncwarp();
             if (lane == 0) mbarArrive(&S.sfree[b]);
           }
 #pragma unroll
-          for (int c2 = 0; c2 < 2; ++c2) {
-            int const ch = hh * 2 + c2;
-            uint32_t hi[4], lo[4];
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-              int const pr = ch * 4 + e;                 // pair index within the warp's 16 pairs
-              float4 const qa = cc[2 * pr], qb = cc[2 * pr + 1];
-              uint64_t const dx = f2sub(p1x, f2pack(qa.x, qa.y));
-              uint64_t const dy = f2sub(p1y, f2pack(qa.z, qa.w));
-              uint64_t const dz = f2sub(p1z, f2pack(qb.x, qb.y));
-              uint64_t const r2 = f2fma(dx, dx, f2fma(dy, dy, f2mul(dz, dz)));
-              float r2a, r2b;
-              f2unpack(r2, r2a, r2b);
-              uint64_t y = f2pack(rsqrtApprox(r2a), rsqrtApprox(r2b));
-              // one Newton step on the hardware estimate: y += (-y/2) (r2 y^2 - 1)
-              uint64_t const em = f2fma(f2mul(r2, y), y, mOne);
-              y = f2fma(f2mul(y, mHalf), em, y);
-              float ya, yb;
-              f2unpack(y, ya, yb);
-              ya = r2a > 0.0f ? ya : 0.0f;                // coincident pair contributes 0
-              yb = r2b > 0.0f ? yb : 0.0f;
-              y = f2pack(ya, yb);
-              vsum2 = f2fma(y, f2pack(qb.z, qb.w), vsum2);
-              uint64_t const x = f2mul(y, f2pack(rho[c2 * 8 + 2 * e], rho[c2 * 8 + 2 * e + 1]));
-              float xa, xb;
-              f2unpack(x, xa, xb);
-              // hi = X with the low 16 mantissa bits cleared (exact), lo = BF16(X - hi)
-              uint32_t const b0 = __float_as_uint(xa) & 0xFFFF0000u, b1 = __float_as_uint(xb) & 0xFFFF0000u;
-              hi[e] = __byte_perm(b0, b1, 0x7632);
-              float la, lb;
-              f2unpack(f2sub(x, f2pack(__uint_as_float(b0), __uint_as_float(b1))), la, lb);
-              lo[e] = packBf16(la, lb);
-            }
-            uint32_t const off = sw128(row, half * 4 + ch);
-            *reinterpret_cast<uint4 *>(xhi + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-            *reinterpret_cast<uint4 *>(xlo + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+          for (int e = 0; e < 8; ++e) {
+            int const pr = hh * 8 + e;                  // pair index within the warp's 16 pairs
+            float4 const qa = cc[2 * pr], qb = cc[2 * pr + 1];
+            uint64_t const dx = f2sub(p1x, f2pack(qa.x, qa.y));
+            uint64_t const dy = f2sub(p1y, f2pack(qa.z, qa.w));
+            uint64_t const dz = f2sub(p1z, f2pack(qb.x, qb.y));
+            uint64_t const r2 = f2fma(dx, dx, f2fma(dy, dy, f2mul(dz, dz)));
+            float r2a, r2b;
+            f2unpack(r2, r2a, r2b);
+            uint64_t y = f2pack(rsqrtApprox(r2a), rsqrtApprox(r2b));
+            // one Newton step on the hardware estimate: y += (-y/2) (r2 y^2 - 1)
+            uint64_t const em = f2fma(f2mul(r2, y), y, mOne);
+            y = f2fma(f2mul(y, mHalf), em, y);
+            float ya, yb;
+            f2unpack(y, ya, yb);
+            ya = r2a > 0.0f ? ya : 0.0f;                // coincident pair contributes 0
+            yb = r2b > 0.0f ? yb : 0.0f;
+            y = f2pack(ya, yb);
+            vsum2 = f2fma(y, f2pack(qb.z, qb.w), vsum2);
+            float2 const a2 = sa[pr];
+            uint64_t const rho = f2fma(f2pack(rh[2 * e], rh[2 * e + 1]), k256, f2pack(rx[2 * e], rx[2 * e + 1]));
+            xv[pr] = f2mul(f2mul(y, f2pack(a2.x, a2.y)), rho);
           }
+        }
+        // row maximum of |X'| over the block's 64 r2 points: this warp's 32 and the other half's
+        float mx = 0.0f;
+#pragma unroll
+        for (int pr = 0; pr < 16; ++pr) {
+          float xa, xb;
+          f2unpack(xv[pr], xa, xb);
+          mx = fmaxf(mx, fmaxf(fabsf(xa), fabsf(xb)));
+        }
+        S.rowmax[b][half][row] = mx;
+        __syncwarp();
+        if (lane == 0) mbarArrive(&S.rmax[b][quarter]);
+        if (!(ok = waitBar(&S.rmax[b][quarter], (g >> 1) & 1, abortFlag, P.status, 35))) break;
+        mx = fmaxf(mx, S.rowmax[b][half ^ 1][row]);
+        // scale bs = 2^(15 - E), E = floor(log2 mx) (clamped below), so |X' bs| < 2^16
+        int const E = max(int((__float_as_uint(mx) >> 23) & 0xFF) - 127, kMinExp);
+        float const bs = __uint_as_float(uint32_t(127 + kXExp - E) << 23);
+        double const binv = __longlong_as_double(int64_t(1023 + E - kXExp) << 52);
+        double const fac = rowA * binv;
+        // the X tile is free once GEMM2 of block g - 1 completed
+        if (g >= 1 && !(ok = waitBar(&S.xfree, (g - 1) & 1, abortFlag, P.status, 34))) break;
+        // slices: t = X' bs = 256 h + l, h = rint(t / 256), l = rint(t - 256 h)
+        uint64_t const bb = f2pack(bs, bs);
+        uint8_t * xhi = S.x[0];
+        uint8_t * xlo = S.x[1];
+#pragma unroll
+        for (int ch = 0; ch < 4; ++ch) {
+          uint32_t hi[4], lo[4];
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            uint64_t const t = f2mul(xv[ch * 4 + e], bb);
+            uint64_t const h = f2sub(f2fma(t, kInv256, kMagic), kMagic);
+            uint64_t const l = f2sub(f2add(f2fma(h, kM256, t), kMagic), kMagic);
+            hi[e] = bf16PairExact(h);
+            lo[e] = bf16PairExact(l);
+          }
+          uint32_t const off = sw128(row, half * 4 + ch);
+          *reinterpret_cast<uint4 *>(xhi + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+          *reinterpret_cast<uint4 *>(xlo + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
         }
         float vs0, vs1;
         f2unpack(vsum2, vs0, vs1);
-        float const vsum = vs0 + vs1;
-        vh += double(vsum);
+        vh += double(vs0 + vs1);
         fenceProxyAsync();
         __syncwarp();
-        if (lane == 0) { mbarArrive(&S.xfull[b]); mbarArrive(&S.empty[s]); }
-        if (pendingFlush >= 0) {
-          if (!(ok = flushWindow<NB>(S, tmem + laneBase + TCOL0 + uint32_t(pendingFlush & 1) * NB + half * (NB / 2), uint32_t(pendingFlush),
-                                     acc, lane, abortFlag, P.status)))
-            break;
-          pendingFlush = -1;
-        }
-        int const inWin = jj % P.window;
-        if (inWin == P.window - 1 || jj == nblk - 1) { pendingFlush = int(windowCount); ++windowCount; }
+        if (lane == 0) { mbarArrive(&S.xfull); mbarArrive(&S.empty[s]); }
+        if (pending && !(ok = flushBlock<NB>(S, tAddr, g - 1, cw, pendingFac, acc, lane, abortFlag, P.status))) break;
+        pending = true;
+        pendingFac = fac;
       }
-      if (ok && pendingFlush >= 0)
-        ok = flushWindow<NB>(S, tmem + laneBase + TCOL0 + uint32_t(pendingFlush & 1) * NB + half * (NB / 2), uint32_t(pendingFlush), acc, lane,
-                             abortFlag, P.status);
+      if (ok && pending) ok = flushBlock<NB>(S, tAddr, blockCount + nblk - 1, cw, pendingFac, acc, lane, abortFlag, P.status);
       blockCount += nblk;
       if (!ok) break;
       if (r1 < P.n1) {
@@ -536,7 +617,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           if (col < P.nb) T[col] = acc[c];
         }
       }
-      // the two column-half warps of a row each summed half of the r2 points of every block
+      // the two r2-half warps of a row each summed half of the r2 points of every block
       if (r1 < P.n1) atomicAdd(&P.VH[int64_t(split) * P.vhStride + r1], vh);
     }
     fenceBeforeSync();
@@ -545,22 +626,76 @@ __global__ void __launch_bounds__(NTHREADS, 1)
 }
 
 // ---- operand packing ---------------------------------------------------------------------------------
-// psi [n][ldpsi] FP64 (R columns) -> hi/lo BF16 [npad][RP], zero padded
-__global__ void kPackPsi(int64_t n, int64_t npad, int R, int RP, const double * psi, int ldpsi, __nv_bfloat16 * hi, __nv_bfloat16 * lo)
+// floor(log2 m) clamped below at kMinExp (m = 0 included)
+__device__ __forceinline__ int sliceExponent(double m)
 {
-  for (int64_t idx = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; idx < npad * RP; idx += int64_t(gridDim.x) * blockDim.x) {
-    int64_t const r = idx / RP;
-    int const b = int(idx % RP);
-    float const v = (r < n && b < R) ? float(psi[r * ldpsi + b]) : 0.0f;
-    double const vd = (r < n && b < R) ? psi[r * ldpsi + b] : 0.0;
-    __nv_bfloat16 const h = __float2bfloat16_rn(v);
-    hi[idx] = h;
-    lo[idx] = __float2bfloat16_rn(float(vd - double(__bfloat162float(h))));
+  if (!(m > 0.0)) return kMinExp;
+  int e = 0;
+  frexp(m, &e);   // m = f 2^e, f in [0.5, 1)
+  return max(e - 1, kMinExp);
+}
+
+// t (|t| < 2^24) -> BF16 slices h = rint(t / 65536), m = rint((t - 65536 h) / 256),
+// l = rint(t - 65536 h - 256 m), stored as h, m and l / 256; h, m, l are integers of at most 8
+// significant bits, so each slice is exact
+__device__ __forceinline__ void sliceFactor(double t, __nv_bfloat16 & h, __nv_bfloat16 & m, __nv_bfloat16 & l)
+{
+  double const hd = rint(t * (1.0 / 65536.0));
+  double const r = t - 65536.0 * hd;
+  double const md = rint(r * (1.0 / 256.0));
+  double const ld = rint(r - 256.0 * md);
+  h = __float2bfloat16_rn(float(hd));
+  m = __float2bfloat16_rn(float(md));
+  l = __float2bfloat16_rn(float(ld * (1.0 / 256.0)));
+}
+
+// psi [n][ldpsi] FP64 (R columns) -> fixed-point slices h / m / l BF16 [npad][RP] each (zero padded),
+// and m / 256 when sms is not null, with the inverse row scale ainv [npad]; one warp per row
+__global__ void kPackPsi(int64_t n, int64_t npad, int R, int RP, const double * psi, int ldpsi, __nv_bfloat16 * sh, __nv_bfloat16 * sm,
+                         __nv_bfloat16 * sl, __nv_bfloat16 * sms, float * ainv)
+{
+  int const lane = threadIdx.x & 31;
+  for (int64_t r = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; r < npad; r += (int64_t(gridDim.x) * blockDim.x) >> 5) {
+    double v[2];
+    double m = 0.0;
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      int const b = lane + 32 * u;
+      v[u] = (r < n && b < R) ? psi[r * ldpsi + b] : 0.0;
+      m = fmax(m, fabs(v[u]));
+    }
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    int const E = sliceExponent(m);
+    double const scale = ldexp(1.0, kFactorExp - E);
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      int const b = lane + 32 * u;
+      if (b < RP) {
+        sliceFactor(v[u] * scale, sh[r * RP + b], sm[r * RP + b], sl[r * RP + b]);
+        if (sms) sms[r * RP + b] = __float2bfloat16_rn(__bfloat162float(sm[r * RP + b]) * (1.0f / 256.0f));
+      }
+    }
+    if (lane == 0) ainv[r] = ldexpf(1.0f, E - kFactorExp);
   }
 }
 
-// V [n][ldv] FP64 (nb columns) -> transposed hi/lo BF16 [NB][npad] (tiled transpose)
-__global__ void kPackVt(int64_t n, int64_t npad, int nb, int NB, const double * V, int ldv, __nv_bfloat16 * hi, __nv_bfloat16 * lo)
+// inverse Vt column scales per r2 block: cinv[blk][c] from max_{r2 in blk} |V[r2][c]|
+__global__ void kVtScales(int64_t n, int nBlocks, int nb, int NB, const double * V, int ldv, float * cinv)
+{
+  for (int64_t idx = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; idx < int64_t(nBlocks) * NB; idx += int64_t(gridDim.x) * blockDim.x) {
+    int const c = int(idx % NB);
+    int64_t const blk = idx / NB;
+    double m = 0.0;
+    if (c < nb)
+      for (int64_t r = blk * BK; r < min(n, (blk + 1) * BK); ++r) m = fmax(m, fabs(V[r * ldv + c]));
+    cinv[idx] = ldexpf(1.0f, sliceExponent(m) - kFactorExp);
+  }
+}
+
+// V [n][ldv] FP64 (nb columns) -> transposed fixed-point slices h / m / l BF16 [NB][npad] each (tiled
+// transpose)
+__global__ void kPackVt(int64_t n, int64_t npad, int nb, int NB, const double * V, int ldv, const float * cinv, __nv_bfloat16 * sh,
+                        __nv_bfloat16 * sm, __nv_bfloat16 * sl)
 {
   __shared__ double tile[32][33];
   int64_t const r0 = int64_t(blockIdx.x) * 32;
@@ -575,24 +710,24 @@ __global__ void kPackVt(int64_t n, int64_t npad, int nb, int NB, const double * 
     int const c = c0 + k;
     int64_t const r = r0 + threadIdx.x;
     if (c < NB && r < npad) {
-      double const v = tile[threadIdx.x][k];
-      __nv_bfloat16 const h = __float2bfloat16_rn(float(v));
-      hi[int64_t(c) * npad + r] = h;
-      lo[int64_t(c) * npad + r] = __float2bfloat16_rn(float(v - double(__bfloat162float(h))));
+      double const scale = 1.0 / double(cinv[(r / BK) * NB + c]);   // a power of two
+      int64_t const o = int64_t(c) * npad + r;
+      sliceFactor(tile[threadIdx.x][k] * scale, sh[o], sm[o], sl[o]);
     }
   }
 }
 
-// pts [3][n] (+ coul [n]) -> float4 [npad] (x, y, z, coul); padding points sit far away with 0 weight
-__global__ void kPackCoords(int64_t n, int64_t npad, const double * pts, const double * coul, float4 * out)
+// pts [3][n] -> float4 [npad] (x, y, z, 0); padding points sit far away
+__global__ void kPackCoords(int64_t n, int64_t npad, const double * pts, float4 * out)
 {
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < npad; i += int64_t(gridDim.x) * blockDim.x) {
-    if (i < n) out[i] = make_float4(float(pts[i]), float(pts[n + i]), float(pts[2 * n + i]), coul ? float(coul[i]) : 0.0f);
+    if (i < n) out[i] = make_float4(float(pts[i]), float(pts[n + i]), float(pts[2 * n + i]), 0.0f);
     else out[i] = make_float4(1.0e4f, 1.0e4f, 1.0e4f, 0.0f);
   }
 }
 
-// same in pairs: point pair p -> {x_2p, x_2p+1, y_2p, y_2p+1}, {z_2p, z_2p+1, c_2p, c_2p+1} (npad even)
+// r2 points in pairs: pair p -> {x_2p, x_2p+1, y_2p, y_2p+1}, {z_2p, z_2p+1, c_2p, c_2p+1} with the
+// Coulomb source c (npad even); padding points sit far away with c = 0
 __global__ void kPackCoordPairs(int64_t n, int64_t npad, const double * pts, const double * coul, float4 * out)
 {
   for (int64_t p = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; p < npad / 2; p += int64_t(gridDim.x) * blockDim.x) {
@@ -650,15 +785,39 @@ template <int NB, int RP>
 int launchFlash(tcscf_ctx * ctx, CUtensorMap const * maps, tc::Params const & P, int grid)
 {
   size_t const smem = sizeof(tc::Smem<NB, RP>) + 1024;
+  static_assert(sizeof(tc::Smem<NB, RP>) + 1024 <= 232448, "shared memory per CTA");
   TCSCF_CUDA(ctx, cudaFuncSetAttribute(tc::kFlashTc<NB, RP>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-  tc::kFlashTc<NB, RP><<<grid, tc::NTHREADS, smem, ctx->stream>>>(maps[0], maps[1], maps[2], maps[3], maps[4], maps[5], P);
+  tc::kFlashTc<NB, RP><<<grid, tc::NTHREADS, smem, ctx->stream>>>(maps[0], maps[1], maps[2], maps[3], maps[4], maps[5], maps[6], maps[7],
+                                                                  maps[8], maps[9], P);
+  TCSCF_LAUNCH(ctx);
+  return TCSCF_OK;
+}
+
+// bytes of the packed Vt operand: h, m and l slices [NB][n2pad], then the column scales [nBlocks][NB]
+size_t packedVtBytes(int NB, int64_t n2pad)
+{
+  return size_t(3) * NB * n2pad * sizeof(__nv_bfloat16) + size_t(n2pad / tc::BK) * NB * sizeof(float);
+}
+
+int packVt(tcscf_ctx * ctx, int64_t n2, int64_t n2pad, int nb, int NB, const double * V, int ldv, void * out)
+{
+  auto * sh = static_cast<__nv_bfloat16 *>(out);
+  auto * sm = sh + size_t(NB) * n2pad;
+  auto * sl = sm + size_t(NB) * n2pad;
+  auto * cinv = reinterpret_cast<float *>(sl + size_t(NB) * n2pad);
+  int const nBlocks = int(n2pad / tc::BK);
+  tc::kVtScales<<<gridBlocks(int64_t(nBlocks) * NB, 256), 256, 0, ctx->stream>>>(n2, nBlocks, nb, NB, V, ldv, cinv);
+  TCSCF_LAUNCH(ctx);
+  dim3 const tb{32, 8, 1};
+  dim3 const tg{unsigned((n2pad + 31) / 32), unsigned((NB + 31) / 32), 1};
+  tc::kPackVt<<<tg, tb, 0, ctx->stream>>>(n2, n2pad, nb, NB, V, ldv, cinv, sh, sm, sl);
   TCSCF_LAUNCH(ctx);
   return TCSCF_OK;
 }
 
 }  // namespace
 
-int tensorPackedV(tcscf_ctx * ctx, Grid & g2, const double * V, double scale, const void ** hi, const void ** lo)
+int tensorPackedV(tcscf_ctx * ctx, Grid & g2, const double * V, double scale, const void ** packed)
 {
   int const NB = g2.nb <= 64 ? 64 : 128;
   int64_t const n2pad = (g2.n + tc::BK - 1) / tc::BK * tc::BK;
@@ -666,19 +825,13 @@ int tensorPackedV(tcscf_ctx * ctx, Grid & g2, const double * V, double scale, co
     cudaStreamSynchronize(ctx->stream);
     cudaFree(g2.vtCache);
     g2.vtCache = nullptr;
-    TCSCF_CUDA(ctx, cudaMalloc(&g2.vtCache, size_t(2) * NB * n2pad * sizeof(__nv_bfloat16)));
-    auto * vh = static_cast<__nv_bfloat16 *>(g2.vtCache);
-    dim3 const tb{32, 8, 1};
-    dim3 const tg{unsigned((n2pad + 31) / 32), unsigned((NB + 31) / 32), 1};
-    tc::kPackVt<<<tg, tb, 0, ctx->stream>>>(g2.n, n2pad, g2.nb, NB, V, g2.nb, vh, vh + size_t(NB) * n2pad);
-    TCSCF_LAUNCH(ctx);
+    TCSCF_CUDA(ctx, cudaMalloc(&g2.vtCache, packedVtBytes(NB, n2pad)));
+    TCSCF_TRY(packVt(ctx, g2.n, n2pad, g2.nb, NB, V, g2.nb, g2.vtCache));
     g2.vtNB = NB;
     g2.vtN2pad = n2pad;
     g2.vtScale = scale;
   }
-  auto * vh = static_cast<__nv_bfloat16 *>(g2.vtCache);
-  *hi = vh;
-  *lo = vh + size_t(NB) * n2pad;
+  *packed = g2.vtCache;
   return TCSCF_OK;
 }
 
@@ -688,6 +841,7 @@ bool tensorPathAvailable(Contraction const & c, int precision, std::string * why
   if (c.kernel != TCSCF_K_INV_R12) { if (why) *why = "tensor path implements the 1/r12 kernel"; return false; }
   if (c.R < 1 || c.R > 64) { if (why) *why = "density factor rank must be 1..64 for the tensor path"; return false; }
   if (c.ncol > 128) { if (why) *why = "tensor path supports nb <= 128"; return false; }
+  if (c.ncol > 64 && c.R > 32) { if (why) *why = "tensor path supports a density factor rank <= 32 for nb > 64"; return false; }
   if (!encodeTiled()) { if (why) *why = "cuTensorMapEncodeTiled unavailable"; return false; }
   return true;
 }
@@ -711,51 +865,49 @@ int contractTensor(tcscf_ctx * ctx, Contraction const & c, int precision)
   nSplit = (nBlocks + perSplit - 1) / perSplit;
 
   size_t const bf = sizeof(__nv_bfloat16);
-  size_t bytes = 2 * size_t(n1pad) * RP * bf + 2 * size_t(n2pad) * RP * bf + 2 * size_t(NB) * n2pad * bf
-                 + size_t(n1pad) * sizeof(float4) + size_t(n2pad) * sizeof(float4) + 64;
+  bool const haveVt = c.vtPacked != nullptr;
+  size_t const bytes = 4 * size_t(n1pad) * RP * bf + 3 * size_t(n2pad) * RP * bf + (haveVt ? 0 : packedVtBytes(NB, n2pad))
+                       + size_t(n1pad) * sizeof(float4) + size_t(n2pad) * sizeof(float4) + size_t(n1pad + n2pad) * sizeof(float) + 64
+                       + 16 * 256;
   void * p = nullptr;
   TCSCF_TRY(scratch(ctx, "flash_tc_ops", bytes, &p));
   char * q = static_cast<char *>(p);
   auto take = [&](size_t n) { char * r = q; q += (n + 255) & ~size_t(255); return r; };
-  auto * psi1hi = reinterpret_cast<__nv_bfloat16 *>(take(size_t(n1pad) * RP * bf));
-  auto * psi1lo = reinterpret_cast<__nv_bfloat16 *>(take(size_t(n1pad) * RP * bf));
-  auto * psi2hi = reinterpret_cast<__nv_bfloat16 *>(take(size_t(n2pad) * RP * bf));
-  auto * psi2lo = reinterpret_cast<__nv_bfloat16 *>(take(size_t(n2pad) * RP * bf));
-  auto * vthi = reinterpret_cast<__nv_bfloat16 *>(take(size_t(NB) * n2pad * bf));
-  auto * vtlo = reinterpret_cast<__nv_bfloat16 *>(take(size_t(NB) * n2pad * bf));
+  __nv_bfloat16 * psi1s[4];
+  __nv_bfloat16 * psi2s[3];
+  for (auto & a : psi1s) a = reinterpret_cast<__nv_bfloat16 *>(take(size_t(n1pad) * RP * bf));
+  for (auto & a : psi2s) a = reinterpret_cast<__nv_bfloat16 *>(take(size_t(n2pad) * RP * bf));
+  void * vt = haveVt ? const_cast<void *>(c.vtPacked) : take(packedVtBytes(NB, n2pad));
   auto * r1c = reinterpret_cast<float4 *>(take(size_t(n1pad) * sizeof(float4)));
   auto * r2c = reinterpret_cast<float4 *>(take(size_t(n2pad) * sizeof(float4)));
+  auto * a1inv = reinterpret_cast<float *>(take(size_t(n1pad) * sizeof(float)));
+  auto * a2inv = reinterpret_cast<float *>(take(size_t(n2pad) * sizeof(float)));
   int * status = reinterpret_cast<int *>(take(64));
-  bool const haveVt = c.vtHi && c.vtLo;
-  TCSCF_CHECK(ctx, size_t(q - static_cast<char *>(p)) <= bytes + 16 * 256, TCSCF_ERR_INVALID_ARGUMENT, "internal: scratch layout");
+  TCSCF_CHECK(ctx, size_t(q - static_cast<char *>(p)) <= bytes, TCSCF_ERR_INVALID_ARGUMENT, "internal: scratch layout");
+  auto * vts = static_cast<__nv_bfloat16 *>(vt);   // h, m, l slices [NB][n2pad] each
+  auto * cinv = reinterpret_cast<float *>(vts + 3 * size_t(NB) * n2pad);
 
-  // operand preparation (BF16 hi/lo split, transposes, FP32 coordinates)
-  tc::kPackPsi<<<gridBlocks(n1pad * RP, 256), 256, 0, ctx->stream>>>(c.n1, n1pad, c.R, RP, c.psi1, c.ldpsi, psi1hi, psi1lo);
+  // operand preparation (fixed-point BF16 slices with their scales, transposes, FP32 coordinates)
+  tc::kPackPsi<<<gridBlocks(n1pad * 32, 256), 256, 0, ctx->stream>>>(c.n1, n1pad, c.R, RP, c.psi1, c.ldpsi, psi1s[0], psi1s[1], psi1s[2],
+                                                                      psi1s[3], a1inv);
   TCSCF_LAUNCH(ctx);
-  tc::kPackPsi<<<gridBlocks(n2pad * RP, 256), 256, 0, ctx->stream>>>(c.n2, n2pad, c.R, RP, c.psi2, c.ldpsi, psi2hi, psi2lo);
+  tc::kPackPsi<<<gridBlocks(n2pad * 32, 256), 256, 0, ctx->stream>>>(c.n2, n2pad, c.R, RP, c.psi2, c.ldpsi, psi2s[0], psi2s[1], psi2s[2],
+                                                                      nullptr, a2inv);
   TCSCF_LAUNCH(ctx);
-  dim3 const tb{32, 8, 1};
-  dim3 const tg{unsigned((n2pad + 31) / 32), unsigned((NB + 31) / 32), 1};
-  if (haveVt) {
-    vthi = static_cast<__nv_bfloat16 *>(const_cast<void *>(c.vtHi));
-    vtlo = static_cast<__nv_bfloat16 *>(const_cast<void *>(c.vtLo));
-  } else {
-    tc::kPackVt<<<tg, tb, 0, ctx->stream>>>(c.n2, n2pad, c.ncol, NB, c.V, c.ldv, vthi, vtlo);
-    TCSCF_LAUNCH(ctx);
-  }
-  tc::kPackCoords<<<gridBlocks(n1pad, 256), 256, 0, ctx->stream>>>(c.n1, n1pad, c.p1, nullptr, r1c);
+  if (!haveVt) TCSCF_TRY(packVt(ctx, c.n2, n2pad, c.ncol, NB, c.V, c.ldv, vt));
+  tc::kPackCoords<<<gridBlocks(n1pad, 256), 256, 0, ctx->stream>>>(c.n1, n1pad, c.p1, r1c);
   TCSCF_LAUNCH(ctx);
   tc::kPackCoordPairs<<<gridBlocks(n2pad / 2, 256), 256, 0, ctx->stream>>>(c.n2, n2pad, c.p2, c.coul, r2c);
   TCSCF_LAUNCH(ctx);
 
-  CUtensorMap maps[6];
+  CUtensorMap maps[10];
   CUtensorMapSwizzle const psw = RP == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B;
-  bool okm = makeMap(&maps[0], psi1hi, RP, n1pad, RP, tc::BM, psw)
-             && makeMap(&maps[1], psi1lo, RP, n1pad, RP, tc::BM, psw)
-             && makeMap(&maps[2], psi2hi, RP, n2pad, RP, tc::BK, psw)
-             && makeMap(&maps[3], psi2lo, RP, n2pad, RP, tc::BK, psw)
-             && makeMap(&maps[4], vthi, n2pad, NB, tc::BK, NB, CU_TENSOR_MAP_SWIZZLE_128B)
-             && makeMap(&maps[5], vtlo, n2pad, NB, tc::BK, NB, CU_TENSOR_MAP_SWIZZLE_128B);
+  bool okm = true;
+  for (int i = 0; i < 4; ++i) okm = okm && makeMap(&maps[i], psi1s[i], RP, n1pad, RP, tc::BM, psw);
+  for (int i = 0; i < 3; ++i) {
+    okm = okm && makeMap(&maps[4 + i], psi2s[i], RP, n2pad, RP, tc::BK, psw);
+    okm = okm && makeMap(&maps[7 + i], vts + size_t(i) * NB * n2pad, n2pad, NB, tc::BK, NB, CU_TENSOR_MAP_SWIZZLE_128B);
+  }
   TCSCF_CHECK(ctx, okm, TCSCF_ERR_CUDA, "cuTensorMapEncodeTiled failed");
 
   double * Tout = c.T;
@@ -772,14 +924,14 @@ int contractTensor(tcscf_ctx * ctx, Contraction const & c, int precision)
 
   tc::Params P{};
   P.nTiles = nTiles; P.nSplit = nSplit; P.blocksPerSplit = perSplit; P.nBlocks = nBlocks;
-  P.n1 = int(c.n1); P.nb = c.ncol; P.window = ctx->flushWindow;
-  P.r1xyz = r1c; P.r2xyzc = r2c; P.T = Tout; P.VH = VHout; P.ldt = c.ldt;
+  P.n1 = int(c.n1); P.nb = c.ncol;
+  P.r1xyz = r1c; P.r2pairs = r2c; P.a1inv = a1inv; P.a2inv = a2inv; P.cinv = cinv;
+  P.T = Tout; P.VH = VHout; P.ldt = c.ldt;
   P.tStride = int64_t(c.n1) * c.ldt; P.vhStride = c.n1; P.status = status;
   int const grid = std::min(nTiles * nSplit, sms);
   if (NB == 64 && RP == 32) TCSCF_TRY((launchFlash<64, 32>(ctx, maps, P, grid)));
   else if (NB == 64) TCSCF_TRY((launchFlash<64, 64>(ctx, maps, P, grid)));
-  else if (RP == 32) TCSCF_TRY((launchFlash<128, 32>(ctx, maps, P, grid)));
-  else TCSCF_TRY((launchFlash<128, 64>(ctx, maps, P, grid)));
+  else TCSCF_TRY((launchFlash<128, 32>(ctx, maps, P, grid)));
 
   int st = 0;
   TCSCF_CUDA(ctx, cudaMemcpyAsync(&st, status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));

@@ -23,8 +23,7 @@ struct Contraction {
   double * T = nullptr;            // [n1][ldt]
   int ldt = 0;
   double * VH = nullptr;           // [n1] (required when coul != null)
-  const void * vtHi = nullptr;     // optional pre-packed BF16 Vt hi/lo [NB][n2pad] (tensor path)
-  const void * vtLo = nullptr;
+  const void * vtPacked = nullptr; // optional pre-packed Vt of the tensor path (slices and column scales)
   int kernel = TCSCF_K_INV_R12;    // r12 kernel g (vector kernels use `component`)
   int component = 0;
   const tcscf_ochi * jastrow = nullptr;
@@ -35,8 +34,9 @@ int contractFp64(tcscf_ctx * ctx, Contraction const & c);
 // tensor-core (tcgen05) contraction of the same quantity for g = 1/r12 (flash_tc.cu)
 int contractTensor(tcscf_ctx * ctx, Contraction const & c, int precision);
 bool tensorPathAvailable(Contraction const & c, int precision, std::string * why);
-// packs (once per grid) the BF16 hi/lo transposed operand Vt of the tensor path from V [n2][nb]
-int tensorPackedV(tcscf_ctx * ctx, Grid & g2, const double * V, double scale, const void ** hi, const void ** lo);
+// packs (once per grid) the transposed operand Vt of the tensor path from V [n2][nb]: BF16 slices
+// hi/lo [NB][n2pad] followed by the per-block column scales
+int tensorPackedV(tcscf_ctx * ctx, Grid & g2, const double * V, double scale, const void ** packed);
 
 // out[r][c] = sum_s part[s*stride + r*ldPart + c] for r < rows, c < cols (deterministic split sum)
 int sumSplitsLaunch(tcscf_ctx * ctx, int64_t n, int nsplit, int64_t stride, const double * part, double * out, int64_t rows, int cols,

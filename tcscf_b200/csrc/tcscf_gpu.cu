@@ -693,9 +693,8 @@ int fockBuildDevice(tcscf_ctx * ctx, Grid & g1, Grid & g2, int nspin, const doub
   TCSCF_CUDA(ctx, cudaMemsetAsync(GRre, 0, sizeof(double) * size_t(nspin) * nb * nb * 2, ctx->stream));
   bool anyComplex = false;
   double contractionMs = 0;
-  const void * vtHi = nullptr;
-  const void * vtLo = nullptr;
-  if (precision != TCSCF_PREC_FP64) TCSCF_TRY(tensorPackedV(ctx, g2, V, scale, &vtHi, &vtLo));
+  const void * vtPacked = nullptr;
+  if (precision != TCSCF_PREC_FP64) TCSCF_TRY(tensorPackedV(ctx, g2, V, scale, &vtPacked));
   for (int s = 0; s < nspin; ++s) {
     Factor f;
     TCSCF_TRY(factorDensity(ctx, g1, dD + size_t(s) * nb * nb, s, f));
@@ -722,7 +721,7 @@ int fockBuildDevice(tcscf_ctx * ctx, Grid & g1, Grid & g2, int nspin, const doub
       c.n1 = n1; c.n2 = n2; c.R = R; c.ncol = nb;
       c.p1 = g1.pts; c.p2 = g2.pts; c.psi1 = psi1; c.psi2 = psi2; c.ldpsi = ldpsi;
       c.V = V; c.ldv = nb; c.T = part == 0 ? Ts : Ti; c.ldt = ldt;
-      c.vtHi = vtHi; c.vtLo = vtLo;
+      c.vtPacked = vtPacked;
       if (part == 0) {
         kCoulombSource<<<gridBlocks(n2, 256), 256, 0, ctx->stream>>>(n2, R, psi1at2, psi2, ldpsi, g2.w, scale, coul);
         TCSCF_LAUNCH(ctx);
@@ -874,13 +873,6 @@ int tcscf_last_potentials(tcscf_ctx * ctx, double * VH, double * T)
   if (VH) TCSCF_CUDA(ctx, cudaMemcpyAsync(VH, ctx->lastVH, sizeof(double) * ctx->lastN1, cudaMemcpyDeviceToHost, ctx->stream));
   if (T) TCSCF_CUDA(ctx, cudaMemcpyAsync(T, ctx->lastT, sizeof(double) * ctx->lastN1 * ctx->lastNb, cudaMemcpyDeviceToHost, ctx->stream));
   TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  return TCSCF_OK;
-}
-
-int tcscf_set_flush_window(tcscf_ctx * ctx, int blocks)
-{
-  if (!ctx || blocks < 1 || blocks > 4096) return TCSCF_ERR_INVALID_ARGUMENT;
-  ctx->flushWindow = blocks;
   return TCSCF_OK;
 }
 

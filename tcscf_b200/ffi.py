@@ -50,7 +50,6 @@ SIGNATURES: dict[str, tuple] = {
     "tcscf_ctx_stream": (_I, [_P, C.POINTER(_P)]),
     "tcscf_synchronize": (_I, [_P]),
     "tcscf_last_timing": (_I, [_P, _D, _D, C.POINTER(_I)]),
-    "tcscf_set_flush_window": (_I, [_P, _I]),
     "tcscf_last_potentials": (_I, [_P, _D, _D]),
     "tcscf_grid_radial": (_I, [_I, _I, C.c_double, C.c_double, _D, _D]),
     "tcscf_grid_product": (_I, [_I, _D, _D, _I, _D, _D, _D]),

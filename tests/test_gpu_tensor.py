@@ -32,8 +32,7 @@ def he(ctx):
     return w, g, G, h
 
 
-def _compare(G1, G2, D, h, window=4):
-    G1.ctx.set_flush_window(window)
+def _compare(G1, G2, D, h):
     Gd, Fd, Ed = api.fock_build(G1, G2, D, h, precision=ffi.PREC_FP64)
     Gm, Fm, Em = api.fock_build(G1, G2, D, h, precision=ffi.PREC_BF16X3)
     scale = np.abs(Gd).max()
@@ -52,13 +51,12 @@ def test_single_tile_matches_fp64(ctx, he):
     assert dG < G_REL_TOL
 
 
-@pytest.mark.parametrize("window", [1, 4, 16])
-def test_he_full_grid_flush_windows(ctx, he, window):
+def test_he_full_grid(ctx, he):
     w, g, G, h = he
     rng = np.random.default_rng(2)
     D = real_density(w.basis, 1, rng)
-    dE, dG, Em, Ed = _compare(G, G, D, h, window)
-    assert dE < e_tol(Ed), (window, Em, Ed)
+    dE, dG, Em, Ed = _compare(G, G, D, h)
+    assert dE < e_tol(Ed), (Em, Ed)
     assert dG < G_REL_TOL
 
 
