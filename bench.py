@@ -159,6 +159,8 @@ def run_reference(args, rank: int) -> None:
     if rank != 0:
         return
     w = workload(args.workload)
+    if args.nrad:
+        w.nrad = args.nrad
     g = grids.product_grid(w.nrad, w.order)
     D, h = scf_guess_density(w.basis, w.Z, w.n_up)
     vals = []
@@ -179,6 +181,19 @@ def run_reference(args, rank: int) -> None:
 METRIC = "Fock-build s/iter, mixed vs FP64 GPU at |dE|<=1 uEh; % of roofline"
 
 
+def profiled_traffic(name: str):
+    """DRAM bytes per launch of the tensor contraction kernel for this workload, as recorded in the
+    committed ncu summary (profiles/kflashtc_dram_traffic.md: 'traffic_bytes_per_launch <name> <bytes>')."""
+    path = Path(__file__).resolve().parent / "profiles" / "kflashtc_dram_traffic.md"
+    if not path.exists():
+        return None
+    for line in path.read_text().splitlines():
+        parts = line.strip("` ").split()
+        if len(parts) == 3 and parts[0] == "traffic_bytes_per_launch" and parts[1].lower() == name.lower():
+            return float(parts[2])
+    return None
+
+
 def run_ours(args, rank: int, world: int) -> None:
     import torch
 
@@ -189,6 +204,8 @@ def run_ours(args, rank: int, world: int) -> None:
     dev = torch.device("cuda", local)
     prec = {"fp64": ffi.PREC_FP64, "bf16x3": ffi.PREC_BF16X3, "tf32": ffi.PREC_TF32}[args.precision]
     w = workload(args.workload)
+    if args.nrad:
+        w.nrad = args.nrad
     g = grids.product_grid(w.nrad, w.order)
     D, h = scf_guess_density(w.basis, w.Z, w.n_up)
     peaks, peak_kind = load_peaks()
@@ -277,9 +294,13 @@ def run_ours(args, rank: int, world: int) -> None:
                 "traffic": None, "peak_source": "measured FP64 matmul (DESIGN.md)"}
     else:
         peak = peaks["bf16_tflops"]
-        roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
-                "peak_source": f"bf16 dense burst, {peak_kind}",
-                "issued_tensor_tflops": achieved * 3.0, "issued_frac": achieved * 3.0 / peak}
+        # tensor work the kernel issues per (r1, r2) pair: GEMM1 6 slice products of K = RP, GEMM2 4 of N = NB
+        RP = 32 if w.n_up <= 32 else 64   # real closed-shell guess density: factor rank = n_occ
+        NB = 64 if w.nb <= 64 else 128
+        issued = n * n * (2.0 * 6 * RP + 2.0 * 4 * NB) / (c_ms / 1e3) / 1e12
+        roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "traffic": profiled_traffic(w.name), "peak_source": f"bf16 dense burst, {peak_kind}",
+                "issued_tensor_tflops": issued, "issued_frac": issued / peak}
     cpu = None
     if not args.skip_cpu:
         r = cpu_reference(w, g, D, h, budget_s=args.cpu_seconds)
@@ -287,11 +308,13 @@ def run_ours(args, rank: int, world: int) -> None:
                "precompute_s": r["precompute_s"], "iteration_s": r["iteration_s"]}
     line = {"metric": METRIC, "value": s_per_iter, "unit": "s/iter", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": total_ms / args.steps, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-            "dtype": {"fp64": "f64", "bf16x3": "bf16x3 (fp32 accumulate, fp64 flush)", "tf32": "tf32"}[args.precision],
+            "dtype": {"fp64": "f64", "bf16x3": "bf16", "tf32": "tf32"}[args.precision],
             "data": "synthetic",
             "config": {"workload": f"{w.name} RCS Fock build (direct form)", "Z": w.Z, "n_points": n, "n_basis": w.nb,
                        "n_occ": w.n_up, "grid": f"{w.nrad} radial (Gauss-Chebyshev, r=(1+x)/(1-x)) x Lebedev order {w.order}",
-                       "precision": args.precision, "l2": "flushed (256 MB write) between timed steps",
+                       "precision": {"fp64": "fp64", "bf16x3": "bf16 fixed-point slices (24-bit factors, 16-bit kernel tile), "
+                                     "exact fp32 block accumulation, fp64 across blocks", "tf32": "tf32"}[args.precision],
+                       "l2": "flushed (256 MB write) between timed steps",
                        "density": "core-Hamiltonian guess (canonical orthogonalisation)"},
             "energy": E, "contraction_ms": c_ms, "gpu_launches": launches, "roofline": roof, "fp64": fp64,
             "speedup_vs_fp64": (fp64["s_per_iter"] / s_per_iter) if fp64 else None,
@@ -307,6 +330,7 @@ def main() -> None:
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="kr", choices=["kr", "ne", "he"])
     ap.add_argument("--precision", default="bf16x3", choices=["bf16x3", "fp64", "tf32"])
+    ap.add_argument("--nrad", type=int, default=0, help="override the workload's radial points (smaller profiling cases)")
     ap.add_argument("--fp64-steps", type=int, default=2)
     ap.add_argument("--fp64-peak", type=float, default=float(os.environ.get("TCSCF_FP64_PEAK_TFLOPS", "37.0")))
     ap.add_argument("--e2e-steps", type=int, default=2)

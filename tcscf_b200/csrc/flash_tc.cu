@@ -16,9 +16,9 @@
 //                                                     is scaled down by 2^-8 in the result)
 // and the product is 256 A + B in units of the block's scales (GEMM2 keeps h m', l h', h l'/256 of
 // its 16-bit X).  The hi*hi accumulation being exact, the tensor core's FP32 adder rounding cannot
-// bias the result; the products below 2^-24 of the largest term are dropped.  Each block's T is added into per-thread
-// FP64 accumulators with its scales as soon as the block completes.  The kernel matrix g exists
-// only as the BF16 X tile in shared memory.
+// bias the result; the products below 2^-24 of the largest term are dropped.  Each block's T is
+// added into per-thread FP64 accumulators with its scales as soon as the block completes.  The
+// kernel matrix g exists only as the BF16 X tile in shared memory.
 //
 // Warp roles (384 threads, one CTA per SM, persistent over (r1 tile, r2 split) work items):
 //   warp 0      TMA producer: psi1 tile (once per work item), psi2 / Vt blocks (TMA, no multicast),
@@ -929,9 +929,12 @@ int contractTensor(tcscf_ctx * ctx, Contraction const & c, int precision)
   P.T = Tout; P.VH = VHout; P.ldt = c.ldt;
   P.tStride = int64_t(c.n1) * c.ldt; P.vhStride = c.n1; P.status = status;
   int const grid = std::min(nTiles * nSplit, sms);
+  // the contraction kernel alone is bracketed by the context's timing events (tcscf_last_timing)
+  cudaEventRecord(ctx->ev[2], ctx->stream);
   if (NB == 64 && RP == 32) TCSCF_TRY((launchFlash<64, 32>(ctx, maps, P, grid)));
   else if (NB == 64) TCSCF_TRY((launchFlash<64, 64>(ctx, maps, P, grid)));
   else TCSCF_TRY((launchFlash<128, 32>(ctx, maps, P, grid)));
+  cudaEventRecord(ctx->ev[3], ctx->stream);
 
   int st = 0;
   TCSCF_CUDA(ctx, cudaMemcpyAsync(&st, status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));

@@ -728,10 +728,9 @@ int fockBuildDevice(tcscf_ctx * ctx, Grid & g1, Grid & g2, int nspin, const doub
         c.coul = coul;
         c.VH = VH + size_t(s) * n1;
       }
-      cudaEventRecord(ctx->ev[2], ctx->stream);
+      // the contraction routines bracket their main kernel with ev[2] / ev[3]
       if (precision == TCSCF_PREC_FP64) TCSCF_TRY(contractFp64(ctx, c));
       else TCSCF_TRY(contractTensor(ctx, c, precision));
-      cudaEventRecord(ctx->ev[3], ctx->stream);
       TCSCF_CUDA(ctx, cudaEventSynchronize(ctx->ev[3]));
       float ms = 0;
       cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]);
