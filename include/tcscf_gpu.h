@@ -156,6 +156,18 @@ int tcscf_compute_F(tcscf_ctx * ctx, int r1, int r2, int kernel, const tcscf_och
 int tcscf_compute_V(tcscf_ctx * ctx, int r1, int r2, int kernel, const tcscf_ochi * jastrow, double * V, int keep, int * vji);
 int tcscf_tensor_destroy(tcscf_ctx * ctx, int handle);
 
+/* ---- 4- and 6-index tensors (integrateAll.hpp:147-442) --------------------------------------- */
+/* integrateAllR1R2<USE_GRADIENT> (integrateAll.hpp:221-317): r1 a 3-D grid, r2 a 2-D grid with the
+ * same basis; scalar kernel (value form, answer[b1][b2][b3][b4]) or, with use_gradient, a vector
+ * kernel dotted into the r2 basis gradients (answer[b2][b1][b4][b3], integrateAll.hpp:302).
+ * answer: nb^4 complex in host memory. */
+int tcscf_integrate_all_r1r2(tcscf_ctx * ctx, int r1, int r2, int use_gradient, int kernel, const tcscf_ochi * jastrow,
+                             double * answer);
+/* threeElectronIntegrals (integrateAll.hpp:361-442): r1, r2 3-D grids, same-spin grad u;
+ * answer[p][q][r][s][t][u] = sum_r1 w1 conj(phi_p) phi_s V(r1,q,t) . V(r1,r,u), nb^6 complex in host
+ * memory (nb <= 32). */
+int tcscf_three_electron_integrals(tcscf_ctx * ctx, int r1, int r2, const tcscf_ochi * jastrow, double * answer);
+
 /* ---- per-iteration Fock build ---------------------------------------------------------------- */
 /* Direct form: G from the density without any stored Fji.  Same result as calculateIaa /
  * calculateFai / assembly (HartreeFock.cpp:817-843 RCS, :925-956 UOS) on Fji = computeF(r1, r2,

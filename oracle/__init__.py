@@ -180,6 +180,26 @@ def compute_V(p1, p2, w2, vals2, basis_n: int, kernel: int, u: Ochi):
     return V
 
 
+def integrate_all_r1r2(use_gradient: bool, p1, w1, vals1, p2, w2, vals2, grads2, nb: int, kernel: int, u: Ochi | None):
+    """integrateAllR1R2 (r1 3-D complex values, r2 2-D real values / complex gradients): [nb]^4 complex."""
+    out = np.empty((nb,) * 4, dtype=np.complex128)
+    lib().oracle_integrate_all_r1r2(int(use_gradient), _p(np.ascontiguousarray(p1)), _p(np.ascontiguousarray(w1)),
+                                    C.c_int64(p1.shape[1]), _p(np.ascontiguousarray(vals1)), _p(np.ascontiguousarray(p2)),
+                                    _p(np.ascontiguousarray(w2)), C.c_int64(p2.shape[1]), _p(np.ascontiguousarray(vals2)),
+                                    _p(None if grads2 is None else np.ascontiguousarray(grads2)), nb, kernel,
+                                    C.byref(u) if u else None, _p(out))
+    return out
+
+
+def three_electron_integrals(p1, w1, vals1, p2, w2, vals2, nb: int, u: Ochi):
+    """threeElectronIntegrals (same-spin grad u): [nb]^6 complex."""
+    out = np.empty((nb,) * 6, dtype=np.complex128)
+    lib().oracle_three_electron_integrals(_p(np.ascontiguousarray(p1)), _p(np.ascontiguousarray(w1)), C.c_int64(p1.shape[1]),
+                                          _p(np.ascontiguousarray(vals1)), _p(np.ascontiguousarray(p2)), _p(np.ascontiguousarray(w2)),
+                                          C.c_int64(p2.shape[1]), _p(np.ascontiguousarray(vals2)), nb, C.byref(u), _p(out))
+    return out
+
+
 def fock_build(F, vals1, w1, D, h, respect_symmetry: bool = True):
     D = np.ascontiguousarray(D, dtype=np.complex128)
     if D.ndim == 2:

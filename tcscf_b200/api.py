@@ -187,6 +187,28 @@ def computeV(r1Grid: QMCGrid, r2Grid: QMCGrid, kernel: int, jastrow: ffi.Ochi, k
     return (V, DeviceTensor(ctx, h.value)) if keep else V
 
 
+def integrateAllR1R2(r1Grid: QMCGrid, r2Grid: QMCGrid, kernel: int, jastrow: ffi.Ochi | None = None,
+                     use_gradient: bool = False) -> np.ndarray:
+    """integrateAllR1R2<USE_GRADIENT> (integrateAll.hpp:221-317): r1 a 3-D grid, r2 a 2-D grid.
+    Value form: answer[b1][b2][b3][b4]; gradient form (vector kernel . r2 basis gradients):
+    answer[b2][b1][b4][b3].  Complex [nb]^4."""
+    ctx = r1Grid.ctx
+    nb = r1Grid.nBasis()
+    out = np.empty((nb,) * 4, dtype=np.complex128)
+    _raise(ffi.lib().tcscf_integrate_all_r1r2(ctx.handle, r1Grid.id, r2Grid.id, int(use_gradient), kernel,
+                                              C.byref(jastrow) if jastrow is not None else None, ffi.dptr(out)), ctx.handle)
+    return out
+
+
+def threeElectronIntegrals(r1Grid: QMCGrid, r2Grid: QMCGrid, jastrow: ffi.Ochi) -> np.ndarray:
+    """threeElectronIntegrals (integrateAll.hpp:361-442): complex [nb]^6, answer[p][q][r][s][t][u]."""
+    ctx = r1Grid.ctx
+    nb = r1Grid.nBasis()
+    out = np.empty((nb,) * 6, dtype=np.complex128)
+    _raise(ffi.lib().tcscf_three_electron_integrals(ctx.handle, r1Grid.id, r2Grid.id, C.byref(jastrow), ffi.dptr(out)), ctx.handle)
+    return out
+
+
 def _check_shapes(D: np.ndarray, h: np.ndarray, nb: int) -> None:
     """CHECK_BOUNDS_3(density, nSpin, nBasis, nBasis) / CHECK_BOUNDS_2(oneElectronTerms, nBasis, nBasis)."""
     if D.ndim != 3 or D.shape[0] not in (1, 2) or D.shape[1:] != (nb, nb) or h.shape != (nb, nb):

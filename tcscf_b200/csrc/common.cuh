@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <cublas_v2.h>
 #include <cusolverDn.h>
 #include <cstdint>
 #include <map>
@@ -66,6 +67,7 @@ struct tcscf_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
   cusolverDnHandle_t solver = nullptr;
+  cublasHandle_t blas = nullptr;   // created on first use (4- and 6-index tensors)
   std::string err;
   std::map<int, tcscf::Grid> grids;
   std::map<int, tcscf::Tensor> tensors;

@@ -835,6 +835,7 @@ int tcscf_ctx_destroy(tcscf_ctx * ctx)
   for (auto & kv : ctx->scratch) cudaFree(kv.second.p);
   for (auto & e : ctx->ev) cudaEventDestroy(e);
   if (ctx->solver) cusolverDnDestroy(ctx->solver);
+  if (ctx->blas) cublasDestroy(ctx->blas);
   cudaStreamDestroy(ctx->stream);
   delete ctx;
   return TCSCF_OK;

@@ -62,6 +62,8 @@ SIGNATURES: dict[str, tuple] = {
     "tcscf_grid_basis_values": (_I, [_P, _I, _D, _D]),
     "tcscf_overlap_core_quadrature": (_I, [_P, _I, _I, _D, _D]),
     "tcscf_overlap_core_quadrature_static": (_I, [_P, _I, _I, _D, _D]),
+    "tcscf_integrate_all_r1r2": (_I, [_P, _I, _I, _I, _I, C.POINTER(Ochi), _D]),
+    "tcscf_three_electron_integrals": (_I, [_P, _I, _I, C.POINTER(Ochi), _D]),
     "tcscf_compute_F": (_I, [_P, _I, _I, _I, C.POINTER(Ochi), _D, _I, C.POINTER(_I)]),
     "tcscf_compute_V": (_I, [_P, _I, _I, _I, C.POINTER(Ochi), _D, _I, C.POINTER(_I)]),
     "tcscf_tensor_destroy": (_I, [_P, _I]),
