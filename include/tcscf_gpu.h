@@ -193,6 +193,26 @@ int tcscf_scf(tcscf_ctx * ctx, int r1, int r2, int nspin, int n_up, int n_down, 
               int respect_symmetry, int precision, double tol, int max_iter, double * energy, int * iterations,
               double * density, double * eigenvalues);
 
+/* ---- transcorrelated Fock build and SCF (TCHartreeFock, HartreeFock.cpp:102-609, :1007-1362) ---- */
+/* One TC Fock build from device-resident tensors: Fji same / opposite spin (computeF with
+ * TCSCF_K_TC_SCALAR_SAME / _OPPO) and Vji same / opposite (computeV with TCSCF_K_GRAD_U_SAME / _OPPO),
+ * all on the r1 grid, whose basis gradients must be stored.  density [2][nb][nb] complex; occupied
+ * orbitals occ_up / occ_down complex, column-major nb x n_up / nb x n_down (occupiedOrbitals,
+ * PERM_JI); h real [nb][nb].  Outputs (any may be NULL): G2, G3, Fock [2][nb][nb] complex (after the
+ * symmetry mask), energy = sum D(i,j) (h + G2/2 - G3/3)(j,i). */
+int tcscf_tc_fock_build(tcscf_ctx * ctx, int r1, int fji_same, int fji_oppo, int vji_same, int vji_oppo, int n_up, int n_down,
+                        const double * density, const double * occ_up, const double * occ_down, const double * h,
+                        int respect_symmetry, double * G2, double * G3, double * fock, double * energy);
+/* TCHartreeFock::compute: zero initial density, TC Fock build, the non-Hermitian pencil F C = S C e
+ * solved on the device (Cholesky of S, cusolverDnXgeev), eigenvalues sorted by real part, occupied
+ * vectors orthogonalised by the S-metric modified Gram-Schmidt of orthogonalization.hpp:136-154,
+ * until |dE| < tol.  S real [nb][nb].  Outputs: energy, iterations, density [2][nb][nb], and the
+ * occupied pseudo-energies [2][nb] (first n_up / n_down entries; may be NULL).
+ * Returns TCSCF_ERR_NOT_CONVERGED after max_iter. */
+int tcscf_tc_scf(tcscf_ctx * ctx, int r1, int fji_same, int fji_oppo, int vji_same, int vji_oppo, const double * S, const double * h,
+                 int n_up, int n_down, int respect_symmetry, double tol, int max_iter, double * energy, int * iterations,
+                 double * density, double * pseudo_energies);
+
 #ifdef __cplusplus
 }
 #endif

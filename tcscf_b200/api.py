@@ -209,6 +209,53 @@ def threeElectronIntegrals(r1Grid: QMCGrid, r2Grid: QMCGrid, jastrow: ffi.Ochi) 
     return out
 
 
+def tc_fock_build(r1Grid: QMCGrid, Fs: DeviceTensor, Fo: DeviceTensor, Vs: DeviceTensor, Vo: DeviceTensor, n_up: int, n_down: int,
+                  density: np.ndarray, occ_up: np.ndarray, occ_down: np.ndarray, h: np.ndarray, respect_symmetry: bool = True):
+    """One transcorrelated Fock build (HartreeFock.cpp:1150-1224) from device tensors.
+    occ_up / occ_down: occupied orbitals as [n_occ][nb] rows (column-major nb x n_occ).
+    Returns (G2, G3, Fock, energy)."""
+    ctx = r1Grid.ctx
+    nb = r1Grid.nBasis()
+    D = np.ascontiguousarray(density, dtype=np.complex128)
+    cu = np.ascontiguousarray(occ_up, dtype=np.complex128).reshape(n_up, nb) if n_up else None
+    cd = np.ascontiguousarray(occ_down, dtype=np.complex128).reshape(n_down, nb) if n_down else None
+    hh = np.ascontiguousarray(h, dtype=np.float64)
+    G2, G3, F = (np.empty((2, nb, nb), dtype=np.complex128) for _ in range(3))
+    e = C.c_double()
+    _raise(ffi.lib().tcscf_tc_fock_build(ctx.handle, r1Grid.id, Fs.handle, Fo.handle, Vs.handle, Vo.handle, n_up, n_down,
+                                         ffi.dptr(D), ffi.dptr(cu), ffi.dptr(cd), ffi.dptr(hh), int(respect_symmetry),
+                                         ffi.dptr(G2), ffi.dptr(G3), ffi.dptr(F), C.byref(e)), ctx.handle)
+    return G2, G3, F, e.value
+
+
+class TCHartreeFock:
+    """TCHartreeFock::compute (HartreeFock.hpp:386-394, HartreeFock.cpp:1007-1362) on device tensors."""
+
+    def __init__(self, n_up: int, n_down: int):
+        self.n_up, self.n_down = n_up, n_down
+        self.energy = None
+        self.iterations = 0
+        self.density = None
+        self.pseudo_energies = None
+
+    def compute(self, overlap: np.ndarray, h: np.ndarray, r1Grid: QMCGrid, Fs: DeviceTensor, Fo: DeviceTensor, Vs: DeviceTensor,
+                Vo: DeviceTensor, respect_symmetry: bool = True, tol: float = 1e-5, max_iter: int = 200) -> float:
+        ctx = r1Grid.ctx
+        nb = r1Grid.nBasis()
+        D = np.empty((2, nb, nb), dtype=np.complex128)
+        pe = np.zeros((2, nb))
+        e, it = C.c_double(), C.c_int()
+        code = ffi.lib().tcscf_tc_scf(ctx.handle, r1Grid.id, Fs.handle, Fo.handle, Vs.handle, Vo.handle,
+                                      ffi.dptr(np.ascontiguousarray(overlap, dtype=np.float64)),
+                                      ffi.dptr(np.ascontiguousarray(h, dtype=np.float64)), self.n_up, self.n_down, int(respect_symmetry),
+                                      float(tol), int(max_iter), C.byref(e), C.byref(it), ffi.dptr(D), ffi.dptr(pe))
+        self.energy, self.iterations, self.density, self.pseudo_energies = e.value, it.value, D, pe
+        if code == ffi.ERR_NOT_CONVERGED:
+            raise ConvergenceError(ffi.lib().tcscf_last_error(ctx.handle).decode())
+        _raise(code, ctx.handle)
+        return self.energy
+
+
 def _check_shapes(D: np.ndarray, h: np.ndarray, nb: int) -> None:
     """CHECK_BOUNDS_3(density, nSpin, nBasis, nBasis) / CHECK_BOUNDS_2(oneElectronTerms, nBasis, nBasis)."""
     if D.ndim != 3 or D.shape[0] not in (1, 2) or D.shape[1:] != (nb, nb) or h.shape != (nb, nb):

@@ -38,6 +38,12 @@ bool tensorPathAvailable(Contraction const & c, int precision, std::string * why
 // hi/lo [NB][n2pad] followed by the per-block column scales
 int tensorPackedV(tcscf_ctx * ctx, Grid & g2, const double * V, double scale, const void ** packed);
 
+// F = h + G - G3 (G3 may be null), masked where h == 0 when respectSym, and the compensated energy
+// factor * sum D(i,j) (h + G/2 - G3/3)(j,i) (constructSCFOperator, HartreeFock.cpp:48-98); G is
+// written back masked
+int finalizeLaunch(tcscf_ctx * ctx, int nspin, int nb, const double * h, double2 * G, const double2 * G3, const double2 * D, int respectSym,
+                   double factor, double2 * fock, double * energy);
+
 // out[r][c] = sum_s part[s*stride + r*ldPart + c] for r < rows, c < cols (deterministic split sum)
 int sumSplitsLaunch(tcscf_ctx * ctx, int64_t n, int nsplit, int64_t stride, const double * part, double * out, int64_t rows, int cols,
                     int ldOut, int ldPart);

@@ -549,6 +549,14 @@ __global__ void kDensityFromOrbitals(int nb, int nocc, const double2 * C, double
 
 }  // namespace
 
+int finalizeLaunch(tcscf_ctx * ctx, int nspin, int nb, const double * h, double2 * G, const double2 * G3, const double2 * D, int respectSym,
+                   double factor, double2 * fock, double * energy)
+{
+  kFinalize<<<1, 512, 0, ctx->stream>>>(nspin, nb, h, G, G3, D, respectSym, factor, fock, energy);
+  TCSCF_LAUNCH(ctx);
+  return TCSCF_OK;
+}
+
 // ------------------------------------------------------------------------------------------------
 // Fock-build pipeline
 // ------------------------------------------------------------------------------------------------

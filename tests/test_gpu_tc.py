@@ -1,0 +1,90 @@
+"""Transcorrelated Fock build and SCF on the GPU vs the oracle (TCHartreeFock, HartreeFock.cpp:1007-1362).
+
+The F and V tensors are computed on the GPU (tcscf_compute_F / tcscf_compute_V, themselves checked
+against the oracle in test_gpu_parity.py) and by the oracle, so each TC build compares the whole
+chain.  FP64 throughout: G2, G3 and F agree to 1e-10 of their largest element, the energy to
+1e-10 Eh; the SCF energies (different eigen-solvers: LAPACK zggev in the oracle, Cholesky +
+cusolverDnXgeev here) to 1e-8 Eh at a 1e-10 convergence threshold.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from tcscf_b200 import api, ffi, grids
+from tcscf_b200 import basis as wl
+
+pytestmark = pytest.mark.gpu
+
+U = dict(a=1.0, a12=1.0, terms=[((1, 0, 0), -0.5, -0.25)])   # HartreeFockTest.cpp:351-360 sign convention
+BASIS = wl.expand(0, [0.6, 1.5, 3.6, 8.5]) + wl.expand(1, [1.2])   # 7 functions
+Z, NUP, NDOWN = 4, 2, 2
+
+
+@pytest.fixture(scope="module")
+def tc_setup(ctx):
+    g1 = grids.qmc_grid(3, 192, 51)
+    g2 = grids.qmc_grid(3, 768, 52)
+    G1 = api.QMCGrid(ctx, g1)
+    G1.setBasisFunctions(BASIS, storeGradients=True)
+    G2 = api.QMCGrid(ctx, g2)
+    G2.setBasisFunctions(BASIS)
+    u = ffi.ochi_struct(U["a"], U["a12"], U["terms"])
+    uo = oracle.ochi(U["a"], U["a12"], U["terms"])
+    t = {}
+    t["Fs"] = api.computeF(G1, G2, ffi.K_TC_SCALAR_SAME, u, keep=True, copy=False)[1]
+    t["Fo"] = api.computeF(G1, G2, ffi.K_TC_SCALAR_OPPO, u, keep=True, copy=False)[1]
+    t["Vs"] = api.computeV(G1, G2, ffi.K_GRAD_U_SAME, u, keep=True, copy=False)[1]
+    t["Vo"] = api.computeV(G1, G2, ffi.K_GRAD_U_OPPO, u, keep=True, copy=False)[1]
+    vals2 = oracle.basis_values(g2.points, BASIS)
+    vals1, grads1 = oracle.basis_values(g1.points, BASIS, gradients=True)
+    nb = len(BASIS)
+    o = dict(Fs=oracle.compute_F(g1.points, g2.points, g2.weights, vals2, nb, ffi.K_TC_SCALAR_SAME, uo),
+             Fo=oracle.compute_F(g1.points, g2.points, g2.weights, vals2, nb, ffi.K_TC_SCALAR_OPPO, uo),
+             Vs=oracle.compute_V(g1.points, g2.points, g2.weights, vals2, nb, ffi.K_GRAD_U_SAME, uo),
+             Vo=oracle.compute_V(g1.points, g2.points, g2.weights, vals2, nb, ffi.K_GRAD_U_OPPO, uo),
+             vals1=vals1, grads1=grads1, w1=g1.weights)
+    S, h = api.overlap_core(BASIS, Z)
+    yield G1, t, o, S, h
+    for d in t.values():
+        d.close()
+
+
+def _random_orbitals(nb, n, rng):
+    return (rng.normal(size=(n, nb)) + 1j * rng.normal(size=(n, nb))) * 0.3
+
+
+def test_tc_fock_build_matches_oracle(ctx, tc_setup):
+    G1, t, o, S, h = tc_setup
+    nb = len(BASIS)
+    rng = np.random.default_rng(7)
+    occ = [_random_orbitals(nb, NUP, rng), _random_orbitals(nb, NDOWN, rng)]
+    D = np.stack([c.T @ c.conj() for c in occ])        # D(u,v) = sum_a C(u,a) conj(C(v,a))
+    for sym in (True, False):
+        G2, G3, F, E = api.tc_fock_build(G1, t["Fs"], t["Fo"], t["Vs"], t["Vo"], NUP, NDOWN, D, occ[0], occ[1], h, sym)
+        G2r, G3r, Fr, Er = oracle.tc_fock_build(o["Fs"], o["Fo"], o["Vs"], o["Vo"], o["vals1"], o["grads1"], o["w1"], D, NUP, NDOWN,
+                                                occ[0], occ[1], h, sym)
+        for a, b in ((G2, G2r), (G3, G3r), (F, Fr)):
+            np.testing.assert_allclose(a, b, rtol=0, atol=1e-10 * max(1.0, np.abs(b).max()))
+        assert abs(E - Er) < 1e-10 * max(1.0, abs(Er)), (E, Er)
+
+
+def test_tc_scf_matches_oracle(ctx, tc_setup):
+    G1, t, o, S, h = tc_setup
+    scf = api.TCHartreeFock(NUP, NDOWN)
+    E = scf.compute(S, h, G1, t["Fs"], t["Fo"], t["Vs"], t["Vo"], tol=1e-10, max_iter=200)
+    st, Er, itr, Dr, per = oracle.tc_scf(o["Fs"], o["Fo"], o["Vs"], o["Vo"], o["vals1"], o["grads1"], o["w1"], S, h, NUP, NDOWN,
+                                         tol=1e-10, max_iter=200)
+    assert st == 0
+    assert abs(E - Er) < 1e-8, (E, Er, scf.iterations, itr)
+    np.testing.assert_allclose(scf.pseudo_energies[:, :NUP], per[:, :NUP], rtol=0, atol=1e-7)
+    np.testing.assert_allclose(scf.density, Dr, rtol=0, atol=1e-6 * np.abs(Dr).max())
+
+
+def test_tc_argument_checks(ctx, tc_setup):
+    G1, t, o, S, h = tc_setup
+    nb = len(BASIS)
+    D = np.zeros((2, nb, nb), dtype=np.complex128)
+    occ = np.zeros((NUP, nb), dtype=np.complex128)
+    with pytest.raises(ffi.TcscfError) as e:      # V handle where an F handle belongs
+        api.tc_fock_build(G1, t["Vs"], t["Fo"], t["Vs"], t["Vo"], NUP, NDOWN, D, occ, occ, h)
+    assert e.value.code == ffi.ERR_INVALID_ARGUMENT
