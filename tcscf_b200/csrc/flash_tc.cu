@@ -40,6 +40,8 @@ constexpr int BM = 128;        // r1 rows per tile
 constexpr int BK = 64;         // r2 points per block
 // TMA stages: three when the tile shapes leave room in shared memory
 __host__ __device__ constexpr int stagesFor(int NB, int RP) { return NB == 64 && RP == 32 ? 3 : 2; }
+// X tile buffers: two (GEMM2 of block g - 1 overlaps the writing of block g) where shared memory allows
+__host__ __device__ constexpr int xBuffersFor(int NB, int RP) { return NB == 64 && RP == 64 ? 1 : 2; }
 constexpr int NCW = 8;         // compute warps
 constexpr int NTHREADS = 384;  // warpgroup 0: TMA, MMA, 2 idle warps; warpgroups 1-2: compute
 // register split: 384 threads x 168 at launch = 64512 = 128 x 56 (producer warpgroup) + 256 x 224
@@ -65,7 +67,8 @@ template <int NB, int RP>
 struct __align__(1024) Smem {
   static constexpr int NSTAGE = stagesFor(NB, RP);
   uint8_t v[NSTAGE][3][NB * BK * 2];       // Vt block h / m / l/256: SW128 K-major [NB rows][64]
-  uint8_t x[2][BM * BK * 2];               // X tile h / l:   SW128 K-major [128 rows][64]
+  static constexpr int XBUF = xBuffersFor(NB, RP);
+  uint8_t x[XBUF][2][BM * BK * 2];         // X tile h / l per buffer: SW128 K-major [128 rows][64]
   uint8_t psi2[NSTAGE][3][BK * RP * 2];    // psi2 block h / m / l/256: K-major [64 rows][RP]
   uint8_t psi1[4][BM * RP * 2];            // psi1 tile h / m / l/256 / m/256: K-major [128 rows][RP]
   float4 coords[NSTAGE][BK];               // r2 block as 32 pairs {x0,x1,y0,y1}{z0,z1,c0,c1}
@@ -74,7 +77,7 @@ struct __align__(1024) Smem {
   float cinvT[NCW][2][NB / 2];             // each compute warp's copy of its columns' cinv, by block parity
   float rowmax[2][2][BM];                  // [block parity][r2 half][row] max |X'| of the half
   uint64_t full[NSTAGE], empty[NSTAGE];
-  uint64_t sfull[2], sfree[2], xfull, xfree;
+  uint64_t sfull[2], sfree[2], xfull[2], xfree[2];   // xfull / xfree: per X buffer
   uint64_t rmax[2][4];                     // [block parity][lane quarter]: both r2 halves posted their maxima
   uint64_t tfull, tfree;
   uint64_t p1full, p1free, done;
@@ -214,7 +217,13 @@ __device__ __forceinline__ void tmemLoad16(uint32_t taddr, float * v)
 #pragma unroll
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
-__device__ __forceinline__ void tmemWaitLoad() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+// wait for the outstanding TMEM loads into a and b; the register operands keep every use of a and b
+// after the wait (the asm statements are volatile, so their order is kept)
+__device__ __forceinline__ void tmemWaitLoad(float (&a)[16], float (&b)[16])
+{
+  asm volatile("tcgen05.wait::ld.sync.aligned;" : "+f"(a[0]), "+f"(a[1]), "+f"(a[2]), "+f"(a[3]), "+f"(a[4]), "+f"(a[5]), "+f"(a[6]), "+f"(a[7]), "+f"(a[8]), "+f"(a[9]), "+f"(a[10]), "+f"(a[11]), "+f"(a[12]), "+f"(a[13]), "+f"(a[14]), "+f"(a[15]) :: "memory");
+  asm volatile("" : "+f"(b[0]), "+f"(b[1]), "+f"(b[2]), "+f"(b[3]), "+f"(b[4]), "+f"(b[5]), "+f"(b[6]), "+f"(b[7]), "+f"(b[8]), "+f"(b[9]), "+f"(b[10]), "+f"(b[11]), "+f"(b[12]), "+f"(b[13]), "+f"(b[14]), "+f"(b[15]) :: "memory");
+}
 
 // ---- packed FP32 pairs (sm_100 f32x2 arithmetic on 64-bit register pairs) ---------------------
 __device__ __forceinline__ uint64_t f2pack(float a, float b)
@@ -279,22 +288,30 @@ __device__ __forceinline__ bool flushBlock(SmemT & S, uint32_t taddr, uint32_t f
   fenceAfterSync();
   float const * cs = S.cinvT[cw][f & 1];
   uint64_t const k256 = f2pack(256.0f, 256.0f);
+  constexpr int NQ = NB / 32;   // chunks of 16 columns; the loads of chunk q + 1 overlap the work on chunk q
+  float hh[2][16], mm[2][16];
+  tmemLoad16(taddr, hh[0]);
+  tmemLoad16(taddr + NB, mm[0]);
+  tmemWaitLoad(hh[0], mm[0]);
 #pragma unroll
-  for (int q = 0; q < NB / 32; ++q) {
-    float hh[16], mm[16];
-    tmemLoad16(taddr + q * 16, hh);
-    tmemLoad16(taddr + NB + q * 16, mm);
-    tmemWaitLoad();
+  for (int q = 0; q < NQ; ++q) {
+    int const cur = q & 1;
+    if (q + 1 < NQ) {
+      tmemLoad16(taddr + (q + 1) * 16, hh[cur ^ 1]);
+      tmemLoad16(taddr + NB + (q + 1) * 16, mm[cur ^ 1]);
+    }
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
       float2 const c2 = *reinterpret_cast<float2 const *>(cs + q * 16 + 2 * i);
       // 256 hh + cross is the block's exact integer sum up to one FP32 rounding; cinv is a power of two
-      uint64_t const v = f2mul(f2fma(f2pack(hh[2 * i], hh[2 * i + 1]), k256, f2pack(mm[2 * i], mm[2 * i + 1])), f2pack(c2.x, c2.y));
+      uint64_t const v =
+          f2mul(f2fma(f2pack(hh[cur][2 * i], hh[cur][2 * i + 1]), k256, f2pack(mm[cur][2 * i], mm[cur][2 * i + 1])), f2pack(c2.x, c2.y));
       float va, vb;
       f2unpack(v, va, vb);
       acc[q * 16 + 2 * i] = fma(double(va), fac, acc[q * 16 + 2 * i]);
       acc[q * 16 + 2 * i + 1] = fma(double(vb), fac, acc[q * 16 + 2 * i + 1]);
     }
+    if (q + 1 < NQ) tmemWaitLoad(hh[cur ^ 1], mm[cur ^ 1]);
   }
   fenceBeforeSync();
   __syncwarp();
@@ -315,6 +332,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   extern __shared__ uint8_t smemRaw[];
   Smem<NB, RP> & S = *reinterpret_cast<Smem<NB, RP> *>((reinterpret_cast<uintptr_t>(smemRaw) + 1023) & ~uintptr_t(1023));
   constexpr int NSTAGE = stagesFor(NB, RP);
+  constexpr int XBUF = xBuffersFor(NB, RP);
   int const warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   volatile int * abortFlag = &S.abort;
 
@@ -326,9 +344,9 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     for (int s = 0; s < NSTAGE; ++s) { mbarInit(&S.full[s], 1); mbarInit(&S.empty[s], 1 + NCW); }
     for (int b = 0; b < 2; ++b) {
       mbarInit(&S.sfull[b], 1); mbarInit(&S.sfree[b], NCW);
+      mbarInit(&S.xfull[b], NCW); mbarInit(&S.xfree[b], 1);
       for (int q = 0; q < 4; ++q) mbarInit(&S.rmax[b][q], 2);
     }
-    mbarInit(&S.xfull, NCW); mbarInit(&S.xfree, 1);
     mbarInit(&S.tfull, 1); mbarInit(&S.tfree, NCW);
     mbarInit(&S.p1full, 1); mbarInit(&S.p1free, 1); mbarInit(&S.done, 1);
     S.abort = 0;
@@ -396,6 +414,10 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     if (lane == 0) {
       constexpr uint32_t idesc1 = instrDescBf16(BM, BK);
       constexpr uint32_t idesc2 = instrDescBf16(BM, NB);
+      // h x [h'; m'] in one MMA: the h and m slices of an operand are adjacent in shared memory (so
+      // the B rows continue), and the two accumulators are adjacent in TMEM (A then B)
+      constexpr uint32_t idesc1x2 = instrDescBf16(BM, 2 * BK);
+      constexpr uint32_t idesc2x2 = instrDescBf16(BM, 2 * NB);
       uint32_t const aPsi1[4] = {smemAddr(S.psi1[0]), smemAddr(S.psi1[1]), smemAddr(S.psi1[2]), smemAddr(S.psi1[3])};
       uint32_t blockCount = 0;   // global block counter: selects stage, rho / X buffers, T phase
       uint32_t p1Use = 0;
@@ -424,12 +446,11 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           for (int k = 0; k < RP / 16; ++k) {
             uint32_t const acc = k > 0 ? 1u : 0u;
             // B: h m' + m h' + h l'/256 + l/256 h' + m/256 m'; A: h h'
-            mmaBf16(dX, da(0, k), db(1, k), idesc1, acc);
+            mmaBf16(dHH, da(0, k), db(0, k), idesc1x2, acc);   // A += h h', B += h m'
             mmaBf16(dX, da(1, k), db(0, k), idesc1, 1);
             mmaBf16(dX, da(0, k), db(2, k), idesc1, 1);
             mmaBf16(dX, da(2, k), db(0, k), idesc1, 1);
             mmaBf16(dX, da(3, k), db(1, k), idesc1, 1);
-            mmaBf16(dHH, da(0, k), db(0, k), idesc1, acc);
           }
           mmaCommit(&S.sfull[b]);
           return true;
@@ -441,21 +462,21 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           int const s = g % NSTAGE, b = g & 1;
           // the T accumulators are free once the compute warps flushed block g - 1
           if (g >= 1 && !(ok = waitBar(&S.tfree, (g - 1) & 1, abortFlag, P.status, 24))) break;
-          if (!(ok = waitBar(&S.xfull, g & 1, abortFlag, P.status, 25))) break;
+          int const xb = g % XBUF;
+          if (!(ok = waitBar(&S.xfull[xb], (g / XBUF) & 1, abortFlag, P.status, 25))) break;
           fenceAfterSync();
           uint32_t const dHH = tmem + TCOL0, dX = dHH + NB;
-          uint32_t const aX[2] = {smemAddr(S.x[0]), smemAddr(S.x[1])};
+          uint32_t const aX[2] = {smemAddr(S.x[xb][0]), smemAddr(S.x[xb][1])};
           uint32_t const bV[3] = {smemAddr(S.v[s][0]), smemAddr(S.v[s][1]), smemAddr(S.v[s][2])};
 #pragma unroll
           for (int k = 0; k < BK / 16; ++k) {
             uint32_t const acc = k > 0 ? 1u : 0u;
             // B: hX mV + lX hV + hX lV/256; A: hX hV
-            mmaBf16(dX, smemDesc(aX[0] + 32 * k, 1024, 2), smemDesc(bV[1] + 32 * k, 1024, 2), idesc2, acc);
+            mmaBf16(dHH, smemDesc(aX[0] + 32 * k, 1024, 2), smemDesc(bV[0] + 32 * k, 1024, 2), idesc2x2, acc);   // A += hX hV, B += hX mV
             mmaBf16(dX, smemDesc(aX[1] + 32 * k, 1024, 2), smemDesc(bV[0] + 32 * k, 1024, 2), idesc2, 1);
             mmaBf16(dX, smemDesc(aX[0] + 32 * k, 1024, 2), smemDesc(bV[2] + 32 * k, 1024, 2), idesc2, 1);
-            mmaBf16(dHH, smemDesc(aX[0] + 32 * k, 1024, 2), smemDesc(bV[0] + 32 * k, 1024, 2), idesc2, acc);
           }
-          mmaCommit(&S.xfree);
+          mmaCommit(&S.xfree[xb]);
           mmaCommit(&S.empty[s]);
           mmaCommit(&S.tfull);
           if (jj == nblk - 1) mmaCommit(&S.p1free);
@@ -525,7 +546,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           float rh[16], rx[16];
           tmemLoad16(rhoAddr + hh * 16, rh);
           tmemLoad16(rhoAddr + BK + hh * 16, rx);
-          tmemWaitLoad();
+          tmemWaitLoad(rh, rx);
           if (hh == 1) {
             // both rho accumulators of this warp's columns are read: the buffer is free for GEMM1
             fenceBeforeSync();
@@ -575,12 +596,13 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         float const bs = __uint_as_float(uint32_t(127 + kXExp - E) << 23);
         double const binv = __longlong_as_double(int64_t(1023 + E - kXExp) << 52);
         double const fac = rowA * binv;
-        // the X tile is free once GEMM2 of block g - 1 completed
-        if (g >= 1 && !(ok = waitBar(&S.xfree, (g - 1) & 1, abortFlag, P.status, 34))) break;
+        // X buffer xb is free once GEMM2 of block g - XBUF completed
+        int const xb = g % XBUF;
+        if (g >= uint32_t(XBUF) && !(ok = waitBar(&S.xfree[xb], ((g / XBUF) - 1) & 1, abortFlag, P.status, 34))) break;
         // slices: t = X' bs = 256 h + l, h = rint(t / 256), l = rint(t - 256 h)
         uint64_t const bb = f2pack(bs, bs);
-        uint8_t * xhi = S.x[0];
-        uint8_t * xlo = S.x[1];
+        uint8_t * xhi = S.x[xb][0];
+        uint8_t * xlo = S.x[xb][1];
 #pragma unroll
         for (int ch = 0; ch < 4; ++ch) {
           uint32_t hi[4], lo[4];
@@ -601,7 +623,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         vh += double(vs0 + vs1);
         fenceProxyAsync();
         __syncwarp();
-        if (lane == 0) { mbarArrive(&S.xfull); mbarArrive(&S.empty[s]); }
+        if (lane == 0) { mbarArrive(&S.xfull[xb]); mbarArrive(&S.empty[s]); }
         if (pending && !(ok = flushBlock<NB>(S, tAddr, g - 1, cw, pendingFac, acc, lane, abortFlag, P.status))) break;
         pending = true;
         pendingFac = fac;
