@@ -180,6 +180,14 @@ int tcscf_fock_build(tcscf_ctx * ctx, int r1, int r2, int nspin, const double * 
  * NULL); the work is ordered on the context stream, which is synchronised before returning. */
 int tcscf_fock_build_device(tcscf_ctx * ctx, int r1, int r2, int nspin, const double * density, const double * h,
                             int respect_symmetry, int precision, double * G, double * fock, double * energy);
+/* Batched RCS Fock builds: instance k uses grids r1[k], r2[k], density[k] ([nb][nb] complex) and
+ * h[k]; energy[k] receives its energy and, when fock and fock[k] are not NULL, fock[k] its Fock
+ * matrix.  At BF16X3 the r12 contractions of all instances run in one persistent launch per tile
+ * class (instances whose density factor is complex in the real-harmonic basis are built on their
+ * own); FP64 builds the instances one after another.  Per-instance results are those of
+ * tcscf_fock_build_device. */
+int tcscf_fock_build_batch(tcscf_ctx * ctx, int count, const int * r1, const int * r2, const double * const * density,
+                           const double * const * h, int respect_symmetry, int precision, double * energy, double * const * fock);
 /* Same, from a device-resident Fji handle (the reference's precompute form). */
 int tcscf_fock_build_precomputed(tcscf_ctx * ctx, int r1, int fji, int nspin, const double * density, const double * h,
                                  int respect_symmetry, double * G, double * fock, double * energy);

@@ -209,6 +209,26 @@ def threeElectronIntegrals(r1Grid: QMCGrid, r2Grid: QMCGrid, jastrow: ffi.Ochi) 
     return out
 
 
+def fock_build_batch(r1Grids, r2Grids, densities, hs, respect_symmetry: bool = True, precision: int = ffi.PREC_BF16X3,
+                     want_fock: bool = False):
+    """Batched RCS Fock builds (one persistent tensor-core launch per tile class for the whole batch).
+    Returns the energies [count] (and the Fock matrices when want_fock)."""
+    count = len(r1Grids)
+    ctx = r1Grids[0].ctx
+    D = [np.ascontiguousarray(d, dtype=np.complex128).reshape(g.nBasis(), g.nBasis()) for d, g in zip(densities, r1Grids)]
+    H = [np.ascontiguousarray(h, dtype=np.float64) for h in hs]
+    F = [np.empty_like(d) for d in D] if want_fock else None
+    r1 = (C.c_int * count)(*[g.id for g in r1Grids])
+    r2 = (C.c_int * count)(*[g.id for g in r2Grids])
+    dp = (ffi._D * count)(*[ffi.dptr(d) for d in D])
+    hp = (ffi._D * count)(*[ffi.dptr(h) for h in H])
+    fp = (ffi._D * count)(*[ffi.dptr(f) for f in F]) if F else None
+    e = np.empty(count)
+    _raise(ffi.lib().tcscf_fock_build_batch(ctx.handle, count, r1, r2, dp, hp, int(respect_symmetry), precision, ffi.dptr(e), fp),
+           ctx.handle)
+    return (e, F) if want_fock else e
+
+
 def tc_fock_build(r1Grid: QMCGrid, Fs: DeviceTensor, Fo: DeviceTensor, Vs: DeviceTensor, Vo: DeviceTensor, n_up: int, n_down: int,
                   density: np.ndarray, occ_up: np.ndarray, occ_down: np.ndarray, h: np.ndarray, respect_symmetry: bool = True):
     """One transcorrelated Fock build (HartreeFock.cpp:1150-1224) from device tensors.

@@ -31,6 +31,9 @@
 #include <cuda.h>
 #include <cuda_bf16.h>
 
+#include <algorithm>
+#include <vector>
+
 #include "kernels.cuh"
 
 namespace tcscf {
@@ -85,21 +88,26 @@ struct __align__(1024) Smem {
   int abort;
 };
 
+using Instance = TensorInstance;
+constexpr int kMapsPerInstance = kTensorMapsPerInstance;
+
 struct Params {
-  int nTiles, nSplit, blocksPerSplit, nBlocks;   // r2 blocks in total, per split
-  int n1;                                          // real r1 rows
-  int nb;                                          // real columns of T
-  const float4 * r1xyz;                            // [n1pad] x, y, z, 0
-  const float4 * r2pairs;                          // [nBlocks*64] r2 points in pair layout
-  const float * a1inv;                             // [n1pad] 1 / psi1 row scale
-  const float * a2inv;                             // [nBlocks*64] 1 / psi2 row scale
-  const float * cinv;                              // [nBlocks][NB] 1 / Vt column scale
-  double * T;                                      // [nSplit][n1][ldt]
-  double * VH;                                     // [nSplit][n1]
-  int ldt;
-  int64_t tStride, vhStride;
-  int * status;                                    // device status word (0 = ok)
+  int nItems;
+  const int4 * items;       // work items (instance, r1 tile, r2 split, 0); null: one instance, item = tile * nSplit + split
+  const Instance * inst;    // [instances] in device memory
+  int * status;             // device status word (0 = ok)
 };
+
+__device__ __forceinline__ void decodeItem(Params const & P, int item, int & inst, int & tile, int & split)
+{
+  if (P.items) {
+    int4 const it = P.items[item];
+    inst = it.x; tile = it.y; split = it.z;
+  } else {
+    int const ns = P.inst[0].nSplit;
+    inst = 0; tile = item / ns; split = item % ns;
+  }
+}
 
 // ---- PTX helpers --------------------------------------------------------------------------------
 __device__ __forceinline__ uint32_t smemAddr(const void * p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
@@ -322,12 +330,7 @@ __device__ __forceinline__ bool flushBlock(SmemT & S, uint32_t taddr, uint32_t f
 // ---- the kernel ------------------------------------------------------------------------------------
 template <int NB, int RP>
 __global__ void __launch_bounds__(NTHREADS, 1)
-    kFlashTc(const __grid_constant__ CUtensorMap mapPsi1H, const __grid_constant__ CUtensorMap mapPsi1M,
-             const __grid_constant__ CUtensorMap mapPsi1L, const __grid_constant__ CUtensorMap mapPsi1Ms,
-             const __grid_constant__ CUtensorMap mapPsi2H,
-             const __grid_constant__ CUtensorMap mapPsi2M, const __grid_constant__ CUtensorMap mapPsi2L,
-             const __grid_constant__ CUtensorMap mapVH, const __grid_constant__ CUtensorMap mapVM,
-             const __grid_constant__ CUtensorMap mapVL, Params P)
+    kFlashTc(Params P)
 {
   extern __shared__ uint8_t smemRaw[];
   Smem<NB, RP> & S = *reinterpret_cast<Smem<NB, RP> *>((reinterpret_cast<uintptr_t>(smemRaw) + 1023) & ~uintptr_t(1023));
@@ -361,7 +364,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
   fenceAfterSync();
   uint32_t const tmem = S.tmemBase;
 
-  int const nItems = P.nTiles * P.nSplit;
+  int const nItems = P.nItems;
 
   if (warp < 4) {
     asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;" ::"n"(kRegsProducer));
@@ -372,15 +375,15 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       uint32_t p1Use = 0;
       bool ok = true;
       for (int item = blockIdx.x; item < nItems && ok; item += gridDim.x) {
-        int const tile = item / P.nSplit, split = item % P.nSplit;
-        int const jb = split * P.blocksPerSplit;
-        int const je = min(P.nBlocks, jb + P.blocksPerSplit);
+        int ii, tile, split;
+        decodeItem(P, item, ii, tile, split);
+        Instance const * I = P.inst + ii;
+        CUtensorMap const * maps = I->maps;
+        int const jb = split * I->blocksPerSplit;
+        int const je = min(I->nBlocks, jb + I->blocksPerSplit);
         if (p1Use > 0 && !(ok = waitBar(&S.p1free, (p1Use - 1) & 1, abortFlag, P.status, 11))) break;
         mbarArriveTx(&S.p1full, kPsi1Bytes);
-        tmaLoad2d(S.psi1[0], &mapPsi1H, 0, tile * BM, &S.p1full);
-        tmaLoad2d(S.psi1[1], &mapPsi1M, 0, tile * BM, &S.p1full);
-        tmaLoad2d(S.psi1[2], &mapPsi1L, 0, tile * BM, &S.p1full);
-        tmaLoad2d(S.psi1[3], &mapPsi1Ms, 0, tile * BM, &S.p1full);
+        for (int k = 0; k < 4; ++k) tmaLoad2d(S.psi1[k], maps + k, 0, tile * BM, &S.p1full);
         ++p1Use;
         for (int j = jb; j < je; ++j) {
           uint32_t const q = issuedLoads++;
@@ -388,15 +391,11 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           // use u = q / NSTAGE of stage s needs consumption u - 1 of it
           if (q >= uint32_t(NSTAGE) && !(ok = waitBar(&S.empty[s], ((q / NSTAGE) - 1) & 1, abortFlag, P.status, 12))) break;
           mbarArriveTx(&S.full[s], kStageBytes);
-          tmaLoad2d(S.psi2[s][0], &mapPsi2H, 0, j * BK, &S.full[s]);
-          tmaLoad2d(S.psi2[s][1], &mapPsi2M, 0, j * BK, &S.full[s]);
-          tmaLoad2d(S.psi2[s][2], &mapPsi2L, 0, j * BK, &S.full[s]);
-          tmaLoad2d(S.v[s][0], &mapVH, j * BK, 0, &S.full[s]);
-          tmaLoad2d(S.v[s][1], &mapVM, j * BK, 0, &S.full[s]);
-          tmaLoad2d(S.v[s][2], &mapVL, j * BK, 0, &S.full[s]);
-          bulkLoad(S.coords[s], P.r2pairs + int64_t(j) * BK, BK * sizeof(float4), &S.full[s]);
-          bulkLoad(S.a2inv[s], P.a2inv + int64_t(j) * BK, BK * sizeof(float), &S.full[s]);
-          bulkLoad(S.cinv[s], P.cinv + int64_t(j) * NB, NB * sizeof(float), &S.full[s]);
+          for (int k = 0; k < 3; ++k) tmaLoad2d(S.psi2[s][k], maps + 4 + k, 0, j * BK, &S.full[s]);
+          for (int k = 0; k < 3; ++k) tmaLoad2d(S.v[s][k], maps + 7 + k, j * BK, 0, &S.full[s]);
+          bulkLoad(S.coords[s], I->r2pairs + int64_t(j) * BK, BK * sizeof(float4), &S.full[s]);
+          bulkLoad(S.a2inv[s], I->a2inv + int64_t(j) * BK, BK * sizeof(float), &S.full[s]);
+          bulkLoad(S.cinv[s], I->cinv + int64_t(j) * NB, NB * sizeof(float), &S.full[s]);
         }
       }
       // drain: every issued load lands before the CTA can exit (bounded)
@@ -423,9 +422,11 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       uint32_t p1Use = 0;
       bool ok = true;
       for (int item = blockIdx.x; item < nItems && ok; item += gridDim.x) {
-        int const split = item % P.nSplit;
-        int const jb = split * P.blocksPerSplit;
-        int const je = min(P.nBlocks, jb + P.blocksPerSplit);
+        int ii, tile, split;
+        decodeItem(P, item, ii, tile, split);
+        Instance const * I = P.inst + ii;
+        int const jb = split * I->blocksPerSplit;
+        int const je = min(I->nBlocks, jb + I->blocksPerSplit);
         int const nblk = je - jb;
         if (!(ok = waitBar(&S.p1full, p1Use & 1, abortFlag, P.status, 21))) break;
         ++p1Use;
@@ -459,7 +460,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         for (int jj = 0; jj < nblk && ok; ++jj) {
           if (jj + 1 < nblk && !(ok = gemm1(jj + 1))) break;
           uint32_t const g = base + jj;
-          int const s = g % NSTAGE, b = g & 1;
+          int const s = g % NSTAGE;
           // the T accumulators are free once the compute warps flushed block g - 1
           if (g >= 1 && !(ok = waitBar(&S.tfree, (g - 1) & 1, abortFlag, P.status, 24))) break;
           int const xb = g % XBUF;
@@ -512,15 +513,17 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     uint64_t const kMagic = f2pack(12582912.0f, 12582912.0f);   // 1.5 * 2^23: adding it rounds |x| < 2^22 to an integer
     uint64_t const mOne = f2pack(-1.0f, -1.0f), mHalf = f2pack(-0.5f, -0.5f);
     for (int item = blockIdx.x; item < nItems && ok; item += gridDim.x) {
-      int const tile = item / P.nSplit, split = item % P.nSplit;
-      int const jb = split * P.blocksPerSplit;
-      int const je = min(P.nBlocks, jb + P.blocksPerSplit);
+      int ii, tile, split;
+      decodeItem(P, item, ii, tile, split);
+      Instance const * I = P.inst + ii;
+      int const jb = split * I->blocksPerSplit;
+      int const je = min(I->nBlocks, jb + I->blocksPerSplit);
       int const nblk = je - jb;
       int const r1 = tile * BM + row;
-      float4 const p1 = P.r1xyz[r1];
+      float4 const p1 = I->r1xyz[r1];
       // rho = 2^24 a1inv a2inv (256 A + B), X' = g a2inv (256 A + B) = X / (2^24 a1inv), and a block's
       // sum_r2 X' Vt = 2^16 (256 A + B) / (bs c): T += 2^40 a1inv / bs * cinv (256 A + B)
-      double const rowA = 1099511627776.0 * double(P.a1inv[r1]);
+      double const rowA = 1099511627776.0 * double(I->a1inv[r1]);
 #pragma unroll
       for (int c = 0; c < NB / 2; ++c) acc[c] = 0.0;
       double vh = 0.0;
@@ -631,16 +634,18 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       if (ok && pending) ok = flushBlock<NB>(S, tAddr, blockCount + nblk - 1, cw, pendingFac, acc, lane, abortFlag, P.status);
       blockCount += nblk;
       if (!ok) break;
-      if (r1 < P.n1) {
-        double * T = P.T + int64_t(split) * P.tStride + int64_t(r1) * P.ldt;
+      int const n1 = I->n1;
+      if (r1 < n1) {
+        int const nbReal = I->nb;
+        double * T = I->T + int64_t(split) * I->tStride + int64_t(r1) * I->ldt;
 #pragma unroll
         for (int c = 0; c < NB / 2; ++c) {
           int const col = half * (NB / 2) + c;
-          if (col < P.nb) T[col] = acc[c];
+          if (col < nbReal) T[col] = acc[c];
         }
       }
       // the two r2-half warps of a row each summed half of the r2 points of every block
-      if (r1 < P.n1) atomicAdd(&P.VH[int64_t(split) * P.vhStride + r1], vh);
+      if (r1 < n1) atomicAdd(&I->VH[int64_t(split) * I->vhStride + r1], vh);
     }
     fenceBeforeSync();
     __syncthreads();
@@ -804,15 +809,22 @@ bool makeMap(CUtensorMap * m, void * base, uint64_t inner, uint64_t outer, uint3
 }
 
 template <int NB, int RP>
-int launchFlash(tcscf_ctx * ctx, CUtensorMap const * maps, tc::Params const & P, int grid)
+int launchFlash(tcscf_ctx * ctx, tc::Params const & P, int grid)
 {
   size_t const smem = sizeof(tc::Smem<NB, RP>) + 1024;
   static_assert(sizeof(tc::Smem<NB, RP>) + 1024 <= 232448, "shared memory per CTA");
   TCSCF_CUDA(ctx, cudaFuncSetAttribute(tc::kFlashTc<NB, RP>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-  tc::kFlashTc<NB, RP><<<grid, tc::NTHREADS, smem, ctx->stream>>>(maps[0], maps[1], maps[2], maps[3], maps[4], maps[5], maps[6], maps[7],
-                                                                  maps[8], maps[9], P);
+  tc::kFlashTc<NB, RP><<<grid, tc::NTHREADS, smem, ctx->stream>>>(P);
   TCSCF_LAUNCH(ctx);
   return TCSCF_OK;
+}
+
+int launchClass(tcscf_ctx * ctx, int NB, int RP, tc::Params const & P, int grid)
+{
+  if (NB == 64 && RP == 32) return launchFlash<64, 32>(ctx, P, grid);
+  if (NB == 64 && RP == 64) return launchFlash<64, 64>(ctx, P, grid);
+  if (NB == 128 && RP == 32) return launchFlash<128, 32>(ctx, P, grid);
+  return fail(ctx, TCSCF_ERR_UNSUPPORTED, "no tensor kernel for this tile class");
 }
 
 // bytes of the packed Vt operand: h, m and l slices [NB][n2pad], then the column scales [nBlocks][NB]
@@ -868,44 +880,82 @@ bool tensorPathAvailable(Contraction const & c, int precision, std::string * why
   return true;
 }
 
-int contractTensor(tcscf_ctx * ctx, Contraction const & c, int precision)
+namespace {
+
+int smCount()
 {
-  std::string why;
-  if (!tensorPathAvailable(c, precision, &why)) return fail(ctx, TCSCF_ERR_UNSUPPORTED, why);
-  int const NB = c.ncol <= 64 ? 64 : 128;
-  int const RP = c.R <= 32 ? 32 : 64;
-  int64_t const n1pad = (c.n1 + tc::BM - 1) / tc::BM * tc::BM;
-  int64_t const n2pad = (c.n2 + tc::BK - 1) / tc::BK * tc::BK;
-  int const nTiles = int(n1pad / tc::BM);
-  int const nBlocks = int(n2pad / tc::BK);
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  // split r2 when there are fewer tiles than SMs (partials summed deterministically afterwards)
-  int nSplit = std::max(1, std::min(sms / std::max(1, nTiles), nBlocks / 4));
-  int const perSplit = (nBlocks + nSplit - 1) / nSplit;
-  nSplit = (nBlocks + perSplit - 1) / perSplit;
+  return sms;
+}
 
+struct Shape {
+  int NB, RP;
+  int64_t n1pad, n2pad;
+  int nTiles, nBlocks, nSplit, perSplit;
+};
+
+Shape shapeOf(Contraction const & c, int sms)
+{
+  Shape sh{};
+  sh.NB = c.ncol <= 64 ? 64 : 128;
+  sh.RP = c.R <= 32 ? 32 : 64;
+  sh.n1pad = (c.n1 + tc::BM - 1) / tc::BM * tc::BM;
+  sh.n2pad = (c.n2 + tc::BK - 1) / tc::BK * tc::BK;
+  sh.nTiles = int(sh.n1pad / tc::BM);
+  sh.nBlocks = int(sh.n2pad / tc::BK);
+  // split r2 when there are fewer tiles than SMs (partials summed deterministically afterwards)
+  sh.nSplit = std::max(1, std::min(sms / std::max(1, sh.nTiles), sh.nBlocks / 4));
+  sh.perSplit = (sh.nBlocks + sh.nSplit - 1) / sh.nSplit;
+  sh.nSplit = (sh.nBlocks + sh.perSplit - 1) / sh.perSplit;
+  return sh;
+}
+
+size_t align256(size_t n) { return (n + 255) & ~size_t(255); }
+
+}  // namespace
+
+size_t tensorArenaBytes(Contraction const & c)
+{
+  Shape const sh = shapeOf(c, smCount());
   size_t const bf = sizeof(__nv_bfloat16);
-  bool const haveVt = c.vtPacked != nullptr;
-  size_t const bytes = 4 * size_t(n1pad) * RP * bf + 3 * size_t(n2pad) * RP * bf + (haveVt ? 0 : packedVtBytes(NB, n2pad))
-                       + size_t(n1pad) * sizeof(float4) + size_t(n2pad) * sizeof(float4) + size_t(n1pad + n2pad) * sizeof(float) + 64
-                       + 16 * 256;
-  void * p = nullptr;
-  TCSCF_TRY(scratch(ctx, "flash_tc_ops", bytes, &p));
-  char * q = static_cast<char *>(p);
-  auto take = [&](size_t n) { char * r = q; q += (n + 255) & ~size_t(255); return r; };
+  size_t b = 4 * align256(size_t(sh.n1pad) * sh.RP * bf) + 3 * align256(size_t(sh.n2pad) * sh.RP * bf);
+  if (!c.vtPacked) b += align256(packedVtBytes(sh.NB, sh.n2pad));
+  b += align256(size_t(sh.n1pad) * sizeof(float4)) + align256(size_t(sh.n2pad) * sizeof(float4));
+  b += align256(size_t(sh.n1pad) * sizeof(float)) + align256(size_t(sh.n2pad) * sizeof(float));
+  if (sh.nSplit > 1 || !c.VH) b += align256(sizeof(double) * size_t(sh.nSplit) * c.n1 * (c.ldt + 1));
+  return b + 256;
+}
+
+int tensorPrepare(tcscf_ctx * ctx, Contraction const & c, int precision, void * arena, size_t arenaBytes, TensorPrep & tp)
+{
+  std::string why;
+  if (!tensorPathAvailable(c, precision, &why)) return fail(ctx, TCSCF_ERR_UNSUPPORTED, why);
+  TCSCF_CHECK(ctx, arenaBytes >= tensorArenaBytes(c), TCSCF_ERR_INVALID_ARGUMENT, "internal: tensor arena too small");
+  Shape const sh = shapeOf(c, smCount());
+  int const NB = sh.NB, RP = sh.RP;
+  int64_t const n1pad = sh.n1pad, n2pad = sh.n2pad;
+  size_t const bf = sizeof(__nv_bfloat16);
+  char * q = reinterpret_cast<char *>((reinterpret_cast<uintptr_t>(arena) + 255) & ~uintptr_t(255));
+  auto take = [&](size_t n) { char * r = q; q += align256(n); return r; };
   __nv_bfloat16 * psi1s[4];
   __nv_bfloat16 * psi2s[3];
   for (auto & a : psi1s) a = reinterpret_cast<__nv_bfloat16 *>(take(size_t(n1pad) * RP * bf));
   for (auto & a : psi2s) a = reinterpret_cast<__nv_bfloat16 *>(take(size_t(n2pad) * RP * bf));
-  void * vt = haveVt ? const_cast<void *>(c.vtPacked) : take(packedVtBytes(NB, n2pad));
+  void * vt = c.vtPacked ? const_cast<void *>(c.vtPacked) : take(packedVtBytes(NB, n2pad));
   auto * r1c = reinterpret_cast<float4 *>(take(size_t(n1pad) * sizeof(float4)));
   auto * r2c = reinterpret_cast<float4 *>(take(size_t(n2pad) * sizeof(float4)));
   auto * a1inv = reinterpret_cast<float *>(take(size_t(n1pad) * sizeof(float)));
   auto * a2inv = reinterpret_cast<float *>(take(size_t(n2pad) * sizeof(float)));
-  int * status = reinterpret_cast<int *>(take(64));
-  TCSCF_CHECK(ctx, size_t(q - static_cast<char *>(p)) <= bytes, TCSCF_ERR_INVALID_ARGUMENT, "internal: scratch layout");
+  double * Tout = c.T;
+  double * VHout = c.VH;
+  if (sh.nSplit > 1 || !c.VH) {
+    // split partials (and a Coulomb sink when the caller does not want the potential)
+    double * sp = reinterpret_cast<double *>(take(sizeof(double) * size_t(sh.nSplit) * c.n1 * (c.ldt + 1)));
+    if (sh.nSplit > 1) Tout = sp;
+    VHout = sp + size_t(sh.nSplit) * c.n1 * c.ldt;
+  }
   auto * vts = static_cast<__nv_bfloat16 *>(vt);   // h, m, l slices [NB][n2pad] each
   auto * cinv = reinterpret_cast<float *>(vts + 3 * size_t(NB) * n2pad);
 
@@ -916,58 +966,112 @@ int contractTensor(tcscf_ctx * ctx, Contraction const & c, int precision)
   tc::kPackPsi<<<gridBlocks(n2pad * 32, 256), 256, 0, ctx->stream>>>(c.n2, n2pad, c.R, RP, c.psi2, c.ldpsi, psi2s[0], psi2s[1], psi2s[2],
                                                                       nullptr, a2inv);
   TCSCF_LAUNCH(ctx);
-  if (!haveVt) TCSCF_TRY(packVt(ctx, c.n2, n2pad, c.ncol, NB, c.V, c.ldv, vt));
+  if (!c.vtPacked) TCSCF_TRY(packVt(ctx, c.n2, n2pad, c.ncol, NB, c.V, c.ldv, vt));
   tc::kPackCoords<<<gridBlocks(n1pad, 256), 256, 0, ctx->stream>>>(c.n1, n1pad, c.p1, r1c);
   TCSCF_LAUNCH(ctx);
   tc::kPackCoordPairs<<<gridBlocks(n2pad / 2, 256), 256, 0, ctx->stream>>>(c.n2, n2pad, c.p2, c.coul, r2c);
   TCSCF_LAUNCH(ctx);
+  TCSCF_CUDA(ctx, cudaMemsetAsync(VHout, 0, sizeof(double) * size_t(sh.nSplit) * c.n1, ctx->stream));
 
-  CUtensorMap maps[10];
   CUtensorMapSwizzle const psw = RP == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B;
   bool okm = true;
-  for (int i = 0; i < 4; ++i) okm = okm && makeMap(&maps[i], psi1s[i], RP, n1pad, RP, tc::BM, psw);
+  for (int i = 0; i < 4; ++i) okm = okm && makeMap(&tp.maps[i], psi1s[i], RP, n1pad, RP, tc::BM, psw);
   for (int i = 0; i < 3; ++i) {
-    okm = okm && makeMap(&maps[4 + i], psi2s[i], RP, n2pad, RP, tc::BK, psw);
-    okm = okm && makeMap(&maps[7 + i], vts + size_t(i) * NB * n2pad, n2pad, NB, tc::BK, NB, CU_TENSOR_MAP_SWIZZLE_128B);
+    okm = okm && makeMap(&tp.maps[4 + i], psi2s[i], RP, n2pad, RP, tc::BK, psw);
+    okm = okm && makeMap(&tp.maps[7 + i], vts + size_t(i) * NB * n2pad, n2pad, NB, tc::BK, NB, CU_TENSOR_MAP_SWIZZLE_128B);
   }
   TCSCF_CHECK(ctx, okm, TCSCF_ERR_CUDA, "cuTensorMapEncodeTiled failed");
 
-  double * Tout = c.T;
-  double * VHout = c.VH;
-  void * sp = nullptr;
-  if (nSplit > 1 || !c.VH) {
-    // split partials (and a Coulomb sink when the caller does not want the potential)
-    TCSCF_TRY(scratch(ctx, "flash_tc_split", sizeof(double) * size_t(nSplit) * c.n1 * (c.ldt + 1), &sp));
-    if (nSplit > 1) Tout = static_cast<double *>(sp);
-    VHout = static_cast<double *>(sp) + size_t(nSplit) * c.n1 * c.ldt;
+  tc::Instance & I = tp.inst;
+  I = tc::Instance{};
+  I.nTiles = sh.nTiles; I.nSplit = sh.nSplit; I.blocksPerSplit = sh.perSplit; I.nBlocks = sh.nBlocks;
+  I.n1 = int(c.n1); I.nb = c.ncol; I.ldt = c.ldt;
+  I.r1xyz = r1c; I.r2pairs = r2c; I.a1inv = a1inv; I.a2inv = a2inv; I.cinv = cinv;
+  I.T = Tout; I.VH = VHout;
+  I.tStride = int64_t(c.n1) * c.ldt; I.vhStride = c.n1;
+  tp.NB = NB; tp.RP = RP;
+  tp.c = c;
+  return TCSCF_OK;
+}
+
+int tensorRun(tcscf_ctx * ctx, TensorPrep * const * preps, int count)
+{
+  int const sms = smCount();
+  // instance table and tensor maps in device memory (maps 64-byte aligned), then the work items
+  size_t const instBytes = align256(sizeof(tc::Instance) * count);
+  size_t const mapBytes = align256(sizeof(CUtensorMap) * tc::kMapsPerInstance * count);
+  size_t itemsTotal = 0;
+  for (int k = 0; k < count; ++k) itemsTotal += size_t(preps[k]->inst.nTiles) * preps[k]->inst.nSplit;
+  void * p = nullptr;
+  TCSCF_TRY(scratch(ctx, "flash_tc_table", instBytes + mapBytes + align256(sizeof(int4) * itemsTotal) + 256, &p));
+  auto * dInst = static_cast<tc::Instance *>(p);
+  auto * dMaps = reinterpret_cast<CUtensorMap *>(static_cast<char *>(p) + instBytes);
+  auto * dItems = reinterpret_cast<int4 *>(static_cast<char *>(p) + instBytes + mapBytes);
+  int * dStatus = reinterpret_cast<int *>(static_cast<char *>(p) + instBytes + mapBytes + align256(sizeof(int4) * itemsTotal));
+  std::vector<tc::Instance> hInst(count);
+  std::vector<CUtensorMap> hMaps(size_t(count) * tc::kMapsPerInstance);
+  for (int k = 0; k < count; ++k) {
+    hInst[k] = preps[k]->inst;
+    hInst[k].maps = dMaps + size_t(k) * tc::kMapsPerInstance;
+    for (int m = 0; m < tc::kMapsPerInstance; ++m) hMaps[size_t(k) * tc::kMapsPerInstance + m] = preps[k]->maps[m];
   }
-  TCSCF_CUDA(ctx, cudaMemsetAsync(VHout, 0, sizeof(double) * size_t(nSplit) * c.n1, ctx->stream));
-  TCSCF_CUDA(ctx, cudaMemsetAsync(status, 0, sizeof(int), ctx->stream));
+  TCSCF_CUDA(ctx, cudaMemcpyAsync(dInst, hInst.data(), sizeof(tc::Instance) * count, cudaMemcpyHostToDevice, ctx->stream));
+  TCSCF_CUDA(ctx, cudaMemcpyAsync(dMaps, hMaps.data(), sizeof(CUtensorMap) * hMaps.size(), cudaMemcpyHostToDevice, ctx->stream));
+  TCSCF_CUDA(ctx, cudaMemsetAsync(dStatus, 0, sizeof(int), ctx->stream));
 
-  tc::Params P{};
-  P.nTiles = nTiles; P.nSplit = nSplit; P.blocksPerSplit = perSplit; P.nBlocks = nBlocks;
-  P.n1 = int(c.n1); P.nb = c.ncol;
-  P.r1xyz = r1c; P.r2pairs = r2c; P.a1inv = a1inv; P.a2inv = a2inv; P.cinv = cinv;
-  P.T = Tout; P.VH = VHout; P.ldt = c.ldt;
-  P.tStride = int64_t(c.n1) * c.ldt; P.vhStride = c.n1; P.status = status;
-  int const grid = std::min(nTiles * nSplit, sms);
-  // the contraction kernel alone is bracketed by the context's timing events (tcscf_last_timing)
+  // one persistent launch per tile class; within it, work items longest first, dealt round-robin
+  std::vector<int4> hItems;
+  hItems.reserve(itemsTotal);
+  size_t offset = 0;
   cudaEventRecord(ctx->ev[2], ctx->stream);
-  if (NB == 64 && RP == 32) TCSCF_TRY((launchFlash<64, 32>(ctx, maps, P, grid)));
-  else if (NB == 64) TCSCF_TRY((launchFlash<64, 64>(ctx, maps, P, grid)));
-  else TCSCF_TRY((launchFlash<128, 32>(ctx, maps, P, grid)));
+  for (int cls = 0; cls < 3; ++cls) {
+    int const NB = cls == 2 ? 128 : 64, RP = cls == 1 ? 64 : 32;
+    std::vector<int4> items;
+    for (int k = 0; k < count; ++k) {
+      if (preps[k]->NB != NB || preps[k]->RP != RP) continue;
+      tc::Instance const & I = preps[k]->inst;
+      for (int t = 0; t < I.nTiles; ++t)
+        for (int sp = 0; sp < I.nSplit; ++sp) items.push_back(make_int4(k, t, sp, std::min(I.nBlocks - sp * I.blocksPerSplit, I.blocksPerSplit)));
+    }
+    if (items.empty()) continue;
+    std::stable_sort(items.begin(), items.end(), [](int4 const & a, int4 const & b) { return a.w > b.w; });
+    TCSCF_CUDA(ctx, cudaMemcpyAsync(dItems + offset, items.data(), sizeof(int4) * items.size(), cudaMemcpyHostToDevice, ctx->stream));
+    tc::Params P{};
+    P.nItems = int(items.size());
+    P.items = count == 1 ? nullptr : dItems + offset;
+    P.inst = dInst;
+    P.status = dStatus;
+    TCSCF_TRY(launchClass(ctx, NB, RP, P, std::min(int(items.size()), sms)));
+    offset += items.size();
+  }
   cudaEventRecord(ctx->ev[3], ctx->stream);
-
   int st = 0;
-  TCSCF_CUDA(ctx, cudaMemcpyAsync(&st, status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  TCSCF_CUDA(ctx, cudaMemcpyAsync(&st, dStatus, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   if (st != 0) return fail(ctx, TCSCF_ERR_TIMEOUT, "tensor-core contraction: bounded wait expired (code " + std::to_string(st) + ")");
-  if (nSplit > 1) {
-    int64_t const n = int64_t(c.n1) * c.ncol;
-    TCSCF_TRY(sumSplitsLaunch(ctx, n, nSplit, int64_t(c.n1) * c.ldt, Tout, c.T, c.n1, c.ncol, c.ldt, c.ldt));
-    if (c.VH) TCSCF_TRY(sumSplitsLaunch(ctx, c.n1, nSplit, c.n1, VHout, c.VH, c.n1, 1, 1, 1));
+  for (int k = 0; k < count; ++k) {
+    tc::Instance const & I = preps[k]->inst;
+    Contraction const & c = preps[k]->c;
+    if (I.nSplit > 1) {
+      int64_t const n = int64_t(c.n1) * c.ncol;
+      TCSCF_TRY(sumSplitsLaunch(ctx, n, I.nSplit, int64_t(c.n1) * c.ldt, I.T, c.T, c.n1, c.ncol, c.ldt, c.ldt));
+      if (c.VH) TCSCF_TRY(sumSplitsLaunch(ctx, c.n1, I.nSplit, c.n1, I.VH, c.VH, c.n1, 1, 1, 1));
+    }
   }
   return TCSCF_OK;
+}
+
+int contractTensor(tcscf_ctx * ctx, Contraction const & c, int precision)
+{
+  std::string why;
+  if (!tensorPathAvailable(c, precision, &why)) return fail(ctx, TCSCF_ERR_UNSUPPORTED, why);
+  size_t const bytes = tensorArenaBytes(c);
+  void * p = nullptr;
+  TCSCF_TRY(scratch(ctx, "flash_tc_ops", bytes, &p));
+  TensorPrep tp;
+  TCSCF_TRY(tensorPrepare(ctx, c, precision, p, bytes, tp));
+  TensorPrep * one = &tp;
+  return tensorRun(ctx, &one, 1);
 }
 
 }  // namespace tcscf

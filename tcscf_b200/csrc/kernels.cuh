@@ -1,6 +1,8 @@
 // Internal launcher interfaces shared by the translation units of libtcscf_gpu.so.
 #pragma once
 
+#include <cuda.h>
+
 #include "common.cuh"
 
 namespace tcscf {
@@ -43,6 +45,41 @@ int tensorPackedV(tcscf_ctx * ctx, Grid & g2, const double * V, double scale, co
 // written back masked
 int finalizeLaunch(tcscf_ctx * ctx, int nspin, int nb, const double * h, double2 * G, const double2 * G3, const double2 * D, int respectSym,
                    double factor, double2 * fock, double * energy);
+
+// One contraction problem as the tensor kernel sees it (device pointers); a launch covers one or many
+// of them (batched builds), all with the same tile shapes NB, RP.
+struct TensorInstance {
+  int nTiles, nSplit, blocksPerSplit, nBlocks;   // r1 tiles; r2 splits; r2 blocks per split and in total
+  int n1;                                          // real r1 rows
+  int nb;                                          // real columns of T
+  int ldt, pad;
+  const float4 * r1xyz;                            // [n1pad] x, y, z, 0
+  const float4 * r2pairs;                          // [nBlocks*64] r2 points in pair layout
+  const float * a1inv;                             // [n1pad] 1 / psi1 row scale
+  const float * a2inv;                             // [nBlocks*64] 1 / psi2 row scale
+  const float * cinv;                              // [nBlocks][NB] 1 / Vt column scale
+  double * T;                                      // [nSplit][n1][ldt]
+  double * VH;                                     // [nSplit][n1]
+  int64_t tStride, vhStride;
+  const CUtensorMap * maps;                        // device memory, 64-byte aligned: psi1 h/m/l/m/256, psi2 h/m/l, Vt h/m/l
+};
+constexpr int kTensorMapsPerInstance = 10;
+
+// a contraction whose operands are packed (tensorPrepare) and ready for tensorRun
+struct TensorPrep {
+  int NB = 0, RP = 0;
+  Contraction c;
+  TensorInstance inst{};
+  CUtensorMap maps[kTensorMapsPerInstance];
+};
+
+// Batched tensor contractions: the operands of one contraction are packed into a caller-provided
+// device arena of tensorArenaBytes(c) bytes (tensorPrepare); any number of prepared contractions then
+// run in one persistent launch per tile class (tensorRun), which also sums the r2-split partials
+// into c.T / c.VH.
+size_t tensorArenaBytes(Contraction const & c);
+int tensorPrepare(tcscf_ctx * ctx, Contraction const & c, int precision, void * arena, size_t arenaBytes, TensorPrep & tp);
+int tensorRun(tcscf_ctx * ctx, TensorPrep * const * preps, int count);
 
 // out[r][c] = sum_s part[s*stride + r*ldPart + c] for r < rows, c < cols (deterministic split sum)
 int sumSplitsLaunch(tcscf_ctx * ctx, int64_t n, int nsplit, int64_t stride, const double * part, double * out, int64_t rows, int cols,

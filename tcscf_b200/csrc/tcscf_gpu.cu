@@ -775,6 +775,124 @@ int fockBuildDevice(tcscf_ctx * ctx, Grid & g1, Grid & g2, int nspin, const doub
   return TCSCF_OK;
 }
 
+// Batched RCS Fock builds (tcscf_fock_build_batch): every instance's density is factored and its
+// tensor operands packed into its own arena; then all tensor contractions run in one persistent
+// launch per tile class, and each instance's Fock matrix and energy are finished.  Instances whose
+// density factor is complex in the real-harmonic basis, or whose shape the tensor path does not
+// take, are built on their own with fockBuildDevice.
+int fockBuildBatch(tcscf_ctx * ctx, int count, Grid * const * g1s, Grid * const * g2s, const double2 * const * dDs, const double * const * dHs,
+                   int respectSym, int precision, double2 * const * dGs, double2 * const * dFs, double * const * dEs)
+{
+  cudaEventRecord(ctx->ev[0], ctx->stream);
+  int const launch0 = ctx->launchCount;
+  // shared temporaries (consumed in stream order by each instance's packing before the next reuses them)
+  int64_t maxN1 = 0, maxN2 = 0;
+  int maxNb = 0;
+  for (int k = 0; k < count; ++k) {
+    maxN1 = std::max(maxN1, g1s[k]->n);
+    maxN2 = std::max(maxN2, g2s[k]->n);
+    maxNb = std::max(maxNb, g1s[k]->nb);
+  }
+  size_t const tmpBytes = sizeof(double) * (size_t(maxN2) * maxNb + size_t(maxN1) * maxNb + 2 * size_t(maxN2) * maxNb + size_t(maxN2));
+  void * tp = nullptr;
+  TCSCF_TRY(scratch(ctx, "batch_tmp", tmpBytes, &tp));
+  double * V = static_cast<double *>(tp);
+  double * psi1 = V + size_t(maxN2) * maxNb;
+  double * psi2 = psi1 + size_t(maxN1) * maxNb;
+  double * psi1at2 = psi2 + size_t(maxN2) * maxNb;
+  double * coul = psi1at2 + size_t(maxN2) * maxNb;
+
+  // per-instance persistent buffers: T, VH, GR and the tensor arena
+  std::vector<Contraction> cs(count);
+  std::vector<char> tensorOk(count, 0);
+  std::vector<size_t> offs(count + 1, 0);
+  std::vector<size_t> arenaBytes(count, 0);
+  for (int k = 0; k < count; ++k) {
+    Grid & g1 = *g1s[k];
+    Grid & g2 = *g2s[k];
+    int const nb = g1.nb;
+    Contraction & c = cs[k];
+    c.n1 = g1.n; c.n2 = g2.n; c.R = std::min(nb, 32); c.ncol = nb; c.ldpsi = nb; c.ldt = nb;
+    c.p1 = g1.pts; c.p2 = g2.pts;
+    arenaBytes[k] = tensorArenaBytes(c);
+    size_t const own = (sizeof(double) * (size_t(g1.n) * nb + g1.n + size_t(nb) * nb) + 255) & ~size_t(255);
+    offs[k + 1] = offs[k] + own + ((arenaBytes[k] + 255) & ~size_t(255));
+  }
+  void * bp = nullptr;
+  TCSCF_TRY(scratch(ctx, "batch_arena", offs[count] + 256, &bp));
+  std::vector<TensorPrep> preps(count);
+  std::vector<TensorPrep *> ready;
+  for (int k = 0; k < count; ++k) {
+    Grid & g1 = *g1s[k];
+    Grid & g2 = *g2s[k];
+    int const nb = g1.nb;
+    int64_t const n1 = g1.n, n2 = g2.n;
+    double const scale = g2.ndim == 2 ? 2 * kPi : 1.0;
+    char * base = static_cast<char *>(bp) + offs[k];
+    double * T = reinterpret_cast<double *>(base);
+    double * VH = T + size_t(n1) * nb;
+    double * GR = VH + n1;
+    void * arena = base + ((sizeof(double) * (size_t(n1) * nb + n1 + size_t(nb) * nb) + 255) & ~size_t(255));
+    Factor f;
+    TCSCF_TRY(factorDensity(ctx, g1, dDs[k], 0, f));
+    Contraction & c = cs[k];
+    c.R = f.R;
+    c.T = T; c.VH = VH; c.V = V; c.ldv = nb;
+    c.psi1 = psi1; c.psi2 = psi2; c.coul = coul;
+    std::string why;
+    bool const eligible = precision == TCSCF_PREC_BF16X3 && f.R > 0 && !f.complex && tensorPathAvailable(c, precision, &why) &&
+                          tensorArenaBytes(c) <= arenaBytes[k];
+    if (!eligible) continue;
+    kWeightedBasis<<<gridBlocks(n2 * nb, 256), 256, 0, ctx->stream>>>(n2, nb, g2.phiR, g2.w, scale, V);
+    TCSCF_LAUNCH(ctx);
+    const void * vtPacked = nullptr;
+    TCSCF_TRY(tensorPackedV(ctx, g2, V, scale, &vtPacked));
+    c.vtPacked = vtPacked;
+    size_t const sm = sizeof(double) * size_t(nb) * f.R;
+    kOrbitals<<<gridBlocks(n1 * f.R, 256), 256, sm, ctx->stream>>>(n1, nb, f.R, g1.phiR, f.X1, f.ldx, psi1, nb);
+    TCSCF_LAUNCH(ctx);
+    kOrbitals<<<gridBlocks(n2 * f.R, 256), 256, sm, ctx->stream>>>(n2, nb, f.R, g2.phiR, f.X2, f.ldx, psi2, nb);
+    TCSCF_LAUNCH(ctx);
+    kOrbitals<<<gridBlocks(n2 * f.R, 256), 256, sm, ctx->stream>>>(n2, nb, f.R, g2.phiR, f.X1, f.ldx, psi1at2, nb);
+    TCSCF_LAUNCH(ctx);
+    kCoulombSource<<<gridBlocks(n2, 256), 256, 0, ctx->stream>>>(n2, f.R, psi1at2, psi2, nb, g2.w, scale, coul);
+    TCSCF_LAUNCH(ctx);
+    TCSCF_TRY(tensorPrepare(ctx, c, precision, arena, arenaBytes[k], preps[k]));
+    tensorOk[k] = 1;
+    ready.push_back(&preps[k]);
+  }
+  if (!ready.empty()) TCSCF_TRY(tensorRun(ctx, ready.data(), int(ready.size())));
+  float contractionMs = 0;
+  if (!ready.empty()) {
+    TCSCF_CUDA(ctx, cudaEventSynchronize(ctx->ev[3]));
+    cudaEventElapsedTime(&contractionMs, ctx->ev[2], ctx->ev[3]);
+  }
+  for (int k = 0; k < count; ++k) {
+    Grid & g1 = *g1s[k];
+    int const nb = g1.nb;
+    if (!tensorOk[k]) {
+      TCSCF_TRY(fockBuildDevice(ctx, g1, *g2s[k], 1, dDs[k], dHs[k], respectSym, precision, dGs[k], dFs[k], dEs[k]));
+      continue;
+    }
+    Contraction const & c = cs[k];
+    double * GR = c.VH + g1.n;
+    TCSCF_CUDA(ctx, cudaMemsetAsync(GR, 0, sizeof(double) * nb * nb, ctx->stream));
+    TCSCF_TRY(reduceFockReal(ctx, g1.n, nb, g1.phiR, g1.w, c.VH, 2.0, c.T, nb, 1.0, GR));
+    kRealToReference<<<gridBlocks(int64_t(nb) * nb, 256), 256, 0, ctx->stream>>>(1, nb, g1.dsto, GR, nullptr, dGs[k]);
+    TCSCF_LAUNCH(ctx);
+    kFinalize<<<1, 512, 0, ctx->stream>>>(1, nb, dHs[k], dGs[k], nullptr, dDs[k], respectSym, 2.0, dFs[k], dEs[k]);
+    TCSCF_LAUNCH(ctx);
+  }
+  cudaEventRecord(ctx->ev[1], ctx->stream);
+  TCSCF_CUDA(ctx, cudaEventSynchronize(ctx->ev[1]));
+  float tot = 0;
+  cudaEventElapsedTime(&tot, ctx->ev[0], ctx->ev[1]);
+  ctx->lastTotalMs = tot;
+  ctx->lastContractionMs = contractionMs;
+  ctx->lastLaunches = ctx->launchCount - launch0;
+  return TCSCF_OK;
+}
+
 int validateBasis(tcscf_ctx * ctx, const tcscf_sto * basis, int nb, std::vector<DevSto> & out)
 {
   TCSCF_CHECK(ctx, basis && nb > 0, TCSCF_ERR_INVALID_ARGUMENT, "empty basis");
@@ -1205,6 +1323,54 @@ int tcscf_tensor_destroy(tcscf_ctx * ctx, int handle)
   cudaStreamSynchronize(ctx->stream);
   cudaFree(it->second.d);
   ctx->tensors.erase(it);
+  return TCSCF_OK;
+}
+
+int tcscf_fock_build_batch(tcscf_ctx * ctx, int count, const int * r1, const int * r2, const double * const * density,
+                           const double * const * h, int respect_symmetry, int precision, double * energy, double * const * fock)
+{
+  if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  TCSCF_CHECK(ctx, count >= 1 && r1 && r2 && density && h && energy, TCSCF_ERR_INVALID_ARGUMENT, "batch: count, grids, densities, h and energy are required");
+  TCSCF_CHECK(ctx, precision == TCSCF_PREC_FP64 || precision == TCSCF_PREC_BF16X3, TCSCF_ERR_INVALID_ARGUMENT, "unknown precision");
+  std::vector<Grid *> g1s(count), g2s(count);
+  size_t io = 0;
+  for (int k = 0; k < count; ++k) {
+    g1s[k] = findGrid(ctx, r1[k]);
+    g2s[k] = findGrid(ctx, r2[k]);
+    TCSCF_TRY(checkBasisPair(ctx, g1s[k], g2s[k]));
+    TCSCF_CHECK(ctx, density[k] && h[k], TCSCF_ERR_INVALID_ARGUMENT, "batch: every instance needs a density and h");
+    size_t const nn = size_t(g1s[k]->nb) * g1s[k]->nb;
+    io += sizeof(double2) * 3 * nn + sizeof(double) * nn + 256;
+  }
+  void * p = nullptr;
+  TCSCF_TRY(scratch(ctx, "batch_io", io + sizeof(double) * count + 256, &p));
+  std::vector<const double2 *> dD(count);
+  std::vector<const double *> dH(count);
+  std::vector<double2 *> dG(count), dF(count);
+  std::vector<double *> dE(count);
+  char * q = static_cast<char *>(p);
+  double * energies = reinterpret_cast<double *>(q);
+  q += (sizeof(double) * count + 255) & ~size_t(255);
+  for (int k = 0; k < count; ++k) {
+    size_t const nn = size_t(g1s[k]->nb) * g1s[k]->nb;
+    auto * d = reinterpret_cast<double2 *>(q);
+    dD[k] = d; dG[k] = d + nn; dF[k] = d + 2 * nn;
+    auto * hh = reinterpret_cast<double *>(d + 3 * nn);
+    dH[k] = hh;
+    dE[k] = energies + k;
+    q += (sizeof(double2) * 3 * nn + sizeof(double) * nn + 255) & ~size_t(255);
+    TCSCF_CUDA(ctx, cudaMemcpyAsync(d, density[k], sizeof(double2) * nn, cudaMemcpyHostToDevice, ctx->stream));
+    TCSCF_CUDA(ctx, cudaMemcpyAsync(hh, h[k], sizeof(double) * nn, cudaMemcpyHostToDevice, ctx->stream));
+  }
+  TCSCF_TRY(fockBuildBatch(ctx, count, g1s.data(), g2s.data(), dD.data(), dH.data(), respect_symmetry, precision, dG.data(), dF.data(), dE.data()));
+  TCSCF_CUDA(ctx, cudaMemcpyAsync(energy, energies, sizeof(double) * count, cudaMemcpyDeviceToHost, ctx->stream));
+  for (int k = 0; k < count; ++k)
+    if (fock && fock[k])
+      TCSCF_CUDA(ctx, cudaMemcpyAsync(fock[k], dF[k], sizeof(double2) * g1s[k]->nb * g1s[k]->nb, cudaMemcpyDeviceToHost, ctx->stream));
+  TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  for (int k = 0; k < count; ++k)
+    if (!(energy[k] == energy[k]) || std::isinf(energy[k])) return fail(ctx, TCSCF_ERR_NONFINITE, "non-finite energy in batch instance " + std::to_string(k));
   return TCSCF_OK;
 }
 
