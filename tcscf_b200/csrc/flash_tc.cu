@@ -43,8 +43,12 @@ constexpr int BM = 128;        // r1 rows per tile
 constexpr int BK = 64;         // r2 points per block
 // TMA stages: three when the tile shapes leave room in shared memory
 __host__ __device__ constexpr int stagesFor(int NB, int RP) { return NB == 64 && RP == 32 ? 3 : 2; }
-// X tile buffers: two (GEMM2 of block g - 1 overlaps the writing of block g) where shared memory allows
-__host__ __device__ constexpr int xBuffersFor(int NB, int RP) { return NB == 64 && RP == 64 ? 1 : 2; }
+// X precision: XS = 2 slices (16 bits, u s in [2^15, 2^16)) or XS = 3 (24 bits, stored as the four
+// slices h, m, l/256, m/256); its tile buffers: two (GEMM2 of block g - 1 overlaps the writing of
+// block g) where shared memory allows
+__host__ __device__ constexpr int xSlicesFor(int XS) { return XS == 3 ? 4 : 2; }
+__host__ __device__ constexpr int xBuffersFor(int NB, int RP, int XS) { return XS == 3 || (NB == 64 && RP == 64) ? 1 : 2; }
+__host__ __device__ constexpr int xExpFor(int XS) { return XS == 3 ? 23 : 15; }
 constexpr int NCW = 8;         // compute warps
 constexpr int NTHREADS = 384;  // warpgroup 0: TMA, MMA, 2 idle warps; warpgroups 1-2: compute
 // register split: 384 threads x 168 at launch = 64512 = 128 x 56 (producer warpgroup) + 256 x 224
@@ -58,7 +62,6 @@ constexpr uint32_t kSuspendHintNs = 1000000;
 // the three-slice factors, 15 for the two-slice X; entries of a row whose maximum is below
 // 2^kMinExp are sliced against 2^kMinExp
 constexpr int kFactorExp = 23;
-constexpr int kXExp = 15;
 constexpr int kMinExp = -100;
 
 // TMEM columns: rho buffers b = 0, 1 at 128 b (hi*hi) and 128 b + 64 (cross); T at TCOL0 (hi*hi) and
@@ -66,12 +69,12 @@ constexpr int kMinExp = -100;
 constexpr uint32_t TCOL0 = 256;
 
 // RP: padded rank of rho (GEMM1 K): 32 (64-byte rows, 64B swizzle) or 64 (128-byte rows, 128B swizzle)
-template <int NB, int RP>
+template <int NB, int RP, int XS>
 struct __align__(1024) Smem {
   static constexpr int NSTAGE = stagesFor(NB, RP);
   uint8_t v[NSTAGE][3][NB * BK * 2];       // Vt block h / m / l/256: SW128 K-major [NB rows][64]
-  static constexpr int XBUF = xBuffersFor(NB, RP);
-  uint8_t x[XBUF][2][BM * BK * 2];         // X tile h / l per buffer: SW128 K-major [128 rows][64]
+  static constexpr int XBUF = xBuffersFor(NB, RP, XS);
+  uint8_t x[XBUF][xSlicesFor(XS)][BM * BK * 2];   // X tile slices per buffer: SW128 K-major [128 rows][64]
   uint8_t psi2[NSTAGE][3][BK * RP * 2];    // psi2 block h / m / l/256: K-major [64 rows][RP]
   uint8_t psi1[4][BM * RP * 2];            // psi1 tile h / m / l/256 / m/256: K-major [128 rows][RP]
   float4 coords[NSTAGE][BK];               // r2 block as 32 pairs {x0,x1,y0,y1}{z0,z1,c0,c1}
@@ -328,14 +331,16 @@ __device__ __forceinline__ bool flushBlock(SmemT & S, uint32_t taddr, uint32_t f
 }
 
 // ---- the kernel ------------------------------------------------------------------------------------
-template <int NB, int RP>
+template <int NB, int RP, int XS>
 __global__ void __launch_bounds__(NTHREADS, 1)
     kFlashTc(Params P)
 {
   extern __shared__ uint8_t smemRaw[];
-  Smem<NB, RP> & S = *reinterpret_cast<Smem<NB, RP> *>((reinterpret_cast<uintptr_t>(smemRaw) + 1023) & ~uintptr_t(1023));
+  Smem<NB, RP, XS> & S = *reinterpret_cast<Smem<NB, RP, XS> *>((reinterpret_cast<uintptr_t>(smemRaw) + 1023) & ~uintptr_t(1023));
   constexpr int NSTAGE = stagesFor(NB, RP);
-  constexpr int XBUF = xBuffersFor(NB, RP);
+  constexpr int XBUF = xBuffersFor(NB, RP, XS);
+  constexpr int XSL = xSlicesFor(XS);
+  constexpr int kXExp = xExpFor(XS);
   int const warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   volatile int * abortFlag = &S.abort;
 
@@ -467,15 +472,27 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           if (!(ok = waitBar(&S.xfull[xb], (g / XBUF) & 1, abortFlag, P.status, 25))) break;
           fenceAfterSync();
           uint32_t const dHH = tmem + TCOL0, dX = dHH + NB;
-          uint32_t const aX[2] = {smemAddr(S.x[xb][0]), smemAddr(S.x[xb][1])};
+          uint32_t aX[XSL];
+#pragma unroll
+          for (int k = 0; k < XSL; ++k) aX[k] = smemAddr(S.x[xb][k]);
           uint32_t const bV[3] = {smemAddr(S.v[s][0]), smemAddr(S.v[s][1]), smemAddr(S.v[s][2])};
+          auto dxa = [&](int sl, int k) { return smemDesc(aX[sl] + 32 * k, 1024, 2); };
+          auto dvb = [&](int sl, int k) { return smemDesc(bV[sl] + 32 * k, 1024, 2); };
 #pragma unroll
           for (int k = 0; k < BK / 16; ++k) {
             uint32_t const acc = k > 0 ? 1u : 0u;
-            // B: hX mV + lX hV + hX lV/256; A: hX hV
-            mmaBf16(dHH, smemDesc(aX[0] + 32 * k, 1024, 2), smemDesc(bV[0] + 32 * k, 1024, 2), idesc2x2, acc);   // A += hX hV, B += hX mV
-            mmaBf16(dX, smemDesc(aX[1] + 32 * k, 1024, 2), smemDesc(bV[0] + 32 * k, 1024, 2), idesc2, 1);
-            mmaBf16(dX, smemDesc(aX[0] + 32 * k, 1024, 2), smemDesc(bV[2] + 32 * k, 1024, 2), idesc2, 1);
+            mmaBf16(dHH, dxa(0, k), dvb(0, k), idesc2x2, acc);   // A += hX hV, B += hX mV
+            if constexpr (XS == 3) {
+              // B += mX hV + hX lV/256 + m/256 mV + l/256 hV
+              mmaBf16(dX, dxa(1, k), dvb(0, k), idesc2, 1);
+              mmaBf16(dX, dxa(0, k), dvb(2, k), idesc2, 1);
+              mmaBf16(dX, dxa(3, k), dvb(1, k), idesc2, 1);
+              mmaBf16(dX, dxa(2, k), dvb(0, k), idesc2, 1);
+            } else {
+              // B += lX hV + hX lV/256
+              mmaBf16(dX, dxa(1, k), dvb(0, k), idesc2, 1);
+              mmaBf16(dX, dxa(0, k), dvb(2, k), idesc2, 1);
+            }
           }
           mmaCommit(&S.xfree[xb]);
           mmaCommit(&S.empty[s]);
@@ -511,6 +528,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     double acc[NB / 2];
     uint64_t const k256 = f2pack(256.0f, 256.0f), kInv256 = f2pack(1.0f / 256.0f, 1.0f / 256.0f), kM256 = f2pack(-256.0f, -256.0f);
     uint64_t const kMagic = f2pack(12582912.0f, 12582912.0f);   // 1.5 * 2^23: adding it rounds |x| < 2^22 to an integer
+    uint64_t const kInv65536 = f2pack(1.0f / 65536.0f, 1.0f / 65536.0f), kM65536 = f2pack(-65536.0f, -65536.0f);
     uint64_t const mOne = f2pack(-1.0f, -1.0f), mHalf = f2pack(-0.5f, -0.5f);
     for (int item = blockIdx.x; item < nItems && ok; item += gridDim.x) {
       int ii, tile, split;
@@ -522,8 +540,9 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       int const r1 = tile * BM + row;
       float4 const p1 = I->r1xyz[r1];
       // rho = 2^24 a1inv a2inv (256 A + B), X' = g a2inv (256 A + B) = X / (2^24 a1inv), and a block's
-      // sum_r2 X' Vt = 2^16 (256 A + B) / (bs c): T += 2^40 a1inv / bs * cinv (256 A + B)
-      double const rowA = 1099511627776.0 * double(I->a1inv[r1]);
+      // sum_r2 X' Vt = 2^16 (256 A + B) / (bs c) (XS = 2) or 2^24 (256 A + B) / (bs c) (XS = 3):
+      // T += 2^40 (or 2^48) a1inv / bs * cinv (256 A + B)
+      double const rowA = (XS == 3 ? 281474976710656.0 : 1099511627776.0) * double(I->a1inv[r1]);   // 2^48 or 2^40
 #pragma unroll
       for (int c = 0; c < NB / 2; ++c) acc[c] = 0.0;
       double vh = 0.0;
@@ -594,7 +613,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         if (lane == 0) mbarArrive(&S.rmax[b][quarter]);
         if (!(ok = waitBar(&S.rmax[b][quarter], (g >> 1) & 1, abortFlag, P.status, 35))) break;
         mx = fmaxf(mx, S.rowmax[b][half ^ 1][row]);
-        // scale bs = 2^(15 - E), E = floor(log2 mx) (clamped below), so |X' bs| < 2^16
+        // scale bs = 2^(kXExp - E), E = floor(log2 mx) (clamped below), so |X' bs| < 2^(kXExp + 1)
         int const E = max(int((__float_as_uint(mx) >> 23) & 0xFF) - 127, kMinExp);
         float const bs = __uint_as_float(uint32_t(127 + kXExp - E) << 23);
         double const binv = __longlong_as_double(int64_t(1023 + E - kXExp) << 52);
@@ -602,24 +621,44 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         // X buffer xb is free once GEMM2 of block g - XBUF completed
         int const xb = g % XBUF;
         if (g >= uint32_t(XBUF) && !(ok = waitBar(&S.xfree[xb], ((g / XBUF) - 1) & 1, abortFlag, P.status, 34))) break;
-        // slices: t = X' bs = 256 h + l, h = rint(t / 256), l = rint(t - 256 h)
         uint64_t const bb = f2pack(bs, bs);
-        uint8_t * xhi = S.x[xb][0];
-        uint8_t * xlo = S.x[xb][1];
 #pragma unroll
         for (int ch = 0; ch < 4; ++ch) {
-          uint32_t hi[4], lo[4];
-#pragma unroll
-          for (int e = 0; e < 4; ++e) {
-            uint64_t const t = f2mul(xv[ch * 4 + e], bb);
-            uint64_t const h = f2sub(f2fma(t, kInv256, kMagic), kMagic);
-            uint64_t const l = f2sub(f2add(f2fma(h, kM256, t), kMagic), kMagic);
-            hi[e] = bf16PairExact(h);
-            lo[e] = bf16PairExact(l);
-          }
           uint32_t const off = sw128(row, half * 4 + ch);
-          *reinterpret_cast<uint4 *>(xhi + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-          *reinterpret_cast<uint4 *>(xlo + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+          if constexpr (XS == 3) {
+            // t = X' bs = 65536 h + 256 m + l: h = rint(t / 65536), m = rint(r / 256), l = rint(r - 256 m),
+            // r = t - 65536 h; slices h, m, l/256, m/256
+            uint32_t sh[4], sm[4], sl[4], sms[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              uint64_t const t = f2mul(xv[ch * 4 + e], bb);
+              uint64_t const h = f2sub(f2fma(t, kInv65536, kMagic), kMagic);
+              uint64_t const r = f2fma(h, kM65536, t);
+              uint64_t const m = f2sub(f2fma(r, kInv256, kMagic), kMagic);
+              uint64_t const l = f2sub(f2add(f2fma(m, kM256, r), kMagic), kMagic);
+              sh[e] = bf16PairExact(h);
+              sm[e] = bf16PairExact(m);
+              sl[e] = bf16PairExact(f2mul(l, kInv256));
+              sms[e] = bf16PairExact(f2mul(m, kInv256));
+            }
+            *reinterpret_cast<uint4 *>(S.x[xb][0] + off) = make_uint4(sh[0], sh[1], sh[2], sh[3]);
+            *reinterpret_cast<uint4 *>(S.x[xb][1] + off) = make_uint4(sm[0], sm[1], sm[2], sm[3]);
+            *reinterpret_cast<uint4 *>(S.x[xb][2] + off) = make_uint4(sl[0], sl[1], sl[2], sl[3]);
+            *reinterpret_cast<uint4 *>(S.x[xb][3] + off) = make_uint4(sms[0], sms[1], sms[2], sms[3]);
+          } else {
+            // t = X' bs = 256 h + l, h = rint(t / 256), l = rint(t - 256 h)
+            uint32_t hi[4], lo[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              uint64_t const t = f2mul(xv[ch * 4 + e], bb);
+              uint64_t const h = f2sub(f2fma(t, kInv256, kMagic), kMagic);
+              uint64_t const l = f2sub(f2add(f2fma(h, kM256, t), kMagic), kMagic);
+              hi[e] = bf16PairExact(h);
+              lo[e] = bf16PairExact(l);
+            }
+            *reinterpret_cast<uint4 *>(S.x[xb][0] + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+            *reinterpret_cast<uint4 *>(S.x[xb][1] + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+          }
         }
         float vs0, vs1;
         f2unpack(vsum2, vs0, vs1);
@@ -808,22 +847,25 @@ bool makeMap(CUtensorMap * m, void * base, uint64_t inner, uint64_t outer, uint3
             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-template <int NB, int RP>
+template <int NB, int RP, int XS>
 int launchFlash(tcscf_ctx * ctx, tc::Params const & P, int grid)
 {
-  size_t const smem = sizeof(tc::Smem<NB, RP>) + 1024;
-  static_assert(sizeof(tc::Smem<NB, RP>) + 1024 <= 232448, "shared memory per CTA");
-  TCSCF_CUDA(ctx, cudaFuncSetAttribute(tc::kFlashTc<NB, RP>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-  tc::kFlashTc<NB, RP><<<grid, tc::NTHREADS, smem, ctx->stream>>>(P);
+  size_t const smem = sizeof(tc::Smem<NB, RP, XS>) + 1024;
+  static_assert(sizeof(tc::Smem<NB, RP, XS>) + 1024 <= 232448, "shared memory per CTA");
+  TCSCF_CUDA(ctx, cudaFuncSetAttribute(tc::kFlashTc<NB, RP, XS>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  tc::kFlashTc<NB, RP, XS><<<grid, tc::NTHREADS, smem, ctx->stream>>>(P);
   TCSCF_LAUNCH(ctx);
   return TCSCF_OK;
 }
 
-int launchClass(tcscf_ctx * ctx, int NB, int RP, tc::Params const & P, int grid)
+// tile classes: (NB, RP, XS)
+constexpr int kClasses[5][3] = {{64, 32, 2}, {64, 32, 3}, {64, 64, 2}, {128, 32, 2}, {128, 32, 3}};
+
+int launchClass(tcscf_ctx * ctx, int NB, int RP, int XS, tc::Params const & P, int grid)
 {
-  if (NB == 64 && RP == 32) return launchFlash<64, 32>(ctx, P, grid);
-  if (NB == 64 && RP == 64) return launchFlash<64, 64>(ctx, P, grid);
-  if (NB == 128 && RP == 32) return launchFlash<128, 32>(ctx, P, grid);
+  if (NB == 64 && RP == 32) return XS == 3 ? launchFlash<64, 32, 3>(ctx, P, grid) : launchFlash<64, 32, 2>(ctx, P, grid);
+  if (NB == 64 && RP == 64 && XS == 2) return launchFlash<64, 64, 2>(ctx, P, grid);
+  if (NB == 128 && RP == 32) return XS == 3 ? launchFlash<128, 32, 3>(ctx, P, grid) : launchFlash<128, 32, 2>(ctx, P, grid);
   return fail(ctx, TCSCF_ERR_UNSUPPORTED, "no tensor kernel for this tile class");
 }
 
@@ -891,7 +933,7 @@ int smCount()
 }
 
 struct Shape {
-  int NB, RP;
+  int NB, RP, XS;
   int64_t n1pad, n2pad;
   int nTiles, nBlocks, nSplit, perSplit;
 };
@@ -901,6 +943,10 @@ Shape shapeOf(Contraction const & c, int sms)
   Shape sh{};
   sh.NB = c.ncol <= 64 ? 64 : 128;
   sh.RP = c.R <= 32 ? 32 : 64;
+  // 24-bit X below 2^18 r2 points: on coarser grids a 64-point r2 block spans a wider range of
+  // g * rho within a row, and the 16-bit slicing error averages over fewer pairs (rank padding 64
+  // leaves no shared memory for the extra slices)
+  sh.XS = (sh.RP == 32 && c.n2 < (int64_t(1) << 18)) ? 3 : 2;
   sh.n1pad = (c.n1 + tc::BM - 1) / tc::BM * tc::BM;
   sh.n2pad = (c.n2 + tc::BK - 1) / tc::BK * tc::BK;
   sh.nTiles = int(sh.n1pad / tc::BM);
@@ -989,7 +1035,7 @@ int tensorPrepare(tcscf_ctx * ctx, Contraction const & c, int precision, void * 
   I.r1xyz = r1c; I.r2pairs = r2c; I.a1inv = a1inv; I.a2inv = a2inv; I.cinv = cinv;
   I.T = Tout; I.VH = VHout;
   I.tStride = int64_t(c.n1) * c.ldt; I.vhStride = c.n1;
-  tp.NB = NB; tp.RP = RP;
+  tp.NB = NB; tp.RP = RP; tp.XS = sh.XS;
   tp.c = c;
   return TCSCF_OK;
 }
@@ -1024,11 +1070,11 @@ int tensorRun(tcscf_ctx * ctx, TensorPrep * const * preps, int count)
   hItems.reserve(itemsTotal);
   size_t offset = 0;
   cudaEventRecord(ctx->ev[2], ctx->stream);
-  for (int cls = 0; cls < 3; ++cls) {
-    int const NB = cls == 2 ? 128 : 64, RP = cls == 1 ? 64 : 32;
+  for (auto const & cl : kClasses) {
+    int const NB = cl[0], RP = cl[1], XS = cl[2];
     std::vector<int4> items;
     for (int k = 0; k < count; ++k) {
-      if (preps[k]->NB != NB || preps[k]->RP != RP) continue;
+      if (preps[k]->NB != NB || preps[k]->RP != RP || preps[k]->XS != XS) continue;
       tc::Instance const & I = preps[k]->inst;
       for (int t = 0; t < I.nTiles; ++t)
         for (int sp = 0; sp < I.nSplit; ++sp) items.push_back(make_int4(k, t, sp, std::min(I.nBlocks - sp * I.blocksPerSplit, I.blocksPerSplit)));
@@ -1041,7 +1087,7 @@ int tensorRun(tcscf_ctx * ctx, TensorPrep * const * preps, int count)
     P.items = count == 1 ? nullptr : dItems + offset;
     P.inst = dInst;
     P.status = dStatus;
-    TCSCF_TRY(launchClass(ctx, NB, RP, P, std::min(int(items.size()), sms)));
+    TCSCF_TRY(launchClass(ctx, NB, RP, XS, P, std::min(int(items.size()), sms)));
     offset += items.size();
   }
   cudaEventRecord(ctx->ev[3], ctx->stream);

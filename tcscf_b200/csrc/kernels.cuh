@@ -67,7 +67,7 @@ constexpr int kTensorMapsPerInstance = 10;
 
 // a contraction whose operands are packed (tensorPrepare) and ready for tensorRun
 struct TensorPrep {
-  int NB = 0, RP = 0;
+  int NB = 0, RP = 0, XS = 2;   // Vt tile columns, rank padding, X slices (2: 16 bits, 3: 24 bits)
   Contraction c;
   TensorInstance inst{};
   CUtensorMap maps[kTensorMapsPerInstance];
