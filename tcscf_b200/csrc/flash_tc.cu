@@ -17,8 +17,9 @@
 // and the product is 256 A + B in units of the block's scales (GEMM2 keeps h m', l h', h l'/256 of
 // its 16-bit X).  The hi*hi accumulation being exact, the tensor core's FP32 adder rounding cannot
 // bias the result; the products below 2^-24 of the largest term are dropped.  Each block's T is
-// added into per-thread FP64 accumulators with its scales as soon as the block completes.  The
-// kernel matrix g exists only as the BF16 X tile in shared memory.
+// added with its scales, as soon as the block completes, into per-thread double-float accumulators
+// (FP32 hi + lo updated by the error-free TwoSum; about 48 bits, no FP64 or conversion pipe work).
+// The kernel matrix g exists only as the BF16 X tile in shared memory.
 //
 // Warp roles (384 threads, one CTA per SM, persistent over (r1 tile, r2 split) work items):
 //   warp 0      TMA producer: psi1 tile (once per work item), psi2 / Vt blocks (TMA, no multicast),
@@ -289,16 +290,18 @@ __device__ __forceinline__ uint32_t bf16PairExact(uint64_t ab)
   return __byte_perm(__float_as_uint(a), __float_as_uint(b), 0x7632);
 }
 
-// Adds the finished block f (this thread's row, NB/2 columns of T) into the FP64 accumulators with the
-// block's scales and hands the TMEM accumulators back to the MMA issuer.
+// Adds the finished block f (this thread's row, NB/2 columns of T) with the block's scales into the
+// double-float accumulators (hi + lo per column, FP32 pairs of columns) by the error-free TwoSum,
+// and hands the TMEM accumulators back to the MMA issuer.
 template <int NB, class SmemT>
-__device__ __forceinline__ bool flushBlock(SmemT & S, uint32_t taddr, uint32_t f, int cw, double fac, double (&acc)[NB / 2], int lane,
-                                           volatile int * abortFlag, int * status)
+__device__ __forceinline__ bool flushBlock(SmemT & S, uint32_t taddr, uint32_t f, int cw, float fac, uint64_t (&hi)[NB / 4],
+                                           uint64_t (&lo)[NB / 4], int lane, volatile int * abortFlag, int * status)
 {
   if (!waitBar(&S.tfull, f & 1, abortFlag, status, 31)) return false;
   fenceAfterSync();
   float const * cs = S.cinvT[cw][f & 1];
   uint64_t const k256 = f2pack(256.0f, 256.0f);
+  uint64_t const ff = f2pack(fac, fac);
   constexpr int NQ = NB / 32;   // chunks of 16 columns; the loads of chunk q + 1 overlap the work on chunk q
   float hh[2][16], mm[2][16];
   tmemLoad16(taddr, hh[0]);
@@ -314,13 +317,17 @@ __device__ __forceinline__ bool flushBlock(SmemT & S, uint32_t taddr, uint32_t f
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
       float2 const c2 = *reinterpret_cast<float2 const *>(cs + q * 16 + 2 * i);
-      // 256 hh + cross is the block's exact integer sum up to one FP32 rounding; cinv is a power of two
-      uint64_t const v =
-          f2mul(f2fma(f2pack(hh[cur][2 * i], hh[cur][2 * i + 1]), k256, f2pack(mm[cur][2 * i], mm[cur][2 * i + 1])), f2pack(c2.x, c2.y));
-      float va, vb;
-      f2unpack(v, va, vb);
-      acc[q * 16 + 2 * i] = fma(double(va), fac, acc[q * 16 + 2 * i]);
-      acc[q * 16 + 2 * i + 1] = fma(double(vb), fac, acc[q * 16 + 2 * i + 1]);
+      // 256 hh + cross is the block's exact integer sum up to one FP32 rounding; cinv and fac are powers
+      // of two, so x is that sum in the units of T
+      uint64_t const x = f2mul(f2fma(f2pack(hh[cur][2 * i], hh[cur][2 * i + 1]), k256, f2pack(mm[cur][2 * i], mm[cur][2 * i + 1])),
+                               f2mul(f2pack(c2.x, c2.y), ff));
+      // TwoSum: s + e == hi + x exactly
+      int const p = q * 8 + i;
+      uint64_t const sum = f2add(hi[p], x);
+      uint64_t const bp = f2sub(sum, hi[p]);
+      uint64_t const err = f2add(f2sub(hi[p], f2sub(sum, bp)), f2sub(x, bp));
+      lo[p] = f2add(lo[p], err);
+      hi[p] = sum;
     }
     if (q + 1 < NQ) tmemWaitLoad(hh[cur ^ 1], mm[cur ^ 1]);
   }
@@ -525,7 +532,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     uint32_t const tAddr = tmem + laneBase + TCOL0 + uint32_t(half * (NB / 2));
     uint32_t blockCount = 0;
     bool ok = true;
-    double acc[NB / 2];
+    uint64_t ahi[NB / 4], alo[NB / 4];   // T of this thread's row and columns as FP32 hi + lo, column pairs
     uint64_t const k256 = f2pack(256.0f, 256.0f), kInv256 = f2pack(1.0f / 256.0f, 1.0f / 256.0f), kM256 = f2pack(-256.0f, -256.0f);
     uint64_t const kMagic = f2pack(12582912.0f, 12582912.0f);   // 1.5 * 2^23: adding it rounds |x| < 2^22 to an integer
     uint64_t const kInv65536 = f2pack(1.0f / 65536.0f, 1.0f / 65536.0f), kM65536 = f2pack(-65536.0f, -65536.0f);
@@ -542,11 +549,11 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       // rho = 2^24 a1inv a2inv (256 A + B), X' = g a2inv (256 A + B) = X / (2^24 a1inv), and a block's
       // sum_r2 X' Vt = 2^16 (256 A + B) / (bs c) (XS = 2) or 2^24 (256 A + B) / (bs c) (XS = 3):
       // T += 2^40 (or 2^48) a1inv / bs * cinv (256 A + B)
-      double const rowA = (XS == 3 ? 281474976710656.0 : 1099511627776.0) * double(I->a1inv[r1]);   // 2^48 or 2^40
+      float const rowA = (XS == 3 ? 281474976710656.0f : 1099511627776.0f) * I->a1inv[r1];   // 2^48 or 2^40, a power of two
 #pragma unroll
-      for (int c = 0; c < NB / 2; ++c) acc[c] = 0.0;
+      for (int c = 0; c < NB / 4; ++c) { ahi[c] = 0; alo[c] = 0; }
       double vh = 0.0;
-      double pendingFac = 0.0;
+      float pendingFac = 0.0f;
       bool pending = false;   // block g - 1 still to be flushed
       uint64_t const p1x = f2pack(p1.x, p1.x), p1y = f2pack(p1.y, p1.y), p1z = f2pack(p1.z, p1.z);
       for (int jj = 0; jj < nblk && ok; ++jj) {
@@ -616,8 +623,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         // scale bs = 2^(kXExp - E), E = floor(log2 mx) (clamped below), so |X' bs| < 2^(kXExp + 1)
         int const E = max(int((__float_as_uint(mx) >> 23) & 0xFF) - 127, kMinExp);
         float const bs = __uint_as_float(uint32_t(127 + kXExp - E) << 23);
-        double const binv = __longlong_as_double(int64_t(1023 + E - kXExp) << 52);
-        double const fac = rowA * binv;
+        float const binv = __uint_as_float(uint32_t(127 + E - kXExp) << 23);   // 2^(E - kXExp), E >= -100
+        float const fac = rowA * binv;   // a power of two (0 when below FP32 range: those blocks add nothing measurable)
         // X buffer xb is free once GEMM2 of block g - XBUF completed
         int const xb = g % XBUF;
         if (g >= uint32_t(XBUF) && !(ok = waitBar(&S.xfree[xb], ((g / XBUF) - 1) & 1, abortFlag, P.status, 34))) break;
@@ -666,11 +673,11 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         fenceProxyAsync();
         __syncwarp();
         if (lane == 0) { mbarArrive(&S.xfull[xb]); mbarArrive(&S.empty[s]); }
-        if (pending && !(ok = flushBlock<NB>(S, tAddr, g - 1, cw, pendingFac, acc, lane, abortFlag, P.status))) break;
+        if (pending && !(ok = flushBlock<NB>(S, tAddr, g - 1, cw, pendingFac, ahi, alo, lane, abortFlag, P.status))) break;
         pending = true;
         pendingFac = fac;
       }
-      if (ok && pending) ok = flushBlock<NB>(S, tAddr, blockCount + nblk - 1, cw, pendingFac, acc, lane, abortFlag, P.status);
+      if (ok && pending) ok = flushBlock<NB>(S, tAddr, blockCount + nblk - 1, cw, pendingFac, ahi, alo, lane, abortFlag, P.status);
       blockCount += nblk;
       if (!ok) break;
       int const n1 = I->n1;
@@ -680,7 +687,10 @@ __global__ void __launch_bounds__(NTHREADS, 1)
 #pragma unroll
         for (int c = 0; c < NB / 2; ++c) {
           int const col = half * (NB / 2) + c;
-          if (col < nbReal) T[col] = acc[c];
+          float h0, h1, l0, l1;
+          f2unpack(ahi[c / 2], h0, h1);
+          f2unpack(alo[c / 2], l0, l1);
+          if (col < nbReal) T[col] = (c & 1) ? double(h1) + double(l1) : double(h0) + double(l0);
         }
       }
       // the two r2-half warps of a row each summed half of the r2 points of every block
