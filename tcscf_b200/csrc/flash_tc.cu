@@ -229,6 +229,20 @@ __device__ __forceinline__ void tmemLoad16(uint32_t taddr, float * v)
 #pragma unroll
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
+__device__ __forceinline__ void tmemLoad8(uint32_t taddr, float * v)
+{
+  uint32_t r[8];
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+               : "r"(taddr));
+#pragma unroll
+  for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
+}
+__device__ __forceinline__ void tmemWaitLoad8(float (&a)[8], float (&b)[8])
+{
+  asm volatile("tcgen05.wait::ld.sync.aligned;" : "+f"(a[0]), "+f"(a[1]), "+f"(a[2]), "+f"(a[3]), "+f"(a[4]), "+f"(a[5]), "+f"(a[6]), "+f"(a[7]) :: "memory");
+  asm volatile("" : "+f"(b[0]), "+f"(b[1]), "+f"(b[2]), "+f"(b[3]), "+f"(b[4]), "+f"(b[5]), "+f"(b[6]), "+f"(b[7]) :: "memory");
+}
 // wait for the outstanding TMEM loads into a and b; the register operands keep every use of a and b
 // after the wait (the asm statements are volatile, so their order is kept)
 __device__ __forceinline__ void tmemWaitLoad(float (&a)[16], float (&b)[16])
@@ -302,34 +316,34 @@ __device__ __forceinline__ bool flushBlock(SmemT & S, uint32_t taddr, uint32_t f
   float const * cs = S.cinvT[cw][f & 1];
   uint64_t const k256 = f2pack(256.0f, 256.0f);
   uint64_t const ff = f2pack(fac, fac);
-  constexpr int NQ = NB / 32;   // chunks of 16 columns; the loads of chunk q + 1 overlap the work on chunk q
-  float hh[2][16], mm[2][16];
-  tmemLoad16(taddr, hh[0]);
-  tmemLoad16(taddr + NB, mm[0]);
-  tmemWaitLoad(hh[0], mm[0]);
+  constexpr int NQ = NB / 16;   // chunks of 8 columns; the loads of chunk q + 1 overlap the work on chunk q
+  float hh[2][8], mm[2][8];
+  tmemLoad8(taddr, hh[0]);
+  tmemLoad8(taddr + NB, mm[0]);
+  tmemWaitLoad8(hh[0], mm[0]);
 #pragma unroll
   for (int q = 0; q < NQ; ++q) {
     int const cur = q & 1;
     if (q + 1 < NQ) {
-      tmemLoad16(taddr + (q + 1) * 16, hh[cur ^ 1]);
-      tmemLoad16(taddr + NB + (q + 1) * 16, mm[cur ^ 1]);
+      tmemLoad8(taddr + (q + 1) * 8, hh[cur ^ 1]);
+      tmemLoad8(taddr + NB + (q + 1) * 8, mm[cur ^ 1]);
     }
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      float2 const c2 = *reinterpret_cast<float2 const *>(cs + q * 16 + 2 * i);
+    for (int i = 0; i < 4; ++i) {
+      float2 const c2 = *reinterpret_cast<float2 const *>(cs + q * 8 + 2 * i);
       // 256 hh + cross is the block's exact integer sum up to one FP32 rounding; cinv and fac are powers
       // of two, so x is that sum in the units of T
       uint64_t const x = f2mul(f2fma(f2pack(hh[cur][2 * i], hh[cur][2 * i + 1]), k256, f2pack(mm[cur][2 * i], mm[cur][2 * i + 1])),
                                f2mul(f2pack(c2.x, c2.y), ff));
       // TwoSum: s + e == hi + x exactly
-      int const p = q * 8 + i;
+      int const p = q * 4 + i;
       uint64_t const sum = f2add(hi[p], x);
       uint64_t const bp = f2sub(sum, hi[p]);
       uint64_t const err = f2add(f2sub(hi[p], f2sub(sum, bp)), f2sub(x, bp));
       lo[p] = f2add(lo[p], err);
       hi[p] = sum;
     }
-    if (q + 1 < NQ) tmemWaitLoad(hh[cur ^ 1], mm[cur ^ 1]);
+    if (q + 1 < NQ) tmemWaitLoad8(hh[cur ^ 1], mm[cur ^ 1]);
   }
   fenceBeforeSync();
   __syncwarp();
