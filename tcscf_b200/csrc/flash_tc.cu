@@ -10,7 +10,9 @@
 // column of Vt carries a power-of-two scale s chosen from its largest entry.  The per-point factors
 // psi1, psi2 and Vt (whose rounding is shared by every pair a point takes part in) keep 24 bits:
 // u s in [2^23, 2^24) is written as 65536 h + 256 m + l with integers |h| <= 256, |m|, |l| <= 128
-// (round to nearest, each exact in BF16); X keeps 16 bits, u s = 256 h + l.  Per r2 block:
+// (round to nearest, each exact in BF16); X keeps 16 bits, u s = 256 h + l, or 24 bits like the
+// factors when r2 has fewer than 2^18 points.  X's lowest slice l enters only B, so it is stored as
+// the BF16 nearest to the remainder (8 significant bits) instead of an integer.  Per r2 block:
 //   A = sum h h'                      (integers below 2^16 each, a K <= 64 sum below 2^23: exact)
 //   B = sum h m' + m h' + (h l' + l h' + m m')/256   (the level 2^-8 below A; its own FP32 rounding
 //                                                     is scaled down by 2^-8 in the result)
@@ -294,6 +296,15 @@ __device__ __forceinline__ float rsqrtApprox(float x)
 __device__ __forceinline__ uint32_t sw128(int row, int chunk)
 {
   return uint32_t((row >> 3) * 1024 + (row & 7) * 128 + ((chunk ^ (row & 7)) << 4));
+}
+
+// the BF16 pair {a, b} rounded to nearest
+__device__ __forceinline__ uint32_t bf16PairRn(uint64_t ab)
+{
+  float a, b;
+  f2unpack(ab, a, b);
+  __nv_bfloat162 const h = __floats2bfloat162_rn(a, b);
+  return *reinterpret_cast<uint32_t const *>(&h);
 }
 
 // the BF16 pair {a, b} of two FP32 values whose low 16 mantissa bits are zero (exact truncation)
@@ -647,7 +658,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         for (int ch = 0; ch < 4; ++ch) {
           uint32_t const off = sw128(row, half * 4 + ch);
           if constexpr (XS == 3) {
-            // t = X' bs = 65536 h + 256 m + l: h = rint(t / 65536), m = rint(r / 256), l = rint(r - 256 m),
+            // t = X' bs = 65536 h + 256 m + l: h = rint(t / 65536), m = rint(r / 256), l = r - 256 m,
             // r = t - 65536 h; slices h, m, l/256, m/256
             uint32_t sh[4], sm[4], sl[4], sms[4];
 #pragma unroll
@@ -656,10 +667,11 @@ __global__ void __launch_bounds__(NTHREADS, 1)
               uint64_t const h = f2sub(f2fma(t, kInv65536, kMagic), kMagic);
               uint64_t const r = f2fma(h, kM65536, t);
               uint64_t const m = f2sub(f2fma(r, kInv256, kMagic), kMagic);
-              uint64_t const l = f2sub(f2add(f2fma(m, kM256, r), kMagic), kMagic);
+              // the lowest slice only feeds the cross accumulator, which rounds 2^-8 below the result:
+              // it is stored rounded to nearest BF16 (8 significant bits), not rounded to an integer
               sh[e] = bf16PairExact(h);
               sm[e] = bf16PairExact(m);
-              sl[e] = bf16PairExact(f2mul(l, kInv256));
+              sl[e] = bf16PairRn(f2mul(f2fma(m, kM256, r), kInv256));
               sms[e] = bf16PairExact(f2mul(m, kInv256));
             }
             *reinterpret_cast<uint4 *>(S.x[xb][0] + off) = make_uint4(sh[0], sh[1], sh[2], sh[3]);
@@ -667,15 +679,15 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             *reinterpret_cast<uint4 *>(S.x[xb][2] + off) = make_uint4(sl[0], sl[1], sl[2], sl[3]);
             *reinterpret_cast<uint4 *>(S.x[xb][3] + off) = make_uint4(sms[0], sms[1], sms[2], sms[3]);
           } else {
-            // t = X' bs = 256 h + l, h = rint(t / 256), l = rint(t - 256 h)
+            // t = X' bs = 256 h + l, h = rint(t / 256), l = t - 256 h (rounded to nearest BF16: it only
+            // feeds the cross accumulator)
             uint32_t hi[4], lo[4];
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
               uint64_t const t = f2mul(xv[ch * 4 + e], bb);
               uint64_t const h = f2sub(f2fma(t, kInv256, kMagic), kMagic);
-              uint64_t const l = f2sub(f2add(f2fma(h, kM256, t), kMagic), kMagic);
               hi[e] = bf16PairExact(h);
-              lo[e] = bf16PairExact(l);
+              lo[e] = bf16PairRn(f2fma(h, kM256, t));
             }
             *reinterpret_cast<uint4 *>(S.x[xb][0] + off) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
             *reinterpret_cast<uint4 *>(S.x[xb][1] + off) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
