@@ -296,6 +296,16 @@ def run_ours(args, rank: int, world: int) -> None:
     if prec == ffi.PREC_FP64:
         roof = {"bound": "fp64", "achieved": achieved, "peak": args.fp64_peak, "unit": "TFLOP/s", "frac": achieved / args.fp64_peak,
                 "traffic": None, "peak_source": "measured FP64 matmul (DESIGN.md)"}
+    elif prec == ffi.PREC_TF32:
+        # TF32 dense rate is half the BF16 rate (nominal 1.1 vs 2.25 PFLOP/s): half the measured BF16 burst
+        peak = peaks["bf16_tflops"] / 2
+        RP = 32                            # TF32 launches hold rank 32 (larger ranks run in chunks)
+        NB = 64 if w.nb <= 64 else 128
+        chunks = -(-w.n_up // RP)
+        issued = n * n * chunks * (2.0 * RP + 2.0 * NB) / (c_ms / 1e3) / 1e12
+        roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "traffic": None, "peak_source": f"tf32 dense = half the bf16 dense burst, {peak_kind}",
+                "issued_tensor_tflops": issued, "issued_frac": issued / peak}
     else:
         peak = peaks["bf16_tflops"]
         # tensor work the kernel issues per (r1, r2) pair: GEMM1 6 slice products of K = RP, GEMM2 4 of N = NB
@@ -316,8 +326,11 @@ def run_ours(args, rank: int, world: int) -> None:
             "data": "synthetic",
             "config": {"workload": f"{w.name} RCS Fock build (direct form)", "Z": w.Z, "n_points": n, "n_basis": w.nb,
                        "n_occ": w.n_up, "grid": f"{w.nrad} radial (Gauss-Chebyshev, r=(1+x)/(1-x)) x Lebedev order {w.order}",
-                       "precision": {"fp64": "fp64", "bf16x3": "bf16 fixed-point slices (24-bit factors, 16-bit kernel tile), "
-                                     "exact fp32 block accumulation, fp64 across blocks", "tf32": "tf32"}[args.precision],
+                       "precision": {"fp64": "fp64",
+                                     "bf16x3": "bf16 fixed-point slices (24-bit factors, 16- or 24-bit kernel tile), exact fp32 "
+                                               "accumulation of the leading slices per 64-point block, double-float across blocks",
+                                     "tf32": "tf32 operands (10-bit mantissa, round to nearest), fp32 accumulation per 64-point "
+                                             "block, double-float across blocks"}[args.precision],
                        "l2": "flushed (256 MB write) between timed steps",
                        "density": "core-Hamiltonian guess (canonical orthogonalisation)"},
             "energy": E, "contraction_ms": c_ms, "gpu_launches": launches, "roofline": roof, "fp64": fp64,

@@ -72,10 +72,13 @@ typedef enum tcscf_kernel {
   TCSCF_K_GRAD_U_OPPO = 4
 } tcscf_kernel;
 
-/* Precision of the r12 contraction.  FP64: CUDA-core FP64 throughout.  BF16X3: tcgen05 tensor
- * cores with hi+lo BF16 operand pairs (3 products) in fixed point (power-of-two scale per row /
- * column / r2 block), so the FP32 accumulation in TMEM of each r2 block of 64 is exact; every block
- * is added into FP64.  TF32: reserved (returns TCSCF_ERR_UNSUPPORTED). */
+/* Precision of the r12 contraction (the direct Fock build; the precompute form and the TC tensors
+ * are FP64).  FP64: CUDA-core FP64 throughout.  BF16X3: tcgen05 tensor cores on fixed-point BF16
+ * slices of every operand (24 bits for the orbital factors and the weighted basis, 16 or 24 bits for
+ * g * rho; power-of-two scales per row / column / r2 block of 64), so the tensor-core sum of the
+ * leading slices is exact; each block is added into double-float (FP32 hi + lo) accumulators.
+ * TF32: tcgen05 kind::tf32 on operands rounded to TF32 (10 explicit mantissa bits), FP32
+ * accumulation within an r2 block of 64, blocks added into double-float accumulators. */
 typedef enum tcscf_precision {
   TCSCF_PREC_FP64 = 0,
   TCSCF_PREC_BF16X3 = 1,

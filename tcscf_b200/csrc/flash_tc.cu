@@ -37,13 +37,11 @@
 #include <algorithm>
 #include <vector>
 
-#include "kernels.cuh"
+#include "tc_device.cuh"
 
 namespace tcscf {
 namespace tc {
 
-constexpr int BM = 128;        // r1 rows per tile
-constexpr int BK = 64;         // r2 points per block
 // TMA stages: three when the tile shapes leave room in shared memory
 __host__ __device__ constexpr int stagesFor(int NB, int RP) { return NB == 64 && RP == 32 ? 3 : 2; }
 // X precision: XS = 2 slices (16 bits, u s in [2^15, 2^16)) or XS = 3 (24 bits, stored as the four
@@ -52,15 +50,6 @@ __host__ __device__ constexpr int stagesFor(int NB, int RP) { return NB == 64 &&
 __host__ __device__ constexpr int xSlicesFor(int XS) { return XS == 3 ? 4 : 2; }
 __host__ __device__ constexpr int xBuffersFor(int NB, int RP, int XS) { return XS == 3 || (NB == 64 && RP == 64) ? 1 : 2; }
 __host__ __device__ constexpr int xExpFor(int XS) { return XS == 3 ? 23 : 15; }
-constexpr int NCW = 8;         // compute warps
-constexpr int NTHREADS = 384;  // warpgroup 0: TMA, MMA, 2 idle warps; warpgroups 1-2: compute
-// register split: 384 threads x 168 at launch = 64512 = 128 x 56 (producer warpgroup) + 256 x 224
-constexpr int kRegsLaunch = 168, kRegsProducer = 56, kRegsCompute = 224;
-static_assert(128 * kRegsProducer + 256 * kRegsCompute <= NTHREADS * kRegsLaunch, "register split exceeds the launch allocation");
-constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s per wait
-// a waiting thread sleeps in mbarrier.try_wait (woken when the phase completes) instead of spinning
-// on the issue slots the compute warps need
-constexpr uint32_t kSuspendHintNs = 1000000;
 // slicing: scale = 2^(k - floor(log2 max|u|)) puts the largest entry in [2^k, 2^(k+1)): k = 23 for
 // the three-slice factors, 15 for the two-slice X; entries of a row whose maximum is below
 // 2^kMinExp are sliced against 2^kMinExp
@@ -94,107 +83,6 @@ struct __align__(1024) Smem {
   int abort;
 };
 
-using Instance = TensorInstance;
-constexpr int kMapsPerInstance = kTensorMapsPerInstance;
-
-struct Params {
-  int nItems;
-  const int4 * items;       // work items (instance, r1 tile, r2 split, 0); null: one instance, item = tile * nSplit + split
-  const Instance * inst;    // [instances] in device memory
-  int * status;             // device status word (0 = ok)
-};
-
-__device__ __forceinline__ void decodeItem(Params const & P, int item, int & inst, int & tile, int & split)
-{
-  if (P.items) {
-    int4 const it = P.items[item];
-    inst = it.x; tile = it.y; split = it.z;
-  } else {
-    int const ns = P.inst[0].nSplit;
-    inst = 0; tile = item / ns; split = item % ns;
-  }
-}
-
-// ---- PTX helpers --------------------------------------------------------------------------------
-__device__ __forceinline__ uint32_t smemAddr(const void * p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
-
-__device__ __forceinline__ unsigned long long globalTimer()
-{
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
-__device__ __forceinline__ void mbarInit(uint64_t * b, uint32_t count)
-{
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smemAddr(b)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbarArrive(uint64_t * b)
-{
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smemAddr(b)) : "memory");
-}
-__device__ __forceinline__ void mbarArriveTx(uint64_t * b, uint32_t bytes)
-{
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smemAddr(b)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ bool mbarTryWait(uint64_t * b, uint32_t parity)
-{
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(smemAddr(b)), "r"(parity), "r"(kSuspendHintNs)
-      : "memory");
-  return ok != 0;
-}
-
-// Bounded wait; returns false (after recording the failure) when the limit expires or another role
-// has already aborted.
-__device__ __forceinline__ bool waitBar(uint64_t * b, uint32_t parity, volatile int * abortFlag, int * status, int code)
-{
-  if (mbarTryWait(b, parity)) return true;
-  unsigned long long const t0 = globalTimer();
-  while (true) {
-    if (mbarTryWait(b, parity)) return true;
-    if (*abortFlag) return false;
-    if (globalTimer() - t0 > kWaitLimitNs) {
-      *abortFlag = 1;
-      atomicCAS(status, 0, code);
-      return false;
-    }
-  }
-}
-
-__device__ __forceinline__ void tmaLoad2d(void * dst, const CUtensorMap * map, int x, int y, uint64_t * bar)
-{
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(smemAddr(dst)),
-      "l"(map), "r"(x), "r"(y), "r"(smemAddr(bar))
-      : "memory");
-}
-
-__device__ __forceinline__ void bulkLoad(void * dst, const void * src, uint32_t bytes, uint64_t * bar)
-{
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smemAddr(dst)), "l"(src),
-               "r"(bytes), "r"(smemAddr(bar))
-               : "memory");
-}
-
-// UMMA shared-memory descriptor (K-major): start address, stride byte offset between 8-row groups,
-// version 1, swizzle mode (2 = 128B, 4 = 64B).
-__device__ __forceinline__ uint64_t smemDesc(uint32_t addr, uint32_t sbo, uint32_t swizzle)
-{
-  uint64_t d = 0;
-  d |= uint64_t((addr >> 4) & 0x3FFF);
-  d |= uint64_t(1) << 16;                          // leading byte offset (unused for swizzled K-major)
-  d |= uint64_t((sbo >> 4) & 0x3FFF) << 32;
-  d |= uint64_t(1) << 46;                          // descriptor version (sm_100)
-  d |= uint64_t(swizzle & 7) << 61;
-  return d;
-}
-
 // instruction descriptor: kind::f16, A = B = BF16 (K-major), D = F32, shape M x N
 __host__ __device__ constexpr uint32_t instrDescBf16(int M, int N)
 {
@@ -209,93 +97,6 @@ __device__ __forceinline__ void mmaBf16(uint32_t tmemD, uint64_t a, uint64_t b, 
       "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmemD),
       "l"(a), "l"(b), "r"(idesc), "r"(accumulate)
       : "memory");
-}
-
-__device__ __forceinline__ void mmaCommit(uint64_t * bar)
-{
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smemAddr(bar)) : "memory");
-}
-
-__device__ __forceinline__ void fenceBeforeSync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void fenceAfterSync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void fenceProxyAsync() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-
-__device__ __forceinline__ void tmemLoad16(uint32_t taddr, float * v)
-{
-  uint32_t r[16];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]),
-        "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
-#pragma unroll
-  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
-}
-__device__ __forceinline__ void tmemLoad8(uint32_t taddr, float * v)
-{
-  uint32_t r[8];
-  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
-               : "r"(taddr));
-#pragma unroll
-  for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
-}
-__device__ __forceinline__ void tmemWaitLoad8(float (&a)[8], float (&b)[8])
-{
-  asm volatile("tcgen05.wait::ld.sync.aligned;" : "+f"(a[0]), "+f"(a[1]), "+f"(a[2]), "+f"(a[3]), "+f"(a[4]), "+f"(a[5]), "+f"(a[6]), "+f"(a[7]) :: "memory");
-  asm volatile("" : "+f"(b[0]), "+f"(b[1]), "+f"(b[2]), "+f"(b[3]), "+f"(b[4]), "+f"(b[5]), "+f"(b[6]), "+f"(b[7]) :: "memory");
-}
-// wait for the outstanding TMEM loads into a and b; the register operands keep every use of a and b
-// after the wait (the asm statements are volatile, so their order is kept)
-__device__ __forceinline__ void tmemWaitLoad(float (&a)[16], float (&b)[16])
-{
-  asm volatile("tcgen05.wait::ld.sync.aligned;" : "+f"(a[0]), "+f"(a[1]), "+f"(a[2]), "+f"(a[3]), "+f"(a[4]), "+f"(a[5]), "+f"(a[6]), "+f"(a[7]), "+f"(a[8]), "+f"(a[9]), "+f"(a[10]), "+f"(a[11]), "+f"(a[12]), "+f"(a[13]), "+f"(a[14]), "+f"(a[15]) :: "memory");
-  asm volatile("" : "+f"(b[0]), "+f"(b[1]), "+f"(b[2]), "+f"(b[3]), "+f"(b[4]), "+f"(b[5]), "+f"(b[6]), "+f"(b[7]), "+f"(b[8]), "+f"(b[9]), "+f"(b[10]), "+f"(b[11]), "+f"(b[12]), "+f"(b[13]), "+f"(b[14]), "+f"(b[15]) :: "memory");
-}
-
-// ---- packed FP32 pairs (sm_100 f32x2 arithmetic on 64-bit register pairs) ---------------------
-__device__ __forceinline__ uint64_t f2pack(float a, float b)
-{
-  uint64_t d;
-  asm("mov.b64 %0, {%1, %2};" : "=l"(d) : "f"(a), "f"(b));
-  return d;
-}
-__device__ __forceinline__ void f2unpack(uint64_t v, float & a, float & b) { asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v)); }
-__device__ __forceinline__ uint64_t f2add(uint64_t a, uint64_t b)
-{
-  uint64_t d;
-  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-  return d;
-}
-__device__ __forceinline__ uint64_t f2sub(uint64_t a, uint64_t b)
-{
-  uint64_t d;
-  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-  return d;
-}
-__device__ __forceinline__ uint64_t f2mul(uint64_t a, uint64_t b)
-{
-  uint64_t d;
-  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
-  return d;
-}
-__device__ __forceinline__ uint64_t f2fma(uint64_t a, uint64_t b, uint64_t c)
-{
-  uint64_t d;
-  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
-  return d;
-}
-__device__ __forceinline__ float rsqrtApprox(float x)
-{
-  float y;
-  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-  return y;
-}
-
-// byte offset of element (row, k) in a K-major SW128 tile of 64 BF16 columns
-__device__ __forceinline__ uint32_t sw128(int row, int chunk)
-{
-  return uint32_t((row >> 3) * 1024 + (row & 7) * 128 + ((chunk ^ (row & 7)) << 4));
 }
 
 // the BF16 pair {a, b} rounded to nearest
@@ -852,12 +653,6 @@ __global__ void kPackCoordPairs(int64_t n, int64_t npad, const double * pts, con
 // ------------------------------------------------------------------------------------------------------
 // host side
 // ------------------------------------------------------------------------------------------------------
-namespace {
-
-using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *, const cuuint64_t *,
-                                   const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
-                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
 EncodeTiledFn encodeTiled()
 {
   static EncodeTiledFn fn = nullptr;
@@ -870,17 +665,25 @@ EncodeTiledFn encodeTiled()
   return fn;
 }
 
-// 2-D BF16 tensor map: inner extent `inner` (contiguous), `outer` rows, box (boxInner, boxOuter)
-bool makeMap(CUtensorMap * m, void * base, uint64_t inner, uint64_t outer, uint32_t boxInner, uint32_t boxOuter, CUtensorMapSwizzle sw)
+bool makeMap2d(CUtensorMap * m, CUtensorMapDataType type, uint32_t elemBytes, void * base, uint64_t inner, uint64_t outer, uint32_t boxInner,
+               uint32_t boxOuter, CUtensorMapSwizzle sw)
 {
   EncodeTiledFn fn = encodeTiled();
   if (!fn) return false;
   cuuint64_t dims[2] = {inner, outer};
-  cuuint64_t strides[1] = {inner * 2};
+  cuuint64_t strides[1] = {inner * elemBytes};
   cuuint32_t box[2] = {boxInner, boxOuter};
   cuuint32_t es[2] = {1, 1};
-  return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, sw,
-            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+  return fn(m, type, 2, base, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, sw, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+namespace {
+
+// 2-D BF16 tensor map: inner extent `inner` (contiguous), `outer` rows, box (boxInner, boxOuter)
+bool makeMap(CUtensorMap * m, void * base, uint64_t inner, uint64_t outer, uint32_t boxInner, uint32_t boxOuter, CUtensorMapSwizzle sw)
+{
+  return makeMap2d(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, inner, outer, boxInner, boxOuter, sw);
 }
 
 template <int NB, int RP, int XS>
@@ -894,11 +697,12 @@ int launchFlash(tcscf_ctx * ctx, tc::Params const & P, int grid)
   return TCSCF_OK;
 }
 
-// tile classes: (NB, RP, XS)
-constexpr int kClasses[5][3] = {{64, 32, 2}, {64, 32, 3}, {64, 64, 2}, {128, 32, 2}, {128, 32, 3}};
+// tile classes: (NB, RP, XS); XS = 0 is the TF32 kernel
+constexpr int kClasses[7][3] = {{64, 32, 2}, {64, 32, 3}, {64, 64, 2}, {128, 32, 2}, {128, 32, 3}, {64, 32, 0}, {128, 32, 0}};
 
 int launchClass(tcscf_ctx * ctx, int NB, int RP, int XS, tc::Params const & P, int grid)
 {
+  if (XS == 0) return launchTf32(ctx, NB, P, grid);
   if (NB == 64 && RP == 32) return XS == 3 ? launchFlash<64, 32, 3>(ctx, P, grid) : launchFlash<64, 32, 2>(ctx, P, grid);
   if (NB == 64 && RP == 64 && XS == 2) return launchFlash<64, 64, 2>(ctx, P, grid);
   if (NB == 128 && RP == 32) return XS == 3 ? launchFlash<128, 32, 3>(ctx, P, grid) : launchFlash<128, 32, 2>(ctx, P, grid);
@@ -949,11 +753,11 @@ int tensorPackedV(tcscf_ctx * ctx, Grid & g2, const double * V, double scale, co
 
 bool tensorPathAvailable(Contraction const & c, int precision, std::string * why)
 {
-  if (precision != TCSCF_PREC_BF16X3) { if (why) *why = "only the bf16x3 tensor path is built"; return false; }
+  if (precision != TCSCF_PREC_BF16X3 && precision != TCSCF_PREC_TF32) { if (why) *why = "not a tensor-core precision"; return false; }
   if (c.kernel != TCSCF_K_INV_R12) { if (why) *why = "tensor path implements the 1/r12 kernel"; return false; }
-  if (c.R < 1 || c.R > 64) { if (why) *why = "density factor rank must be 1..64 for the tensor path"; return false; }
+  if (c.R < 1) { if (why) *why = "empty density factor"; return false; }
   if (c.ncol > 128) { if (why) *why = "tensor path supports nb <= 128"; return false; }
-  if (c.ncol > 64 && c.R > 32) { if (why) *why = "tensor path supports a density factor rank <= 32 for nb > 64"; return false; }
+  if (c.R > tensorRankLimit(c, precision)) { if (why) *why = "one tensor launch holds a density factor rank <= 32 (TF32, or nb > 64) or 64"; return false; }
   if (!encodeTiled()) { if (why) *why = "cuTensorMapEncodeTiled unavailable"; return false; }
   return true;
 }
@@ -974,15 +778,16 @@ struct Shape {
   int nTiles, nBlocks, nSplit, perSplit;
 };
 
-Shape shapeOf(Contraction const & c, int sms)
+Shape shapeOf(Contraction const & c, int sms, int precision)
 {
   Shape sh{};
   sh.NB = c.ncol <= 64 ? 64 : 128;
   sh.RP = c.R <= 32 ? 32 : 64;
   // 24-bit X below 2^18 r2 points: on coarser grids a 64-point r2 block spans a wider range of
   // g * rho within a row, and the 16-bit slicing error averages over fewer pairs (rank padding 64
-  // leaves no shared memory for the extra slices)
-  sh.XS = (sh.RP == 32 && c.n2 < (int64_t(1) << 18)) ? 3 : 2;
+  // leaves no shared memory for the extra slices); the TF32 kernel (XS = 0) has rank padding 32
+  if (precision == TCSCF_PREC_TF32) sh.XS = 0;
+  else sh.XS = (sh.RP == 32 && c.n2 < (int64_t(1) << 18)) ? 3 : 2;
   sh.n1pad = (c.n1 + tc::BM - 1) / tc::BM * tc::BM;
   sh.n2pad = (c.n2 + tc::BK - 1) / tc::BK * tc::BK;
   sh.nTiles = int(sh.n1pad / tc::BM);
@@ -998,12 +803,16 @@ size_t align256(size_t n) { return (n + 255) & ~size_t(255); }
 
 }  // namespace
 
-size_t tensorArenaBytes(Contraction const & c)
+size_t tensorArenaBytes(Contraction const & c, int precision)
 {
-  Shape const sh = shapeOf(c, smCount());
+  Shape const sh = shapeOf(c, smCount(), precision);
   size_t const bf = sizeof(__nv_bfloat16);
-  size_t b = 4 * align256(size_t(sh.n1pad) * sh.RP * bf) + 3 * align256(size_t(sh.n2pad) * sh.RP * bf);
-  if (!c.vtPacked) b += align256(packedVtBytes(sh.NB, sh.n2pad));
+  size_t b = 0;
+  if (precision == TCSCF_PREC_TF32) b += align256(tf32OperandBytes(sh.NB, sh.n1pad, sh.n2pad));
+  else {
+    b += 4 * align256(size_t(sh.n1pad) * sh.RP * bf) + 3 * align256(size_t(sh.n2pad) * sh.RP * bf);
+    if (!c.vtPacked) b += align256(packedVtBytes(sh.NB, sh.n2pad));
+  }
   b += align256(size_t(sh.n1pad) * sizeof(float4)) + align256(size_t(sh.n2pad) * sizeof(float4));
   b += align256(size_t(sh.n1pad) * sizeof(float)) + align256(size_t(sh.n2pad) * sizeof(float));
   if (sh.nSplit > 1 || !c.VH) b += align256(sizeof(double) * size_t(sh.nSplit) * c.n1 * (c.ldt + 1));
@@ -1014,18 +823,24 @@ int tensorPrepare(tcscf_ctx * ctx, Contraction const & c, int precision, void * 
 {
   std::string why;
   if (!tensorPathAvailable(c, precision, &why)) return fail(ctx, TCSCF_ERR_UNSUPPORTED, why);
-  TCSCF_CHECK(ctx, arenaBytes >= tensorArenaBytes(c), TCSCF_ERR_INVALID_ARGUMENT, "internal: tensor arena too small");
-  Shape const sh = shapeOf(c, smCount());
+  TCSCF_CHECK(ctx, arenaBytes >= tensorArenaBytes(c, precision), TCSCF_ERR_INVALID_ARGUMENT, "internal: tensor arena too small");
+  Shape const sh = shapeOf(c, smCount(), precision);
   int const NB = sh.NB, RP = sh.RP;
+  bool const tf32 = precision == TCSCF_PREC_TF32;
   int64_t const n1pad = sh.n1pad, n2pad = sh.n2pad;
   size_t const bf = sizeof(__nv_bfloat16);
   char * q = reinterpret_cast<char *>((reinterpret_cast<uintptr_t>(arena) + 255) & ~uintptr_t(255));
   auto take = [&](size_t n) { char * r = q; q += align256(n); return r; };
-  __nv_bfloat16 * psi1s[4];
-  __nv_bfloat16 * psi2s[3];
-  for (auto & a : psi1s) a = reinterpret_cast<__nv_bfloat16 *>(take(size_t(n1pad) * RP * bf));
-  for (auto & a : psi2s) a = reinterpret_cast<__nv_bfloat16 *>(take(size_t(n2pad) * RP * bf));
-  void * vt = c.vtPacked ? const_cast<void *>(c.vtPacked) : take(packedVtBytes(NB, n2pad));
+  __nv_bfloat16 * psi1s[4] = {};
+  __nv_bfloat16 * psi2s[3] = {};
+  void * vt = nullptr;
+  void * tf32Ops = nullptr;
+  if (tf32) tf32Ops = take(tf32OperandBytes(NB, n1pad, n2pad));
+  else {
+    for (auto & a : psi1s) a = reinterpret_cast<__nv_bfloat16 *>(take(size_t(n1pad) * RP * bf));
+    for (auto & a : psi2s) a = reinterpret_cast<__nv_bfloat16 *>(take(size_t(n2pad) * RP * bf));
+    vt = c.vtPacked ? const_cast<void *>(c.vtPacked) : take(packedVtBytes(NB, n2pad));
+  }
   auto * r1c = reinterpret_cast<float4 *>(take(size_t(n1pad) * sizeof(float4)));
   auto * r2c = reinterpret_cast<float4 *>(take(size_t(n2pad) * sizeof(float4)));
   auto * a1inv = reinterpret_cast<float *>(take(size_t(n1pad) * sizeof(float)));
@@ -1038,6 +853,22 @@ int tensorPrepare(tcscf_ctx * ctx, Contraction const & c, int precision, void * 
     if (sh.nSplit > 1) Tout = sp;
     VHout = sp + size_t(sh.nSplit) * c.n1 * c.ldt;
   }
+  tc::kPackCoords<<<gridBlocks(n1pad, 256), 256, 0, ctx->stream>>>(c.n1, n1pad, c.p1, r1c);
+  TCSCF_LAUNCH(ctx);
+  tc::kPackCoordPairs<<<gridBlocks(n2pad / 2, 256), 256, 0, ctx->stream>>>(c.n2, n2pad, c.p2, c.coul, r2c);
+  TCSCF_LAUNCH(ctx);
+  TCSCF_CUDA(ctx, cudaMemsetAsync(VHout, 0, sizeof(double) * size_t(sh.nSplit) * c.n1, ctx->stream));
+  tc::Instance & I = tp.inst;
+  I = tc::Instance{};
+  I.nTiles = sh.nTiles; I.nSplit = sh.nSplit; I.blocksPerSplit = sh.perSplit; I.nBlocks = sh.nBlocks;
+  I.n1 = int(c.n1); I.nb = c.ncol; I.ldt = c.ldt;
+  I.r1xyz = r1c; I.r2pairs = r2c;
+  I.T = Tout; I.VH = VHout;
+  I.tStride = int64_t(c.n1) * c.ldt; I.vhStride = c.n1;
+  tp.NB = NB; tp.RP = RP; tp.XS = sh.XS;
+  tp.c = c;
+  if (tf32) return tf32PackOperands(ctx, c, NB, n1pad, n2pad, tf32Ops, tp.maps);
+
   auto * vts = static_cast<__nv_bfloat16 *>(vt);   // h, m, l slices [NB][n2pad] each
   auto * cinv = reinterpret_cast<float *>(vts + 3 * size_t(NB) * n2pad);
 
@@ -1049,11 +880,6 @@ int tensorPrepare(tcscf_ctx * ctx, Contraction const & c, int precision, void * 
                                                                       nullptr, a2inv);
   TCSCF_LAUNCH(ctx);
   if (!c.vtPacked) TCSCF_TRY(packVt(ctx, c.n2, n2pad, c.ncol, NB, c.V, c.ldv, vt));
-  tc::kPackCoords<<<gridBlocks(n1pad, 256), 256, 0, ctx->stream>>>(c.n1, n1pad, c.p1, r1c);
-  TCSCF_LAUNCH(ctx);
-  tc::kPackCoordPairs<<<gridBlocks(n2pad / 2, 256), 256, 0, ctx->stream>>>(c.n2, n2pad, c.p2, c.coul, r2c);
-  TCSCF_LAUNCH(ctx);
-  TCSCF_CUDA(ctx, cudaMemsetAsync(VHout, 0, sizeof(double) * size_t(sh.nSplit) * c.n1, ctx->stream));
 
   CUtensorMapSwizzle const psw = RP == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B;
   bool okm = true;
@@ -1063,20 +889,11 @@ int tensorPrepare(tcscf_ctx * ctx, Contraction const & c, int precision, void * 
     okm = okm && makeMap(&tp.maps[7 + i], vts + size_t(i) * NB * n2pad, n2pad, NB, tc::BK, NB, CU_TENSOR_MAP_SWIZZLE_128B);
   }
   TCSCF_CHECK(ctx, okm, TCSCF_ERR_CUDA, "cuTensorMapEncodeTiled failed");
-
-  tc::Instance & I = tp.inst;
-  I = tc::Instance{};
-  I.nTiles = sh.nTiles; I.nSplit = sh.nSplit; I.blocksPerSplit = sh.perSplit; I.nBlocks = sh.nBlocks;
-  I.n1 = int(c.n1); I.nb = c.ncol; I.ldt = c.ldt;
-  I.r1xyz = r1c; I.r2pairs = r2c; I.a1inv = a1inv; I.a2inv = a2inv; I.cinv = cinv;
-  I.T = Tout; I.VH = VHout;
-  I.tStride = int64_t(c.n1) * c.ldt; I.vhStride = c.n1;
-  tp.NB = NB; tp.RP = RP; tp.XS = sh.XS;
-  tp.c = c;
+  I.a1inv = a1inv; I.a2inv = a2inv; I.cinv = cinv;
   return TCSCF_OK;
 }
 
-int tensorRun(tcscf_ctx * ctx, TensorPrep * const * preps, int count)
+int tensorRun(tcscf_ctx * ctx, TensorPrep * const * preps, int count, bool recordStart)
 {
   int const sms = smCount();
   // instance table and tensor maps in device memory (maps 64-byte aligned), then the work items
@@ -1105,7 +922,7 @@ int tensorRun(tcscf_ctx * ctx, TensorPrep * const * preps, int count)
   std::vector<int4> hItems;
   hItems.reserve(itemsTotal);
   size_t offset = 0;
-  cudaEventRecord(ctx->ev[2], ctx->stream);
+  if (recordStart) cudaEventRecord(ctx->ev[2], ctx->stream);
   for (auto const & cl : kClasses) {
     int const NB = cl[0], RP = cl[1], XS = cl[2];
     std::vector<int4> items;
@@ -1143,17 +960,58 @@ int tensorRun(tcscf_ctx * ctx, TensorPrep * const * preps, int count)
   return TCSCF_OK;
 }
 
-int contractTensor(tcscf_ctx * ctx, Contraction const & c, int precision)
+namespace {
+
+// T[r][j] += A[r][j] for j < ncol (leading dimension ld)
+__global__ void kAddInto(int64_t n1, int ncol, int ld, const double * A, double * T)
+{
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n1 * ncol; i += int64_t(gridDim.x) * blockDim.x) {
+    int64_t const r = i / ncol;
+    int const j = int(i % ncol);
+    T[r * ld + j] += A[r * ld + j];
+  }
+}
+
+int contractTensorOnce(tcscf_ctx * ctx, Contraction const & c, int precision, bool recordStart)
 {
   std::string why;
   if (!tensorPathAvailable(c, precision, &why)) return fail(ctx, TCSCF_ERR_UNSUPPORTED, why);
-  size_t const bytes = tensorArenaBytes(c);
+  size_t const bytes = tensorArenaBytes(c, precision);
   void * p = nullptr;
   TCSCF_TRY(scratch(ctx, "flash_tc_ops", bytes, &p));
   TensorPrep tp;
   TCSCF_TRY(tensorPrepare(ctx, c, precision, p, bytes, tp));
   TensorPrep * one = &tp;
-  return tensorRun(ctx, &one, 1);
+  return tensorRun(ctx, &one, 1, recordStart);
+}
+
+}  // namespace
+
+int tensorRankLimit(Contraction const & c, int precision) { return precision == TCSCF_PREC_TF32 || c.ncol > 64 ? 32 : 64; }
+
+int contractTensor(tcscf_ctx * ctx, Contraction const & c, int precision)
+{
+  int const lim = tensorRankLimit(c, precision);
+  if (c.R <= lim) return contractTensorOnce(ctx, c, precision, true);
+  // rho is linear in the density factor: a rank beyond what one launch's psi tiles hold (32 for TF32
+  // or with nb > 64, 64 otherwise) is contracted in column chunks whose T add up (the Coulomb potential,
+  // which does not depend on the factor, with the first); ev[2] / ev[3] span all chunks
+  double * tmp = nullptr;
+  TCSCF_TRY(scratch(ctx, "flash_tc_rank_chunk", sizeof(double) * size_t(c.n1) * c.ldt, reinterpret_cast<void **>(&tmp)));
+  for (int r0 = 0; r0 < c.R; r0 += lim) {
+    Contraction ck = c;
+    ck.R = std::min(lim, c.R - r0);
+    ck.psi1 = c.psi1 + r0;
+    ck.psi2 = c.psi2 + r0;
+    if (r0 > 0) { ck.coul = nullptr; ck.VH = nullptr; ck.T = tmp; }
+    TCSCF_TRY(contractTensorOnce(ctx, ck, precision, r0 == 0));
+    if (r0 > 0) {
+      kAddInto<<<gridBlocks(c.n1 * c.ncol, 256), 256, 0, ctx->stream>>>(c.n1, c.ncol, c.ldt, tmp, c.T);
+      TCSCF_LAUNCH(ctx);
+    }
+  }
+  cudaEventRecord(ctx->ev[3], ctx->stream);
+  return TCSCF_OK;
 }
 
 }  // namespace tcscf

@@ -33,9 +33,13 @@ struct Contraction {
 
 int contractFp64(tcscf_ctx * ctx, Contraction const & c);
 
-// tensor-core (tcgen05) contraction of the same quantity for g = 1/r12 (flash_tc.cu)
+// tensor-core (tcgen05) contraction of the same quantity for g = 1/r12: split-BF16 (flash_tc.cu) or
+// TF32 (flash_tf32.cu)
 int contractTensor(tcscf_ctx * ctx, Contraction const & c, int precision);
+// one launch of the tensor path (contractTensor splits a larger density factor rank into chunks of
+// tensorRankLimit columns)
 bool tensorPathAvailable(Contraction const & c, int precision, std::string * why);
+int tensorRankLimit(Contraction const & c, int precision);
 // packs (once per grid) the transposed operand Vt of the tensor path from V [n2][nb]: BF16 slices
 // hi/lo [NB][n2pad] followed by the per-block column scales
 int tensorPackedV(tcscf_ctx * ctx, Grid & g2, const double * V, double scale, const void ** packed);
@@ -67,7 +71,7 @@ constexpr int kTensorMapsPerInstance = 10;
 
 // a contraction whose operands are packed (tensorPrepare) and ready for tensorRun
 struct TensorPrep {
-  int NB = 0, RP = 0, XS = 2;   // Vt tile columns, rank padding, X slices (2: 16 bits, 3: 24 bits)
+  int NB = 0, RP = 0, XS = 2;   // Vt tile columns, rank padding, X slices (2: 16 bits, 3: 24 bits; 0: the TF32 kernel)
   Contraction c;
   TensorInstance inst{};
   CUtensorMap maps[kTensorMapsPerInstance];
@@ -77,9 +81,9 @@ struct TensorPrep {
 // device arena of tensorArenaBytes(c) bytes (tensorPrepare); any number of prepared contractions then
 // run in one persistent launch per tile class (tensorRun), which also sums the r2-split partials
 // into c.T / c.VH.
-size_t tensorArenaBytes(Contraction const & c);
+size_t tensorArenaBytes(Contraction const & c, int precision = TCSCF_PREC_BF16X3);
 int tensorPrepare(tcscf_ctx * ctx, Contraction const & c, int precision, void * arena, size_t arenaBytes, TensorPrep & tp);
-int tensorRun(tcscf_ctx * ctx, TensorPrep * const * preps, int count);
+int tensorRun(tcscf_ctx * ctx, TensorPrep * const * preps, int count, bool recordStart = true);
 
 // out[r][c] = sum_s part[s*stride + r*ldPart + c] for r < rows, c < cols (deterministic split sum)
 int sumSplitsLaunch(tcscf_ctx * ctx, int64_t n, int nsplit, int64_t stride, const double * part, double * out, int64_t rows, int cols,

@@ -702,7 +702,7 @@ int fockBuildDevice(tcscf_ctx * ctx, Grid & g1, Grid & g2, int nspin, const doub
   bool anyComplex = false;
   double contractionMs = 0;
   const void * vtPacked = nullptr;
-  if (precision != TCSCF_PREC_FP64) TCSCF_TRY(tensorPackedV(ctx, g2, V, scale, &vtPacked));
+  if (precision == TCSCF_PREC_BF16X3) TCSCF_TRY(tensorPackedV(ctx, g2, V, scale, &vtPacked));
   for (int s = 0; s < nspin; ++s) {
     Factor f;
     TCSCF_TRY(factorDensity(ctx, g1, dD + size_t(s) * nb * nb, s, f));
@@ -814,7 +814,7 @@ int fockBuildBatch(tcscf_ctx * ctx, int count, Grid * const * g1s, Grid * const 
     Contraction & c = cs[k];
     c.n1 = g1.n; c.n2 = g2.n; c.R = std::min(nb, 32); c.ncol = nb; c.ldpsi = nb; c.ldt = nb;
     c.p1 = g1.pts; c.p2 = g2.pts;
-    arenaBytes[k] = tensorArenaBytes(c);
+    arenaBytes[k] = tensorArenaBytes(c, precision);
     size_t const own = (sizeof(double) * (size_t(g1.n) * nb + g1.n + size_t(nb) * nb) + 255) & ~size_t(255);
     offs[k + 1] = offs[k] + own + ((arenaBytes[k] + 255) & ~size_t(255));
   }
@@ -840,13 +840,13 @@ int fockBuildBatch(tcscf_ctx * ctx, int count, Grid * const * g1s, Grid * const 
     c.T = T; c.VH = VH; c.V = V; c.ldv = nb;
     c.psi1 = psi1; c.psi2 = psi2; c.coul = coul;
     std::string why;
-    bool const eligible = precision == TCSCF_PREC_BF16X3 && f.R > 0 && !f.complex && tensorPathAvailable(c, precision, &why) &&
-                          tensorArenaBytes(c) <= arenaBytes[k];
+    bool const eligible = (precision == TCSCF_PREC_BF16X3 || precision == TCSCF_PREC_TF32) && f.R > 0 && !f.complex &&
+                          tensorPathAvailable(c, precision, &why) && tensorArenaBytes(c, precision) <= arenaBytes[k];
     if (!eligible) continue;
     kWeightedBasis<<<gridBlocks(n2 * nb, 256), 256, 0, ctx->stream>>>(n2, nb, g2.phiR, g2.w, scale, V);
     TCSCF_LAUNCH(ctx);
     const void * vtPacked = nullptr;
-    TCSCF_TRY(tensorPackedV(ctx, g2, V, scale, &vtPacked));
+    if (precision == TCSCF_PREC_BF16X3) TCSCF_TRY(tensorPackedV(ctx, g2, V, scale, &vtPacked));
     c.vtPacked = vtPacked;
     size_t const sm = sizeof(double) * size_t(nb) * f.R;
     kOrbitals<<<gridBlocks(n1 * f.R, 256), 256, sm, ctx->stream>>>(n1, nb, f.R, g1.phiR, f.X1, f.ldx, psi1, nb);
@@ -1332,7 +1332,7 @@ int tcscf_fock_build_batch(tcscf_ctx * ctx, int count, const int * r1, const int
   if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
   cudaSetDevice(ctx->device);
   TCSCF_CHECK(ctx, count >= 1 && r1 && r2 && density && h && energy, TCSCF_ERR_INVALID_ARGUMENT, "batch: count, grids, densities, h and energy are required");
-  TCSCF_CHECK(ctx, precision == TCSCF_PREC_FP64 || precision == TCSCF_PREC_BF16X3, TCSCF_ERR_INVALID_ARGUMENT, "unknown precision");
+  TCSCF_CHECK(ctx, precision >= TCSCF_PREC_FP64 && precision <= TCSCF_PREC_TF32, TCSCF_ERR_INVALID_ARGUMENT, "unknown precision");
   std::vector<Grid *> g1s(count), g2s(count);
   size_t io = 0;
   for (int k = 0; k < count; ++k) {

@@ -60,5 +60,19 @@ def test_batch_fp64_and_arguments(ctx):
         _, _, Ed = api.fock_build(G, G, Ds[k], h, precision=ffi.PREC_FP64)
         assert abs(E[k] - Ed) < 1e-12 * max(1.0, abs(Ed))
     with pytest.raises(ffi.TcscfError) as e:
-        api.fock_build_batch(Gs, Gs, Ds, hs, precision=ffi.PREC_TF32)
+        api.fock_build_batch(Gs, Gs, Ds, hs, precision=7)
     assert e.value.code == ffi.ERR_INVALID_ARGUMENT
+
+
+def test_batch_tf32_matches_single_builds(ctx):
+    # the TF32 tile classes run in the same persistent launches: each instance's result is the one its
+    # own build gives (same tiles, splits and summation order)
+    inst = _instances(ctx, 3, 11)
+    rng = np.random.default_rng(13)
+    Ds = [real_density(w.basis, max(1, min(w.n_up, 4)), rng) for w, G, h in inst]
+    Gs = [G for w, G, h in inst]
+    hs = [h for w, G, h in inst]
+    E = api.fock_build_batch(Gs, Gs, Ds, hs, precision=ffi.PREC_TF32)
+    for k, (w, G, h) in enumerate(inst):
+        _, _, Et = api.fock_build(G, G, Ds[k], h, precision=ffi.PREC_TF32)
+        assert E[k] == Et, (k, E[k], Et)
