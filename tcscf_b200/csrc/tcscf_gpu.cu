@@ -284,6 +284,89 @@ __global__ void kHermitianCopy(int nb, const double2 * DR, double2 * Z)
 }
 
 // factor matrices X1, X2 [nb][ldx] from the kept eigenpairs (real case): X2 = v sqrt|l|, X1 = sign(l) X2
+constexpr int kCholeskyMaxNb = 128;
+
+// Pivoted (diagonal-pivoting) Cholesky factorisation of the real symmetric density A [nb][nb]:
+// A = L L^T with the R columns of L written to X1 and X2 ([nb][ldx], both L).  Stops when the largest
+// remaining diagonal is <= 1e-12 of the largest initial diagonal; info = {R, 0}, or {R, 1} when the
+// remainder is not negligible (largest |entry| above 1e-10 of the largest initial diagonal: the
+// density is not positive semi-definite and the caller factors it by eigen-decomposition).  One
+// block of 256 threads; shared memory nb * nb doubles (nb <= 128).
+__global__ void __launch_bounds__(256) kPivotedCholesky(int nb, const double * A, int ldx, double * X1, double * X2, int * info)
+{
+  extern __shared__ double S[];
+  __shared__ double lcol[kCholeskyMaxNb];
+  __shared__ int done[kCholeskyMaxNb];
+  __shared__ double rv[256];
+  __shared__ int ri[256];
+  int const t = threadIdx.x;
+  for (int i = t; i < nb * nb; i += 256) S[i] = A[i];
+  for (int i = t; i < nb; i += 256) done[i] = 0;
+  __syncthreads();
+  // block reduction of (value, index): largest value, smallest index among equals
+  auto argmax = [&](double v, int idx, double & bv, int & bi) {
+    rv[t] = v;
+    ri[t] = idx;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+      if (t < o) {
+        double const w = rv[t + o];
+        int const wi = ri[t + o];
+        if (w > rv[t] || (w == rv[t] && wi >= 0 && (ri[t] < 0 || wi < ri[t]))) { rv[t] = w; ri[t] = wi; }
+      }
+      __syncthreads();
+    }
+    bv = rv[0];
+    bi = ri[0];
+    __syncthreads();
+  };
+  double d0 = 0;
+  int unused = 0;
+  {
+    double m = 0;
+    for (int i = t; i < nb; i += 256) m = fmax(m, S[i * nb + i]);
+    argmax(m, -1, d0, unused);
+  }
+  double const tol = 1e-12 * d0;
+  int R = 0;
+  for (; R < nb; ++R) {
+    double best = -1.0;
+    int bi = -1;
+    for (int i = t; i < nb; i += 256)
+      if (!done[i] && S[i * nb + i] > best) { best = S[i * nb + i]; bi = i; }
+    double pv;
+    int p;
+    argmax(best, bi, pv, p);
+    if (p < 0 || !(pv > tol)) break;
+    double const sq = sqrt(pv), inv = 1.0 / sq;
+    for (int i = t; i < nb; i += 256) {
+      double const l = done[i] ? 0.0 : (i == p ? sq : S[i * nb + p] * inv);
+      lcol[i] = l;
+      X1[int64_t(i) * ldx + R] = l;
+      X2[int64_t(i) * ldx + R] = l;
+    }
+    __syncthreads();
+    for (int idx = t; idx < nb * nb; idx += 256) S[idx] -= lcol[idx / nb] * lcol[idx % nb];
+    if (t == 0) done[p] = 1;
+    __syncthreads();
+  }
+  double r = 0;
+  for (int idx = t; idx < nb * nb; idx += 256)
+    if (!done[idx / nb] && !done[idx % nb]) r = fmax(r, fabs(S[idx]));
+  double rmax;
+  argmax(r, -1, rmax, unused);
+  if (t == 0) {
+    info[0] = R;
+    info[1] = (rmax > 1e-10 * d0 || !(rmax == rmax)) ? 1 : 0;
+  }
+}
+
+// status of a density the pivoted Cholesky does not take (nb > 128): factor by eigen-decomposition
+__global__ void kMarkIndefinite(int * info)
+{
+  if (threadIdx.x == 0) { info[0] = 0; info[1] = 1; }
+}
+
 __global__ void kRealFactors(int nb, int nkeep, const int * keep, const double * W, const double * V, int ldx, double * X1, double * X2)
 {
   for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < nb * nkeep; idx += gridDim.x * blockDim.x) {
@@ -571,36 +654,84 @@ struct Factor {
 
 // Factor the spin density's real-harmonic form DR = X1 X2^T (real) or, for a density that is not
 // real in the real-harmonic basis, into the real/imaginary pair described in kComplexFactors.
-int factorDensity(tcscf_ctx * ctx, Grid & g, const double2 * dD, int spin, Factor & f)
+// Device buffers of one density factorisation: the real-harmonic density DR, its symmetrised real
+// part A, the factors X1 (X1im) and X2 [nb][ldx], and the status {max |Re DR|, max |Im DR|} with the
+// pivoted-Cholesky rank and flag behind it (FactorStatus).
+struct FactorStatus {
+  double maxAbs[2];
+  int rank, indefinite;
+};
+struct FactorBufs {
+  double2 * DR = nullptr;
+  double * A = nullptr;
+  double * X1 = nullptr, * X1im = nullptr, * X2 = nullptr;
+  FactorStatus * status = nullptr;
+};
+size_t factorBufBytes(int nb)
+{
+  size_t const nn = size_t(nb) * nb;
+  return nn * sizeof(double2) + nn * sizeof(double) + 3 * nn * 2 * sizeof(double) + 2 * sizeof(FactorStatus) + 256;
+}
+FactorBufs carveFactorBufs(void * p, int nb)
+{
+  size_t const nn = size_t(nb) * nb;
+  char * base = static_cast<char *>(p);
+  FactorBufs b;
+  b.DR = reinterpret_cast<double2 *>(base); base += nn * sizeof(double2);
+  b.A = reinterpret_cast<double *>(base); base += nn * sizeof(double);
+  b.X1 = reinterpret_cast<double *>(base); base += nn * 2 * sizeof(double);
+  b.X1im = reinterpret_cast<double *>(base); base += nn * 2 * sizeof(double);
+  b.X2 = reinterpret_cast<double *>(base); base += nn * 2 * sizeof(double);
+  b.status = reinterpret_cast<FactorStatus *>(base);
+  return b;
+}
+
+// Launches (no host synchronisation) the real-harmonic transform of the spin density, its split
+// into real and imaginary magnitudes, and the pivoted Cholesky factorisation of its real part.
+int factorLaunch(tcscf_ctx * ctx, Grid & g, const double2 * dD, FactorBufs const & b)
 {
   int const nb = g.nb;
   size_t const nn = size_t(nb) * nb;
-  void * p = nullptr;
-  TCSCF_TRY(scratch(ctx, spin ? "fac1" : "fac0", nn * sizeof(double2) * 3 + nn * sizeof(double) * 8 + 64 * sizeof(double) + nb * sizeof(int) + 4096, &p));
-  char * base = static_cast<char *>(p);
-  double2 * DR = reinterpret_cast<double2 *>(base); base += nn * sizeof(double2);
-  double2 * Z = reinterpret_cast<double2 *>(base); base += nn * sizeof(double2) * 2;
-  double * A = reinterpret_cast<double *>(base); base += nn * sizeof(double);
-  double * W = reinterpret_cast<double *>(base); base += nn * sizeof(double);
-  f.X1 = reinterpret_cast<double *>(base); base += nn * sizeof(double) * 2;
-  f.X1im = reinterpret_cast<double *>(base); base += nn * sizeof(double) * 2;
-  f.X2 = reinterpret_cast<double *>(base); base += nn * sizeof(double) * 2;
-  double * maxAbs = reinterpret_cast<double *>(base); base += 64 * sizeof(double);
-  int * keep = reinterpret_cast<int *>(base);
-  f.ldx = 2 * nb;
+  kDensityToReal<<<gridBlocks(nn, 256), 256, 0, ctx->stream>>>(1, nb, g.dsto, dD, b.DR);
+  TCSCF_LAUNCH(ctx);
+  kSplitDensity<<<1, 256, 0, ctx->stream>>>(nb, b.DR, b.A, b.status->maxAbs);
+  TCSCF_LAUNCH(ctx);
+  if (nb <= kCholeskyMaxNb) {
+    TCSCF_CUDA(ctx, cudaFuncSetAttribute(kPivotedCholesky, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(double) * kCholeskyMaxNb * kCholeskyMaxNb)));
+    kPivotedCholesky<<<1, 256, sizeof(double) * nn, ctx->stream>>>(nb, b.A, 2 * nb, b.X1, b.X2, &b.status->rank);
+    TCSCF_LAUNCH(ctx);
+  } else {
+    kMarkIndefinite<<<1, 32, 0, ctx->stream>>>(&b.status->rank);
+    TCSCF_LAUNCH(ctx);
+  }
+  return TCSCF_OK;
+}
 
-  kDensityToReal<<<gridBlocks(nn, 256), 256, 0, ctx->stream>>>(1, nb, g.dsto, dD, DR);
-  TCSCF_LAUNCH(ctx);
-  kSplitDensity<<<1, 256, 0, ctx->stream>>>(nb, DR, A, maxAbs);
-  TCSCF_LAUNCH(ctx);
-  double hmax[2];
-  TCSCF_CUDA(ctx, cudaMemcpyAsync(hmax, maxAbs, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-  TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+// Completes the factorisation from the status read back to the host: the pivoted Cholesky factor
+// (X1 = X2 = L) when the density is real and positive semi-definite in the real-harmonic basis,
+// otherwise the eigen-decomposition (real: DR = X1 X2^T with X1 = V sign(l) sqrt|l|, X2 = V sqrt|l|;
+// complex: the real/imaginary pair described in kComplexFactors), keeping the eigenvalues above
+// 1e-12 of the largest.
+int factorFinish(tcscf_ctx * ctx, Grid & g, FactorBufs const & b, FactorStatus const & st, Factor & f)
+{
+  int const nb = g.nb;
+  size_t const nn = size_t(nb) * nb;
+  f.X1 = b.X1; f.X1im = b.X1im; f.X2 = b.X2;
+  f.ldx = 2 * nb;
+  double const hmax[2] = {st.maxAbs[0], st.maxAbs[1]};
   if (!(hmax[0] == hmax[0]) || !(hmax[1] == hmax[1])) return fail(ctx, TCSCF_ERR_NONFINITE, "non-finite density");
   f.complex = hmax[1] > 1e-13 * std::max(hmax[0], 1e-300);
   if (hmax[0] == 0 && hmax[1] == 0) { f.R = 0; return TCSCF_OK; }
+  if (!f.complex && !st.indefinite) { f.R = st.rank; return TCSCF_OK; }
 
-  int * devInfo = reinterpret_cast<int *>(maxAbs + 8);
+  void * p = nullptr;
+  TCSCF_TRY(scratch(ctx, "fac_eig", nn * sizeof(double2) * 2 + nn * sizeof(double) + 64 * sizeof(double) + nb * sizeof(int) + 1024, &p));
+  char * base = static_cast<char *>(p);
+  double2 * Z = reinterpret_cast<double2 *>(base); base += nn * sizeof(double2) * 2;
+  double * W = reinterpret_cast<double *>(base); base += nn * sizeof(double);
+  int * devInfo = reinterpret_cast<int *>(base); base += 64 * sizeof(double);
+  int * keep = reinterpret_cast<int *>(base);
+  double * A = b.A;
   int lwork = 0;
   std::vector<double> hW(nb);
   if (!f.complex) {
@@ -611,7 +742,7 @@ int factorDensity(tcscf_ctx * ctx, Grid & g, const double2 * dD, int spin, Facto
     if (cusolverDnDsyevd(ctx->solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, nb, A, nb, W, static_cast<double *>(wk), lwork, devInfo) != CUSOLVER_STATUS_SUCCESS)
       return fail(ctx, TCSCF_ERR_LINALG, "cusolverDnDsyevd failed");
   } else {
-    kHermitianCopy<<<gridBlocks(nn, 256), 256, 0, ctx->stream>>>(nb, DR, Z);
+    kHermitianCopy<<<gridBlocks(nn, 256), 256, 0, ctx->stream>>>(nb, b.DR, Z);
     TCSCF_LAUNCH(ctx);
     if (cusolverDnZheevd_bufferSize(ctx->solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, nb, reinterpret_cast<cuDoubleComplex *>(Z), nb, W, &lwork) != CUSOLVER_STATUS_SUCCESS)
       return fail(ctx, TCSCF_ERR_LINALG, "cusolverDnZheevd_bufferSize failed");
@@ -645,6 +776,20 @@ int factorDensity(tcscf_ctx * ctx, Grid & g, const double2 * dD, int spin, Facto
   // host vectors go out of scope only after the stream has consumed `keep`
   TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return TCSCF_OK;
+}
+
+// Factor the spin density's real-harmonic form DR = X1 X2^T (one host synchronisation when the
+// pivoted Cholesky factor applies; see factorFinish).
+int factorDensity(tcscf_ctx * ctx, Grid & g, const double2 * dD, int spin, Factor & f)
+{
+  void * p = nullptr;
+  TCSCF_TRY(scratch(ctx, spin ? "fac1" : "fac0", factorBufBytes(g.nb), &p));
+  FactorBufs const b = carveFactorBufs(p, g.nb);
+  TCSCF_TRY(factorLaunch(ctx, g, dD, b));
+  FactorStatus st;
+  TCSCF_CUDA(ctx, cudaMemcpyAsync(&st, b.status, sizeof(FactorStatus), cudaMemcpyDeviceToHost, ctx->stream));
+  TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return factorFinish(ctx, g, b, st, f);
 }
 
 int checkBasisPair(tcscf_ctx * ctx, Grid * g1, Grid * g2)
@@ -820,6 +965,23 @@ int fockBuildBatch(tcscf_ctx * ctx, int count, Grid * const * g1s, Grid * const 
   }
   void * bp = nullptr;
   TCSCF_TRY(scratch(ctx, "batch_arena", offs[count] + 256, &bp));
+  // every instance's density factorisation is launched first, with one host synchronisation for all
+  std::vector<size_t> fOffs(count + 1, 0);
+  for (int k = 0; k < count; ++k) fOffs[k + 1] = fOffs[k] + ((factorBufBytes(g1s[k]->nb) + 255) & ~size_t(255));
+  void * fp = nullptr;
+  TCSCF_TRY(scratch(ctx, "batch_factors", fOffs[count] + 256, &fp));
+  void * sp = nullptr;
+  TCSCF_TRY(scratch(ctx, "batch_factor_status", sizeof(FactorStatus) * count + 256, &sp));
+  auto * dStatus = static_cast<FactorStatus *>(sp);
+  std::vector<FactorBufs> fbufs(count);
+  for (int k = 0; k < count; ++k) {
+    fbufs[k] = carveFactorBufs(static_cast<char *>(fp) + fOffs[k], g1s[k]->nb);
+    TCSCF_TRY(factorLaunch(ctx, *g1s[k], dDs[k], fbufs[k]));
+    TCSCF_CUDA(ctx, cudaMemcpyAsync(dStatus + k, fbufs[k].status, sizeof(FactorStatus), cudaMemcpyDeviceToDevice, ctx->stream));
+  }
+  std::vector<FactorStatus> hStatus(count);
+  TCSCF_CUDA(ctx, cudaMemcpyAsync(hStatus.data(), dStatus, sizeof(FactorStatus) * count, cudaMemcpyDeviceToHost, ctx->stream));
+  TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   std::vector<TensorPrep> preps(count);
   std::vector<TensorPrep *> ready;
   for (int k = 0; k < count; ++k) {
@@ -834,7 +996,7 @@ int fockBuildBatch(tcscf_ctx * ctx, int count, Grid * const * g1s, Grid * const 
     double * GR = VH + n1;
     void * arena = base + ((sizeof(double) * (size_t(n1) * nb + n1 + size_t(nb) * nb) + 255) & ~size_t(255));
     Factor f;
-    TCSCF_TRY(factorDensity(ctx, g1, dDs[k], 0, f));
+    TCSCF_TRY(factorFinish(ctx, g1, fbufs[k], hStatus[k], f));
     Contraction & c = cs[k];
     c.R = f.R;
     c.T = T; c.VH = VH; c.V = V; c.ldv = nb;
