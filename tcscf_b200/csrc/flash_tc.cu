@@ -20,7 +20,7 @@
 // its 16-bit X).  The hi*hi accumulation being exact, the tensor core's FP32 adder rounding cannot
 // bias the result; the products below 2^-24 of the largest term are dropped.  Each block's T is
 // added with its scales, as soon as the block completes, into per-thread double-float accumulators
-// (FP32 hi + lo updated by the error-free TwoSum; about 48 bits, no FP64 or conversion pipe work).
+// (FP32 hi + lo updated by Fast2Sum; about 48 bits, no FP64 or conversion pipe work).
 // The kernel matrix g exists only as the BF16 X tile in shared memory.
 //
 // Warp roles (384 threads, one CTA per SM, persistent over (r1 tile, r2 split) work items):
@@ -117,7 +117,7 @@ __device__ __forceinline__ uint32_t bf16PairExact(uint64_t ab)
 }
 
 // Adds the finished block f (this thread's row, NB/2 columns of T) with the block's scales into the
-// double-float accumulators (hi + lo per column, FP32 pairs of columns) by the error-free TwoSum,
+// double-float accumulators (hi + lo per column, FP32 pairs of columns) by Fast2Sum,
 // and hands the TMEM accumulators back to the MMA issuer.
 template <int NB, class SmemT>
 __device__ __forceinline__ bool flushBlock(SmemT & S, uint32_t taddr, uint32_t f, int cw, float fac, uint64_t (&hi)[NB / 4],
@@ -147,12 +147,12 @@ __device__ __forceinline__ bool flushBlock(SmemT & S, uint32_t taddr, uint32_t f
       // of two, so x is that sum in the units of T
       uint64_t const x = f2mul(f2fma(f2pack(hh[cur][2 * i], hh[cur][2 * i + 1]), k256, f2pack(mm[cur][2 * i], mm[cur][2 * i + 1])),
                                f2mul(f2pack(c2.x, c2.y), ff));
-      // TwoSum: s + e == hi + x exactly
       int const p = q * 4 + i;
+      // Fast2Sum: hi + x == sum + (x - (sum - hi)) exactly when |hi| >= |x|, which holds once a
+      // row's sum has absorbed its first blocks; otherwise the compensation is approximate at the
+      // level of the rounding of the smaller term
       uint64_t const sum = f2add(hi[p], x);
-      uint64_t const bp = f2sub(sum, hi[p]);
-      uint64_t const err = f2add(f2sub(hi[p], f2sub(sum, bp)), f2sub(x, bp));
-      lo[p] = f2add(lo[p], err);
+      lo[p] = f2add(lo[p], f2sub(x, f2sub(sum, hi[p])));
       hi[p] = sum;
     }
     if (q + 1 < NQ) tmemWaitLoad8(hh[cur ^ 1], mm[cur ^ 1]);

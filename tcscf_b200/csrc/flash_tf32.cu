@@ -10,7 +10,7 @@
 // nearest): psi1, psi2 and Vt when they are packed, X when it is written to shared memory.  No
 // scales are needed (TF32 keeps the FP32 exponent range).  Each block's FP32 tensor-core sum is
 // added, as soon as the block completes, into per-thread double-float accumulators (FP32 hi + lo,
-// error-free TwoSum), so the only approximations are the TF32 operand roundings and the FP32
+// Fast2Sum), so the only approximations are the TF32 operand roundings and the FP32
 // accumulation inside one 64-point block.
 //
 // Shared-memory operands are K-major with the 128-byte swizzle: a 128-byte row holds 32 FP32 values,
@@ -80,7 +80,7 @@ __device__ __forceinline__ void tmemWait8(float (&a)[8])
 }
 
 // Adds the finished block f (this thread's row, NB/2 columns of T) into the double-float
-// accumulators by the error-free TwoSum and hands the TMEM accumulator back to the MMA issuer.
+// accumulators by Fast2Sum and hands the TMEM accumulator back to the MMA issuer.
 template <int NB, class SmemT>
 __device__ __forceinline__ bool flushTf32(SmemT & S, uint32_t taddr, uint32_t f, uint64_t (&hi)[NB / 4], uint64_t (&lo)[NB / 4], int lane,
                                           volatile int * abortFlag, int * status)
@@ -99,10 +99,11 @@ __device__ __forceinline__ bool flushTf32(SmemT & S, uint32_t taddr, uint32_t f,
     for (int i = 0; i < 4; ++i) {
       uint64_t const x = f2pack(tt[cur][2 * i], tt[cur][2 * i + 1]);
       int const p = q * 4 + i;
+      // Fast2Sum: hi + x == sum + (x - (sum - hi)) exactly when |hi| >= |x|, which holds once a
+      // row's sum has absorbed its first blocks; otherwise the compensation is approximate at the
+      // level of the rounding of the smaller term
       uint64_t const sum = f2add(hi[p], x);
-      uint64_t const bp = f2sub(sum, hi[p]);
-      uint64_t const err = f2add(f2sub(hi[p], f2sub(sum, bp)), f2sub(x, bp));
-      lo[p] = f2add(lo[p], err);
+      lo[p] = f2add(lo[p], f2sub(x, f2sub(sum, hi[p])));
       hi[p] = sum;
     }
     if (q + 1 < NQ) tmemWait8(tt[cur ^ 1]);

@@ -361,6 +361,67 @@ __global__ void __launch_bounds__(256) kPivotedCholesky(int nb, const double * A
   }
 }
 
+// One-sided Jacobi (Hestenes) orthogonalisation of the R = info[0] factor columns L [nb][ldx] of X1
+// (skipped when info[1] flags an indefinite density): L <- L W with W orthogonal, chosen so that the
+// columns of L W are mutually orthogonal; X X^T = L L^T is unchanged and X's columns become the
+// density's eigenvectors scaled by the square roots of its eigenvalues (the factor the fixed-point
+// and TF32 contractions are accurate with: no cancellation between columns).  The result goes to
+// X1 and X2.  One block of 256 threads: column pairs in round-robin order, one pair per warp at a
+// time; at most 30 sweeps, ending when every pair is orthogonal to 1e-15 of its norms.
+__global__ void __launch_bounds__(256) kOrthogonalizeFactor(int nb, int ldx, double * X1, double * X2, const int * info)
+{
+  extern __shared__ double Lc[];   // [R][nb]: column a at Lc + a * nb
+  __shared__ int rotated;
+  int const R = info[0];
+  if (info[1] || R < 2) return;
+  int const t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  for (int idx = t; idx < R * nb; idx += 256) Lc[idx] = X1[int64_t(idx % nb) * ldx + idx / nb];
+  __syncthreads();
+  int const Rp = R + (R & 1);   // an even number of slots (the last one idle when R is odd)
+  for (int sweep = 0; sweep < 30; ++sweep) {
+    if (t == 0) rotated = 0;
+    __syncthreads();
+    for (int step = 0; step < Rp - 1; ++step) {
+      for (int k = warp; k < Rp / 2; k += 8) {
+        int const a = k == 0 ? Rp - 1 : (step + k) % (Rp - 1);
+        int const b = k == 0 ? step : (step - k + Rp - 1) % (Rp - 1);
+        if (a >= R || b >= R) continue;
+        double * ca = Lc + a * nb;
+        double * cb = Lc + b * nb;
+        double al = 0, be = 0, ga = 0;
+        for (int i = lane; i < nb; i += 32) {
+          al += ca[i] * ca[i];
+          be += cb[i] * cb[i];
+          ga += ca[i] * cb[i];
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+          al += __shfl_xor_sync(0xffffffffu, al, o);
+          be += __shfl_xor_sync(0xffffffffu, be, o);
+          ga += __shfl_xor_sync(0xffffffffu, ga, o);
+        }
+        if (!(fabs(ga) > 1e-15 * sqrt(al * be))) continue;
+        double const zeta = (be - al) / (2.0 * ga);
+        double const tn = copysign(1.0, zeta) / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+        double const c = 1.0 / sqrt(1.0 + tn * tn), sn = c * tn;
+        for (int i = lane; i < nb; i += 32) {
+          double const x = ca[i], y = cb[i];
+          ca[i] = c * x - sn * y;
+          cb[i] = sn * x + c * y;
+        }
+        if (lane == 0) rotated = 1;
+      }
+      __syncthreads();
+    }
+    if (!rotated) break;
+    __syncthreads();
+  }
+  for (int idx = t; idx < R * nb; idx += 256) {
+    int64_t const o = int64_t(idx % nb) * ldx + idx / nb;
+    X1[o] = Lc[idx];
+    X2[o] = Lc[idx];
+  }
+}
+
 // status of a density the pivoted Cholesky does not take (nb > 128): factor by eigen-decomposition
 __global__ void kMarkIndefinite(int * info)
 {
@@ -700,6 +761,9 @@ int factorLaunch(tcscf_ctx * ctx, Grid & g, const double2 * dD, FactorBufs const
     TCSCF_CUDA(ctx, cudaFuncSetAttribute(kPivotedCholesky, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(double) * kCholeskyMaxNb * kCholeskyMaxNb)));
     kPivotedCholesky<<<1, 256, sizeof(double) * nn, ctx->stream>>>(nb, b.A, 2 * nb, b.X1, b.X2, &b.status->rank);
     TCSCF_LAUNCH(ctx);
+    TCSCF_CUDA(ctx, cudaFuncSetAttribute(kOrthogonalizeFactor, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(double) * kCholeskyMaxNb * kCholeskyMaxNb)));
+    kOrthogonalizeFactor<<<1, 256, sizeof(double) * nn, ctx->stream>>>(nb, 2 * nb, b.X1, b.X2, &b.status->rank);
+    TCSCF_LAUNCH(ctx);
   } else {
     kMarkIndefinite<<<1, 32, 0, ctx->stream>>>(&b.status->rank);
     TCSCF_LAUNCH(ctx);
@@ -708,7 +772,8 @@ int factorLaunch(tcscf_ctx * ctx, Grid & g, const double2 * dD, FactorBufs const
 }
 
 // Completes the factorisation from the status read back to the host: the pivoted Cholesky factor
-// (X1 = X2 = L) when the density is real and positive semi-definite in the real-harmonic basis,
+// with orthogonalised columns (X1 = X2 = L W) when the density is real and positive semi-definite in
+// the real-harmonic basis,
 // otherwise the eigen-decomposition (real: DR = X1 X2^T with X1 = V sign(l) sqrt|l|, X2 = V sqrt|l|;
 // complex: the real/imaginary pair described in kComplexFactors), keeping the eigenvalues above
 // 1e-12 of the largest.
