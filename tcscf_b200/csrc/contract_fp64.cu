@@ -256,26 +256,29 @@ __global__ void kSumSplits(int64_t n, int nsplit, int64_t stride, const double *
 
 // ---- real Fock reduction:  out[k][l] = sum_r w[r] phi[r][k] (cJ phi[r][l] VH[r] - sgnT T[r][l]) ----
 constexpr int RB = 16;      // rows per step
-constexpr int RCH = 1024;   // rows per block
+constexpr int RCH = 1024;   // rows per block (complex reduction; the real one sizes its row chunks per call)
 
-__global__ void __launch_bounds__(NT) kReduceReal(int64_t n1, int nb, const double * phi, const double * w, const double * VH,
+// one block: `rch` rows (a multiple of RB) into a W x W tile of out (W = 64 or 128; 16 x 16 threads, TT x TT each)
+template <int W>
+__global__ void __launch_bounds__(NT) kReduceReal(int64_t n1, int nb, int rch, const double * phi, const double * w, const double * VH,
                                                   double cJ, const double * T, int ldt, double sgnT, double * part)
 {
-  __shared__ __align__(16) double sA[RB][BN];
-  __shared__ __align__(16) double sY[RB][BN];
+  constexpr int TT = W / 16;
+  __shared__ __align__(16) double sA[RB][W];
+  __shared__ __align__(16) double sY[RB][W];
   int const tid = threadIdx.x;
-  int const kg = blockIdx.y * BN, lg = blockIdx.z * BN;
-  int64_t const rbeg = int64_t(blockIdx.x) * RCH, rend = min(n1, rbeg + RCH);
+  int const kg = blockIdx.y * W, lg = blockIdx.z * W;
+  int64_t const rbeg = int64_t(blockIdx.x) * rch, rend = min(n1, rbeg + rch);
   int const tk = tid >> 4, tl = tid & 15;
-  double acc[8][8];
+  double acc[TT][TT];
 #pragma unroll
-  for (int i = 0; i < 8; ++i)
+  for (int i = 0; i < TT; ++i)
 #pragma unroll
-    for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
+    for (int j = 0; j < TT; ++j) acc[i][j] = 0.0;
   for (int64_t r0 = rbeg; r0 < rend; r0 += RB) {
     __syncthreads();
-    for (int idx = tid; idx < RB * BN; idx += NT) {
-      int const rr = idx / BN, c = idx % BN;
+    for (int idx = tid; idx < RB * W; idx += NT) {
+      int const rr = idx / W, c = idx % W;
       int64_t const r = r0 + rr;
       double av = 0.0, yv = 0.0;
       if (r < rend) {
@@ -294,28 +297,28 @@ __global__ void __launch_bounds__(NT) kReduceReal(int64_t n1, int nb, const doub
     __syncthreads();
 #pragma unroll 2
     for (int rr = 0; rr < RB; ++rr) {
-      double av[8], bv[8];
+      double av[TT], bv[TT];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        double2 const x = *reinterpret_cast<double2 const *>(&sA[rr][tk * 8 + 2 * q]);
-        double2 const y = *reinterpret_cast<double2 const *>(&sY[rr][tl * 8 + 2 * q]);
+      for (int q = 0; q < TT / 2; ++q) {
+        double2 const x = *reinterpret_cast<double2 const *>(&sA[rr][tk * TT + 2 * q]);
+        double2 const y = *reinterpret_cast<double2 const *>(&sY[rr][tl * TT + 2 * q]);
         av[2 * q] = x.x; av[2 * q + 1] = x.y;
         bv[2 * q] = y.x; bv[2 * q + 1] = y.y;
       }
 #pragma unroll
-      for (int i = 0; i < 8; ++i)
+      for (int i = 0; i < TT; ++i)
 #pragma unroll
-        for (int j = 0; j < 8; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
+        for (int j = 0; j < TT; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
     }
   }
   double * out = part + int64_t(blockIdx.x) * nb * nb;
 #pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    int const k = kg + tk * 8 + i;
+  for (int i = 0; i < TT; ++i) {
+    int const k = kg + tk * TT + i;
     if (k >= nb) continue;
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      int const l = lg + tl * 8 + j;
+    for (int j = 0; j < TT; ++j) {
+      int const l = lg + tl * TT + j;
       if (l < nb) out[k * nb + l] = acc[i][j];
     }
   }
@@ -485,13 +488,20 @@ int sumSplitsLaunch(tcscf_ctx * ctx, int64_t n, int nsplit, int64_t stride, cons
 int reduceFockReal(tcscf_ctx * ctx, int64_t n1, int nb, const double * phi, const double * w1, const double * VH, double cJ,
                    const double * T, int ldt, double sgnT, double * out)
 {
-  int const g = (nb + BN - 1) / BN;
-  int64_t const chunks = (n1 + RCH - 1) / RCH;
+  // output tile 64 wide when nb <= 64; row chunks sized for about two blocks per SM (16 to 1024 rows)
+  int const W = nb <= 64 ? 64 : 128;
+  int const g = (nb + W - 1) / W;
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+  int64_t const want = (n1 + 2 * sms * g * g - 1) / (2 * sms * g * g);
+  int const rch = int(std::min<int64_t>(1024, std::max<int64_t>(RB, (want + RB - 1) / RB * RB)));
+  int64_t const chunks = (n1 + rch - 1) / rch;
   void * p = nullptr;
   TCSCF_TRY(scratch(ctx, "reduce_real", size_t(chunks) * nb * nb * sizeof(double), &p));
   double * part = static_cast<double *>(p);
   dim3 grid{unsigned(chunks), unsigned(g), unsigned(g)};
-  kReduceReal<<<grid, NT, 0, ctx->stream>>>(n1, nb, phi, w1, VH, cJ, T, ldt, sgnT, part);
+  if (W == 64) kReduceReal<64><<<grid, NT, 0, ctx->stream>>>(n1, nb, rch, phi, w1, VH, cJ, T, ldt, sgnT, part);
+  else kReduceReal<128><<<grid, NT, 0, ctx->stream>>>(n1, nb, rch, phi, w1, VH, cJ, T, ldt, sgnT, part);
   TCSCF_LAUNCH(ctx);
   int const n = nb * nb;
   kSumChunks<<<(n + 255) / 256, 256, 0, ctx->stream>>>(n, int(chunks), part, out);

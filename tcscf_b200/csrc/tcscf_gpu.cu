@@ -1057,8 +1057,7 @@ int fockBuildBatch(tcscf_ctx * ctx, int count, Grid * const * g1s, Grid * const 
     double const scale = g2.ndim == 2 ? 2 * kPi : 1.0;
     char * base = static_cast<char *>(bp) + offs[k];
     double * T = reinterpret_cast<double *>(base);
-    double * VH = T + size_t(n1) * nb;
-    double * GR = VH + n1;
+    double * VH = T + size_t(n1) * nb;   // followed by the instance's [nb][nb] reduction output
     void * arena = base + ((sizeof(double) * (size_t(n1) * nb + n1 + size_t(nb) * nb) + 255) & ~size_t(255));
     Factor f;
     TCSCF_TRY(factorFinish(ctx, g1, fbufs[k], hStatus[k], f));
