@@ -45,10 +45,21 @@ typedef enum tcscf_status {
   TCSCF_ERR_NO_DEVICE = 8
 } tcscf_status;
 
-/* Slater-type orbital (SlaterTypeOrbital.hpp:27-37): alpha = orbital exponent zeta. */
+/* Atomic basis function families; every function is radial(r) * Y_lm(theta, phi) and one basis
+ * holds one family (the reference's QMCGrid::setBasisFunctions is a template over the family). */
+typedef enum tcscf_basis_family {
+  TCSCF_BASIS_STO = 0,      /* SlaterTypeOrbital (SlaterTypeOrbital.hpp:27-106): N r^(n-1) e^(-alpha r), n >= 1 */
+  TCSCF_BASIS_OCHI = 1,     /* OchiBasisFunction (OchiBasis.hpp:14-110): N r^l L_n^(2l+2)(2 alpha r) e^(-alpha r), n >= 0 */
+  TCSCF_BASIS_HYDROGEN = 2  /* HydrogenLikeBasisFunction (HydrogenLikeBasis.hpp:11-60): alpha = Z, beta = Z / n,
+                               N r^l L_(n-l-1)^(2l+1)(2 beta r) e^(-beta r); values only (the reference has no gradient) */
+} tcscf_basis_family;
+
+/* One basis function (SlaterTypeOrbital / OchiBasisFunction / HydrogenLikeBasisFunction constructor
+ * arguments): alpha = orbital exponent (STO, Ochi) or nuclear charge Z (hydrogen-like); family is a
+ * tcscf_basis_family (0 = STO). */
 typedef struct tcscf_sto {
   double alpha;
-  int32_t n, l, m, pad;
+  int32_t n, l, m, family;
 } tcscf_sto;
 
 /* Ochi / Boys-Handy Jastrow factor (jastrowFunctions.hpp:9-115):
@@ -127,7 +138,14 @@ int tcscf_grid_qmc(int ndim, int64_t n, const double * u, double * pts, double *
  * un-vendored mppmu/qmc lattice generator (qmcWrapper.hpp:94-141). */
 int tcscf_sobol(int ndim, int64_t n, uint64_t seed, double * u);
 
-/* ---- analytic one-electron matrices (SlaterTypeOrbital.hpp:134-181) -------------------------- */
+/* ---- analytic one-electron matrices -----------------------------------------------------------
+ * STO: SlaterTypeOrbital.hpp:134-181.  Ochi: overlap = [n, l, m equal] (OchiBasis.hpp:118-125), core
+ * element from the radial integral of fnl fnl / r (OchiBasis.hpp:130-155) on the reference driver's
+ * 1000-point Chebyshev-Gauss grid with the Treutler-Ahlrichs M4 map (a = 1, eps = 0.9,
+ * HartreeFockTest.cpp:364-367); functions of different exponents have no core element
+ * (TCSCF_ERR_INVALID_ARGUMENT).  Hydrogen-like: overlap = [l, m equal] x the radial integral of
+ * R1 R2 r^2 on the same grid (the generic AtomicBasis.hpp overlap), core element -Z^2 / (2 n^2) when
+ * n, l, m are equal (HydrogenLikeBasis.hpp:70-82).  One family per call. */
 int tcscf_overlap_core_analytic(const tcscf_sto * basis, int nb, int Z, double * S, double * H);
 
 /* ---- device-resident grids (QMCGrid, integrateAll.hpp:12-142) ------------------------------- */

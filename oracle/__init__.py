@@ -23,7 +23,7 @@ _D = C.POINTER(C.c_double)
 
 
 class Sto(C.Structure):
-    _fields_ = [("alpha", C.c_double), ("n", C.c_int32), ("l", C.c_int32), ("m", C.c_int32), ("pad", C.c_int32)]
+    _fields_ = [("alpha", C.c_double), ("n", C.c_int32), ("l", C.c_int32), ("m", C.c_int32), ("family", C.c_int32)]
 
 
 class Ochi(C.Structure):
@@ -67,6 +67,7 @@ def _sto(basis):
     arr = (Sto * len(basis))()
     for i, b in enumerate(basis):
         arr[i].alpha, arr[i].n, arr[i].l, arr[i].m = float(b[0]), int(b[1]), int(b[2]), int(b[3])
+        arr[i].family = int(b[4]) if len(b) > 4 else 0
     return arr
 
 

@@ -36,7 +36,7 @@ namespace {
 
 constexpr double PI = 3.141592653589793238462643383279502884;
 
-struct Sto { double alpha; int32_t n, l, m; int32_t pad; };          // == tcscf_sto
+struct Sto { double alpha; int32_t n, l, m; int32_t family; };       // == tcscf_sto (family 0 STO, 1 Ochi, 2 hydrogen-like)
 struct Ochi { double a, a12; int32_t nterms, pad; int32_t S[8][3]; double c[8][2]; };  // == tcscf_ochi
 
 struct Vec3 { double x, y, z; };
@@ -54,9 +54,31 @@ cplx sphericalHarmonic(int l, int m, double theta, double phi)
 double stoNormalization(double alpha, int n)
 { return std::pow(2 * alpha, n) * std::sqrt(2 * alpha / factorial(2 * n)); }
 
-// SlaterTypeOrbital.hpp:57-58
+// mathFunctions.hpp:101-110
+double truncatedFactorial(int max, int min) { double r = 1; for (int i = min + 1; i <= max; ++i) r *= i; return r; }
+
+// OchiBasis.hpp:25-32 and HydrogenLikeBasis.hpp:22-30 (beta = Z / n)
+double ochiNormalization(double alpha, int n, int l) { return std::pow(2 * alpha, l + 1.5) / std::sqrt(truncatedFactorial(n + 2 * l + 2, n)); }
+double hydrogenNormalization(double Z, int n, int l)
+{ return -std::pow(2 * (Z / n), l + 1.5) / std::sqrt(2 * n * truncatedFactorial(n + l, n - l - 1)); }
+double basisNormalization(Sto const & b)
+{
+  if (b.family == 1) return ochiNormalization(b.alpha, b.n, b.l);
+  if (b.family == 2) return hydrogenNormalization(b.alpha, b.n, b.l);
+  return stoNormalization(b.alpha, b.n);
+}
+
+// SlaterTypeOrbital.hpp:57-58; OchiBasis.hpp:51-53; HydrogenLikeBasis.hpp:44-47 (assocLaguerre is
+// std::assoc_laguerre, mathFunctions.hpp:144-148)
 double radialComponent(Sto const & b, double nrm, double r)
-{ return nrm * std::pow(r, b.n - 1) * std::exp(-b.alpha * r); }
+{
+  if (b.family == 1) return nrm * std::pow(r, b.l) * std::assoc_laguerre(b.n, 2 * b.l + 2, 2 * b.alpha * r) * std::exp(-b.alpha * r);
+  if (b.family == 2) {
+    double const beta = b.alpha / b.n;
+    return nrm * std::pow(r, b.l) * std::assoc_laguerre(b.n - b.l - 1, 2 * b.l + 1, 2 * beta * r) * std::exp(-beta * r);
+  }
+  return nrm * std::pow(r, b.n - 1) * std::exp(-b.alpha * r);
+}
 
 // mathFunctions.hpp:240-261 (Cartesian::toSpherical)
 void toSpherical(double x, double y, double z, double & r, double & th, double & ph)
@@ -72,7 +94,13 @@ CVec3 stoGradient(Sto const & b, double nrm, double r, double th, double ph)
   int const n = b.n, l = b.l, m = b.m;
   double const radial = radialComponent(b, nrm, r);
   cplx const Ylm = sphericalHarmonic(l, m, th, ph);
-  double const dRadialPart = ((n - 1) / r - b.alpha) * radial;
+  double dRadialPart = ((n - 1) / r - b.alpha) * radial;
+  if (b.family == 1) {
+    // OchiBasis.hpp:64-72
+    double const dLaguerrePart = (n > 0) * -2 * b.alpha * nrm * std::pow(r, l) * std::exp(-b.alpha * r) *
+                                 (n > 0 ? std::assoc_laguerre(n - 1, 2 * l + 3, 2 * b.alpha * r) : 0.0);
+    dRadialPart = (l / r - b.alpha) * radial + dLaguerrePart;
+  }
   cplx const Ylmp1 = double(l != m) * std::sqrt(double((l - m) * (l + m + 1))) * cExp(-ph) * sphericalHarmonic(l, m + 1, th, ph);
   cplx const rHat = dRadialPart * Ylm;
   cplx const thetaHat = (double(m) * Ylm / std::tan(th) + Ylmp1) * radial / r;
@@ -442,7 +470,7 @@ void oracle_qmc_grid(int ndim, int64_t N, double const * u, double * pts, double
 void oracle_basis_values(double const * pts, int64_t N, int ndim, Sto const * basis, int nb, double * vals, double * grads)
 {
   std::vector<double> nrm(nb);
-  for (int b = 0; b < nb; ++b) nrm[b] = stoNormalization(basis[b].alpha, basis[b].n);
+  for (int b = 0; b < nb; ++b) nrm[b] = basisNormalization(basis[b]);
 #pragma omp parallel for schedule(static)
   for (int64_t i = 0; i < N; ++i) {
     Vec3 const p = point(pts, ndim, N, i);
@@ -470,6 +498,39 @@ double oracle_sto_normalization(double alpha, int n) { return stoNormalization(a
 // HartreeFockTest.cpp:370-381.  S, H row-major [nb][nb] (S(i,j) symmetric, real).
 void oracle_overlap_core(Sto const * basis, int nb, int Z, double * S, double * H)
 {
+  if (basis[0].family != 0) {
+    // Ochi (OchiBasis.hpp:118-155) and hydrogen-like (HydrogenLikeBasis.hpp:70-82; the generic overlap
+    // of AtomicBasis.hpp:19-31 reduced to its radial integral) on the reference driver's core grid:
+    // ChebyshevGauss(1000) with TreutlerAhlrichsM4(1, 0.9) (HartreeFockTest.cpp:364-367)
+    int const nr = 1000;
+    std::vector<double> r(nr), w(nr);
+    oracle_radial_grid(nr, 3, 1.0, 0.9, r.data(), w.data());
+    for (int i = 0; i < nb; ++i)
+      for (int j = 0; j < nb; ++j) {
+        Sto const & b1 = basis[i];
+        Sto const & b2 = basis[j];
+        double const n1 = basisNormalization(b1), n2 = basisNormalization(b2);
+        bool const lm = b1.l == b2.l && b1.m == b2.m;
+        double sv = 0, hv = 0;
+        if (b1.family == 1) {
+          sv = (b1.n == b2.n) && lm;
+          if (lm) {
+            double integral = 0;   // integrate<1>(grid, fnl1(r) / r * fnl2(r)), fnl = radial * r
+            for (int k = 0; k < nr; ++k)
+              integral += w[k] * (radialComponent(b1, n1, r[k]) * r[k]) * (1 / r[k]) * (radialComponent(b2, n2, r[k]) * r[k]);
+            double const coeff = b1.alpha * (b1.l + 1) * (1 + 2 * std::min(b1.n, b2.n) / double(2 * b1.l + 3)) - Z;
+            hv = coeff * integral - (b1.n == b2.n) * std::pow(b1.alpha, 2) / 2;
+          }
+        } else {
+          if (lm)
+            for (int k = 0; k < nr; ++k) sv += w[k] * radialComponent(b1, n1, r[k]) * radialComponent(b2, n2, r[k]) * r[k] * r[k];
+          if (b1.n == b2.n && lm) hv = -std::pow(Z, 2) / (2.0 * std::pow(b1.n, 2));
+        }
+        S[i * nb + j] = sv;
+        H[i * nb + j] = hv;
+      }
+    return;
+  }
   for (int i = 0; i < nb; ++i)
     for (int j = 0; j < nb; ++j) {
       Sto const & b1 = basis[i];

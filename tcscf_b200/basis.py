@@ -10,11 +10,24 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-Basis = list  # list of (alpha, n, l, m)
+Basis = list  # list of (alpha, n, l, m) Slater-type orbitals, or (alpha, n, l, m, family)
 
 
 def expand(l: int, zetas) -> Basis:
     return [(float(z), l + 1, l, m) for z in zetas for m in range(-l, l + 1)]
+
+
+def ochi_functions(n_max: int, l_max: int, alpha: float) -> Basis:
+    """Ochi functions (family 1) for n = 0..n_max, l = 0..l_max, m = -l..l in the order of
+    createBasisFunctions (src/unitTests/HartreeFockTest.cpp:153-172)."""
+    return [(float(alpha), n, l, m, 1) for n in range(n_max + 1) for l in range(l_max + 1) for m in range(-l, l + 1)]
+
+
+def hydrogen_functions(n_max: int, l_max: int, Z: int) -> Basis:
+    """Hydrogen-like functions (family 2, alpha = Z) for n = 1..n_max, l = 0..min(l_max, n - 1),
+    m = -l..l.  createBasisFunctions (src/unitTests/HartreeFockTest.cpp:178-198) runs l up to
+    min(l_max, n), which the constructor's l < n check (HydrogenLikeBasis.hpp:33) rejects at l = n."""
+    return [(float(Z), n, l, m, 2) for n in range(1, n_max + 1) for l in range(min(l_max, n - 1) + 1) for m in range(-l, l + 1)]
 
 
 def even_tempered(counts: dict[int, int], z0: float, ratio: float) -> Basis:
@@ -35,14 +48,16 @@ def real_harmonic_unitary(basis: Basis) -> np.ndarray:
     """U with phi^R = U phi: m > 0 -> (phi_m + phi_-m)/sqrt2, m < 0 -> (phi_|m| - phi_-|m|)/(i sqrt2)
     (the reference's Y_l^m = P_l^|m| e^{i m phi} convention, mathFunctions.hpp:126-139)."""
     nb = len(basis)
-    idx = {tuple(b): i for i, b in enumerate(basis)}
+    key = lambda b: (b[0], b[1], b[2], b[3], b[4] if len(b) > 4 else 0)
+    idx = {key(b): i for i, b in enumerate(basis)}
     U = np.zeros((nb, nb), dtype=complex)
     h = 1 / np.sqrt(2)
-    for k, (a, n, l, m) in enumerate(basis):
+    for k, b in enumerate(basis):
+        a, n, l, m, fam = key(b)
         if m == 0:
             U[k, k] = 1
             continue
-        p = idx[(a, n, l, -m)]
+        p = idx[(a, n, l, -m, fam)]
         if m > 0:
             U[k, k], U[k, p] = h, h
         else:

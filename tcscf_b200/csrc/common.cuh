@@ -5,12 +5,14 @@
 #include <cuda_runtime.h>
 #include <cublas_v2.h>
 #include <cusolverDn.h>
+#include <cmath>
 #include <cstdint>
 #include <map>
 #include <string>
 #include <vector>
 
 #include "../../include/tcscf_gpu.h"
+#include "basis.cuh"
 
 namespace tcscf {
 
@@ -19,13 +21,7 @@ constexpr double kPi = 3.141592653589793238462643383279502884;
 
 // Per basis function data the device evaluators read (SlaterTypeOrbital.hpp:27-37 fields plus the
 // real-harmonic type used by the tensor paths).
-struct DevSto {
-  double alpha, norm;
-  int n, l, m;
-  int rtype;    // 0: m == 0, 1: cos-type (m > 0), 2: sin-type (m < 0)
-  int partner;  // index of the -m function (-1 for m == 0)
-  int pad;
-};
+
 
 struct Grid {
   int64_t n = 0;

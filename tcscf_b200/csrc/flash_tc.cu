@@ -963,7 +963,7 @@ int tensorRun(tcscf_ctx * ctx, TensorPrep * const * preps, int count, bool recor
 namespace {
 
 // T[r][j] += A[r][j] for j < ncol (leading dimension ld)
-__global__ void kAddInto(int64_t n1, int ncol, int ld, const double * A, double * T)
+__global__ void kAddTChunk(int64_t n1, int ncol, int ld, const double * A, double * T)
 {
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n1 * ncol; i += int64_t(gridDim.x) * blockDim.x) {
     int64_t const r = i / ncol;
@@ -1006,7 +1006,7 @@ int contractTensor(tcscf_ctx * ctx, Contraction const & c, int precision)
     if (r0 > 0) { ck.coul = nullptr; ck.VH = nullptr; ck.T = tmp; }
     TCSCF_TRY(contractTensorOnce(ctx, ck, precision, r0 == 0));
     if (r0 > 0) {
-      kAddInto<<<gridBlocks(c.n1 * c.ncol, 256), 256, 0, ctx->stream>>>(c.n1, c.ncol, c.ldt, tmp, c.T);
+      kAddTChunk<<<gridBlocks(c.n1 * c.ncol, 256), 256, 0, ctx->stream>>>(c.n1, c.ncol, c.ldt, tmp, c.T);
       TCSCF_LAUNCH(ctx);
     }
   }

@@ -1,11 +1,13 @@
 // Host-side grid generation of libtcscf_gpu.so (negligible work, no device involvement):
 // Chebyshev-Gauss radial rules with the reference's changes of variables, radial x angular product
 // grids, the QMCGrid point mapping and a seeded scrambled Sobol point source.
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <vector>
 
 #include "../../include/tcscf_gpu.h"
+#include "basis.cuh"
 
 namespace {
 constexpr double kPi = 3.141592653589793238462643383279502884;
@@ -34,6 +36,64 @@ void directionNumbers(int dim, uint32_t v[32])
   }
   for (int k = 1; k <= 32; ++k) v[k - 1] = m[k] << (32 - k);
 }
+// Ochi and hydrogen-like one-electron matrices (tcscf_overlap_core_analytic).  Radial integrals use
+// the reference driver's core grid: 1000-point Chebyshev-Gauss with the Treutler-Ahlrichs M4 map,
+// a = 1, eps = 0.9 (HartreeFockTest.cpp:364-367).
+int overlapCoreLaguerre(const tcscf_sto * basis, int nb, int Z, double * S, double * H)
+{
+  int const nr = 1000;
+  std::vector<double> r(nr), w(nr);
+  tcscf_grid_radial(nr, TCSCF_MAP_TREUTLER_AHLRICHS_M4, 1.0, 0.9, r.data(), w.data());
+  std::vector<tcscf::DevSto> d(nb);
+  std::vector<double> R(size_t(nb) * nr);
+  for (int b = 0; b < nb; ++b) {
+    tcscf_sto const & s = basis[b];
+    if (s.n < (s.family == TCSCF_BASIS_OCHI ? 0 : 1) || s.l < std::abs(s.m) || !(s.alpha > 0)) return TCSCF_ERR_INVALID_ARGUMENT;
+    if (s.family == TCSCF_BASIS_HYDROGEN && s.l >= s.n) return TCSCF_ERR_INVALID_ARGUMENT;
+    d[b].alpha = s.family == TCSCF_BASIS_HYDROGEN ? s.alpha / s.n : s.alpha;
+    d[b].norm = tcscf::basisNormalization(s);
+    d[b].n = s.n; d[b].l = s.l; d[b].m = s.m; d[b].family = s.family;
+    for (int k = 0; k < nr; ++k) {
+      double dR = 0;
+      tcscf::basisRadial(d[b], r[k], R[size_t(b) * nr + k], dR);
+    }
+  }
+  for (int i = 0; i < nb; ++i)
+    for (int j = 0; j < nb; ++j) {
+      tcscf_sto const & b1 = basis[i];
+      tcscf_sto const & b2 = basis[j];
+      bool const lm = b1.l == b2.l && b1.m == b2.m;
+      double s = 0, h = 0;
+      if (b1.family == TCSCF_BASIS_OCHI) {
+        // OchiBasis.hpp:118-125: orthonormal by construction, whatever the exponents
+        s = (b1.n == b2.n && lm) ? 1.0 : 0.0;
+        if (H) {
+          // OchiBasis.hpp:130-155
+          if (b1.alpha != b2.alpha) return TCSCF_ERR_INVALID_ARGUMENT;
+          if (lm) {
+            double integral = 0;   // sum_k w fnl1 fnl2 / r with fnl = R r
+            for (int k = 0; k < nr; ++k) integral += w[k] * R[size_t(i) * nr + k] * r[k] * R[size_t(j) * nr + k];
+            double const a = b1.alpha;
+            double const coeff = a * (b1.l + 1) * (1 + 2 * std::min(b1.n, b2.n) / double(2 * b1.l + 3)) - Z;
+            h = coeff * integral - (b1.n == b2.n) * a * a / 2;
+          }
+        }
+      } else {
+        // the generic overlap (AtomicBasis.hpp:19-31) reduces to the radial integral of R1 R2 r^2
+        if (lm) {
+          double integral = 0;
+          for (int k = 0; k < nr; ++k) integral += w[k] * R[size_t(i) * nr + k] * R[size_t(j) * nr + k] * r[k] * r[k];
+          s = integral;
+        }
+        // HydrogenLikeBasis.hpp:70-82
+        if (b1.n == b2.n && lm) h = -double(Z) * Z / (2.0 * b1.n * b1.n);
+      }
+      if (S) S[i * nb + j] = s;
+      if (H) H[i * nb + j] = h;
+    }
+  return TCSCF_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -150,6 +210,10 @@ int tcscf_sobol(int ndim, int64_t n, uint64_t seed, double * u)
 int tcscf_overlap_core_analytic(const tcscf_sto * basis, int nb, int Z, double * S, double * H)
 {
   if (!basis || nb <= 0 || (!S && !H)) return TCSCF_ERR_INVALID_ARGUMENT;
+  int const family = basis[0].family;
+  for (int i = 0; i < nb; ++i)
+    if (basis[i].family != family || family < TCSCF_BASIS_STO || family > TCSCF_BASIS_HYDROGEN) return TCSCF_ERR_INVALID_ARGUMENT;
+  if (family != TCSCF_BASIS_STO) return overlapCoreLaguerre(basis, nb, Z, S, H);
   auto fact = [](int k) { double r = 1; for (int i = 2; i <= k; ++i) r *= i; return r; };
   auto nrm = [&](tcscf_sto const & b) { return std::pow(2 * b.alpha, b.n) * std::sqrt(2 * b.alpha / fact(2 * b.n)); };
   auto ovl = [](int sn, double sa) { return std::tgamma(sn + 1) / std::pow(sa, sn + 1); };

@@ -71,7 +71,8 @@ __device__ double sphLegendre(int l, int m, double x, double s)
 }
 
 // QMCGrid::setBasisFunctions (integrateAll.hpp:88-137) with SlaterTypeOrbital::operator() and
-// ::gradient (SlaterTypeOrbital.hpp:51-106).  One thread per (point, function), function index
+// ::gradient (SlaterTypeOrbital.hpp:51-106), or the Ochi / hydrogen-like radial parts (basisRadial;
+// OchiBasisFunction::gradient, OchiBasis.hpp:58-107, shares the angular terms of the STO gradient).  One thread per (point, function), function index
 // fastest, so every store is coalesced.  Also writes the real-harmonic values phiR used by the
 // contraction kernels: cos-type sqrt2 R P cos(|m| phi) for m > 0, sin-type sqrt2 R P sin(|m| phi)
 // for m < 0, R P for m == 0.
@@ -88,7 +89,8 @@ __global__ void kBasis(int64_t n, int nb, int ndim, const double * __restrict__ 
     double const st = sqrt(x * x + y * y) / r;
     double const ph = atan2(y, x);
     DevSto const s = sto[b];
-    double const R = s.norm * ipow(r, s.n - 1) * exp(-s.alpha * r);
+    double R, dR;
+    basisRadial(s, r, R, dR);
     int const am = s.m < 0 ? -s.m : s.m;
     double const P = sphLegendre(s.l, am, ct, st);
     double sn, cs;
@@ -107,7 +109,7 @@ __global__ void kBasis(int64_t n, int nb, int ndim, const double * __restrict__ 
       // SlaterTypeOrbital.hpp:63-106, arithmetic kept (including its m < 0 and pole behaviour)
       double const th = acos(ct);
       double const l = s.l, m = s.m;
-      double const dRadialPart = ((s.n - 1) / r - s.alpha) * R;
+      double const dRadialPart = dR;
       double const ylmRe = P * cs, ylmIm = P * sn;
       double const c1 = (s.l != s.m) ? sqrt((l - m) * (l + m + 1)) : 0.0;
       int const m1 = s.m + 1;
@@ -866,7 +868,7 @@ int checkBasisPair(tcscf_ctx * ctx, Grid * g1, Grid * g2)
   for (int b = 0; b < g1->nb; ++b) {
     tcscf_sto const & a = g1->basis[b];
     tcscf_sto const & c = g2->basis[b];
-    TCSCF_CHECK(ctx, a.alpha == c.alpha && a.n == c.n && a.l == c.l && a.m == c.m, TCSCF_ERR_INVALID_ARGUMENT,
+    TCSCF_CHECK(ctx, a.alpha == c.alpha && a.n == c.n && a.l == c.l && a.m == c.m && a.family == c.family, TCSCF_ERR_INVALID_ARGUMENT,
                 "r1 and r2 grids carry different basis sets");
   }
   return TCSCF_OK;
@@ -1123,22 +1125,38 @@ int validateBasis(tcscf_ctx * ctx, const tcscf_sto * basis, int nb, std::vector<
 {
   TCSCF_CHECK(ctx, basis && nb > 0, TCSCF_ERR_INVALID_ARGUMENT, "empty basis");
   out.resize(nb);
-  auto fact = [](int k) { double r = 1; for (int i = 2; i <= k; ++i) r *= i; return r; };
   for (int b = 0; b < nb; ++b) {
     tcscf_sto const & s = basis[b];
-    // SlaterTypeOrbital.hpp:34-36
-    TCSCF_CHECK(ctx, s.n >= 1 && s.n >= s.l && s.l >= std::abs(s.m), TCSCF_ERR_INVALID_ARGUMENT, "invalid STO quantum numbers");
+    TCSCF_CHECK(ctx, s.family == basis[0].family, TCSCF_ERR_INVALID_ARGUMENT, "a basis holds one family of functions");
     TCSCF_CHECK(ctx, s.l <= kMaxL, TCSCF_ERR_UNSUPPORTED, "angular momentum above 12");
-    TCSCF_CHECK(ctx, s.alpha > 0, TCSCF_ERR_INVALID_ARGUMENT, "non-positive STO exponent");
+    TCSCF_CHECK(ctx, s.l >= std::abs(s.m), TCSCF_ERR_INVALID_ARGUMENT, "|m| > l");
+    if (s.family == TCSCF_BASIS_STO) {
+      // SlaterTypeOrbital.hpp:34-36
+      TCSCF_CHECK(ctx, s.n >= 1 && s.n >= s.l, TCSCF_ERR_INVALID_ARGUMENT, "invalid STO quantum numbers");
+      TCSCF_CHECK(ctx, s.alpha > 0, TCSCF_ERR_INVALID_ARGUMENT, "non-positive STO exponent");
+    } else if (s.family == TCSCF_BASIS_OCHI) {
+      // OchiBasis.hpp:33-34
+      TCSCF_CHECK(ctx, s.n >= 0, TCSCF_ERR_INVALID_ARGUMENT, "negative Ochi Laguerre degree");
+      TCSCF_CHECK(ctx, s.alpha > 0, TCSCF_ERR_INVALID_ARGUMENT, "non-positive Ochi exponent");
+    } else if (s.family == TCSCF_BASIS_HYDROGEN) {
+      // HydrogenLikeBasis.hpp:31-34
+      TCSCF_CHECK(ctx, s.alpha > 0 && s.n >= 1 && s.l < s.n, TCSCF_ERR_INVALID_ARGUMENT, "invalid hydrogen-like quantum numbers or Z");
+    } else {
+      return fail(ctx, TCSCF_ERR_INVALID_ARGUMENT, "unknown basis family");
+    }
     DevSto d{};
-    d.alpha = s.alpha;
-    d.norm = std::pow(2 * s.alpha, s.n) * std::sqrt(2 * s.alpha / fact(2 * s.n));
+    d.alpha = s.family == TCSCF_BASIS_HYDROGEN ? s.alpha / s.n : s.alpha;
+    d.norm = basisNormalization(s);
     d.n = s.n; d.l = s.l; d.m = s.m;
+    d.family = s.family;
     d.rtype = s.m == 0 ? 0 : (s.m > 0 ? 1 : 2);
     d.partner = -1;
     if (s.m != 0) {
       for (int c = 0; c < nb; ++c)
-        if (basis[c].alpha == s.alpha && basis[c].n == s.n && basis[c].l == s.l && basis[c].m == -s.m) { d.partner = c; break; }
+        if (basis[c].alpha == s.alpha && basis[c].n == s.n && basis[c].l == s.l && basis[c].m == -s.m && basis[c].family == s.family) {
+          d.partner = c;
+          break;
+        }
       TCSCF_CHECK(ctx, d.partner >= 0, TCSCF_ERR_UNSUPPORTED, "basis lacks the -m partner of an m != 0 function");
     }
     out[b] = d;
@@ -1270,6 +1288,8 @@ int tcscf_grid_set_basis(tcscf_ctx * ctx, int grid, const tcscf_sto * basis, int
   TCSCF_CHECK(ctx, g, TCSCF_ERR_INVALID_ARGUMENT, "unknown grid handle");
   std::vector<DevSto> ds;
   TCSCF_TRY(validateBasis(ctx, basis, nb, ds));
+  TCSCF_CHECK(ctx, !(gradients && basis[0].family == TCSCF_BASIS_HYDROGEN), TCSCF_ERR_UNSUPPORTED,
+              "hydrogen-like functions have no gradient (HydrogenLikeBasis.hpp:51-55)");
   cudaStreamSynchronize(ctx->stream);
   cudaFree(g->dsto); cudaFree(g->phiR); cudaFree(g->vals); cudaFree(g->grads); cudaFree(g->vtCache);
   g->dsto = nullptr; g->phiR = g->vals = g->grads = nullptr;

@@ -26,11 +26,12 @@ ERR_NO_DEVICE = 8
 
 K_INV_R12, K_TC_SCALAR_SAME, K_TC_SCALAR_OPPO, K_GRAD_U_SAME, K_GRAD_U_OPPO = range(5)
 PREC_FP64, PREC_BF16X3, PREC_TF32 = 0, 1, 2
+BASIS_STO, BASIS_OCHI, BASIS_HYDROGEN = 0, 1, 2
 MAP_NONE, MAP_LINEAR, MAP_X_OVER_1MX, MAP_TREUTLER_AHLRICHS_M4, MAP_ONE_PLUS_X = range(5)
 
 
 class Sto(C.Structure):
-    _fields_ = [("alpha", C.c_double), ("n", C.c_int32), ("l", C.c_int32), ("m", C.c_int32), ("pad", C.c_int32)]
+    _fields_ = [("alpha", C.c_double), ("n", C.c_int32), ("l", C.c_int32), ("m", C.c_int32), ("family", C.c_int32)]
 
 
 class Ochi(C.Structure):
@@ -114,9 +115,12 @@ def check(code: int, ctx=None) -> None:
 
 
 def sto_array(basis) -> "C.Array":
+    """basis: (alpha, n, l, m) Slater-type orbitals, or (alpha, n, l, m, family) with family one of
+    BASIS_STO, BASIS_OCHI, BASIS_HYDROGEN (alpha = Z for the hydrogen-like family)."""
     arr = (Sto * len(basis))()
     for i, b in enumerate(basis):
         arr[i].alpha, arr[i].n, arr[i].l, arr[i].m = float(b[0]), int(b[1]), int(b[2]), int(b[3])
+        arr[i].family = int(b[4]) if len(b) > 4 else BASIS_STO
     return arr
 
 

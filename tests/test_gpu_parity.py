@@ -26,18 +26,7 @@ def real_density(basis, nocc, rng):
     """A density that is real in the real-harmonic basis (the closed-shell SCF case): built from
     orbitals that are real combinations of cos/sin-type functions."""
     nb = len(basis)
-    idx = {b: i for i, b in enumerate(basis)}
-    U = np.zeros((nb, nb), dtype=complex)
-    h = 1 / np.sqrt(2)
-    for k, (a, n, l, m) in enumerate(basis):
-        if m == 0:
-            U[k, k] = 1
-        elif m > 0:
-            p = idx[(a, n, l, -m)]
-            U[k, k], U[k, p] = h, h
-        else:
-            p = idx[(a, n, l, -m)]
-            U[k, p], U[k, k] = -1j * h, 1j * h
+    U = wl.real_harmonic_unitary(basis)
     CR = rng.normal(size=(nb, nocc)) * 0.3          # real-basis orbital coefficients
     C = U.T @ CR                                   # psi = sum_k CR_k phiR_k = sum_i (U^T CR)_i phi_i
     return C @ C.conj().T
