@@ -138,6 +138,13 @@ int tcscf_grid_qmc(int ndim, int64_t n, const double * u, double * pts, double *
  * un-vendored mppmu/qmc lattice generator (qmcWrapper.hpp:94-141). */
 int tcscf_sobol(int ndim, int64_t n, uint64_t seed, double * u);
 
+/* loadSTO (SlaterTypeOrbital.cpp:24-75): the STO basis of an element from the ADF-style basis-set
+ * library <directory>/<basisSet>/<element> (basisSet one of TZ3P, QZ6P, ATZ3P, AQZ6P), functions with
+ * l <= maxL expanded over m = -l..l.  out may be NULL to query *count; otherwise at most capacity
+ * functions are written.  Host only. */
+int tcscf_load_sto(const char * directory, const char * basisSet, const char * element, int maxL, tcscf_sto * out, int capacity,
+                   int * count);
+
 /* ---- analytic one-electron matrices -----------------------------------------------------------
  * STO: SlaterTypeOrbital.hpp:134-181.  Ochi: overlap = [n, l, m equal] (OchiBasis.hpp:118-125), core
  * element from the radial integral of fnl fnl / r (OchiBasis.hpp:130-155) on the reference driver's

@@ -135,6 +135,17 @@ class QMCGrid:
             self._id = C.c_int()
 
 
+def loadSTO(directory: str, basisSet: str, element: str, maxL: int) -> list:
+    """loadSTO (SlaterTypeOrbital.cpp:24-75): the (alpha, n, l, m) Slater-type orbitals of `element`
+    in the basis-set library `directory`/`basisSet` (TZ3P, QZ6P, ATZ3P or AQZ6P), l <= maxL."""
+    n = C.c_int()
+    args = (str(directory).encode(), basisSet.encode(), element.encode(), int(maxL))
+    ffi.check(ffi.lib().tcscf_load_sto(*args, None, 0, C.byref(n)))
+    arr = (ffi.Sto * max(1, n.value))()
+    ffi.check(ffi.lib().tcscf_load_sto(*args, arr, n.value, C.byref(n)))
+    return [(arr[i].alpha, arr[i].n, arr[i].l, arr[i].m) for i in range(n.value)]
+
+
 def overlap_core(basis, Z: int) -> tuple[np.ndarray, np.ndarray]:
     """Analytic overlap and core-Hamiltonian matrices (SlaterTypeOrbital.hpp:134-181)."""
     nb = len(basis)

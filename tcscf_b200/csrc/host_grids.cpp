@@ -2,6 +2,11 @@
 // Chebyshev-Gauss radial rules with the reference's changes of variables, radial x angular product
 // grids, the QMCGrid point mapping and a seeded scrambled Sobol point source.
 #include <algorithm>
+#include <filesystem>
+#include <fstream>
+#include <sstream>
+#include <string>
+#include <unordered_set>
 #include <cmath>
 #include <cstdint>
 #include <vector>
@@ -234,6 +239,48 @@ int tcscf_overlap_core_analytic(const tcscf_sto * basis, int nb, int Z, double *
       if (S) S[i * nb + j] = s;
       if (H) H[i * nb + j] = h;
     }
+  return TCSCF_OK;
+}
+
+// loadSTO (SlaterTypeOrbital.cpp:24-75): the BASIS block of <directory>/<basisSet>/<element>, one
+// "<n><S|P|D|F> <alpha>" entry per line up to END, each expanded over m = -l..l, entries above maxL
+// skipped.  out may be null (count only); otherwise at most capacity functions are written and
+// *count is the total.  The reference aborts on an unknown basis set, a missing basis-set directory or
+// an unparsable line: those return TCSCF_ERR_INVALID_ARGUMENT here.  A missing element file gives
+// an empty basis, as the reference's (its existence check is disabled).
+int tcscf_load_sto(const char * directory, const char * basisSet, const char * element, int maxL, tcscf_sto * out, int capacity,
+                   int * count)
+{
+  if (!directory || !basisSet || !element || !count || capacity < 0) return TCSCF_ERR_INVALID_ARGUMENT;
+  static std::unordered_set<std::string> const valid = {"TZ3P", "QZ6P", "ATZ3P", "AQZ6P"};
+  if (!valid.count(basisSet)) return TCSCF_ERR_INVALID_ARGUMENT;
+  std::filesystem::path const dir = std::filesystem::path(directory) / basisSet;
+  std::error_code ec;
+  if (!std::filesystem::is_directory(dir, ec)) return TCSCF_ERR_INVALID_ARGUMENT;
+  std::ifstream contents(dir / element);
+  int total = 0;
+  for (std::string line; std::getline(contents, line);) {
+    if (line.rfind("BASIS", 0) != 0) continue;
+    while (std::getline(contents, line) && line.rfind("END", 0) != 0) {
+      int n;
+      char type;
+      double alpha;
+      std::istringstream ls(line);
+      if (ls >> n >> type >> alpha) {
+        int const l = type == 'S' ? 0 : type == 'P' ? 1 : type == 'D' ? 2 : type == 'F' ? 3 : -1;
+        if (l < 0) return TCSCF_ERR_INVALID_ARGUMENT;   // spdfToL, SlaterTypeOrbital.cpp:11-21
+        if (l > maxL) continue;
+        for (int m = -l; m <= l; ++m) {
+          if (out && total < capacity) out[total] = tcscf_sto{alpha, n, l, m, TCSCF_BASIS_STO};
+          ++total;
+        }
+      } else if (!line.empty()) {
+        return TCSCF_ERR_INVALID_ARGUMENT;
+      }
+    }
+    break;
+  }
+  *count = total;
   return TCSCF_OK;
 }
 
