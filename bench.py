@@ -5,7 +5,7 @@ energy) for the workload's density on its radial x Lebedev grid.  `value` is dev
 with every input resident in HBM; `e2e` is the same through the public C ABI from host buffers
 (grid upload, device basis evaluation, Fock build, G/Fock/energy back to the host).
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload kr|ne|he]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload kr|ne|he|batch|scf]
                   [--precision bf16x3|fp64|tf32]
 
 Under torchrun (N > 1) every rank runs an independent replica (the Fock build does not shard in
@@ -399,13 +399,71 @@ def run_batch(args, rank: int) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_scf(args, rank: int) -> None:
+    """Full RCS SCF of the Kr configuration to |dE| < 1e-8 Eh: split-BF16 and FP64 Fock builds in the plain
+    Roothaan iteration of the reference (at most --scf-max-iter iterations), split BF16 with Pulay DIIS
+    (history --diis), and the FP64 SCF converged to 1e-10 Eh as the energy reference; all with the
+    real-harmonic eigen-solve (real densities throughout, one contraction per build).  Each SCF starts
+    from the zero density (core-Hamiltonian first step, as the reference); wall time around the public
+    call."""
+    import torch
+
+    from tcscf_b200 import api, ffi, grids
+
+    if rank != 0:
+        return
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+    w = workload("kr")
+    if args.nrad:
+        w.nrad = args.nrad
+    g = grids.product_grid(w.nrad, w.order)
+    ctx = api.Context(int(os.environ.get("LOCAL_RANK", 0)))
+    G = api.QMCGrid(ctx, g)
+    G.setBasisFunctions(w.basis)
+    S, h = api.overlap_core(w.basis, w.Z)
+    # the 1e-8 runs time the configuration; the mixed-precision energy is compared with the FP64 SCF
+    # converged to 1e-10 (the split-BF16 energy settles to its own precision, ~1e-9 Eh per build, so it
+    # is not itself run to 1e-10)
+    runs = [("bf16x3_plain", ffi.PREC_BF16X3, 0, 1e-8), ("bf16x3_diis", ffi.PREC_BF16X3, args.diis, 1e-8),
+            ("fp64_plain", ffi.PREC_FP64, 0, 1e-8), ("fp64_plain_1e-10", ffi.PREC_FP64, 0, 1e-10)]
+    res = {}
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", 0))) as clk:
+        for name, prec, nd, tol in runs:
+            hf = api.RCSHartreeFock(w.n_up, w.n_down, w.nb)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            try:
+                E, ok = hf.compute(S, h, G, G, precision=prec, tol=tol, max_iter=args.scf_max_iter, diis=nd,
+                                   real_eigensolve=True), True
+            except ffi.TcscfError as e:
+                if e.code != ffi.ERR_NOT_CONVERGED:
+                    raise
+                E, ok = None, False
+            torch.cuda.synchronize()
+            res[name] = {"converged": ok, "energy": E, "iterations": hf.numberOfConvergenceLoops(),
+                         "seconds": time.perf_counter() - t0, "diis": nd, "tol": tol}
+    m, f, ft = res["bf16x3_plain"], res["fp64_plain"], res["fp64_plain_1e-10"]
+    line = {"metric": "Kr RCS SCF to |dE| < 1e-8 Eh, wall s (split-BF16 Fock builds)", "value": m["seconds"], "unit": "s",
+            "n_gpus": 1, "steps": 1, "warmup": 0, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16", "data": "synthetic",
+            "config": {"workload": f"Kr RCS SCF (direct-form Fock builds), {w.nrad} radial x Lebedev order {w.order}",
+                       "n_points": g.n, "n_basis": w.nb, "n_occ": w.n_up, "start": "zero density (core-Hamiltonian step)"},
+            "runs": res,
+            "dE_mixed_vs_fp64_converged": (m["energy"] - ft["energy"]) if m["converged"] and ft["converged"] else None,
+            "speedup_vs_fp64": f["seconds"] / m["seconds"], "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="kr", choices=["kr", "ne", "he", "batch"])
+    ap.add_argument("--workload", default="kr", choices=["kr", "ne", "he", "batch", "scf"],
+                    help="scf: full Kr SCF to 1e-8 Eh (split BF16 and FP64, plain iteration and DIIS)")
+    ap.add_argument("--diis", type=int, default=8, help="DIIS history of --workload scf")
+    ap.add_argument("--scf-max-iter", type=int, default=50, help="iteration limit of --workload scf (the reference's RCS limit)")
     ap.add_argument("--precision", default="bf16x3", choices=["bf16x3", "fp64", "tf32"])
     ap.add_argument("--nrad", type=int, default=0, help="override the workload's radial points (smaller profiling cases)")
     ap.add_argument("--fp64-steps", type=int, default=2)
@@ -432,6 +490,8 @@ def main() -> None:
             run_reference(args, rank)
         elif args.workload == "batch":
             run_batch(args, rank)
+        elif args.workload == "scf":
+            run_scf(args, rank)
         else:
             run_ours(args, rank, world)
     finally:

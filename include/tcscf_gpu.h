@@ -221,8 +221,19 @@ int tcscf_fock_build_precomputed(tcscf_ctx * ctx, int r1, int fji, int nspin, co
                                  int respect_symmetry, double * G, double * fock, double * energy);
 
 /* ---- SCF drivers (RCSHartreeFock/UOSHartreeFock::compute, HartreeFock.cpp:785-1003) ---------- */
+/* Options of tcscf_scf on this context (no reference counterpart; the defaults, 0 and 0, reproduce
+ * the reference's plain Roothaan iteration with the complex eigen-solver).  diis in 2..16: the
+ * eigen-solve of every iteration after the first takes the combination of the last `diis` Fock
+ * matrices that minimises the norm of the combined commutator errors F D S - S D F; the energy and
+ * the |dE| < tol test are unchanged.  real_eigensolve != 0: a Fock matrix that is real in the
+ * real-harmonic basis is diagonalised there as a real symmetric problem, so the density stays real
+ * (half the factor rank, one contraction per build) when the aufbau occupation splits a degenerate
+ * shell; in that case the occupied member of the shell differs from the complex solver's arbitrary
+ * choice, as it may between LAPACK builds. */
+int tcscf_set_scf_options(tcscf_ctx * ctx, int diis, int real_eigensolve);
 /* Zero initial density, Fock build (direct form at `precision`), FP64 generalized Hermitian
- * eigen-solve on the device (upper triangle, as LAPACK zhegvd in the reference), new density,
+ * eigen-solve on the device (upper triangle, as LAPACK zhegvd in the reference; see
+ * tcscf_set_scf_options for the real-harmonic alternative), new density,
  * until |dE| < tol or max_iter.  S real [nb][nb].  Outputs: energy, iterations, density, eigenvalues
  * [nspin][nb].  Returns TCSCF_ERR_NOT_CONVERGED after max_iter. */
 int tcscf_scf(tcscf_ctx * ctx, int r1, int r2, int nspin, int n_up, int n_down, const double * S, const double * h,

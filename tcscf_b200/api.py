@@ -342,7 +342,10 @@ class _SCF:
 
     def compute(self, overlap: np.ndarray, oneElectronTerms: np.ndarray, r1Grid: QMCGrid, r2Grid: QMCGrid,
                 respectOneElectronSymmetry: bool = True, precision: int = ffi.PREC_FP64, tol: float = 1e-5,
-                max_iter: int | None = None) -> float:
+                max_iter: int | None = None, diis: int = 0, real_eigensolve: bool = False) -> float:
+        """diis: Pulay DIIS history length; real_eigensolve: diagonalise a Fock matrix that is real in the
+        real-harmonic basis there (real densities when a degenerate shell is partly occupied).  The
+        defaults (0, False) iterate plain Roothaan steps with the complex solver, as the reference."""
         ctx = r1Grid.ctx
         S = np.ascontiguousarray(np.real(overlap), dtype=np.float64)
         hh = np.ascontiguousarray(oneElectronTerms, dtype=np.float64)
@@ -351,10 +354,14 @@ class _SCF:
             raise ffi.TcscfError(ffi.ERR_INVALID_ARGUMENT, "overlap / oneElectronTerms do not match nBasis")
         e = C.c_double()
         it = C.c_int()
-        code = ffi.lib().tcscf_scf(ctx.handle, r1Grid.id, r2Grid.id, self.nspin, self.nElectrons[0], self.nElectrons[1],
-                                   ffi.dptr(S), ffi.dptr(hh), int(respectOneElectronSymmetry), precision, tol,
-                                   max_iter or self.max_iter, C.byref(e), C.byref(it), ffi.dptr(self.density),
-                                   ffi.dptr(self.eigenvalues))
+        _raise(ffi.lib().tcscf_set_scf_options(ctx.handle, int(diis), int(real_eigensolve)), ctx.handle)
+        try:
+            code = ffi.lib().tcscf_scf(ctx.handle, r1Grid.id, r2Grid.id, self.nspin, self.nElectrons[0], self.nElectrons[1],
+                                       ffi.dptr(S), ffi.dptr(hh), int(respectOneElectronSymmetry), precision, tol,
+                                       max_iter or self.max_iter, C.byref(e), C.byref(it), ffi.dptr(self.density),
+                                       ffi.dptr(self.eigenvalues))
+        finally:
+            ffi.lib().tcscf_set_scf_options(ctx.handle, 0, 0)
         self._iter = it.value
         _raise(code, ctx.handle)
         return e.value

@@ -72,6 +72,8 @@ struct tcscf_ctx {
   double lastContractionMs = 0, lastTotalMs = 0;
   int lastLaunches = 0;
   int launchCount = 0;
+  int diisSize = 0;   // Pulay DIIS history length of tcscf_scf (0: plain Roothaan iterations)
+  int realEigen = 0;  // tcscf_scf solves a Fock matrix that is real in the real-harmonic basis there
   std::map<std::string, tcscf::Scratch> scratch;
   // device buffers of the most recent direct Fock build (for tcscf_last_potentials)
   const double * lastVH = nullptr;

@@ -783,11 +783,11 @@ Shape shapeOf(Contraction const & c, int sms, int precision)
   Shape sh{};
   sh.NB = c.ncol <= 64 ? 64 : 128;
   sh.RP = c.R <= 32 ? 32 : 64;
-  // 24-bit X below 2^18 r2 points: on coarser grids a 64-point r2 block spans a wider range of
-  // g * rho within a row, and the 16-bit slicing error averages over fewer pairs (rank padding 64
-  // leaves no shared memory for the extra slices); the TF32 kernel (XS = 0) has rank padding 32
+  // 24-bit X wherever shared memory holds its four slices (rank padding 32; 64 leaves no room): with
+  // 16-bit X the converged Kr SCF energy (406,000 points) was 1.5e-6 Eh from FP64, with 24-bit X
+  // 9e-8, for a 9 % slower kernel; the TF32 kernel (XS = 0) has rank padding 32
   if (precision == TCSCF_PREC_TF32) sh.XS = 0;
-  else sh.XS = (sh.RP == 32 && c.n2 < (int64_t(1) << 18)) ? 3 : 2;
+  else sh.XS = sh.RP == 32 ? 3 : 2;
   sh.n1pad = (c.n1 + tc::BM - 1) / tc::BM * tc::BM;
   sh.n2pad = (c.n2 + tc::BK - 1) / tc::BK * tc::BK;
   sh.nTiles = int(sh.n1pad / tc::BM);

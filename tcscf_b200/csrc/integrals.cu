@@ -114,15 +114,6 @@ __global__ void kPermute6(int nb, const double2 * __restrict__ C, double2 * __re
   }
 }
 
-int blas(tcscf_ctx * ctx, cublasHandle_t * out)
-{
-  if (!ctx->blas) {
-    if (cublasCreate(&ctx->blas) != CUBLAS_STATUS_SUCCESS) return fail(ctx, TCSCF_ERR_CUDA, "cublasCreate failed");
-  }
-  if (cublasSetStream(ctx->blas, ctx->stream) != CUBLAS_STATUS_SUCCESS) return fail(ctx, TCSCF_ERR_CUDA, "cublasSetStream failed");
-  *out = ctx->blas;
-  return TCSCF_OK;
-}
 
 int checkPair(tcscf_ctx * ctx, Grid * g1, Grid * g2, int ndim2)
 {
@@ -162,7 +153,7 @@ int tcscf_integrate_all_r1r2(tcscf_ctx * ctx, int r1, int r2, int use_gradient, 
   int const nb = g1->nb;
   int64_t const nn = int64_t(nb) * nb, n1 = g1->n, n2 = g2->n;
   cublasHandle_t h = nullptr;
-  TCSCF_TRY(blas(ctx, &h));
+  TCSCF_TRY(blasHandle(ctx, &h));
 
   // r2 side B[r1][(b2,b4)]: real (value form, computeF on the 2-D grid, 2 pi included) or complex
   int fid = 0;
@@ -233,7 +224,7 @@ int tcscf_three_electron_integrals(tcscf_ctx * ctx, int r1, int r2, const tcscf_
   int64_t const nn = int64_t(nb) * nb, n4 = nn * nn, n6 = n4 * nn, n1 = g1->n;
   TCSCF_CHECK(ctx, nb <= 32, TCSCF_ERR_UNSUPPORTED, "threeElectronIntegrals: nb <= 32 (the nb^6 output exceeds device memory beyond)");
   cublasHandle_t h = nullptr;
-  TCSCF_TRY(blas(ctx, &h));
+  TCSCF_TRY(blasHandle(ctx, &h));
   int vid = 0;
   TCSCF_TRY(tcscf_compute_V(ctx, r1, r2, TCSCF_K_GRAD_U_SAME, jastrow, nullptr, 1, &vid));
   const double2 * V = reinterpret_cast<const double2 *>(ctx->tensors[vid].d);

@@ -33,6 +33,9 @@ struct Contraction {
 
 int contractFp64(tcscf_ctx * ctx, Contraction const & c);
 
+// the context's cuBLAS handle (created on first use), bound to the context stream
+int blasHandle(tcscf_ctx * ctx, cublasHandle_t * out);
+
 // tensor-core (tcgen05) contraction of the same quantity for g = 1/r12: split-BF16 (flash_tc.cu) or
 // TF32 (flash_tf32.cu)
 int contractTensor(tcscf_ctx * ctx, Contraction const & c, int precision);

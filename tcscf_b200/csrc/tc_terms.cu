@@ -334,13 +334,6 @@ Tensor const * findTensor(tcscf_ctx * ctx, int id)
   return it == ctx->tensors.end() ? nullptr : &it->second;
 }
 
-int blasHandle(tcscf_ctx * ctx, cublasHandle_t * out)
-{
-  if (!ctx->blas && cublasCreate(&ctx->blas) != CUBLAS_STATUS_SUCCESS) return fail(ctx, TCSCF_ERR_CUDA, "cublasCreate failed");
-  if (cublasSetStream(ctx->blas, ctx->stream) != CUBLAS_STATUS_SUCCESS) return fail(ctx, TCSCF_ERR_CUDA, "cublasSetStream failed");
-  *out = ctx->blas;
-  return TCSCF_OK;
-}
 
 struct TcInputs {
   Grid * g1 = nullptr;

@@ -18,6 +18,14 @@ int fail(tcscf_ctx * ctx, int code, std::string const & msg)
   return code;
 }
 
+int blasHandle(tcscf_ctx * ctx, cublasHandle_t * out)
+{
+  if (!ctx->blas && cublasCreate(&ctx->blas) != CUBLAS_STATUS_SUCCESS) return fail(ctx, TCSCF_ERR_CUDA, "cublasCreate failed");
+  if (cublasSetStream(ctx->blas, ctx->stream) != CUBLAS_STATUS_SUCCESS) return fail(ctx, TCSCF_ERR_CUDA, "cublasSetStream failed");
+  *out = ctx->blas;
+  return TCSCF_OK;
+}
+
 int scratch(tcscf_ctx * ctx, char const * name, size_t bytes, void ** out)
 {
   Scratch & s = ctx->scratch[name];
@@ -693,6 +701,104 @@ __global__ void kDensityFromOrbitals(int nb, int nocc, const double2 * C, double
   }
 }
 
+// real-harmonic density DR(u,v) = sum_a C(u,a) C(v,a) from real eigenvectors C (column-major)
+__global__ void kRealDensity(int nb, int nocc, const double * C, double * DR)
+{
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < nb * nb; idx += gridDim.x * blockDim.x) {
+    int const u = idx / nb, v = idx % nb;
+    double t = 0;
+    for (int a = 0; a < nocc; ++a) t += C[a * nb + u] * C[a * nb + v];
+    DR[idx] = t;
+  }
+}
+
+// ---- Pulay DIIS (optional SCF acceleration; the reference iterates plain Roothaan steps) ---------
+// dots[j] = Re <E[slot], E[j]> (Frobenius product of the commutator error matrices of both spins)
+// for the used history slots j < count, one block per j
+__global__ void kDiisDots(int64_t len, int slot, int count, const double2 * E, double * dots)
+{
+  __shared__ double red[256];
+  int const j = blockIdx.x;
+  if (j >= count) return;
+  double acc = 0;
+  for (int64_t i = threadIdx.x; i < len; i += blockDim.x) {
+    double2 const a = E[int64_t(slot) * len + i], b = E[int64_t(j) * len + i];
+    acc += a.x * b.x + a.y * b.y;
+  }
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) dots[j] = red[0];
+}
+
+// F = sum_j c[j] Fh[j]
+__global__ void kDiisCombine(int64_t len, int count, const double * c, const double2 * Fh, double2 * F)
+{
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < len; i += int64_t(gridDim.x) * blockDim.x) {
+    double2 a = make_double2(0, 0);
+    for (int j = 0; j < count; ++j) {
+      double2 const f = Fh[int64_t(j) * len + i];
+      a.x += c[j] * f.x;
+      a.y += c[j] * f.y;
+    }
+    F[i] = a;
+  }
+}
+
+__global__ void kRealToComplex(int64_t n, const double * a, double2 * b)
+{
+  for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) b[i] = make_double2(a[i], 0.0);
+}
+
+// row-major C = alpha A B + beta C (n x n complex) through column-major cuBLAS: C^T = B^T A^T
+int rowMajorZgemm(tcscf_ctx * ctx, cublasHandle_t h, int n, double2 alpha, const double2 * A, const double2 * B, double2 beta, double2 * C)
+{
+  cuDoubleComplex const al = make_cuDoubleComplex(alpha.x, alpha.y), be = make_cuDoubleComplex(beta.x, beta.y);
+  if (cublasZgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, n, n, n, &al, reinterpret_cast<const cuDoubleComplex *>(B), n,
+                  reinterpret_cast<const cuDoubleComplex *>(A), n, &be, reinterpret_cast<cuDoubleComplex *>(C), n) != CUBLAS_STATUS_SUCCESS)
+    return fail(ctx, TCSCF_ERR_CUDA, "cublasZgemm failed");
+  return TCSCF_OK;
+}
+
+// Solves the DIIS equations [B -1; -1 0] [c; lambda] = [0; -1] (B m x m, row stride ld) by Gaussian
+// elimination with partial pivoting; false when singular
+bool solveDiis(int m, std::vector<double> const & B, int ld, std::vector<double> & c)
+{
+  int const n = m + 1;
+  std::vector<double> A(size_t(n) * (n + 1), 0.0);
+  for (int i = 0; i < m; ++i) {
+    for (int j = 0; j < m; ++j) A[i * (n + 1) + j] = B[i * ld + j];
+    A[i * (n + 1) + m] = -1;
+    A[m * (n + 1) + i] = -1;
+  }
+  A[m * (n + 1) + n] = -1;
+  for (int k = 0; k < n; ++k) {
+    int p = k;
+    for (int i = k + 1; i < n; ++i)
+      if (std::fabs(A[i * (n + 1) + k]) > std::fabs(A[p * (n + 1) + k])) p = i;
+    if (!(std::fabs(A[p * (n + 1) + k]) > 0)) return false;
+    if (p != k)
+      for (int j = 0; j <= n; ++j) std::swap(A[k * (n + 1) + j], A[p * (n + 1) + j]);
+    for (int i = k + 1; i < n; ++i) {
+      double const f = A[i * (n + 1) + k] / A[k * (n + 1) + k];
+      for (int j = k; j <= n; ++j) A[i * (n + 1) + j] -= f * A[k * (n + 1) + j];
+    }
+  }
+  std::vector<double> x(n);
+  for (int i = n - 1; i >= 0; --i) {
+    double t = A[i * (n + 1) + n];
+    for (int j = i + 1; j < n; ++j) t -= A[i * (n + 1) + j] * x[j];
+    x[i] = t / A[i * (n + 1) + i];
+  }
+  c.assign(x.begin(), x.begin() + m);
+  for (double v : c)
+    if (!(v == v)) return false;
+  return true;
+}
+
 }  // namespace
 
 int finalizeLaunch(tcscf_ctx * ctx, int nspin, int nb, const double * h, double2 * G, const double2 * G3, const double2 * D, int respectSym,
@@ -787,7 +893,9 @@ int factorFinish(tcscf_ctx * ctx, Grid & g, FactorBufs const & b, FactorStatus c
   f.ldx = 2 * nb;
   double const hmax[2] = {st.maxAbs[0], st.maxAbs[1]};
   if (!(hmax[0] == hmax[0]) || !(hmax[1] == hmax[1])) return fail(ctx, TCSCF_ERR_NONFINITE, "non-finite density");
-  f.complex = hmax[1] > 1e-13 * std::max(hmax[0], 1e-300);
+  // an imaginary part below 1e-10 of the real part is rounding (SCF densities from the complex
+  // eigen-solver carry ~1e-12): the density is factored as real, dropping it
+  f.complex = hmax[1] > 1e-10 * std::max(hmax[0], 1e-300);
   if (hmax[0] == 0 && hmax[1] == 0) { f.R = 0; return TCSCF_OK; }
   if (!f.complex && !st.indefinite) { f.R = st.rank; return TCSCF_OK; }
 
@@ -1684,6 +1792,15 @@ int tcscf_fock_build_precomputed(tcscf_ctx * ctx, int r1, int fji, int nspin, co
   return TCSCF_OK;
 }
 
+int tcscf_set_scf_options(tcscf_ctx * ctx, int diis, int real_eigensolve)
+{
+  if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
+  TCSCF_CHECK(ctx, diis >= 0 && diis <= 16, TCSCF_ERR_INVALID_ARGUMENT, "DIIS history must be 0..16");
+  ctx->diisSize = diis == 1 ? 0 : diis;
+  ctx->realEigen = real_eigensolve ? 1 : 0;
+  return TCSCF_OK;
+}
+
 int tcscf_scf(tcscf_ctx * ctx, int r1, int r2, int nspin, int n_up, int n_down, const double * S, const double * h, int respect_symmetry,
               int precision, double tol, int max_iter, double * energy, int * iterations, double * density, double * eigenvalues)
 {
@@ -1721,6 +1838,65 @@ int tcscf_scf(tcscf_ctx * ctx, int r1, int r2, int nspin, int n_up, int n_down, 
     return fail(ctx, TCSCF_ERR_LINALG, "cusolverDnZhegvd_bufferSize failed");
   void * wk = nullptr;
   TCSCF_TRY(scratch(ctx, "hegvd_work", sizeof(double2) * size_t(lwork) + 64, &wk));
+  // optional Pulay DIIS: history of Fock matrices and commutator errors FDS - SDF (both spins)
+  int const nd = ctx->diisSize;
+  size_t const len = size_t(nspin) * nn;
+  double2 * Fh = nullptr, * Eh = nullptr, * T1 = nullptr, * T2 = nullptr, * Sc = nullptr, * Fd = nullptr;
+  double * dDots = nullptr, * dCoef = nullptr;
+  cublasHandle_t bh = nullptr;
+  std::vector<double> Bm(size_t(nd) * nd, 0.0), hDots(nd), coef;
+  int count = 0, head = 0;
+  {
+    void * q = nullptr;
+    TCSCF_TRY(scratch(ctx, "scf_diis", sizeof(double2) * (2 * size_t(nd) * len + 3 * nn + len) + sizeof(double) * 2 * (nd + 1) + 1024, &q));
+    Fh = static_cast<double2 *>(q);
+    Eh = Fh + size_t(nd) * len;
+    T1 = Eh + size_t(nd) * len;
+    T2 = T1 + nn;
+    Sc = T2 + nn;
+    Fd = Sc + nn;
+    dDots = reinterpret_cast<double *>(Fd + len);
+    dCoef = dDots + nd + 1;
+    kRealToComplex<<<gridBlocks(int64_t(nn), 256), 256, 0, ctx->stream>>>(int64_t(nn), dS, Sc);
+    TCSCF_LAUNCH(ctx);
+    if (nd > 0) TCSCF_TRY(blasHandle(ctx, &bh));
+  }
+  // Optional real-harmonic eigen-solve (tcscf_set_scf_options): the Fock matrix of a density that is
+  // real in the real-harmonic basis is real there too, and the real symmetric problem
+  // (cusolverDnDsygvd) gives real eigenvectors, so the next density stays real (one rank-nocc tensor
+  // contraction per build) even when the aufbau occupation splits a degenerate shell, where the complex
+  // solver of the reference basis returns arbitrary complex combinations (doubling the factor rank
+  // and the contractions).  Same eigenvalues; when a degenerate level is partly occupied the two
+  // solvers occupy different members of it, so the default keeps the reference's complex path.
+  void * rp = nullptr;
+  TCSCF_TRY(scratch(ctx, "scf_real", sizeof(double2) * 2 * nn + sizeof(double) * 5 * nn + 256, &rp));
+  double2 * FR = static_cast<double2 *>(rp);
+  double2 * SRc = FR + nn;
+  double * Ar = reinterpret_cast<double *>(SRc + nn);
+  double * Br = Ar + nn;
+  double * SRre = Br + nn;
+  double * DRre = SRre + nn;
+  double * fmax = DRre + nn;
+  bool realPath = true;
+  int lworkR = 0;
+  void * wkR = nullptr;
+  {
+    kDensityToReal<<<gridBlocks(nn, 256), 256, 0, ctx->stream>>>(1, nb, g1->dsto, Sc, SRc);
+    TCSCF_LAUNCH(ctx);
+    kSplitDensity<<<1, 256, 0, ctx->stream>>>(nb, SRc, SRre, fmax);
+    TCSCF_LAUNCH(ctx);
+    double hm[2];
+    TCSCF_CUDA(ctx, cudaMemcpyAsync(hm, fmax, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    realPath = ctx->realEigen && hm[1] <= 1e-12 * hm[0];
+    if (realPath) {
+      if (cusolverDnDsygvd_bufferSize(ctx->solver, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, nb, Ar, nb, Br, nb, W,
+                                      &lworkR) != CUSOLVER_STATUS_SUCCESS)
+        return fail(ctx, TCSCF_ERR_LINALG, "cusolverDnDsygvd_bufferSize failed");
+      TCSCF_TRY(scratch(ctx, "sygvd_work", sizeof(double) * size_t(lworkR) + 64, &wkR));
+    }
+  }
+  double2 const one = make_double2(1, 0), zero = make_double2(0, 0), mone = make_double2(-1, 0);
   double e = std::numeric_limits<double>::max();
   for (int it = 0; it < max_iter; ++it) {
     TCSCF_TRY(fockBuildDevice(ctx, *g1, *g2, nspin, dD, dH, respect_symmetry, precision, dG, dF, dE));
@@ -1736,8 +1912,68 @@ int tcscf_scf(tcscf_ctx * ctx, int r1, int r2, int nspin, int n_up, int n_down, 
       return TCSCF_OK;
     }
     e = ne;
+    const double2 * Fuse = dF;
+    if (nd > 0 && it >= 1) {
+      int const slot = head;
+      head = (head + 1) % nd;
+      count = std::min(count + 1, nd);
+      for (int s = 0; s < nspin; ++s) {
+        double2 const * Fs = dF + s * nn;
+        double2 const * Ds = dD + s * nn;
+        double2 * Es = Eh + slot * len + s * nn;
+        TCSCF_TRY(rowMajorZgemm(ctx, bh, nb, one, Ds, Sc, zero, T1));     // D S
+        TCSCF_TRY(rowMajorZgemm(ctx, bh, nb, one, Fs, T1, zero, Es));     // F D S
+        TCSCF_TRY(rowMajorZgemm(ctx, bh, nb, one, Sc, Ds, zero, T2));     // S D
+        TCSCF_TRY(rowMajorZgemm(ctx, bh, nb, mone, T2, Fs, one, Es));     // - S D F
+        TCSCF_CUDA(ctx, cudaMemcpyAsync(Fh + slot * len + s * nn, Fs, sizeof(double2) * nn, cudaMemcpyDeviceToDevice, ctx->stream));
+      }
+      kDiisDots<<<count, 256, 0, ctx->stream>>>(int64_t(len), slot, count, Eh, dDots);
+      TCSCF_LAUNCH(ctx);
+      TCSCF_CUDA(ctx, cudaMemcpyAsync(hDots.data(), dDots, sizeof(double) * count, cudaMemcpyDeviceToHost, ctx->stream));
+      TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+      for (int j = 0; j < count; ++j) Bm[slot * nd + j] = Bm[j * nd + slot] = hDots[j];
+      if (count >= 2) {
+        // equations scaled by the largest error norm for conditioning
+        double mx = 0;
+        for (int j = 0; j < count; ++j) mx = std::max(mx, Bm[j * nd + j]);
+        std::vector<double> Bs(size_t(count) * count);
+        for (int i = 0; i < count; ++i)
+          for (int j = 0; j < count; ++j) Bs[i * count + j] = mx > 0 ? Bm[i * nd + j] / mx : Bm[i * nd + j];
+        if (mx > 0 && solveDiis(count, Bs, count, coef)) {
+          TCSCF_CUDA(ctx, cudaMemcpyAsync(dCoef, coef.data(), sizeof(double) * count, cudaMemcpyHostToDevice, ctx->stream));
+          kDiisCombine<<<gridBlocks(int64_t(len), 256), 256, 0, ctx->stream>>>(int64_t(len), count, dCoef, Fh, Fd);
+          TCSCF_LAUNCH(ctx);
+          Fuse = Fd;
+        }
+      }
+    }
     for (int s = 0; s < nspin; ++s) {
-      kToColumnMajor<<<gridBlocks(nn, 256), 256, 0, ctx->stream>>>(nb, dF + s * nn, dS, A, B);
+      if (realPath) {
+        kDensityToReal<<<gridBlocks(nn, 256), 256, 0, ctx->stream>>>(1, nb, g1->dsto, Fuse + s * nn, FR);
+        TCSCF_LAUNCH(ctx);
+        kSplitDensity<<<1, 256, 0, ctx->stream>>>(nb, FR, Ar, fmax);
+        TCSCF_LAUNCH(ctx);
+        double hm[2];
+        TCSCF_CUDA(ctx, cudaMemcpyAsync(hm, fmax, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        if (!(hm[0] == hm[0]) || !(hm[1] == hm[1])) return fail(ctx, TCSCF_ERR_NONFINITE, "non-finite Fock matrix");
+        if (hm[1] <= 1e-10 * hm[0]) {
+          TCSCF_CUDA(ctx, cudaMemcpyAsync(Br, SRre, sizeof(double) * nn, cudaMemcpyDeviceToDevice, ctx->stream));
+          if (cusolverDnDsygvd(ctx->solver, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, nb, Ar, nb, Br, nb, W + s * nb,
+                               static_cast<double *>(wkR), lworkR, devInfo) != CUSOLVER_STATUS_SUCCESS)
+            return fail(ctx, TCSCF_ERR_LINALG, "cusolverDnDsygvd failed");
+          int info = 0;
+          TCSCF_CUDA(ctx, cudaMemcpyAsync(&info, devInfo, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+          TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+          if (info != 0) return fail(ctx, TCSCF_ERR_LINALG, "generalized eigen-solve failed (info " + std::to_string(info) + ")");
+          kRealDensity<<<gridBlocks(nn, 256), 256, 0, ctx->stream>>>(nb, nocc[s], Ar, DRre);
+          TCSCF_LAUNCH(ctx);
+          kRealToReference<<<gridBlocks(nn, 256), 256, 0, ctx->stream>>>(1, nb, g1->dsto, DRre, nullptr, dD + s * nn);
+          TCSCF_LAUNCH(ctx);
+          continue;
+        }
+      }
+      kToColumnMajor<<<gridBlocks(nn, 256), 256, 0, ctx->stream>>>(nb, Fuse + s * nn, dS, A, B);
       TCSCF_LAUNCH(ctx);
       if (cusolverDnZhegvd(ctx->solver, CUSOLVER_EIG_TYPE_1, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_UPPER, nb,
                            reinterpret_cast<cuDoubleComplex *>(A), nb, reinterpret_cast<cuDoubleComplex *>(B), nb, W + s * nb,

@@ -57,6 +57,7 @@ SIGNATURES: dict[str, tuple] = {
     "tcscf_grid_qmc": (_I, [_I, _I64, _D, _D, _D]),
     "tcscf_sobol": (_I, [_I, _I64, C.c_uint64, _D]),
     "tcscf_overlap_core_analytic": (_I, [C.POINTER(Sto), _I, _I, _D, _D]),
+    "tcscf_set_scf_options": (_I, [_P, _I, _I]),
     "tcscf_load_sto": (_I, [C.c_char_p, C.c_char_p, C.c_char_p, _I, C.POINTER(Sto), _I, C.POINTER(_I)]),
     "tcscf_grid_create": (_I, [_P, _D, _D, _I64, _I, C.POINTER(_I)]),
     "tcscf_grid_destroy": (_I, [_P, _I]),

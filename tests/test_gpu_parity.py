@@ -243,3 +243,25 @@ def test_invalid_arguments_raise(ctx, he_setup):
     hf = api.RCSHartreeFock(1, 1, w.nb)
     with pytest.raises(api.ConvergenceError):
         hf.compute(S, h, G, G, tol=1e-30, max_iter=2)
+
+
+def test_rcs_scf_diis_reaches_the_same_energy(ctx):
+    # optional Pulay DIIS (no reference counterpart): the converged energy of the plain Roothaan
+    # iteration (closed-shell atoms converge in a similar number of steps either way); DIIS off
+    # reproduces the plain iteration exactly
+    w = wl.ne()
+    g = grids.product_grid(24, 17)
+    G = api.QMCGrid(ctx, g)
+    G.setBasisFunctions(w.basis)
+    S, h = api.overlap_core(w.basis, w.Z)
+    plain = api.RCSHartreeFock(w.n_up, w.n_down, w.nb)
+    Ep = plain.compute(S, h, G, G, tol=1e-10, max_iter=200)
+    acc = api.RCSHartreeFock(w.n_up, w.n_down, w.nb)
+    Ed = acc.compute(S, h, G, G, tol=1e-10, max_iter=200, diis=8)
+    assert abs(Ed - Ep) < 1e-8, (Ed, Ep)
+    assert acc.numberOfConvergenceLoops() <= plain.numberOfConvergenceLoops() + 5
+    again = api.RCSHartreeFock(w.n_up, w.n_down, w.nb)
+    assert again.compute(S, h, G, G, tol=1e-10, max_iter=200) == Ep
+    with pytest.raises(ffi.TcscfError) as e:
+        acc.compute(S, h, G, G, diis=17)
+    assert e.value.code == ffi.ERR_INVALID_ARGUMENT
