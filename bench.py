@@ -308,10 +308,11 @@ def run_ours(args, rank: int, world: int) -> None:
                 "issued_tensor_tflops": issued, "issued_frac": issued / peak}
     else:
         peak = peaks["bf16_tflops"]
-        # tensor work the kernel issues per (r1, r2) pair: GEMM1 6 slice products of K = RP, GEMM2 4 of N = NB
+        # tensor work the kernel issues per (r1, r2) pair: GEMM1 6 slice products of K = RP; GEMM2 6 of
+        # N = NB with 24-bit X (rank padding 32), 4 with 16-bit X (rank padding 64)
         RP = 32 if w.n_up <= 32 else 64   # real closed-shell guess density: factor rank = n_occ
         NB = 64 if w.nb <= 64 else 128
-        issued = n * n * (2.0 * 6 * RP + 2.0 * 4 * NB) / (c_ms / 1e3) / 1e12
+        issued = n * n * (2.0 * 6 * RP + 2.0 * (6 if RP == 32 else 4) * NB) / (c_ms / 1e3) / 1e12
         roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                 "traffic": profiled_traffic(w.name), "peak_source": f"bf16 dense burst, {peak_kind}",
                 "issued_tensor_tflops": issued, "issued_frac": issued / peak}
@@ -327,7 +328,7 @@ def run_ours(args, rank: int, world: int) -> None:
             "config": {"workload": f"{w.name} RCS Fock build (direct form)", "Z": w.Z, "n_points": n, "n_basis": w.nb,
                        "n_occ": w.n_up, "grid": f"{w.nrad} radial (Gauss-Chebyshev, r=(1+x)/(1-x)) x Lebedev order {w.order}",
                        "precision": {"fp64": "fp64",
-                                     "bf16x3": "bf16 fixed-point slices (24-bit factors, 16- or 24-bit kernel tile), exact fp32 "
+                                     "bf16x3": "bf16 fixed-point slices (24-bit factors and kernel tile), exact fp32 "
                                                "accumulation of the leading slices per 64-point block, double-float across blocks",
                                      "tf32": "tf32 operands (10-bit mantissa, round to nearest), fp32 accumulation per 64-point "
                                              "block, double-float across blocks"}[args.precision],
