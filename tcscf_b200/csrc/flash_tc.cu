@@ -10,8 +10,8 @@
 // column of Vt carries a power-of-two scale s chosen from its largest entry.  The per-point factors
 // psi1, psi2 and Vt (whose rounding is shared by every pair a point takes part in) keep 24 bits:
 // u s in [2^23, 2^24) is written as 65536 h + 256 m + l with integers |h| <= 256, |m|, |l| <= 128
-// (round to nearest, each exact in BF16); X keeps 16 bits, u s = 256 h + l, or 24 bits like the
-// factors when r2 has fewer than 2^18 points.  X's lowest slice l enters only B, so it is stored as
+// (round to nearest, each exact in BF16); X keeps 24 bits like the factors (four slices) when the
+// rank padding is 32, 16 bits (u s = 256 h + l) when it is 64 and shared memory has no room for more.  X's lowest slice l enters only B, so it is stored as
 // the BF16 nearest to the remainder (8 significant bits) instead of an integer.  Per r2 block:
 //   A = sum h h'                      (integers below 2^16 each, a K <= 64 sum below 2^23: exact)
 //   B = sum h m' + m h' + (h l' + l h' + m m')/256   (the level 2^-8 below A; its own FP32 rounding
