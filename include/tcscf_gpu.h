@@ -250,6 +250,17 @@ int tcscf_scf(tcscf_ctx * ctx, int r1, int r2, int nspin, int n_up, int n_down, 
 int tcscf_tc_fock_build(tcscf_ctx * ctx, int r1, int fji_same, int fji_oppo, int vji_same, int vji_oppo, int n_up, int n_down,
                         const double * density, const double * occ_up, const double * occ_down, const double * h,
                         int respect_symmetry, double * G2, double * G3, double * fock, double * energy);
+/* computeQ (HartreeFock.cpp:613-683; the reference keeps it, and its comparison with the G_3 of
+ * tcscf_tc_fock_build, commented out in TCHartreeFock::compute): the 6-index tensors
+ * Q[j][p][r][i][q][s] = sum_r1 w (conj(b_j) (V_pq . V_rs) b_i + conj(b_p) (V_ji . V_rs) b_q
+ * + conj(b_r) (V_ji . V_pq) b_s) for the same-same, same-opposite and opposite-opposite pairs of the
+ * computeV handles vji_same / vji_oppo on the r1 grid.  Outputs complex [nb]^6 row-major (nb <= 16). */
+int tcscf_tc_compute_q(tcscf_ctx * ctx, int r1, int vji_same, int vji_oppo, double * Qss, double * Qso, double * Qoo);
+/* assembleG (HartreeFock.cpp:687-752, without its debugging checks): G3 [2][nb][nb] complex from the
+ * three Q tensors and the spin densities [2][nb][nb] complex (element (q, p) at [q][p]). */
+int tcscf_tc_assemble_g(tcscf_ctx * ctx, int nb, const double * Qss, const double * Qso, const double * Qoo, const double * density,
+                        double * G3);
+
 /* TCHartreeFock::compute: zero initial density, TC Fock build, the non-Hermitian pencil F C = S C e
  * solved on the device (Cholesky of S, cusolverDnXgeev), eigenvalues sorted by real part, occupied
  * vectors orthogonalised by the S-metric modified Gram-Schmidt of orthogonalization.hpp:136-154,

@@ -260,3 +260,21 @@ def mgs(vectors: np.ndarray, metric_col_major: np.ndarray | None = None) -> np.n
     v = np.ascontiguousarray(vectors, dtype=np.complex128).copy()
     lib().oracle_mgs(_p(v), v.shape[0], v.shape[1], _p(None if metric_col_major is None else np.ascontiguousarray(metric_col_major, dtype=np.complex128)))
     return v
+
+
+def compute_q(w1, vals1, Vs, Vo):
+    """computeQ (HartreeFock.cpp:613-683): (Qss, Qso, Qoo), each complex [nb]^6."""
+    N1, nb = vals1.shape
+    out = [np.empty((nb,) * 6, dtype=np.complex128) for _ in range(3)]
+    lib().oracle_compute_q(C.c_int64(N1), nb, _p(np.ascontiguousarray(w1)), _p(np.ascontiguousarray(vals1, dtype=np.complex128)),
+                           _p(np.ascontiguousarray(Vs)), _p(np.ascontiguousarray(Vo)), _p(out[0]), _p(out[1]), _p(out[2]))
+    return tuple(out)
+
+
+def assemble_g(Qss, Qso, Qoo, D):
+    """assembleG (HartreeFock.cpp:687-752): G3 [2][nb][nb] from the Q tensors and the spin densities."""
+    nb = Qss.shape[0]
+    G3 = np.empty((2, nb, nb), dtype=np.complex128)
+    lib().oracle_assemble_g(nb, _p(np.ascontiguousarray(Qss)), _p(np.ascontiguousarray(Qso)), _p(np.ascontiguousarray(Qoo)),
+                            _p(np.ascontiguousarray(D, dtype=np.complex128)), _p(G3))
+    return G3

@@ -1082,4 +1082,82 @@ void oracle_three_electron_integrals(double const * p1, double const * w1, int64
   }
 }
 
+// computeQ (HartreeFock.cpp:613-683): the 6-index verification tensors of the TC 3-body term,
+// Q[j][p][r][i][q][s] = sum_r1 w (conj(b_j) (V_pq . V_rs) b_i + conj(b_p) (V_ji . V_rs) b_q
+//                                 + conj(b_r) (V_ji . V_pq) b_s)
+// for the same-same (Vs, Vs), same-opposite (Vs, Vo) and opposite-opposite (Vo, Vo) pairs.  vals1
+// complex [N1][nb]; V complex Cartesian [N1][nb][nb][3]; outputs complex [nb]^6 row-major.
+void oracle_compute_q(int64_t N1, int nb, double const * w1, double const * vals1, double const * Vs, double const * Vo, double * Qss,
+                      double * Qso, double * Qoo)
+{
+  cplx const * b = reinterpret_cast<cplx const *>(vals1);
+  cplx const * vs = reinterpret_cast<cplx const *>(Vs);
+  cplx const * vo = reinterpret_cast<cplx const *>(Vo);
+  int64_t const n6 = int64_t(nb) * nb * nb * nb * nb * nb;
+  cplx * ss = reinterpret_cast<cplx *>(Qss);
+  cplx * so = reinterpret_cast<cplx *>(Qso);
+  cplx * oo = reinterpret_cast<cplx *>(Qoo);
+  for (int64_t o = 0; o < n6; ++o) ss[o] = so[o] = oo[o] = 0.0;
+  auto V = [&](cplx const * v, int64_t a, int x, int y, int d) { return v[((a * nb + x) * nb + y) * 3 + d]; };
+  auto dot = [&](cplx const * v1, cplx const * v2, int64_t a, int x1, int y1, int x2, int y2) {
+    return V(v1, a, x1, y1, 0) * V(v2, a, x2, y2, 0) + V(v1, a, x1, y1, 1) * V(v2, a, x2, y2, 1) + V(v1, a, x1, y1, 2) * V(v2, a, x2, y2, 2);
+  };
+  // r1 outermost per j slab (each thread owns the outputs of its j; the reference adds atomically)
+#pragma omp parallel for schedule(dynamic)
+  for (int j = 0; j < nb; ++j)
+    for (int64_t a = 0; a < N1; ++a) {
+      double const w = w1[a];
+      for (int p = 0; p < nb; ++p)
+        for (int r = 0; r < nb; ++r)
+          for (int i = 0; i < nb; ++i)
+            for (int q = 0; q < nb; ++q)
+              for (int s2 = 0; s2 < nb; ++s2) {
+                cplx const bj = std::conj(b[a * nb + j]), bp = std::conj(b[a * nb + p]), br = std::conj(b[a * nb + r]);
+                cplx const bi = b[a * nb + i], bq = b[a * nb + q], bs = b[a * nb + s2];
+                cplx const ss123 = bj * dot(vs, vs, a, p, q, r, s2) * bi, so123 = bj * dot(vs, vo, a, p, q, r, s2) * bi,
+                           oo123 = bj * dot(vo, vo, a, p, q, r, s2) * bi;
+                cplx const ss213 = bp * dot(vs, vs, a, j, i, r, s2) * bq, so213 = bp * dot(vs, vo, a, j, i, r, s2) * bq,
+                           oo213 = bp * dot(vo, vo, a, j, i, r, s2) * bq;
+                cplx const ss312 = br * dot(vs, vs, a, j, i, p, q) * bs, so312 = br * dot(vs, vo, a, j, i, p, q) * bs,
+                           oo312 = br * dot(vo, vo, a, j, i, p, q) * bs;
+                int64_t const o = ((((int64_t(j) * nb + p) * nb + r) * nb + i) * nb + q) * nb + s2;
+                ss[o] += w * (ss123 + ss213 + ss312);
+                so[o] += w * (so123 + so213 + so312);
+                oo[o] += w * (oo123 + oo213 + oo312);
+              }
+    }
+}
+
+// assembleG (HartreeFock.cpp:687-752) without its debugging checks: G3[spin][j][i] from the Q
+// tensors and the spin densities D [2][nb][nb] (element (q, p) at [q][p]).
+void oracle_assemble_g(int nb, double const * Qss, double const * Qso, double const * Qoo, double const * density, double * G3)
+{
+  cplx const * SS = reinterpret_cast<cplx const *>(Qss);
+  cplx const * SO = reinterpret_cast<cplx const *>(Qso);
+  cplx const * OO = reinterpret_cast<cplx const *>(Qoo);
+  cplx const * D = reinterpret_cast<cplx const *>(density);
+  cplx * G = reinterpret_cast<cplx *>(G3);
+  int64_t const nn = int64_t(nb) * nb;
+  auto Q = [&](cplx const * T, int j, int p, int r, int x, int y, int z) {
+    return T[((((int64_t(j) * nb + p) * nb + r) * nb + x) * nb + y) * nb + z];
+  };
+  auto Dm = [&](int spin, int x, int y) { return D[spin * nn + int64_t(x) * nb + y]; };
+  for (int j = 0; j < nb; ++j)
+    for (int i = 0; i < nb; ++i) {
+      cplx value[2] = {0.0, 0.0};
+      for (int p = 0; p < nb; ++p)
+        for (int q = 0; q < nb; ++q)
+          for (int r = 0; r < nb; ++r)
+            for (int s2 = 0; s2 < nb; ++s2)
+              for (int spin = 0; spin < 2; ++spin) {
+                value[spin] += Dm(spin, q, p) * Dm(spin, s2, r) *
+                               (Q(SS, j, p, r, i, q, s2) - Q(SS, j, p, r, i, s2, q) + 2.0 * Q(SS, j, p, r, q, s2, i) - 2.0 * Q(SS, j, p, r, s2, q, i));
+                value[spin] += 2.0 * Dm(spin, q, p) * Dm(!spin, s2, r) * (Q(SO, j, p, r, i, q, s2) - Q(SO, j, p, r, q, i, s2));
+                value[spin] += Dm(!spin, q, p) * Dm(!spin, s2, r) * (Q(OO, j, p, r, i, q, s2) - Q(OO, j, p, r, i, s2, q));
+              }
+      G[0 * nn + int64_t(j) * nb + i] = value[0] / 2.0;
+      G[1 * nn + int64_t(j) * nb + i] = value[1] / 2.0;
+    }
+}
+
 } // extern "C"

@@ -259,6 +259,25 @@ def tc_fock_build(r1Grid: QMCGrid, Fs: DeviceTensor, Fo: DeviceTensor, Vs: Devic
     return G2, G3, F, e.value
 
 
+def tc_compute_q(r1Grid: QMCGrid, Vs: DeviceTensor, Vo: DeviceTensor):
+    """computeQ (HartreeFock.cpp:613-683): (Qss, Qso, Qoo), complex [nb]^6 each, from computeV tensors."""
+    ctx = r1Grid.ctx
+    nb = r1Grid.nBasis()
+    out = [np.empty((nb,) * 6, dtype=np.complex128) for _ in range(3)]
+    _raise(ffi.lib().tcscf_tc_compute_q(ctx.handle, r1Grid.id, Vs.handle, Vo.handle, *(ffi.dptr(o) for o in out)), ctx.handle)
+    return tuple(out)
+
+
+def tc_assemble_g(ctx: Context, Qss: np.ndarray, Qso: np.ndarray, Qoo: np.ndarray, density: np.ndarray) -> np.ndarray:
+    """assembleG (HartreeFock.cpp:687-752): G3 [2][nb][nb] from the Q tensors and the spin densities."""
+    nb = Qss.shape[0]
+    D = np.ascontiguousarray(density, dtype=np.complex128)
+    G3 = np.empty((2, nb, nb), dtype=np.complex128)
+    args = [ffi.dptr(np.ascontiguousarray(q, dtype=np.complex128)) for q in (Qss, Qso, Qoo)]
+    _raise(ffi.lib().tcscf_tc_assemble_g(ctx.handle, nb, *args, ffi.dptr(D), ffi.dptr(G3)), ctx.handle)
+    return G3
+
+
 class TCHartreeFock:
     """TCHartreeFock::compute (HartreeFock.hpp:386-394, HartreeFock.cpp:1007-1362) on device tensors."""
 

@@ -125,6 +125,84 @@ int checkPair(tcscf_ctx * ctx, Grid * g1, Grid * g2, int ndim2)
   return TCSCF_OK;
 }
 
+// Y[a][(p,q),(r,s)] = Vx_pq(a) . Vy_rs(a) (complex Cartesian dot, no conjugate) for r1 rows a0..a0+rows
+__global__ void kVDotV2(int64_t a0, int64_t rows, int nb, const double2 * __restrict__ Vx, const double2 * __restrict__ Vy,
+                        double2 * __restrict__ Y)
+{
+  int64_t const nn = int64_t(nb) * nb, n4 = nn * nn;
+  for (int64_t idx = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; idx < rows * n4; idx += int64_t(gridDim.x) * blockDim.x) {
+    int64_t const a = a0 + idx / n4;
+    int64_t const k = idx % n4;
+    int64_t const pq = k / nn, rs = k % nn;
+    double2 const * x = Vx + (a * nn + pq) * 3;
+    double2 const * y = Vy + (a * nn + rs) * 3;
+    double re = 0, im = 0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      re += x[d].x * y[d].x - x[d].y * y[d].y;
+      im += x[d].x * y[d].y + x[d].y * y[d].x;
+    }
+    Y[idx] = make_double2(re, im);
+  }
+}
+
+// computeQ's three terms from T[(ji)][(pq)][(rs)] = sum_r1 w conj(b_j) b_i (V_pq . V_rs), stored
+// column-major as C[(ji) + nn ((pq) nn + (rs))]:
+// Q[j][p][r][i][q][s] = T[ji][pq][rs] + T[pq][ji][rs] + T[rs][ji][pq]   (HartreeFock.cpp:655-673)
+__global__ void kAssembleQ(int nb, const double2 * __restrict__ C, double2 * __restrict__ Q)
+{
+  int64_t const nn = int64_t(nb) * nb, n6 = nn * nn * nn;
+  auto T = [&](int64_t a, int64_t b, int64_t c) { return C[a + nn * (b * nn + c)]; };
+  for (int64_t idx = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; idx < n6; idx += int64_t(gridDim.x) * blockDim.x) {
+    int64_t k = idx;
+    int const s = int(k % nb); k /= nb;
+    int const q = int(k % nb); k /= nb;
+    int const i = int(k % nb); k /= nb;
+    int const r = int(k % nb); k /= nb;
+    int const p = int(k % nb); k /= nb;
+    int const j = int(k);
+    int64_t const ji = int64_t(j) * nb + i, pq = int64_t(p) * nb + q, rs = int64_t(r) * nb + s;
+    double2 const a = T(ji, pq, rs), b = T(pq, ji, rs), c = T(rs, ji, pq);
+    Q[idx] = make_double2(a.x + b.x + c.x, a.y + b.y + c.y);
+  }
+}
+
+__device__ __forceinline__ double2 cmulQ(double2 a, double2 b) { return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+
+// assembleG (HartreeFock.cpp:687-752, without its debugging checks): one thread per (j, i)
+__global__ void kAssembleG(int nb, const double2 * __restrict__ SS, const double2 * __restrict__ SO, const double2 * __restrict__ OO,
+                           const double2 * __restrict__ D, double2 * __restrict__ G3)
+{
+  int64_t const nn = int64_t(nb) * nb;
+  for (int64_t ji = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; ji < nn; ji += int64_t(gridDim.x) * blockDim.x) {
+    int const j = int(ji / nb), i = int(ji % nb);
+    auto Qv = [&](const double2 * T, int p, int r, int x, int y, int z) {
+      return T[((((int64_t(j) * nb + p) * nb + r) * nb + x) * nb + y) * nb + z];
+    };
+    double2 value[2] = {make_double2(0, 0), make_double2(0, 0)};
+    for (int p = 0; p < nb; ++p)
+      for (int q = 0; q < nb; ++q)
+        for (int r = 0; r < nb; ++r)
+          for (int s = 0; s < nb; ++s) {
+            double2 const ss1 = Qv(SS, p, r, i, q, s), ss2 = Qv(SS, p, r, i, s, q), ss3 = Qv(SS, p, r, q, s, i), ss4 = Qv(SS, p, r, s, q, i);
+            double2 const so1 = Qv(SO, p, r, i, q, s), so2 = Qv(SO, p, r, q, i, s);
+            double2 const oo1 = Qv(OO, p, r, i, q, s), oo2 = Qv(OO, p, r, i, s, q);
+            double2 const tss = make_double2(ss1.x - ss2.x + 2 * ss3.x - 2 * ss4.x, ss1.y - ss2.y + 2 * ss3.y - 2 * ss4.y);
+            double2 const tso = make_double2(2 * (so1.x - so2.x), 2 * (so1.y - so2.y));
+            double2 const too = make_double2(oo1.x - oo2.x, oo1.y - oo2.y);
+            for (int spin = 0; spin < 2; ++spin) {
+              double2 const dqp = D[spin * nn + int64_t(q) * nb + p], dsr = D[spin * nn + int64_t(s) * nb + r];
+              double2 const oqp = D[(1 - spin) * nn + int64_t(q) * nb + p], osr = D[(1 - spin) * nn + int64_t(s) * nb + r];
+              double2 const a = cmulQ(cmulQ(dqp, dsr), tss), b = cmulQ(cmulQ(dqp, osr), tso), c = cmulQ(cmulQ(oqp, osr), too);
+              value[spin].x += a.x + b.x + c.x;
+              value[spin].y += a.y + b.y + c.y;
+            }
+          }
+    G3[ji] = make_double2(value[0].x / 2, value[0].y / 2);
+    G3[nn + ji] = make_double2(value[1].x / 2, value[1].y / 2);
+  }
+}
+
 }  // namespace
 }  // namespace tcscf
 
@@ -258,6 +336,82 @@ int tcscf_three_electron_integrals(tcscf_ctx * ctx, int r1, int r2, const tcscf_
   kPermute6<<<gridBlocks(n6, 256), 256, 0, ctx->stream>>>(nb, C, out);
   TCSCF_LAUNCH(ctx);
   TCSCF_CUDA(ctx, cudaMemcpyAsync(answer, out, sizeof(double2) * size_t(n6), cudaMemcpyDeviceToHost, ctx->stream));
+  TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return TCSCF_OK;
+}
+
+int tcscf_tc_compute_q(tcscf_ctx * ctx, int r1, int vsame, int voppo, double * Qss, double * Qso, double * Qoo)
+{
+  if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  Grid * g1 = findGrid(ctx, r1);
+  TCSCF_CHECK(ctx, g1 && g1->nb > 0 && g1->ndim == 3, TCSCF_ERR_INVALID_ARGUMENT, "computeQ: a 3-D r1 grid with basis values is required");
+  TCSCF_CHECK(ctx, Qss && Qso && Qoo, TCSCF_ERR_INVALID_ARGUMENT, "computeQ: three outputs are required");
+  auto itS = ctx->tensors.find(vsame), itO = ctx->tensors.find(voppo);
+  TCSCF_CHECK(ctx, itS != ctx->tensors.end() && itO != ctx->tensors.end() && itS->second.vec && itO->second.vec, TCSCF_ERR_INVALID_ARGUMENT,
+              "computeQ: two computeV tensor handles are required");
+  int const nb = g1->nb;
+  TCSCF_CHECK(ctx, itS->second.nb == nb && itO->second.nb == nb && itS->second.n1 == g1->n && itO->second.n1 == g1->n,
+              TCSCF_ERR_INVALID_ARGUMENT, "computeQ: the tensors do not match the r1 grid");
+  TCSCF_CHECK(ctx, nb <= 16, TCSCF_ERR_UNSUPPORTED, "computeQ: nb <= 16 (three nb^6 complex tensors)");
+  int64_t const nn = int64_t(nb) * nb, n4 = nn * nn, n6 = n4 * nn, n1 = g1->n;
+  const double2 * Vs = reinterpret_cast<const double2 *>(itS->second.d);
+  const double2 * Vo = reinterpret_cast<const double2 *>(itO->second.d);
+  cublasHandle_t h = nullptr;
+  TCSCF_TRY(blasHandle(ctx, &h));
+  int64_t const chunk = std::max<int64_t>(1, std::min<int64_t>(n1, (int64_t(1) << 26) / n4));
+  size_t const bytes = sizeof(double2) * (size_t(chunk) * nn + size_t(chunk) * n4 + 4 * size_t(n6));
+  void * p = nullptr;
+  TCSCF_TRY(scratch(ctx, "compute_q", bytes, &p));
+  double2 * X = static_cast<double2 *>(p);
+  double2 * Y = X + size_t(chunk) * nn;
+  double2 * C = Y + size_t(chunk) * n4;        // [3][n6]: same-same, same-opposite, opposite-opposite
+  double2 * out = C + 3 * size_t(n6);
+  const double2 * pairs[3][2] = {{Vs, Vs}, {Vs, Vo}, {Vo, Vo}};
+  cuDoubleComplex const one = make_cuDoubleComplex(1, 0), zero = make_cuDoubleComplex(0, 0);
+  for (int64_t a0 = 0; a0 < n1; a0 += chunk) {
+    int64_t const rows = std::min(chunk, n1 - a0);
+    kR1Pairs<<<gridBlocks(rows * nn, 256), 256, 0, ctx->stream>>>(a0, rows, nb, reinterpret_cast<const double2 *>(g1->vals), g1->w, X);
+    TCSCF_LAUNCH(ctx);
+    for (int t = 0; t < 3; ++t) {
+      kVDotV2<<<gridBlocks(rows * n4, 256), 256, 0, ctx->stream>>>(a0, rows, nb, pairs[t][0], pairs[t][1], Y);
+      TCSCF_LAUNCH(ctx);
+      // C_t [(ji)][(pq,rs)] (column-major) += X^T Y over this chunk of r1
+      cublasStatus_t const bs = cublasZgemm(h, CUBLAS_OP_N, CUBLAS_OP_T, int(nn), int(n4), int(rows), &one,
+                                            reinterpret_cast<const cuDoubleComplex *>(X), int(nn), reinterpret_cast<const cuDoubleComplex *>(Y),
+                                            int(n4), a0 == 0 ? &zero : &one, reinterpret_cast<cuDoubleComplex *>(C + t * n6), int(nn));
+      TCSCF_CHECK(ctx, bs == CUBLAS_STATUS_SUCCESS, TCSCF_ERR_CUDA, "cuBLAS ZGEMM failed");
+    }
+  }
+  double * outs[3] = {Qss, Qso, Qoo};
+  for (int t = 0; t < 3; ++t) {
+    kAssembleQ<<<gridBlocks(n6, 256), 256, 0, ctx->stream>>>(nb, C + t * n6, out);
+    TCSCF_LAUNCH(ctx);
+    TCSCF_CUDA(ctx, cudaMemcpyAsync(outs[t], out, sizeof(double2) * size_t(n6), cudaMemcpyDeviceToHost, ctx->stream));
+    TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+  return TCSCF_OK;
+}
+
+int tcscf_tc_assemble_g(tcscf_ctx * ctx, int nb, const double * Qss, const double * Qso, const double * Qoo, const double * density, double * G3)
+{
+  if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  TCSCF_CHECK(ctx, nb >= 1 && nb <= 16 && Qss && Qso && Qoo && density && G3, TCSCF_ERR_INVALID_ARGUMENT,
+              "assembleG: nb in 1..16 and all arrays are required");
+  int64_t const nn = int64_t(nb) * nb, n6 = nn * nn * nn;
+  void * p = nullptr;
+  TCSCF_TRY(scratch(ctx, "assemble_g", sizeof(double2) * (3 * size_t(n6) + 4 * size_t(nn)), &p));
+  double2 * Q = static_cast<double2 *>(p);
+  double2 * D = Q + 3 * size_t(n6);
+  double2 * G = D + 2 * size_t(nn);
+  double const * in[3] = {Qss, Qso, Qoo};
+  for (int t = 0; t < 3; ++t)
+    TCSCF_CUDA(ctx, cudaMemcpyAsync(Q + t * n6, in[t], sizeof(double2) * size_t(n6), cudaMemcpyHostToDevice, ctx->stream));
+  TCSCF_CUDA(ctx, cudaMemcpyAsync(D, density, sizeof(double2) * 2 * size_t(nn), cudaMemcpyHostToDevice, ctx->stream));
+  kAssembleG<<<gridBlocks(nn, 64), 64, 0, ctx->stream>>>(nb, Q, Q + n6, Q + 2 * n6, D, G);
+  TCSCF_LAUNCH(ctx);
+  TCSCF_CUDA(ctx, cudaMemcpyAsync(G3, G, sizeof(double2) * 2 * size_t(nn), cudaMemcpyDeviceToHost, ctx->stream));
   TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return TCSCF_OK;
 }

@@ -88,3 +88,23 @@ def test_tc_argument_checks(ctx, tc_setup):
     with pytest.raises(ffi.TcscfError) as e:      # V handle where an F handle belongs
         api.tc_fock_build(G1, t["Vs"], t["Fo"], t["Vs"], t["Vo"], NUP, NDOWN, D, occ, occ, h)
     assert e.value.code == ffi.ERR_INVALID_ARGUMENT
+
+
+def test_compute_q_and_assemble_g_match_oracle(ctx, tc_setup):
+    # the reference's verification route for the 3-body term (computeQ / assembleG,
+    # HartreeFock.cpp:613-752): device ZGEMMs over r1 against the oracle's loops to 1e-10 of the
+    # largest element; assembleG on the same Q to 1e-12
+    G1, t, o, S, h = tc_setup
+    Q = api.tc_compute_q(G1, t["Vs"], t["Vo"])
+    Qr = oracle.compute_q(o["w1"], o["vals1"], o["Vs"], o["Vo"])
+    for a, b in zip(Q, Qr):
+        np.testing.assert_allclose(a, b, rtol=0, atol=1e-10 * np.abs(b).max())
+    # c_same = c_opposite / 2 here, so Q_so = 2 Q_ss and Q_oo = 4 Q_ss (the reference's own checks)
+    np.testing.assert_allclose(Q[1], 2 * Q[0], rtol=0, atol=1e-12 * np.abs(Q[1]).max())
+    np.testing.assert_allclose(Q[2], 4 * Q[0], rtol=0, atol=1e-12 * np.abs(Q[2]).max())
+    rng = np.random.default_rng(9)
+    occ = [_random_orbitals(len(BASIS), n, rng) for n in (NUP, NDOWN)]
+    D = np.stack([c.T @ c.conj() for c in occ])
+    G3 = api.tc_assemble_g(ctx, *Qr, D)
+    G3r = oracle.assemble_g(*Qr, D)
+    np.testing.assert_allclose(G3, G3r, rtol=0, atol=1e-12 * np.abs(G3r).max())
