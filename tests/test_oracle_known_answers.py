@@ -223,3 +223,22 @@ def test_library_family_overlap_core_matches_oracle():
     Sh, Hh = oracle.overlap_core(wl.hydrogen_functions(3, 2, 2), 2)
     np.testing.assert_allclose(Sh, np.eye(len(Sh)), atol=1e-8)          # orthonormal (same Z)
     assert np.allclose(np.diag(Hh)[:1], -2.0)                          # -Z^2 / 2 for 1s
+
+
+def test_oracle_compute_q_symmetries():
+    # the relations assembleG checks before using Q (HartreeFock.cpp:716-720): with c_same = c_oppo / 2
+    # the gradients satisfy Vo = 2 Vs exactly, so Q_so = 2 Q_ss and Q_oo = 4 Q_ss, and every Q is
+    # symmetric under (p, q) <-> (r, s)
+    from tcscf_b200 import basis as wl
+    b = wl.expand(0, [0.8, 1.7]) + wl.expand(1, [1.2])
+    nb = len(b)
+    g1 = grids.qmc_grid(3, 24, 61)
+    g2 = grids.qmc_grid(3, 64, 62)
+    u = oracle.ochi(1.0, 1.0, [((1, 0, 0), -0.5, -0.25)])
+    vals2 = oracle.basis_values(g2.points, b)
+    Vs = oracle.compute_V(g1.points, g2.points, g2.weights, vals2, nb, ffi.K_GRAD_U_SAME, u)
+    Vo = oracle.compute_V(g1.points, g2.points, g2.weights, vals2, nb, ffi.K_GRAD_U_OPPO, u)
+    Qss, Qso, Qoo = oracle.compute_q(g1.weights, oracle.basis_values(g1.points, b), Vs, Vo)
+    assert np.abs(Qso - 2 * Qss).max() <= 1e-15 * np.abs(Qso).max()
+    assert np.abs(Qoo - 4 * Qss).max() <= 1e-15 * np.abs(Qoo).max()
+    np.testing.assert_allclose(Qss, np.transpose(Qss, (0, 2, 1, 3, 5, 4)), rtol=0, atol=1e-14 * np.abs(Qss).max())
