@@ -219,6 +219,11 @@ int tcscf_fock_build_batch(tcscf_ctx * ctx, int count, const int * r1, const int
 /* Same, from a device-resident Fji handle (the reference's precompute form). */
 int tcscf_fock_build_precomputed(tcscf_ctx * ctx, int r1, int fji, int nspin, const double * density, const double * h,
                                  int respect_symmetry, double * G, double * fock, double * energy);
+/* CUDA-graph use of tcscf_fock_build_batch on this context (no reference counterpart): the batch's
+ * persistent tensor launches are captured into a graph the first time a launch sequence (tile
+ * classes, grid sizes, work-item counts, device tables) occurs and replayed while it repeats, e.g.
+ * over the SCF iterations of one set of instances.  Returns the numbers of captures and replays. */
+int tcscf_batch_graph_stats(tcscf_ctx * ctx, int * captures, int * replays);
 
 /* ---- SCF drivers (RCSHartreeFock/UOSHartreeFock::compute, HartreeFock.cpp:785-1003) ---------- */
 /* Options of tcscf_scf on this context (no reference counterpart; the defaults, 0 and 0, reproduce

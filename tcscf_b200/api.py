@@ -73,6 +73,12 @@ class Context:
     def synchronize(self) -> None:
         _raise(ffi.lib().tcscf_synchronize(self._h), self._h)
 
+    def batch_graph_stats(self) -> tuple[int, int]:
+        """(captures, replays) of the batched builds' CUDA graph on this context."""
+        a, b = C.c_int(), C.c_int()
+        _raise(ffi.lib().tcscf_batch_graph_stats(self._h, C.byref(a), C.byref(b)), self._h)
+        return a.value, b.value
+
     def last_timing(self) -> tuple[float, float, int]:
         a, b, n = C.c_double(), C.c_double(), C.c_int()
         _raise(ffi.lib().tcscf_last_timing(self._h, C.byref(a), C.byref(b), C.byref(n)), self._h)

@@ -73,6 +73,11 @@ struct tcscf_ctx {
   int lastLaunches = 0;
   int launchCount = 0;
   int diisSize = 0;   // Pulay DIIS history length of tcscf_scf (0: plain Roothaan iterations)
+  // CUDA graph of the most recent batched tensor launch sequence and the launch parameters it was
+  // captured with (replayed while a batch repeats them); capture / replay counts
+  cudaGraphExec_t tensorGraph = nullptr;
+  std::vector<uint64_t> tensorGraphKey;
+  int graphCaptures = 0, graphReplays = 0;
   int realEigen = 0;  // tcscf_scf solves a Fock matrix that is real in the real-harmonic basis there
   std::map<std::string, tcscf::Scratch> scratch;
   // device buffers of the most recent direct Fock build (for tcscf_last_potentials)

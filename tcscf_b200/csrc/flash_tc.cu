@@ -919,8 +919,11 @@ int tensorRun(tcscf_ctx * ctx, TensorPrep * const * preps, int count, bool recor
   TCSCF_CUDA(ctx, cudaMemsetAsync(dStatus, 0, sizeof(int), ctx->stream));
 
   // one persistent launch per tile class; within it, work items longest first, dealt round-robin
-  std::vector<int4> hItems;
-  hItems.reserve(itemsTotal);
+  struct Launch {
+    int NB, RP, XS, grid;
+    tc::Params P;
+  };
+  std::vector<Launch> launches;
   size_t offset = 0;
   if (recordStart) cudaEventRecord(ctx->ev[2], ctx->stream);
   for (auto const & cl : kClasses) {
@@ -940,8 +943,44 @@ int tensorRun(tcscf_ctx * ctx, TensorPrep * const * preps, int count, bool recor
     P.items = count == 1 ? nullptr : dItems + offset;
     P.inst = dInst;
     P.status = dStatus;
-    TCSCF_TRY(launchClass(ctx, NB, RP, XS, P, std::min(int(items.size()), sms)));
+    launches.push_back({NB, RP, XS, std::min(int(items.size()), sms), P});
     offset += items.size();
+  }
+  if (count == 1) {
+    for (auto const & l : launches) TCSCF_TRY(launchClass(ctx, l.NB, l.RP, l.XS, l.P, l.grid));
+  } else {
+    // A batch runs as a CUDA graph of its persistent launches, captured once per launch sequence and
+    // replayed while the sequence repeats (every SCF iteration of the same instances): the instance
+    // table, tensor maps and work items the kernels read are refreshed above, before the replay.
+    std::vector<uint64_t> key;
+    for (auto const & l : launches) {
+      key.insert(key.end(), {uint64_t(l.NB), uint64_t(l.RP), uint64_t(l.XS), uint64_t(l.grid), uint64_t(l.P.nItems),
+                             uint64_t(reinterpret_cast<uintptr_t>(l.P.items)), uint64_t(reinterpret_cast<uintptr_t>(l.P.inst)),
+                             uint64_t(reinterpret_cast<uintptr_t>(l.P.status))});
+    }
+    if (!ctx->tensorGraph || ctx->tensorGraphKey != key) {
+      if (ctx->tensorGraph) {
+        cudaGraphExecDestroy(ctx->tensorGraph);
+        ctx->tensorGraph = nullptr;
+      }
+      TCSCF_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed));
+      int lst = TCSCF_OK;
+      for (auto const & l : launches)
+        if (lst == TCSCF_OK) lst = launchClass(ctx, l.NB, l.RP, l.XS, l.P, l.grid);
+      cudaGraph_t graph = nullptr;
+      cudaError_t const ce = cudaStreamEndCapture(ctx->stream, &graph);
+      TCSCF_TRY(lst);
+      TCSCF_CHECK(ctx, ce == cudaSuccess && graph, TCSCF_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+      cudaError_t const ie = cudaGraphInstantiate(&ctx->tensorGraph, graph, 0);
+      cudaGraphDestroy(graph);
+      TCSCF_CHECK(ctx, ie == cudaSuccess, TCSCF_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
+      ctx->tensorGraphKey = key;
+      ++ctx->graphCaptures;
+    } else {
+      ++ctx->graphReplays;
+      ctx->launchCount += int(launches.size());
+    }
+    TCSCF_CUDA(ctx, cudaGraphLaunch(ctx->tensorGraph, ctx->stream));
   }
   cudaEventRecord(ctx->ev[3], ctx->stream);
   int st = 0;

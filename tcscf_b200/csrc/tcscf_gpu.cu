@@ -1312,6 +1312,7 @@ int tcscf_ctx_destroy(tcscf_ctx * ctx)
   for (auto & kv : ctx->tensors) cudaFree(kv.second.d);
   for (auto & kv : ctx->scratch) cudaFree(kv.second.p);
   for (auto & e : ctx->ev) cudaEventDestroy(e);
+  if (ctx->tensorGraph) cudaGraphExecDestroy(ctx->tensorGraph);
   if (ctx->solver) cusolverDnDestroy(ctx->solver);
   if (ctx->blas) cublasDestroy(ctx->blas);
   cudaStreamDestroy(ctx->stream);
@@ -1320,6 +1321,14 @@ int tcscf_ctx_destroy(tcscf_ctx * ctx)
 }
 
 const char * tcscf_last_error(tcscf_ctx * ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int tcscf_batch_graph_stats(tcscf_ctx * ctx, int * captures, int * replays)
+{
+  if (!ctx || !captures || !replays) return TCSCF_ERR_INVALID_ARGUMENT;
+  *captures = ctx->graphCaptures;
+  *replays = ctx->graphReplays;
+  return TCSCF_OK;
+}
 
 int tcscf_ctx_stream(tcscf_ctx * ctx, void ** stream)
 {

@@ -69,6 +69,7 @@ SIGNATURES: dict[str, tuple] = {
     "tcscf_three_electron_integrals": (_I, [_P, _I, _I, C.POINTER(Ochi), _D]),
     "tcscf_fock_build_batch": (_I, [_P, _I, C.POINTER(_I), C.POINTER(_I), C.POINTER(_D), C.POINTER(_D), _I, _I, _D, C.POINTER(_D)]),
     "tcscf_tc_fock_build": (_I, [_P, _I, _I, _I, _I, _I, _I, _I, _D, _D, _D, _D, _I, _D, _D, _D, _D]),
+    "tcscf_batch_graph_stats": (_I, [_P, C.POINTER(_I), C.POINTER(_I)]),
     "tcscf_tc_compute_q": (_I, [_P, _I, _I, _I, _D, _D, _D]),
     "tcscf_tc_assemble_g": (_I, [_P, _I, _D, _D, _D, _D, _D]),
     "tcscf_tc_scf": (_I, [_P, _I, _I, _I, _I, _I, _D, _D, _I, _I, _I, C.c_double, _I, _D, C.POINTER(_I), _D, _D]),

@@ -76,3 +76,27 @@ def test_batch_tf32_matches_single_builds(ctx):
     for k, (w, G, h) in enumerate(inst):
         _, _, Et = api.fock_build(G, G, Ds[k], h, precision=ffi.PREC_TF32)
         assert E[k] == Et, (k, E[k], Et)
+
+
+def test_batch_graph_replays_give_identical_results(ctx):
+    # the batch's persistent launches run as a CUDA graph: captured on the first call with a new launch
+    # sequence, replayed on repeats (fresh device tables each time); results are bit-identical
+    inst = _instances(ctx, 3, 17)
+    rng = np.random.default_rng(19)
+    Ds = [real_density(w.basis, max(1, min(w.n_up, 4)), rng) for w, G, h in inst]
+    Gs = [G for w, G, h in inst]
+    hs = [h for w, G, h in inst]
+    c0, r0 = ctx.batch_graph_stats()
+    E1 = api.fock_build_batch(Gs, Gs, Ds, hs, precision=ffi.PREC_BF16X3)
+    c1, r1 = ctx.batch_graph_stats()
+    E2 = api.fock_build_batch(Gs, Gs, Ds, hs, precision=ffi.PREC_BF16X3)
+    c2, r2 = ctx.batch_graph_stats()
+    assert r2 == r1 + 1 and c2 == c1, (c0, r0, c1, r1, c2, r2)
+    assert np.array_equal(E1, E2)
+    # a different density on the same instances replays the same graph and changes the result
+    Ds2 = [real_density(w.basis, max(1, min(w.n_up, 4)), rng) for w, G, h in inst]
+    E3 = api.fock_build_batch(Gs, Gs, Ds2, hs, precision=ffi.PREC_BF16X3)
+    assert ctx.batch_graph_stats()[1] == r2 + 1
+    for k, (w, G, h) in enumerate(inst):
+        _, _, Es = api.fock_build(G, G, Ds2[k], h, precision=ffi.PREC_BF16X3)
+        assert E3[k] == Es, (k, E3[k], Es)
