@@ -100,3 +100,19 @@ def test_batch_graph_replays_give_identical_results(ctx):
     for k, (w, G, h) in enumerate(inst):
         _, _, Es = api.fock_build(G, G, Ds2[k], h, precision=ffi.PREC_BF16X3)
         assert E3[k] == Es, (k, E3[k], Es)
+
+
+def test_batch_graph_recaptured_for_a_new_launch_sequence(ctx):
+    # another set of instances gives another launch sequence: a fresh capture, and its results still
+    # equal the single builds
+    inst = _instances(ctx, 2, 23)
+    rng = np.random.default_rng(29)
+    Ds = [real_density(w.basis, max(1, min(w.n_up, 4)), rng) for w, G, h in inst]
+    Gs = [G for w, G, h in inst]
+    hs = [h for w, G, h in inst]
+    c0, _ = ctx.batch_graph_stats()
+    E = api.fock_build_batch(Gs, Gs, Ds, hs, precision=ffi.PREC_BF16X3)
+    assert ctx.batch_graph_stats()[0] == c0 + 1
+    for k, (w, G, h) in enumerate(inst):
+        _, _, Es = api.fock_build(G, G, Ds[k], h, precision=ffi.PREC_BF16X3)
+        assert E[k] == Es, (k, E[k], Es)
