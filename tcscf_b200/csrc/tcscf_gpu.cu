@@ -48,13 +48,6 @@ Grid * findGrid(tcscf_ctx * ctx, int id)
 
 namespace {
 
-__device__ __forceinline__ double ipow(double x, int k)
-{
-  double r = 1;
-  for (int i = 0; i < k; ++i) r *= x;
-  return r;
-}
-
 // Fully normalised associated Legendre function with the Condon-Shortley phase,
 // P(l, m, cos t) = (-1)^m sqrt((2l+1)/(4 pi) (l-m)!/(l+m)!) P_l^m(cos t), i.e. Y_l^m(t, 0), evaluated
 // with the standard three-term recurrences in l at fixed m (x = cos t, s = sin t).
