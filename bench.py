@@ -201,7 +201,7 @@ def profiled_traffic(name: str):
 def run_ours(args, rank: int, world: int) -> None:
     import torch
 
-    from tcscf_b200 import api, ffi, grids
+    from tcscf_b200 import api, ffi, grids, replicas
 
     local = int(os.environ.get("LOCAL_RANK", 0))
     torch.cuda.set_device(local)
@@ -235,8 +235,7 @@ def run_ours(args, rank: int, world: int) -> None:
         for _ in range(steps):
             flush.zero_()
             torch.cuda.synchronize()
-            if world > 1:
-                torch.distributed.barrier()
+            replicas.barrier(world)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
             step(precision)
@@ -250,12 +249,8 @@ def run_ours(args, rank: int, world: int) -> None:
 
     with ClockSampler(local) as clk:
         ms, cms, launches, E = timed(prec, args.steps, args.warmup)
-    total_ms = sum(ms)
-    if world > 1:
-        t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
-    s_per_iter = total_ms / 1e3 / (args.steps * world)
+    total_ms = replicas.max_over_ranks(sum(ms), world, dev)
+    s_per_iter = replicas.whole_job_seconds_per_build(total_ms, args.steps, world)
 
     # FP64 comparison (the plain FP64 GPU form) at the same density
     fp64 = None
@@ -477,15 +472,10 @@ def main() -> None:
     ap.add_argument("--skip-cpu", action="store_true")
     args = ap.parse_args()
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    if world > 1:
-        import datetime
+    from tcscf_b200 import replicas
 
-        import torch
-
-        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
-        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    rank, world, local = replicas.env_ranks()
+    replicas.init(world, local)
     try:
         if args.impl == "reference":
             run_reference(args, rank)
@@ -496,10 +486,7 @@ def main() -> None:
         else:
             run_ours(args, rank, world)
     finally:
-        if world > 1:
-            import torch
-
-            torch.distributed.destroy_process_group()
+        replicas.finalize(world)
 
 
 if __name__ == "__main__":
