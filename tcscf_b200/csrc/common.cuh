@@ -64,6 +64,10 @@ struct tcscf_ctx {
   cudaStream_t stream = nullptr;
   cusolverDnHandle_t solver = nullptr;
   cublasHandle_t blas = nullptr;   // created on first use (4- and 6-index tensors)
+  // stream-ordered pool of the grid buffers (points, weights, basis values and gradients, the
+  // packed tensor-path operand): grids created and destroyed between SCF runs reuse its memory
+  // without driver allocations or the device-wide synchronisation of cudaFree
+  cudaMemPool_t gridPool = nullptr;
   std::string err;
   std::map<int, tcscf::Grid> grids;
   std::map<int, tcscf::Tensor> tensors;
@@ -121,6 +125,21 @@ int fail(tcscf_ctx * ctx, int code, std::string const & msg);
 int scratch(tcscf_ctx * ctx, char const * name, size_t bytes, void ** out);
 
 Grid * findGrid(tcscf_ctx * ctx, int id);
+
+// grid buffers from the context's pool, ordered on ctx->stream; every allocation is checked to be
+// 256-byte aligned (vector loads and TMA descriptors rely on it)
+int gridAllocBytes(tcscf_ctx * ctx, void ** p, size_t bytes);
+template <class T> int gridAlloc(tcscf_ctx * ctx, T ** p, size_t bytes)
+{
+  void * q = nullptr;
+  int const st = gridAllocBytes(ctx, &q, bytes);
+  *p = static_cast<T *>(q);
+  return st;
+}
+// returns a grid buffer to the pool in stream order (null is ignored)
+void gridRelease(tcscf_ctx * ctx, void * p);
+// releases every buffer of a grid and clears its pointers
+void gridReleaseAll(tcscf_ctx * ctx, Grid & g);
 
 inline unsigned gridBlocks(int64_t n, int threads)
 {

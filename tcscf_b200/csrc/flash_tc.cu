@@ -738,10 +738,9 @@ int tensorPackedV(tcscf_ctx * ctx, Grid & g2, const double * V, double scale, co
   int const NB = g2.nb <= 64 ? 64 : 128;
   int64_t const n2pad = (g2.n + tc::BK - 1) / tc::BK * tc::BK;
   if (!g2.vtCache || g2.vtNB != NB || g2.vtN2pad != n2pad || g2.vtScale != scale) {
-    cudaStreamSynchronize(ctx->stream);
-    cudaFree(g2.vtCache);
+    gridRelease(ctx, g2.vtCache);
     g2.vtCache = nullptr;
-    TCSCF_CUDA(ctx, cudaMalloc(&g2.vtCache, packedVtBytes(NB, n2pad)));
+    TCSCF_TRY(gridAlloc(ctx, &g2.vtCache, packedVtBytes(NB, n2pad)));
     TCSCF_TRY(packVt(ctx, g2.n, n2pad, g2.nb, NB, V, g2.nb, g2.vtCache));
     g2.vtNB = NB;
     g2.vtN2pad = n2pad;

@@ -46,6 +46,33 @@ Grid * findGrid(tcscf_ctx * ctx, int id)
   return it == ctx->grids.end() ? nullptr : &it->second;
 }
 
+int gridAllocBytes(tcscf_ctx * ctx, void ** p, size_t bytes)
+{
+  *p = nullptr;
+  cudaError_t const e = cudaMallocFromPoolAsync(p, std::max<size_t>(bytes, 256), ctx->gridPool, ctx->stream);
+  if (e != cudaSuccess) return fail(ctx, TCSCF_ERR_CUDA, std::string("grid buffer allocation: ") + cudaGetErrorString(e));
+  if (reinterpret_cast<uintptr_t>(*p) % 256 != 0) {
+    cudaFreeAsync(*p, ctx->stream);
+    *p = nullptr;
+    return fail(ctx, TCSCF_ERR_CUDA, "grid buffer allocation is not 256-byte aligned");
+  }
+  return TCSCF_OK;
+}
+
+void gridRelease(tcscf_ctx * ctx, void * p)
+{
+  if (p) cudaFreeAsync(p, ctx->stream);
+}
+
+void gridReleaseAll(tcscf_ctx * ctx, Grid & g)
+{
+  gridRelease(ctx, g.pts); gridRelease(ctx, g.w); gridRelease(ctx, g.dsto); gridRelease(ctx, g.phiR);
+  gridRelease(ctx, g.vals); gridRelease(ctx, g.grads); gridRelease(ctx, g.vtCache);
+  g.pts = g.w = g.phiR = g.vals = g.grads = nullptr;
+  g.dsto = nullptr;
+  g.vtCache = nullptr;
+}
+
 namespace {
 
 // Fully normalised associated Legendre function with the Condon-Shortley phase,
@@ -1286,6 +1313,21 @@ int tcscf_ctx_create(int device, tcscf_ctx ** out)
   tcscf_ctx * ctx = new tcscf_ctx();
   ctx->device = device;
   if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) { delete ctx; return TCSCF_ERR_CUDA; }
+  {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    if (cudaMemPoolCreate(&ctx->gridPool, &props) != cudaSuccess) {
+      cudaStreamDestroy(ctx->stream);
+      delete ctx;
+      return TCSCF_ERR_CUDA;
+    }
+    // memory of destroyed grids stays in the pool up to this much (a few Kr-sized grids); the rest
+    // goes back to the device at the next synchronisation
+    uint64_t keep = uint64_t(4) << 30;
+    cudaMemPoolSetAttribute(ctx->gridPool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
   for (auto & e : ctx->ev) cudaEventCreate(&e);
   if (cusolverDnCreate(&ctx->solver) != CUSOLVER_STATUS_SUCCESS) { delete ctx; return TCSCF_ERR_CUDA; }
   cusolverDnSetStream(ctx->solver, ctx->stream);
@@ -1298,10 +1340,9 @@ int tcscf_ctx_destroy(tcscf_ctx * ctx)
   if (!ctx) return TCSCF_OK;
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
-  for (auto & kv : ctx->grids) {
-    Grid & g = kv.second;
-    cudaFree(g.pts); cudaFree(g.w); cudaFree(g.dsto); cudaFree(g.phiR); cudaFree(g.vals); cudaFree(g.grads); cudaFree(g.vtCache);
-  }
+  for (auto & kv : ctx->grids) gridReleaseAll(ctx, kv.second);
+  cudaStreamSynchronize(ctx->stream);
+  if (ctx->gridPool) cudaMemPoolDestroy(ctx->gridPool);
   for (auto & kv : ctx->tensors) cudaFree(kv.second.d);
   for (auto & kv : ctx->scratch) cudaFree(kv.second.p);
   for (auto & e : ctx->ev) cudaEventDestroy(e);
@@ -1364,8 +1405,11 @@ int tcscf_grid_create(tcscf_ctx * ctx, const double * points, const double * wei
   Grid g;
   g.n = n;
   g.ndim = ndim;
-  TCSCF_CUDA(ctx, cudaMalloc(&g.pts, sizeof(double) * 3 * n));
-  TCSCF_CUDA(ctx, cudaMalloc(&g.w, sizeof(double) * n));
+  if (gridAlloc(ctx, &g.pts, sizeof(double) * 3 * n) != TCSCF_OK || gridAlloc(ctx, &g.w, sizeof(double) * n) != TCSCF_OK) {
+    std::string const msg = ctx->err;
+    gridReleaseAll(ctx, g);
+    return fail(ctx, TCSCF_ERR_CUDA, msg);
+  }
   if (ndim == 3) TCSCF_CUDA(ctx, cudaMemcpyAsync(g.pts, points, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, ctx->stream));
   else {
     TCSCF_CUDA(ctx, cudaMemcpyAsync(g.pts, points, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
@@ -1385,8 +1429,7 @@ int tcscf_grid_destroy(tcscf_ctx * ctx, int grid)
   if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
   Grid * g = findGrid(ctx, grid);
   TCSCF_CHECK(ctx, g, TCSCF_ERR_INVALID_ARGUMENT, "unknown grid handle");
-  cudaStreamSynchronize(ctx->stream);
-  cudaFree(g->pts); cudaFree(g->w); cudaFree(g->dsto); cudaFree(g->phiR); cudaFree(g->vals); cudaFree(g->grads); cudaFree(g->vtCache);
+  gridReleaseAll(ctx, *g);
   ctx->grids.erase(grid);
   return TCSCF_OK;
 }
@@ -1400,16 +1443,16 @@ int tcscf_grid_set_basis(tcscf_ctx * ctx, int grid, const tcscf_sto * basis, int
   TCSCF_TRY(validateBasis(ctx, basis, nb, ds));
   TCSCF_CHECK(ctx, !(gradients && basis[0].family == TCSCF_BASIS_HYDROGEN), TCSCF_ERR_UNSUPPORTED,
               "hydrogen-like functions have no gradient (HydrogenLikeBasis.hpp:51-55)");
-  cudaStreamSynchronize(ctx->stream);
-  cudaFree(g->dsto); cudaFree(g->phiR); cudaFree(g->vals); cudaFree(g->grads); cudaFree(g->vtCache);
+  gridRelease(ctx, g->dsto); gridRelease(ctx, g->phiR); gridRelease(ctx, g->vals); gridRelease(ctx, g->grads);
+  gridRelease(ctx, g->vtCache);
   g->dsto = nullptr; g->phiR = g->vals = g->grads = nullptr;
   g->vtCache = nullptr;
   g->vtNB = 0;
   g->nb = 0;
-  TCSCF_CUDA(ctx, cudaMalloc(&g->dsto, sizeof(DevSto) * nb));
-  TCSCF_CUDA(ctx, cudaMalloc(&g->phiR, sizeof(double) * g->n * nb));
-  TCSCF_CUDA(ctx, cudaMalloc(&g->vals, sizeof(double) * g->n * nb * (g->ndim == 3 ? 2 : 1)));
-  if (gradients) TCSCF_CUDA(ctx, cudaMalloc(&g->grads, sizeof(double) * g->n * nb * 6));
+  TCSCF_TRY(gridAlloc(ctx, &g->dsto, sizeof(DevSto) * nb));
+  TCSCF_TRY(gridAlloc(ctx, &g->phiR, sizeof(double) * g->n * nb));
+  TCSCF_TRY(gridAlloc(ctx, &g->vals, sizeof(double) * g->n * nb * (g->ndim == 3 ? 2 : 1)));
+  if (gradients) TCSCF_TRY(gridAlloc(ctx, &g->grads, sizeof(double) * g->n * nb * 6));
   TCSCF_CUDA(ctx, cudaMemcpyAsync(g->dsto, ds.data(), sizeof(DevSto) * nb, cudaMemcpyHostToDevice, ctx->stream));
   kBasis<<<gridBlocks(g->n * nb, 256), 256, 0, ctx->stream>>>(g->n, nb, g->ndim, g->pts, g->dsto, g->phiR, g->vals, g->grads);
   TCSCF_LAUNCH(ctx);
