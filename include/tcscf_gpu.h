@@ -156,7 +156,10 @@ int tcscf_load_sto(const char * directory, const char * basisSet, const char * e
 int tcscf_overlap_core_analytic(const tcscf_sto * basis, int nb, int Z, double * S, double * H);
 
 /* ---- device-resident grids (QMCGrid, integrateAll.hpp:12-142) ------------------------------- */
-/* copies points [ndim][n] and weights [n] from host memory; ndim 2 or 3 */
+/* copies points [ndim][n] and weights [n] from host memory; ndim 2 or 3.  Grid buffers come from a
+ * memory pool owned by the context, in the order of its stream: tcscf_grid_destroy returns them to
+ * the pool after the context's queued work, without a device-wide synchronisation, and the pool keeps
+ * up to 4 GiB of freed grid memory for later grids until the context is destroyed. */
 int tcscf_grid_create(tcscf_ctx * ctx, const double * points, const double * weights, int64_t n, int ndim, int * grid);
 int tcscf_grid_destroy(tcscf_ctx * ctx, int grid);
 /* QMCGrid::setBasisFunctions (integrateAll.hpp:88-137): evaluates the STOs (and gradients) on the
