@@ -290,7 +290,7 @@ def run_ours(args, rank: int, world: int) -> None:
     achieved = flops / (c_ms / 1e3) / 1e12
     if prec == ffi.PREC_FP64:
         roof = {"bound": "fp64", "achieved": achieved, "peak": args.fp64_peak, "unit": "TFLOP/s", "frac": achieved / args.fp64_peak,
-                "traffic": None, "peak_source": "measured FP64 matmul (DESIGN.md)"}
+                "traffic": None, "peak_source": "nominal B200 FP64 dense rate (--fp64-peak or TCSCF_FP64_PEAK_TFLOPS overrides)"}
     elif prec == ffi.PREC_TF32:
         # TF32 dense rate is half the BF16 rate (nominal 1.1 vs 2.25 PFLOP/s): half the measured BF16 burst
         peak = peaks["bf16_tflops"] / 2

@@ -41,7 +41,7 @@ typedef enum tcscf_status {
   TCSCF_ERR_NONFINITE = 4,        /* NaN/Inf in an energy or Fock matrix */
   TCSCF_ERR_NOT_CONVERGED = 5,    /* tcscf::ConvergenceError (HartreeFock.hpp:13-19) */
   TCSCF_ERR_LINALG = 6,           /* LvArray::dense::Error (eigen-solve failure) */
-  TCSCF_ERR_UNSUPPORTED = 7,      /* shape or feature outside what this build implements */
+  TCSCF_ERR_UNSUPPORTED = 7,      /* shape or feature outside what this library implements */
   TCSCF_ERR_NO_DEVICE = 8
 } tcscf_status;
 

@@ -2,8 +2,8 @@
 
 ctypes bindings of the CPU restatement in oracle/tcscf_oracle.cpp (built into
 oracle/_build/liboracle.so by oracle/Makefile).  Only tests/, __graft_entry__.smoke() and bench.py's
-cpu_baseline / reference arm may import this package, and only as the checker or the timed CPU
-baseline; the product library never touches it.
+cpu_baseline / reference arm may import this package, and only as the parity reference or the timed
+CPU baseline; the product library never touches it.
 """
 from __future__ import annotations
 

@@ -1,7 +1,7 @@
 // ORACLE — TEST INFRASTRUCTURE ONLY.
 //
 // A CPU restatement (C++17 + OpenMP, FP64) of corbett5/tcscf's grid-quadrature Fock build, used
-// only as the checker by tests/, __graft_entry__.smoke() and the cpu_baseline / reference arm of
+// only as the parity reference by tests/, __graft_entry__.smoke() and the cpu_baseline / reference arm of
 // bench.py.  It is never linked into, loaded by or called from the product library
 // (tcscf_b200/libtcscf_gpu.so).  Every routine cites the reference file:line it follows; loop
 // orders are the reference's except where noted (a transposed basis table is used for the r2

@@ -221,7 +221,7 @@ size_t tf32OperandBytes(int NB, int64_t n1pad, int64_t n2pad);
 int tf32PackOperands(tcscf_ctx * ctx, Contraction const & c, int NB, int64_t n1pad, int64_t n2pad, void * dst, CUtensorMap * maps);
 int launchTf32(tcscf_ctx * ctx, int NB, tc::Params const & P, int grid);
 
-// cuTensorMapEncodeTiled from the driver (null when unavailable)
+// cuTensorMapEncodeTiled from the CUDA driver API (null when unavailable)
 using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *, const cuuint64_t *,
                                    const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
                                    CUtensorMapL2promotion, CUtensorMapFloatOOBfill);

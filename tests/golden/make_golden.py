@@ -1,5 +1,5 @@
 """Generates tests/golden/*.json from the reference sources (run in a container where the reference
-checkout is mounted; the GPU box never needs it).
+checkout is mounted; GPU test runs only read the committed fixtures).
 
   python tests/golden/make_golden.py /path/to/tcscf
 
