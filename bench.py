@@ -215,6 +215,8 @@ def run_ours(args, rank: int, world: int) -> None:
     peaks, peak_kind = load_peaks()
 
     ctx = api.Context(local)
+    if args.autotune:
+        ctx.set_autotune(True)
     G = api.QMCGrid(ctx, g)
     G.setBasisFunctions(w.basis)
     stream = torch.cuda.ExternalStream(ctx.stream(), device=dev)
@@ -328,7 +330,9 @@ def run_ours(args, rank: int, world: int) -> None:
                                      "tf32": "tf32 operands (10-bit mantissa, round to nearest), fp32 accumulation per 64-point "
                                              "block, double-float across blocks"}[args.precision],
                        "l2": "flushed (256 MB write) between timed steps",
-                       "density": "core-Hamiltonian guess (canonical orthogonalisation)"},
+                       "density": "core-Hamiltonian guess (canonical orthogonalisation)",
+                       "schedule": "autotuned r2 split (tuned in the warm-up: shapes, batches, measurements = %s)" % (ctx.autotune_stats(),)
+                       if args.autotune else "fixed rule"},
             "energy": E, "contraction_ms": c_ms, "gpu_launches": launches, "roofline": roof, "fp64": fp64,
             "speedup_vs_fp64": (fp64["s_per_iter"] / s_per_iter) if fp64 else None,
             "e2e": e2e, "cpu_baseline": cpu, "clocks": clk.summary()}
@@ -349,6 +353,8 @@ def run_batch(args, rank: int) -> None:
         return
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
     ctx = api.Context(int(os.environ.get("LOCAL_RANK", 0)))
+    if args.autotune:
+        ctx.set_autotune(True)
     inst = wl.batch()
     Gs, Ds, hs, npts = [], [], [], []
     for w in inst:
@@ -391,7 +397,8 @@ def run_batch(args, rank: int) -> None:
                        "public batched call, inputs resident on the device except the densities"},
             "one_at_a_time_s": t1, "batch_speedup": t1 / tb, "batched_equals_one_at_a_time": bool(np.array_equal(Eb, E1)),
             "dE_vs_fp64_max": float(err.max()), "dE_vs_fp64_median": float(np.median(err)),
-            "dE_rel_vs_fp64_max": float((err / np.abs(E64)).max()), "clocks": clk.summary()}
+            "dE_rel_vs_fp64_max": float((err / np.abs(E64)).max()), "clocks": clk.summary(),
+            "schedule": {"autotune": bool(args.autotune), "tuned_shapes_batches_measurements": ctx.autotune_stats()}}
     print(json.dumps(line), flush=True)
 
 
@@ -470,6 +477,8 @@ def main() -> None:
     ap.add_argument("--skip-fp64", action="store_true")
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--autotune", action="store_true",
+                    help="measure the tensor launch's r2 split per build shape / batch on first use (inside the warm-up)")
     args = ap.parse_args()
 
     from tcscf_b200 import replicas

@@ -228,6 +228,23 @@ int tcscf_fock_build_precomputed(tcscf_ctx * ctx, int r1, int fji, int nspin, co
  * over the SCF iterations of one set of instances.  Returns the numbers of captures and replays. */
 int tcscf_batch_graph_stats(tcscf_ctx * ctx, int * captures, int * replays);
 
+/* Autotuner of the tensor-core Fock build's schedule (no reference counterpart; off by default).
+ * With it on, the first split-BF16 / TF32 direct build of each shape (r1 and r2 points, padded basis
+ * size, padded density rank, precision) times every candidate r2 split of its persistent launch with
+ * CUDA events on the context stream and keeps the fastest for later builds of that shape; the first
+ * tcscf_fock_build_batch of each batch signature (precision, every instance's grid sizes and basis
+ * size) times the split policies {default rule, no split, 2x, 4x} over the whole batch and keeps the
+ * fastest.  The tile class (NB, RP, X precision) stays the fixed rule: it sets the accuracy.  Results
+ * of different splits differ only in the order of the r2 block sums.  Turning it off returns to the
+ * default rule and keeps the measurements. */
+int tcscf_set_autotune(tcscf_ctx * ctx, int enable);
+/* shapes and batch signatures tuned on this context so far, and candidate measurements taken */
+int tcscf_autotune_stats(tcscf_ctx * ctx, int * shapes, int * batches, int * measurements);
+/* host only: the candidate r2 split counts for a launch over n1 x n2 points on a device with sms SMs,
+ * the default rule's first, then 1, 2, 3, 4, 6, 8 while every split keeps at least 16 r2 blocks of 64
+ * points (effective counts, no repeats); writes at most capacity of them and their number to count */
+int tcscf_autotune_split_candidates(int64_t n1, int64_t n2, int sms, int * splits, int capacity, int * count);
+
 /* ---- SCF drivers (RCSHartreeFock/UOSHartreeFock::compute, HartreeFock.cpp:785-1003) ---------- */
 /* Options of tcscf_scf on this context (no reference counterpart; the defaults, 0 and 0, reproduce
  * the reference's plain Roothaan iteration with the complex eigen-solver).  diis in 2..16: the

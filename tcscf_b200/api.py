@@ -79,6 +79,17 @@ class Context:
         _raise(ffi.lib().tcscf_batch_graph_stats(self._h, C.byref(a), C.byref(b)), self._h)
         return a.value, b.value
 
+    def set_autotune(self, enable: bool = True) -> None:
+        """Measure the tensor-path launch schedule (r2 split) per build shape and batch signature on
+        first use and keep the fastest (off by default)."""
+        _raise(ffi.lib().tcscf_set_autotune(self._h, int(bool(enable))), self._h)
+
+    def autotune_stats(self) -> tuple[int, int, int]:
+        """(shapes tuned, batch signatures tuned, candidate measurements) on this context."""
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        _raise(ffi.lib().tcscf_autotune_stats(self._h, C.byref(a), C.byref(b), C.byref(c)), self._h)
+        return a.value, b.value, c.value
+
     def last_timing(self) -> tuple[float, float, int]:
         a, b, n = C.c_double(), C.c_double(), C.c_int()
         _raise(ffi.lib().tcscf_last_timing(self._h, C.byref(a), C.byref(b), C.byref(n)), self._h)

@@ -83,6 +83,16 @@ struct tcscf_ctx {
   std::vector<uint64_t> tensorGraphKey;
   int graphCaptures = 0, graphReplays = 0;
   int realEigen = 0;  // tcscf_scf solves a Fock matrix that is real in the real-harmonic basis there
+  // autotuner (tcscf_set_autotune): the measured r2 split count of the tensor-path launch per shape
+  // {n1, n2, padded nb, padded rank, precision}, the split policy per batch signature, the policy
+  // the batch build applies (1: the default rule, 0: no split, k > 1: k x the default split),
+  // candidate measurements taken, and the two events that time them
+  int autotune = 0;
+  std::map<std::vector<int64_t>, int> tunedSplit;
+  std::map<std::vector<int64_t>, int> tunedBatchPolicy;
+  int batchSplitPolicy = 1;
+  int tuneMeasurements = 0;
+  cudaEvent_t tuneEv[2] = {nullptr, nullptr};
   std::map<std::string, tcscf::Scratch> scratch;
   // device buffers of the most recent direct Fock build (for tcscf_last_potentials)
   const double * lastVH = nullptr;

@@ -771,6 +771,18 @@ int smCount()
   return sms;
 }
 
+int defaultSplit(int nTiles, int nBlocks, int sms) { return std::max(1, std::min(sms / std::max(1, nTiles), nBlocks / 4)); }
+
+// a requested split count after rounding the r2 blocks per split up (what the launch really runs)
+int effectiveSplit(int nBlocks, int want)
+{
+  int const per = (nBlocks + want - 1) / want;
+  return (nBlocks + per - 1) / per;
+}
+
+// the autotuner's largest split: every split keeps at least 16 blocks of 64 r2 points
+int maxTunedSplit(int nBlocks) { return std::max(1, nBlocks / 16); }
+
 struct Shape {
   int NB, RP, XS;
   int64_t n1pad, n2pad;
@@ -791,8 +803,9 @@ Shape shapeOf(Contraction const & c, int sms, int precision)
   sh.n2pad = (c.n2 + tc::BK - 1) / tc::BK * tc::BK;
   sh.nTiles = int(sh.n1pad / tc::BM);
   sh.nBlocks = int(sh.n2pad / tc::BK);
-  // split r2 when there are fewer tiles than SMs (partials summed deterministically afterwards)
-  sh.nSplit = std::max(1, std::min(sms / std::max(1, sh.nTiles), sh.nBlocks / 4));
+  // split r2 when there are fewer tiles than SMs (partials summed deterministically afterwards), or
+  // as the caller (the autotuner) asks
+  sh.nSplit = c.nSplit > 0 ? std::min(c.nSplit, sh.nBlocks) : defaultSplit(sh.nTiles, sh.nBlocks, sms);
   sh.perSplit = (sh.nBlocks + sh.nSplit - 1) / sh.nSplit;
   sh.nSplit = (sh.nBlocks + sh.perSplit - 1) / sh.perSplit;
   return sh;
@@ -801,6 +814,27 @@ Shape shapeOf(Contraction const & c, int sms, int precision)
 size_t align256(size_t n) { return (n + 255) & ~size_t(255); }
 
 }  // namespace
+
+std::vector<int> splitCandidates(int64_t n1, int64_t n2, int sms)
+{
+  int const nTiles = int((n1 + tc::BM - 1) / tc::BM);
+  int const nBlocks = int((n2 + tc::BK - 1) / tc::BK);
+  std::vector<int> out{effectiveSplit(nBlocks, defaultSplit(nTiles, nBlocks, sms))};
+  for (int s : {1, 2, 3, 4, 6, 8}) {
+    if (s > maxTunedSplit(nBlocks)) break;
+    int const e = effectiveSplit(nBlocks, s);
+    if (std::find(out.begin(), out.end(), e) == out.end()) out.push_back(e);
+  }
+  return out;
+}
+
+int splitForPolicy(Contraction const & c, int precision, int policy)
+{
+  if (policy == 1) return 0;
+  if (policy <= 0) return 1;
+  Shape const sh = shapeOf(c, smCount(), precision);
+  return std::max(1, std::min(sh.nSplit * policy, std::max(sh.nSplit, maxTunedSplit(sh.nBlocks))));
+}
 
 size_t tensorArenaBytes(Contraction const & c, int precision)
 {
@@ -1010,7 +1044,7 @@ __global__ void kAddTChunk(int64_t n1, int ncol, int ld, const double * A, doubl
   }
 }
 
-int contractTensorOnce(tcscf_ctx * ctx, Contraction const & c, int precision, bool recordStart)
+int runTensorOnce(tcscf_ctx * ctx, Contraction const & c, int precision, bool recordStart)
 {
   std::string why;
   if (!tensorPathAvailable(c, precision, &why)) return fail(ctx, TCSCF_ERR_UNSUPPORTED, why);
@@ -1021,6 +1055,51 @@ int contractTensorOnce(tcscf_ctx * ctx, Contraction const & c, int precision, bo
   TCSCF_TRY(tensorPrepare(ctx, c, precision, p, bytes, tp));
   TensorPrep * one = &tp;
   return tensorRun(ctx, &one, 1, recordStart);
+}
+
+// Times every candidate split of this contraction (operand packing, the persistent launch and the
+// split sums, between two events on the context stream; the first candidate, the default rule, runs
+// once untimed before) and returns the fastest.  Each run writes the contraction's outputs in full,
+// so the caller's final run leaves them as an untuned build would, up to the order of the r2 sums.
+int tuneSplit(tcscf_ctx * ctx, Contraction const & c, int precision, int * best)
+{
+  std::vector<int> const cand = splitCandidates(c.n1, c.n2, smCount());
+  *best = cand[0];
+  if (cand.size() == 1) return TCSCF_OK;
+  for (auto & e : ctx->tuneEv)
+    if (!e) TCSCF_CUDA(ctx, cudaEventCreate(&e));
+  float bestMs = 0;
+  for (size_t i = 0; i < cand.size(); ++i) {
+    Contraction ck = c;
+    ck.nSplit = cand[i];
+    if (i == 0) TCSCF_TRY(runTensorOnce(ctx, ck, precision, false));
+    TCSCF_CUDA(ctx, cudaEventRecord(ctx->tuneEv[0], ctx->stream));
+    TCSCF_TRY(runTensorOnce(ctx, ck, precision, false));
+    TCSCF_CUDA(ctx, cudaEventRecord(ctx->tuneEv[1], ctx->stream));
+    TCSCF_CUDA(ctx, cudaEventSynchronize(ctx->tuneEv[1]));
+    float ms = 0;
+    TCSCF_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->tuneEv[0], ctx->tuneEv[1]));
+    ++ctx->tuneMeasurements;
+    if (i == 0 || ms < bestMs) { bestMs = ms; *best = cand[i]; }
+  }
+  return TCSCF_OK;
+}
+
+int contractTensorOnce(tcscf_ctx * ctx, Contraction const & c, int precision, bool recordStart)
+{
+  if (!ctx->autotune || c.nSplit > 0) return runTensorOnce(ctx, c, precision, recordStart);
+  std::string why;
+  if (!tensorPathAvailable(c, precision, &why)) return fail(ctx, TCSCF_ERR_UNSUPPORTED, why);
+  std::vector<int64_t> const key{c.n1, c.n2, c.ncol <= 64 ? 64 : 128, c.R <= 32 ? 32 : 64, precision};
+  auto it = ctx->tunedSplit.find(key);
+  if (it == ctx->tunedSplit.end()) {
+    int best = 0;
+    TCSCF_TRY(tuneSplit(ctx, c, precision, &best));
+    it = ctx->tunedSplit.emplace(key, best).first;
+  }
+  Contraction ck = c;
+  ck.nSplit = it->second;
+  return runTensorOnce(ctx, ck, precision, recordStart);
 }
 
 }  // namespace

@@ -29,6 +29,7 @@ struct Contraction {
   int kernel = TCSCF_K_INV_R12;    // r12 kernel g (vector kernels use `component`)
   int component = 0;
   const tcscf_ochi * jastrow = nullptr;
+  int nSplit = 0;                  // r2 split count of the tensor-path launch (0: the default rule)
 };
 
 int contractFp64(tcscf_ctx * ctx, Contraction const & c);
@@ -39,6 +40,13 @@ int blasHandle(tcscf_ctx * ctx, cublasHandle_t * out);
 // tensor-core (tcgen05) contraction of the same quantity for g = 1/r12: split-BF16 (flash_tc.cu) or
 // TF32 (flash_tf32.cu)
 int contractTensor(tcscf_ctx * ctx, Contraction const & c, int precision);
+// r2 split counts the autotuner measures for a tensor-path launch over n1 x n2 points on sms SMs:
+// the default rule's count first, then 1, 2, 3, 4, 6 and 8 where every split keeps at least 16
+// r2 blocks of 64 points (effective counts after rounding the blocks per split, no repeats)
+std::vector<int> splitCandidates(int64_t n1, int64_t n2, int sms);
+// the split count a batch instance gets under a batch split policy (1: the default rule, 0: no
+// split, k > 1: k x the default count, at most the candidates' limit)
+int splitForPolicy(Contraction const & c, int precision, int policy);
 // one launch of the tensor path (contractTensor splits a larger density factor rank into chunks of
 // tensorRankLimit columns)
 bool tensorPathAvailable(Contraction const & c, int precision, std::string * why);

@@ -1154,6 +1154,7 @@ int fockBuildBatch(tcscf_ctx * ctx, int count, Grid * const * g1s, Grid * const 
     Contraction & c = cs[k];
     c.n1 = g1.n; c.n2 = g2.n; c.R = std::min(nb, 32); c.ncol = nb; c.ldpsi = nb; c.ldt = nb;
     c.p1 = g1.pts; c.p2 = g2.pts;
+    c.nSplit = splitForPolicy(c, precision, ctx->batchSplitPolicy);
     arenaBytes[k] = tensorArenaBytes(c, precision);
     size_t const own = (sizeof(double) * (size_t(g1.n) * nb + g1.n + size_t(nb) * nb) + 255) & ~size_t(255);
     offs[k + 1] = offs[k] + own + ((arenaBytes[k] + 255) & ~size_t(255));
@@ -1346,6 +1347,8 @@ int tcscf_ctx_destroy(tcscf_ctx * ctx)
   for (auto & kv : ctx->tensors) cudaFree(kv.second.d);
   for (auto & kv : ctx->scratch) cudaFree(kv.second.p);
   for (auto & e : ctx->ev) cudaEventDestroy(e);
+  for (auto & e : ctx->tuneEv)
+    if (e) cudaEventDestroy(e);
   if (ctx->tensorGraph) cudaGraphExecDestroy(ctx->tensorGraph);
   if (ctx->solver) cusolverDnDestroy(ctx->solver);
   if (ctx->blas) cublasDestroy(ctx->blas);
@@ -1361,6 +1364,33 @@ int tcscf_batch_graph_stats(tcscf_ctx * ctx, int * captures, int * replays)
   if (!ctx || !captures || !replays) return TCSCF_ERR_INVALID_ARGUMENT;
   *captures = ctx->graphCaptures;
   *replays = ctx->graphReplays;
+  return TCSCF_OK;
+}
+
+int tcscf_set_autotune(tcscf_ctx * ctx, int enable)
+{
+  if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
+  ctx->autotune = enable ? 1 : 0;
+  return TCSCF_OK;
+}
+
+int tcscf_autotune_stats(tcscf_ctx * ctx, int * shapes, int * batches, int * measurements)
+{
+  if (!ctx || !shapes || !batches || !measurements) return TCSCF_ERR_INVALID_ARGUMENT;
+  *shapes = int(ctx->tunedSplit.size());
+  *batches = int(ctx->tunedBatchPolicy.size());
+  *measurements = ctx->tuneMeasurements;
+  return TCSCF_OK;
+}
+
+int tcscf_autotune_split_candidates(int64_t n1, int64_t n2, int sms, int * splits, int capacity, int * count)
+{
+  if (n1 <= 0 || n2 <= 0 || sms <= 0 || !count || capacity < 0 || (capacity > 0 && !splits)) return TCSCF_ERR_INVALID_ARGUMENT;
+  if (n1 > (int64_t(1) << 36) || n2 > (int64_t(1) << 36)) return TCSCF_ERR_INVALID_ARGUMENT;  // tile and block counts stay int
+  std::vector<int> const c = splitCandidates(n1, n2, sms);
+  int const n = std::min<int>(capacity, int(c.size()));
+  for (int i = 0; i < n; ++i) splits[i] = c[i];
+  *count = n;
   return TCSCF_OK;
 }
 
@@ -1762,7 +1792,37 @@ int tcscf_fock_build_batch(tcscf_ctx * ctx, int count, const int * r1, const int
     TCSCF_CUDA(ctx, cudaMemcpyAsync(d, density[k], sizeof(double2) * nn, cudaMemcpyHostToDevice, ctx->stream));
     TCSCF_CUDA(ctx, cudaMemcpyAsync(hh, h[k], sizeof(double) * nn, cudaMemcpyHostToDevice, ctx->stream));
   }
-  TCSCF_TRY(fockBuildBatch(ctx, count, g1s.data(), g2s.data(), dD.data(), dH.data(), respect_symmetry, precision, dG.data(), dF.data(), dE.data()));
+  auto build = [&]() {
+    return fockBuildBatch(ctx, count, g1s.data(), g2s.data(), dD.data(), dH.data(), respect_symmetry, precision, dG.data(), dF.data(), dE.data());
+  };
+  if (ctx->autotune && (precision == TCSCF_PREC_BF16X3 || precision == TCSCF_PREC_TF32)) {
+    // batch signature: precision and every instance's grid sizes and basis size
+    std::vector<int64_t> key{precision, count};
+    for (int k = 0; k < count; ++k) key.insert(key.end(), {g1s[k]->n, g2s[k]->n, int64_t(g1s[k]->nb)});
+    auto it = ctx->tunedBatchPolicy.find(key);
+    if (it == ctx->tunedBatchPolicy.end()) {
+      // each policy's whole batch build runs twice and the second (its graph replayed, scratch
+      // grown) is timed between the build's own events; the inputs are read-only, so every run
+      // writes the same outputs up to the order of the r2 sums
+      int best = 1;
+      double bestMs = 0;
+      bool first = true;
+      for (int policy : {1, 0, 2, 4}) {
+        ctx->batchSplitPolicy = policy;
+        int st = build();
+        if (st == TCSCF_OK) st = build();
+        if (st != TCSCF_OK) { ctx->batchSplitPolicy = 1; return st; }
+        ++ctx->tuneMeasurements;
+        if (first || ctx->lastTotalMs < bestMs) { bestMs = ctx->lastTotalMs; best = policy; }
+        first = false;
+      }
+      it = ctx->tunedBatchPolicy.emplace(key, best).first;
+    }
+    ctx->batchSplitPolicy = it->second;
+  }
+  int const bst = build();
+  ctx->batchSplitPolicy = 1;
+  TCSCF_TRY(bst);
   TCSCF_CUDA(ctx, cudaMemcpyAsync(energy, energies, sizeof(double) * count, cudaMemcpyDeviceToHost, ctx->stream));
   for (int k = 0; k < count; ++k)
     if (fock && fock[k])

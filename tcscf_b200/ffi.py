@@ -70,6 +70,9 @@ SIGNATURES: dict[str, tuple] = {
     "tcscf_fock_build_batch": (_I, [_P, _I, C.POINTER(_I), C.POINTER(_I), C.POINTER(_D), C.POINTER(_D), _I, _I, _D, C.POINTER(_D)]),
     "tcscf_tc_fock_build": (_I, [_P, _I, _I, _I, _I, _I, _I, _I, _D, _D, _D, _D, _I, _D, _D, _D, _D]),
     "tcscf_batch_graph_stats": (_I, [_P, C.POINTER(_I), C.POINTER(_I)]),
+    "tcscf_set_autotune": (_I, [_P, _I]),
+    "tcscf_autotune_stats": (_I, [_P, C.POINTER(_I), C.POINTER(_I), C.POINTER(_I)]),
+    "tcscf_autotune_split_candidates": (_I, [C.c_int64, C.c_int64, _I, C.POINTER(_I), _I, C.POINTER(_I)]),
     "tcscf_tc_compute_q": (_I, [_P, _I, _I, _I, _D, _D, _D]),
     "tcscf_tc_assemble_g": (_I, [_P, _I, _D, _D, _D, _D, _D]),
     "tcscf_tc_scf": (_I, [_P, _I, _I, _I, _I, _I, _D, _D, _I, _I, _I, C.c_double, _I, _D, C.POINTER(_I), _D, _D]),
@@ -138,3 +141,12 @@ def ochi_struct(a: float, a12: float, terms) -> Ochi:
             o.S[t][d] = int(S[d])
         o.c[t][0], o.c[t][1] = float(c_oppo), float(c_same)
     return o
+
+
+def autotune_split_candidates(n1: int, n2: int, sms: int = 148) -> list[int]:
+    """Candidate r2 split counts of a tensor-path launch over n1 x n2 points (host only, no device)."""
+    buf = (C.c_int * 16)()
+    n = C.c_int()
+    check(lib().tcscf_autotune_split_candidates(int(n1), int(n2), int(sms), buf, 16, C.byref(n)))
+    return list(buf[: n.value])
+
