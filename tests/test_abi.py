@@ -53,3 +53,32 @@ def test_context_needs_a_device():
     h = C.c_void_p()
     assert ffi.lib().tcscf_ctx_create(0, C.byref(h)) == ffi.ERR_NO_DEVICE
     assert ffi.lib().tcscf_ctx_destroy(None) == ffi.OK
+
+
+def _context_entry_points():
+    """Names of the declared functions whose first parameter is the context."""
+    out = []
+    for h in sorted((ROOT / "include").glob("*.h")):
+        text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
+        out += re.findall(r"^\s*(?:const\s+)?\w+\s*\*?\s*(tcscf_\w+)\s*\(\s*tcscf_ctx\s*\*\s*\w+\s*[,)]", text, flags=re.M)
+    return sorted(set(out))
+
+
+def test_every_context_entry_point_rejects_a_null_context():
+    # the reference aborts on bad arguments (LVARRAY_ERROR_IF_*); the C ABI returns a status
+    # instead, and a null context is refused before any device call, so this runs without a GPU
+    lib = ffi.lib()
+    names = _context_entry_points()
+    assert len(names) >= 30
+    assert set(names) <= set(ffi.SIGNATURES), set(names) - set(ffi.SIGNATURES)
+    for n in names:
+        res, argtypes = ffi.SIGNATURES[n]
+        args = [None] + [0.0 if t is C.c_double else (0 if t in (C.c_int, C.c_int32, C.c_int64, C.c_uint64) else None)
+                         for t in argtypes[1:]]
+        r = getattr(lib, n)(*args)
+        if n == "tcscf_ctx_destroy":
+            assert r == ffi.OK
+        elif n == "tcscf_last_error":
+            assert r == b"null context"
+        else:
+            assert r == ffi.ERR_INVALID_ARGUMENT, n
