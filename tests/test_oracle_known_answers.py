@@ -287,3 +287,26 @@ def test_hydrogen_exchange_integral():
     out = _r12_hydrogen([(1, 1, 0, 0, 2), (1, 2, 1, 0, 2)])
     assert abs(out[0, 1, 1, 0].real - 112 / 6561) < 1e-3
     assert abs(out[0, 1, 1, 0].imag) < 1e-12
+
+
+def test_rcs_fock_build_hydrogen_closed_form():
+    """The RCS Fock build (precomputeIntegrand + computeF, then calculateIaa / calculateFai and the
+    2J - K assembly, HartreeFock.cpp:144-213, 822-850) for one doubly occupied hydrogen 1s (Z = 1) in
+    the basis {1s, 2p0}: G(1s,1s) = 2J - K = J(1s,1s) = 5/8, G(2p0,2p0) = 2 F0(1s,2p) - G1(1s,2p)/3
+    = 2 * 59/243 - 112/6561, G(1s,2p0) = 0 by parity, and the two-electron energy is J(1s,1s) = 5/8
+    (h = 0).  r1: 60 radial x Lebedev 23, r2: 71 radial x Lebedev 29 (3-D, complex F); the symmetry
+    mask is off because h = 0 would zero every element."""
+    basis = [(1, 1, 0, 0, 2), (1, 2, 1, 0, 2)]
+    r1, w1r = oracle.radial_grid(60, ffi.MAP_ONE_PLUS_X)
+    p1, w1 = oracle.product_grid(r1, w1r, grids.lebedev_table(23))
+    r2, w2r = oracle.radial_grid(71, ffi.MAP_ONE_PLUS_X)
+    p2, w2 = oracle.product_grid(r2, w2r, grids.lebedev_table(29))
+    v1 = oracle.basis_values(p1, basis)
+    F = oracle.compute_F(p1, p2, w2, oracle.basis_values(p2, basis), 2)
+    D = np.zeros((1, 2, 2), dtype=np.complex128)
+    D[0, 0, 0] = 1.0
+    G, _, E = oracle.fock_build(F, v1, w1, D, np.zeros((2, 2)), respect_symmetry=False)
+    assert abs(G[0, 0, 0] - 5 / 8) < 1e-3
+    assert abs(G[0, 1, 1] - (2 * 59 / 243 - 112 / 6561)) < 1e-3
+    assert abs(G[0, 0, 1]) < 1e-6 and abs(G[0, 1, 0]) < 1e-6
+    assert abs(E - 5 / 8) < 1e-3
