@@ -329,3 +329,22 @@ def test_rcs_scf_helium_reaches_the_hartree_fock_limit():
     st, E, it, _, _ = oracle.scf(1, 1, 1, F, v1, w1, S, h, tol=1e-10, max_iter=100)
     assert st == 0 and it < 100
     assert abs(E - KA["he_literature"]["hf"]) < 1e-3, E
+
+
+def test_uos_scf_lithium_reaches_the_hartree_fock_limit():
+    """The oracle's UOS SCF (HartreeFock.cpp:890-1003: per-spin Coulomb from both spins, exchange
+    from its own) for Li (1s^2 2s, two spin-up electrons and one spin-down) in eight even-tempered 1s
+    STOs (zeta = 0.3 x 1.9^k) reaches the numerical Hartree-Fock limit of the lithium atom, -7.4327 Eh,
+    within 1e-3 Eh: measured -7.431958 on r1 = 80 radial x Lebedev 29 and r2 = 91 radial x Lebedev
+    35 (-7.432329 with ten functions)."""
+    basis = [(0.3 * 1.9 ** k, 1, 0, 0) for k in range(8)]
+    r1, w1r = oracle.radial_grid(80, ffi.MAP_ONE_PLUS_X)
+    p1, w1 = oracle.product_grid(r1, w1r, grids.lebedev_table(29))
+    r2, w2r = oracle.radial_grid(91, ffi.MAP_ONE_PLUS_X)
+    p2, w2 = oracle.product_grid(r2, w2r, grids.lebedev_table(35))
+    v1 = oracle.basis_values(p1, basis)
+    F = oracle.compute_F(p1, p2, w2, oracle.basis_values(p2, basis), len(basis))
+    S, h = oracle.overlap_core(basis, 3)
+    st, E, it, _, _ = oracle.scf(2, 2, 1, F, v1, w1, S, h, tol=1e-10, max_iter=200)
+    assert st == 0
+    assert abs(E - (-7.4327)) < 1e-3, E
