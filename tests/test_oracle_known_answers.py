@@ -348,3 +348,36 @@ def test_uos_scf_lithium_reaches_the_hartree_fock_limit():
     st, E, it, _, _ = oracle.scf(2, 2, 1, F, v1, w1, S, h, tol=1e-10, max_iter=200)
     assert st == 0
     assert abs(E - (-7.4327)) < 1e-3, E
+
+
+def test_tc_scf_with_zero_jastrow_is_hartree_fock():
+    """With every Jastrow coefficient zero the transcorrelated SCF (TCHartreeFock, HartreeFock.cpp:
+    1007-1362: G2 from the TC scalar kernel 2/r12, G3 and the vector term from grad u = 0, zggev with
+    the sort by real part and the S-metric MGS) is Hartree-Fock: He in six 1s STOs gives the UOS and
+    RCS energies on the same grids to 1e-9 Eh.  The r1 grid is rotated so that no point lies on the
+    z axis, where the reference's STO gradient formula divides by sin(theta)."""
+    from scipy.spatial.transform import Rotation
+
+    basis = [(0.9 * 1.8 ** k, 1, 0, 0) for k in range(6)]
+    nb = len(basis)
+    r1, w1r = oracle.radial_grid(40, ffi.MAP_ONE_PLUS_X)
+    p1, w1 = oracle.product_grid(r1, w1r, grids.lebedev_table(17))
+    p1 = np.ascontiguousarray(Rotation.from_euler("zyx", [0.3, 0.2, 0.1]).as_matrix() @ p1)
+    r2, w2r = oracle.radial_grid(47, ffi.MAP_ONE_PLUS_X)
+    p2, w2 = oracle.product_grid(r2, w2r, grids.lebedev_table(23))
+    v1, g1 = oracle.basis_values(p1, basis, gradients=True)
+    v2 = oracle.basis_values(p2, basis)
+    S, h = oracle.overlap_core(basis, 2)
+    F = oracle.compute_F(p1, p2, w2, v2, nb)
+    st_u, E_uos, _, _, _ = oracle.scf(2, 1, 1, F, v1, w1, S, h, tol=1e-11, max_iter=100)
+    st_r, E_rcs, _, _, _ = oracle.scf(1, 1, 1, F, v1, w1, S, h, tol=1e-11, max_iter=100)
+    u0 = oracle.ochi(1.0, 1.0, [((1, 0, 0), 0.0, 0.0)])
+    Fs = oracle.compute_F(p1, p2, w2, v2, nb, ffi.K_TC_SCALAR_SAME, u0)
+    Fo = oracle.compute_F(p1, p2, w2, v2, nb, ffi.K_TC_SCALAR_OPPO, u0)
+    Vs = oracle.compute_V(p1, p2, w2, v2, nb, ffi.K_GRAD_U_SAME, u0)
+    Vo = oracle.compute_V(p1, p2, w2, v2, nb, ffi.K_GRAD_U_OPPO, u0)
+    np.testing.assert_allclose(Fs, 2 * F, rtol=1e-14, atol=0)
+    assert np.abs(Vs).max() == 0 and np.abs(Vo).max() == 0
+    st_t, E_tc, _, _, _ = oracle.tc_scf(Fs, Fo, Vs, Vo, v1, g1, w1, S, h, 1, 1, tol=1e-11, max_iter=200)
+    assert (st_u, st_r, st_t) == (0, 0, 0)
+    assert abs(E_uos - E_rcs) < 1e-9 and abs(E_tc - E_uos) < 1e-9, (E_rcs, E_uos, E_tc)
