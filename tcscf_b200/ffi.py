@@ -106,7 +106,8 @@ def lib() -> C.CDLL:
 def dptr(a: np.ndarray | None):
     if a is None:
         return None
-    assert a.dtype in (np.float64, np.complex128) and a.flags.c_contiguous, (a.dtype, a.flags)
+    if a.dtype not in (np.float64, np.complex128) or not a.flags.c_contiguous:
+        raise TypeError(f"expected a C-contiguous float64 or complex128 array, got {a.dtype} (contiguous={a.flags.c_contiguous})")
     return a.ctypes.data_as(_D)
 
 
