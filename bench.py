@@ -182,6 +182,48 @@ def run_reference(args, rank: int) -> None:
     print(json.dumps(line), flush=True)
 
 
+def roofline(prec: int, n: int, nb: int, nocc: int, c_ms: float, peaks: dict, peak_kind: str, fp64_peak: float, traffic) -> dict:
+    """The line's roofline object for one Fock build of n points (r1 = r2 grid) whose contraction
+    kernel took c_ms milliseconds."""
+    from tcscf_b200 import ffi
+
+    # algorithmic work per Fock build: F_alg = 2 N^2 (nb nocc + 1), the pair-density count of the direct
+    # build (nb nocc exchange pair densities and the Coulomb density per (r1, r2) pair); this kernel
+    # contracts the same sum in factored form, 2 N^2 (nocc + nb + 1) flops (rho GEMM, exchange GEMM,
+    # Coulomb), reported beside it as kernel_algorithm_tflops
+    flops = 2.0 * n * n * (nb * nocc + 1)
+    kernel_flops = 2.0 * n * n * (nocc + nb + 1)
+    achieved = flops / (c_ms / 1e3) / 1e12
+    kernel_achieved = kernel_flops / (c_ms / 1e3) / 1e12
+    numerator = {"achieved_numerator": "F_alg = 2 N^2 (nb nocc + 1) flops per build (pair-density count)",
+                 "kernel_algorithm_tflops": kernel_achieved}
+    if prec == ffi.PREC_FP64:
+        roof = {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved / fp64_peak,
+                "traffic": None, "peak_source": "nominal B200 FP64 dense rate (--fp64-peak or TCSCF_FP64_PEAK_TFLOPS overrides)",
+                **numerator}
+    elif prec == ffi.PREC_TF32:
+        # TF32 dense rate is half the BF16 rate (nominal 1.1 vs 2.25 PFLOP/s): half the measured BF16 burst
+        peak = peaks["bf16_tflops"] / 2
+        RP = 32                            # TF32 launches hold rank 32 (larger ranks run in chunks)
+        NB = 64 if nb <= 64 else 128
+        chunks = -(-nocc // RP)
+        issued = n * n * chunks * (2.0 * RP + 2.0 * NB) / (c_ms / 1e3) / 1e12
+        roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "traffic": None, "peak_source": f"tf32 dense = half the bf16 dense burst, {peak_kind}",
+                "issued_tensor_tflops": issued, "issued_frac": issued / peak, **numerator}
+    else:
+        peak = peaks["bf16_tflops"]
+        # tensor work the kernel issues per (r1, r2) pair: GEMM1 6 slice products of K = RP; GEMM2 6 of
+        # N = NB with 24-bit X (rank padding 32), 4 with 16-bit X (rank padding 64)
+        RP = 32 if nocc <= 32 else 64   # real closed-shell guess density: factor rank = n_occ
+        NB = 64 if nb <= 64 else 128
+        issued = n * n * (2.0 * 6 * RP + 2.0 * (6 if RP == 32 else 4) * NB) / (c_ms / 1e3) / 1e12
+        roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "traffic": traffic, "peak_source": f"bf16 dense burst, {peak_kind}",
+                "issued_tensor_tflops": issued, "issued_frac": issued / peak, **numerator}
+    return roof
+
+
 METRIC = "Fock-build s/iter, mixed vs FP64 GPU at |dE|<=1 uEh; % of roofline"
 
 
@@ -287,41 +329,8 @@ def run_ours(args, rank: int, world: int) -> None:
     if rank != 0:
         return
     n = g.n
-    # algorithmic work per Fock build: F_alg = 2 N^2 (nb nocc + 1), the pair-density count of the direct
-    # build (nb nocc exchange pair densities and the Coulomb density per (r1, r2) pair); this kernel
-    # contracts the same sum in factored form, 2 N^2 (nocc + nb + 1) flops (rho GEMM, exchange GEMM,
-    # Coulomb), reported beside it as kernel_algorithm_tflops
-    flops = 2.0 * n * n * (w.nb * w.n_up + 1)
-    kernel_flops = 2.0 * n * n * (w.n_up + w.nb + 1)
     c_ms = statistics.median(cms)
-    achieved = flops / (c_ms / 1e3) / 1e12
-    kernel_achieved = kernel_flops / (c_ms / 1e3) / 1e12
-    numerator = {"achieved_numerator": "F_alg = 2 N^2 (nb nocc + 1) flops per build (pair-density count)",
-                 "kernel_algorithm_tflops": kernel_achieved}
-    if prec == ffi.PREC_FP64:
-        roof = {"bound": "fp64", "achieved": achieved, "peak": args.fp64_peak, "unit": "TFLOP/s", "frac": achieved / args.fp64_peak,
-                "traffic": None, "peak_source": "nominal B200 FP64 dense rate (--fp64-peak or TCSCF_FP64_PEAK_TFLOPS overrides)",
-                **numerator}
-    elif prec == ffi.PREC_TF32:
-        # TF32 dense rate is half the BF16 rate (nominal 1.1 vs 2.25 PFLOP/s): half the measured BF16 burst
-        peak = peaks["bf16_tflops"] / 2
-        RP = 32                            # TF32 launches hold rank 32 (larger ranks run in chunks)
-        NB = 64 if w.nb <= 64 else 128
-        chunks = -(-w.n_up // RP)
-        issued = n * n * chunks * (2.0 * RP + 2.0 * NB) / (c_ms / 1e3) / 1e12
-        roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                "traffic": None, "peak_source": f"tf32 dense = half the bf16 dense burst, {peak_kind}",
-                "issued_tensor_tflops": issued, "issued_frac": issued / peak, **numerator}
-    else:
-        peak = peaks["bf16_tflops"]
-        # tensor work the kernel issues per (r1, r2) pair: GEMM1 6 slice products of K = RP; GEMM2 6 of
-        # N = NB with 24-bit X (rank padding 32), 4 with 16-bit X (rank padding 64)
-        RP = 32 if w.n_up <= 32 else 64   # real closed-shell guess density: factor rank = n_occ
-        NB = 64 if w.nb <= 64 else 128
-        issued = n * n * (2.0 * 6 * RP + 2.0 * (6 if RP == 32 else 4) * NB) / (c_ms / 1e3) / 1e12
-        roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                "traffic": profiled_traffic(w.name), "peak_source": f"bf16 dense burst, {peak_kind}",
-                "issued_tensor_tflops": issued, "issued_frac": issued / peak, **numerator}
+    roof = roofline(prec, n, w.nb, w.n_up, c_ms, peaks, peak_kind, args.fp64_peak, profiled_traffic(w.name))
     cpu = None
     if not args.skip_cpu:
         r = cpu_reference(w, g, D, h, budget_s=args.cpu_seconds)
