@@ -54,7 +54,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     OBJ.mkdir(exist_ok=True)
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
         objs = list(ex.map(lambda s: _compile(s, verbose), _sources()))
-    cmd = [NVCC, *ARCH, "-shared", "-o", str(OUT), *map(str, objs), "-lcusolver", "-lcublas", "-lcudart",
+    cmd = [NVCC, *ARCH, "-shared", "-o", str(OUT), *map(str, objs), "-lcusolver", "-lcublas", "-lcudart", "-ldl",
            "-Xlinker", "-rpath,/usr/local/cuda/lib64"]
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <cublas_v2.h>
 #include <cusolverDn.h>
+#include <nvtx3/nvToolsExt.h>
 #include <cmath>
 #include <cstdint>
 #include <map>
@@ -130,6 +131,16 @@ int fail(tcscf_ctx * ctx, int code, std::string const & msg);
     int s_ = (expr);                                                                          \
     if (s_ != TCSCF_OK) return s_;                                                            \
   } while (0)
+
+// NVTX range named after the enclosing C-ABI function: profilers that record NVTX show each call
+// (and filter kernels by it); without such a tool attached the push and pop do nothing
+struct NvtxRange {
+  explicit NvtxRange(char const * name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(NvtxRange const &) = delete;
+  NvtxRange & operator=(NvtxRange const &) = delete;
+};
+#define TCSCF_NVTX() ::tcscf::NvtxRange tcscfNvtxRange_(__func__)
 
 // context-owned scratch buffer, grown on demand and kept until the context is destroyed
 int scratch(tcscf_ctx * ctx, char const * name, size_t bytes, void ** out);

@@ -212,6 +212,7 @@ extern "C" {
 
 int tcscf_integrate_all_r1r2(tcscf_ctx * ctx, int r1, int r2, int use_gradient, int kernel, const tcscf_ochi * jastrow, double * answer)
 {
+  TCSCF_NVTX();
   if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
   cudaSetDevice(ctx->device);
   Grid * g1 = findGrid(ctx, r1);
@@ -290,6 +291,7 @@ int tcscf_integrate_all_r1r2(tcscf_ctx * ctx, int r1, int r2, int use_gradient, 
 
 int tcscf_three_electron_integrals(tcscf_ctx * ctx, int r1, int r2, const tcscf_ochi * jastrow, double * answer)
 {
+  TCSCF_NVTX();
   if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
   cudaSetDevice(ctx->device);
   Grid * g1 = findGrid(ctx, r1);
@@ -342,6 +344,7 @@ int tcscf_three_electron_integrals(tcscf_ctx * ctx, int r1, int r2, const tcscf_
 
 int tcscf_tc_compute_q(tcscf_ctx * ctx, int r1, int vsame, int voppo, double * Qss, double * Qso, double * Qoo)
 {
+  TCSCF_NVTX();
   if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
   cudaSetDevice(ctx->device);
   Grid * g1 = findGrid(ctx, r1);
@@ -395,6 +398,7 @@ int tcscf_tc_compute_q(tcscf_ctx * ctx, int r1, int vsame, int voppo, double * Q
 
 int tcscf_tc_assemble_g(tcscf_ctx * ctx, int nb, const double * Qss, const double * Qso, const double * Qoo, const double * density, double * G3)
 {
+  TCSCF_NVTX();
   if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
   cudaSetDevice(ctx->device);
   TCSCF_CHECK(ctx, nb >= 1 && nb <= 16 && Qss && Qso && Qoo && density && G3, TCSCF_ERR_INVALID_ARGUMENT,

@@ -445,6 +445,7 @@ int tcscf_tc_fock_build(tcscf_ctx * ctx, int r1, int fji_same, int fji_oppo, int
                         const double * density, const double * occ_up, const double * occ_down, const double * h, int respect_symmetry,
                         double * G2, double * G3, double * fock, double * energy)
 {
+  TCSCF_NVTX();
   if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
   cudaSetDevice(ctx->device);
   TcInputs in;
@@ -483,6 +484,7 @@ int tcscf_tc_scf(tcscf_ctx * ctx, int r1, int fji_same, int fji_oppo, int vji_sa
                  int n_up, int n_down, int respect_symmetry, double tol, int max_iter, double * energy, int * iterations, double * density,
                  double * pseudo_energies)
 {
+  TCSCF_NVTX();
   using cplx = std::complex<double>;
   if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
   cudaSetDevice(ctx->device);

@@ -1429,6 +1429,7 @@ int tcscf_last_potentials(tcscf_ctx * ctx, double * VH, double * T)
 
 int tcscf_grid_create(tcscf_ctx * ctx, const double * points, const double * weights, int64_t n, int ndim, int * grid)
 {
+  TCSCF_NVTX();
   if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
   TCSCF_CHECK(ctx, points && weights && grid && n > 0 && (ndim == 2 || ndim == 3), TCSCF_ERR_INVALID_ARGUMENT, "invalid grid arguments");
   cudaSetDevice(ctx->device);
@@ -1466,6 +1467,7 @@ int tcscf_grid_destroy(tcscf_ctx * ctx, int grid)
 
 int tcscf_grid_set_basis(tcscf_ctx * ctx, int grid, const tcscf_sto * basis, int nb, int gradients)
 {
+  TCSCF_NVTX();
   if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
   Grid * g = findGrid(ctx, grid);
   TCSCF_CHECK(ctx, g, TCSCF_ERR_INVALID_ARGUMENT, "unknown grid handle");
@@ -1510,6 +1512,7 @@ int tcscf_grid_basis_values(tcscf_ctx * ctx, int grid, double * values, double *
 
 int tcscf_overlap_core_quadrature(tcscf_ctx * ctx, int grid, int Z, double * S, double * H)
 {
+  TCSCF_NVTX();
   if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
   Grid * g = findGrid(ctx, grid);
   TCSCF_CHECK(ctx, g && g->nb > 0 && g->ndim == 3, TCSCF_ERR_INVALID_ARGUMENT, "needs a 3-D grid with a basis");
@@ -1568,6 +1571,7 @@ int tcscf_overlap_core_quadrature_static(tcscf_ctx * ctx, int grid, int Z, doubl
 int tcscf_fock_build(tcscf_ctx * ctx, int r1, int r2, int nspin, const double * density, const double * h, int respect_symmetry,
                      int precision, double * G, double * fock, double * energy)
 {
+  TCSCF_NVTX();
   if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
   cudaSetDevice(ctx->device);
   Grid * g1 = findGrid(ctx, r1);
@@ -1601,6 +1605,7 @@ int tcscf_fock_build(tcscf_ctx * ctx, int r1, int r2, int nspin, const double * 
 int tcscf_fock_build_device(tcscf_ctx * ctx, int r1, int r2, int nspin, const double * density, const double * h, int respect_symmetry,
                             int precision, double * G, double * fock, double * energy)
 {
+  TCSCF_NVTX();
   if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
   cudaSetDevice(ctx->device);
   Grid * g1 = findGrid(ctx, r1);
@@ -1621,6 +1626,7 @@ int tcscf_fock_build_device(tcscf_ctx * ctx, int r1, int r2, int nspin, const do
 
 int tcscf_compute_F(tcscf_ctx * ctx, int r1, int r2, int kernel, const tcscf_ochi * jastrow, double * F, int keep, int * fji)
 {
+  TCSCF_NVTX();
   if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
   cudaSetDevice(ctx->device);
   Grid * g1 = findGrid(ctx, r1);
@@ -1681,6 +1687,7 @@ int tcscf_compute_F(tcscf_ctx * ctx, int r1, int r2, int kernel, const tcscf_och
 
 int tcscf_compute_V(tcscf_ctx * ctx, int r1, int r2, int kernel, const tcscf_ochi * jastrow, double * V, int keep, int * vji)
 {
+  TCSCF_NVTX();
   if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
   cudaSetDevice(ctx->device);
   Grid * g1 = findGrid(ctx, r1);
@@ -1758,6 +1765,7 @@ int tcscf_tensor_destroy(tcscf_ctx * ctx, int handle)
 int tcscf_fock_build_batch(tcscf_ctx * ctx, int count, const int * r1, const int * r2, const double * const * density,
                            const double * const * h, int respect_symmetry, int precision, double * energy, double * const * fock)
 {
+  TCSCF_NVTX();
   if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
   cudaSetDevice(ctx->device);
   TCSCF_CHECK(ctx, count >= 1 && r1 && r2 && density && h && energy, TCSCF_ERR_INVALID_ARGUMENT, "batch: count, grids, densities, h and energy are required");
@@ -1836,6 +1844,7 @@ int tcscf_fock_build_batch(tcscf_ctx * ctx, int count, const int * r1, const int
 int tcscf_fock_build_precomputed(tcscf_ctx * ctx, int r1, int fji, int nspin, const double * density, const double * h,
                                  int respect_symmetry, double * G, double * fock, double * energy)
 {
+  TCSCF_NVTX();
   if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
   cudaSetDevice(ctx->device);
   Grid * g1 = findGrid(ctx, r1);
@@ -1909,6 +1918,7 @@ int tcscf_set_scf_options(tcscf_ctx * ctx, int diis, int real_eigensolve)
 int tcscf_scf(tcscf_ctx * ctx, int r1, int r2, int nspin, int n_up, int n_down, const double * S, const double * h, int respect_symmetry,
               int precision, double tol, int max_iter, double * energy, int * iterations, double * density, double * eigenvalues)
 {
+  TCSCF_NVTX();
   if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
   cudaSetDevice(ctx->device);
   Grid * g1 = findGrid(ctx, r1);
