@@ -490,7 +490,7 @@ def main() -> None:
     ap.add_argument("--nrad", type=int, default=0, help="override the workload's radial points (smaller profiling cases)")
     ap.add_argument("--fp64-steps", type=int, default=2)
     ap.add_argument("--fp64-peak", type=float, default=float(os.environ.get("TCSCF_FP64_PEAK_TFLOPS", "37.0")))
-    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--ref-seconds", type=float, default=10.0)
     ap.add_argument("--skip-fp64", action="store_true")
