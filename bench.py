@@ -172,10 +172,12 @@ def run_reference(args, rank: int) -> None:
         if i >= args.warmup:
             vals.append(r["s_per_iter"])
     v = statistics.median(vals)
+    dropped, near = grids.coincident_pairs(g, g)   # r1 = r2 grid: the diagonal pairs contribute 0
     line = {"metric": METRIC, "value": v, "unit": "s/iter", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "impl": "reference",
-            "config": {"workload": f"{w.name} RCS Fock build", "n_points": g.n, "n_basis": w.nb, "n_occ": w.n_up},
+            "config": {"workload": f"{w.name} RCS Fock build", "n_points": g.n, "n_basis": w.nb, "n_occ": w.n_up,
+                       "dropped_pairs": dropped, "near_coincident_pairs": near},
             "cpu_baseline": {"value": v, "unit": "s/iter", "cores": r["cores"], "kind": "port", "sample": r["sample"],
                              "precompute_s": r["precompute_s"]},
             "e2e": {"value": v, "unit": "s/iter", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -330,6 +332,7 @@ def run_ours(args, rank: int, world: int) -> None:
     if rank != 0:
         return
     n = g.n
+    dropped, near = grids.coincident_pairs(g, g)   # r1 = r2 grid: the diagonal pairs contribute 0
     c_ms = statistics.median(cms)
     roof = roofline(prec, n, w.nb, w.n_up, c_ms, peaks, peak_kind, args.fp64_peak, profiled_traffic(w.name))
     cpu = None
@@ -350,6 +353,7 @@ def run_ours(args, rank: int, world: int) -> None:
                                              "block, double-float across blocks"}[args.precision],
                        "l2": "flushed (256 MB write) between timed steps",
                        "density": "core-Hamiltonian guess (canonical orthogonalisation)",
+                       "dropped_pairs": dropped, "near_coincident_pairs": near,
                        "schedule": "autotuned r2 split (tuned in the warm-up: shapes, batches, measurements = %s)" % (ctx.autotune_stats(),)
                        if args.autotune else "fixed rule"},
             "energy": E, "contraction_ms": c_ms, "gpu_launches": launches, "roofline": roof, "fp64": fp64,

@@ -75,3 +75,33 @@ def qmc_grid(ndim: int, n: int, seed: int) -> QuadratureGrid:
 def subset(grid: QuadratureGrid, idx) -> QuadratureGrid:
     idx = np.asarray(idx)
     return QuadratureGrid(np.ascontiguousarray(grid.points[:, idx]), np.ascontiguousarray(grid.weights[idx]))
+
+
+def _cartesian(grid: QuadratureGrid) -> np.ndarray:
+    """Points as [N][3]; a 2-D grid's rows are (x, z) with y = 0."""
+    p = grid.points
+    if grid.ndim == 2:
+        return np.stack([p[0], np.zeros_like(p[0]), p[1]], axis=1)
+    return np.ascontiguousarray(p.T)
+
+
+def coincident_pairs(r1: QuadratureGrid, r2: QuadratureGrid, rel_tol: float = 1e-10) -> tuple[int, int]:
+    """(exact, near): the r1 / r2 point pairs with r1 == r2, which every r12 kernel drops (contributes 0,
+    the reference's r12Inv convention, src/unitTests/IntegrationTest.cpp:298-309), and the pairs
+    with 0 < |r1 - r2| <= rel_tol |r1|, where 1/r12 exceeds 1/(rel_tol |r1|) and swamps the quadrature.
+    Near pairs arise when two grids share angular directions and radial nodes up to rounding, e.g.
+    Chebyshev radial rules of n and m points with (n + 1) and (m + 1) sharing a factor."""
+    from scipy.spatial import cKDTree
+
+    a, b = _cartesian(r1), _cartesian(r2)
+    tree = cKDTree(b)
+    radius = rel_tol * np.linalg.norm(a, axis=1)
+    exact = near = 0
+    for i, hits in enumerate(tree.query_ball_point(a, np.maximum(radius, 0.0))):
+        for j in hits:
+            if np.array_equal(a[i], b[j]):
+                exact += 1
+            else:
+                near += 1
+    # a point at the origin has radius 0: query_ball_point returns only exact matches there
+    return exact, near

@@ -68,3 +68,18 @@ def test_workload_sizes():
     assert wl.be_tc().nb == 24
     b = wl.batch()
     assert len(b) == 64 and all(10 <= x.nb <= 80 for x in b)
+
+
+def test_coincident_pairs_are_counted():
+    """Exact r1 == r2 pairs (dropped by every r12 kernel) and pairs equal up to rounding (where 1/r12
+    explodes): Chebyshev rules of 6 and 21 nodes (n + 1 = 6, 21) share two radii up to rounding, and
+    the Lebedev rules of orders 11 and 17 share 14 directions; rules of 10 and 15 nodes share four
+    radii exactly, orders 3 and 5 the six octahedral directions."""
+    g = grids.product_grid(12, 11)
+    assert grids.coincident_pairs(g, g) == (g.n, 0)
+    assert grids.coincident_pairs(grids.product_grid(5, 11), grids.product_grid(20, 17)) == (0, 28)
+    assert grids.coincident_pairs(grids.product_grid(9, 3), grids.product_grid(14, 5)) == (24, 0)
+    assert grids.coincident_pairs(grids.product_grid(8, 11), grids.product_grid(9, 17)) == (0, 0)
+    # a 2-D (x, z) grid is compared in the y = 0 plane
+    g2 = grids.QuadratureGrid(np.ascontiguousarray(g.points[[0, 2]]), g.weights)
+    assert grids.coincident_pairs(g, g2)[0] >= 1
