@@ -108,6 +108,18 @@ def main(ref: Path) -> None:
              ("third", (4, 3, 2), (3, 2, -1), 0.000451565, 0.000064, "src/unitTests/IntegrationTest.cpp:450-483"),
              ("fourth", (4, 2, -2), (5, 3, 1), 0.0317012, 0.0001, "src/unitTests/IntegrationTest.cpp:485-520"),
              ("s_p", (1, 0, 0), (2, 1, 0), None, None, "closed form F0(1s,2p) = 59/243")]
+    # the reference's recorded He study (convergence.sh: RCS, Ochi s functions n = 0..nMax with
+    # -n 1..9 -l 0 -a 1.355, QMC grids --r1 2000 --r2 1000; data.txt: mean and standard deviation
+    # over ten grid draws per basis size)
+    rows = []
+    for line in (ref / "data.txt").read_text().splitlines()[1:]:
+        f = [x.strip() for x in line.split(",")]
+        if len(f) >= 5:
+            rows.append([int(f[0]), float(f[3]), float(f[4])])
+    script = (ref / "convergence.sh").read_text()
+    alpha = float(re.search(r"-a\s+([0-9.]+)", script).group(1))
+    known["he_ochi_study"] = {"Z": 2, "alpha": alpha, "l_max": 0, "rows_nbasis_energy_std": rows,
+                              "src": "data.txt:1-10 (settings convergence.sh:3-6)"}
     known["r12_hydrogen"] = [{"name": n, "a": list(a), "b": list(b), "reference_value": v, "reference_error": e,
                               "exact": hydrogen_coulomb(*a, *b), "src": src} for n, a, b, v, e, src in cases]
     (here / "known_answers.json").write_text(json.dumps(known, indent=1))
