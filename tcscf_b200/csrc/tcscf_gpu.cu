@@ -1330,7 +1330,11 @@ int tcscf_ctx_create(int device, tcscf_ctx ** out)
     cudaMemPoolSetAttribute(ctx->gridPool, cudaMemPoolAttrReleaseThreshold, &keep);
   }
   for (auto & e : ctx->ev) cudaEventCreate(&e);
-  if (cusolverDnCreate(&ctx->solver) != CUSOLVER_STATUS_SUCCESS) { delete ctx; return TCSCF_ERR_CUDA; }
+  if (cusolverDnCreate(&ctx->solver) != CUSOLVER_STATUS_SUCCESS) {
+    ctx->solver = nullptr;
+    tcscf_ctx_destroy(ctx);   // releases the stream, the grid pool and the events made so far
+    return TCSCF_ERR_CUDA;
+  }
   cusolverDnSetStream(ctx->solver, ctx->stream);
   *out = ctx;
   return TCSCF_OK;
