@@ -1655,12 +1655,15 @@ int tcscf_compute_F(tcscf_ctx * ctx, int r1, int r2, int kernel, const tcscf_och
   cudaEventRecord(ctx->ev[0], ctx->stream);
   int const launch0 = ctx->launchCount;
   kPairProducts<<<gridBlocks(n2 * np, 256), 256, 0, ctx->stream>>>(n2, nb, g2->phiR, g2->w, scale, pairs);
-  TCSCF_LAUNCH(ctx);
+  ctx->launchCount++;
+  int st = TCSCF_OK;
+  if (cudaError_t const e = cudaGetLastError(); e != cudaSuccess)   // dOut is released below
+    st = fail(ctx, TCSCF_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
   Contraction c;
   c.n1 = n1; c.n2 = n2; c.R = 0; c.ncol = np; c.p1 = g1->pts; c.p2 = g2->pts; c.V = pairs; c.ldv = np; c.T = FR; c.ldt = np;
   c.kernel = kernel; c.jastrow = jastrow;
   cudaEventRecord(ctx->ev[2], ctx->stream);
-  int st = contractFp64(ctx, c);
+  if (st == TCSCF_OK) st = contractFp64(ctx, c);
   cudaEventRecord(ctx->ev[3], ctx->stream);
   if (st == TCSCF_OK) {
     kPairsToReference<<<gridBlocks(n1 * nb * nb, 256), 256, 0, ctx->stream>>>(n1, nb, g1->dsto, FR, 1, 0, realOut ? 1 : 0, dOut);
@@ -1714,8 +1717,10 @@ int tcscf_compute_V(tcscf_ctx * ctx, int r1, int r2, int kernel, const tcscf_och
   cudaEventRecord(ctx->ev[0], ctx->stream);
   int const launch0 = ctx->launchCount;
   kPairProducts<<<gridBlocks(n2 * np, 256), 256, 0, ctx->stream>>>(n2, nb, g2->phiR, g2->w, 1.0, pairs);
-  TCSCF_LAUNCH(ctx);
+  ctx->launchCount++;
   int st = TCSCF_OK;
+  if (cudaError_t const e = cudaGetLastError(); e != cudaSuccess)   // dOut is released below
+    st = fail(ctx, TCSCF_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
   float contraction = 0;
   for (int comp = 0; comp < 3 && st == TCSCF_OK; ++comp) {
     Contraction c;
