@@ -409,3 +409,20 @@ def test_ochi_basis_convergence_matches_the_reference_he_study():
         assert st == 0
     for nb in (4, 5, 6):
         assert abs((E[nb] - E[10]) - (ref[nb] - ref[10])) < 2e-5, (nb, E[nb] - E[10], ref[nb] - ref[10])
+
+
+@pytest.mark.parametrize("family", ["sto", "ochi", "hydrogen"])
+def test_real_harmonic_unitary_makes_the_basis_real(family):
+    """U (tcscf_b200.basis.real_harmonic_unitary) is unitary and turns the reference's complex
+    functions (Y_l^m = P_l^|m| e^{i m phi}, mathFunctions.hpp:126-139, as the oracle evaluates them)
+    into real ones: m > 0 -> (phi_m + phi_-m)/sqrt 2, m < 0 -> (phi_|m| - phi_-|m|)/(i sqrt 2).  The
+    device contractions run on these real functions; the Fock matrices go back through U."""
+    from tcscf_b200 import basis as wl
+
+    b = {"sto": wl.kr().basis, "ochi": wl.ochi_functions(2, 3, 1.3), "hydrogen": wl.hydrogen_functions(4, 3, 2)}[family]
+    U = wl.real_harmonic_unitary(b)
+    np.testing.assert_allclose(U @ U.conj().T, np.eye(len(b)), atol=1e-15)
+    pts = np.random.default_rng(4).normal(size=(3, 200)) * 2
+    phi = oracle.basis_values(pts, b)                        # [N][nb] complex
+    phiR = phi @ U.T
+    assert np.abs(phiR.imag).max() <= 1e-13 * max(1.0, np.abs(phiR).max())
