@@ -229,9 +229,6 @@ int ggev(int n, cplx * A, cplx * B, cplx * alpha, cplx * beta, cplx * VR)
   return info;
 }
 
-template <typename T> T cj(T v) { return v; }
-template <> cplx cj<cplx>(cplx v) { return std::conj(v); }
-
 // HartreeFock.cpp:183-213 (calculateIaa), Iji element type U, density complex
 template <typename U>
 void calculateIaa(cplx * Iaa, U const * Iji, int64_t N1, int nb, cplx const * D)
