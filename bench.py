@@ -5,7 +5,7 @@ energy) for the workload's density on its radial x Lebedev grid.  `value` is dev
 with every input resident in HBM; `e2e` is the same through the public C ABI from host buffers
 (grid upload, device basis evaluation, Fock build, G/Fock/energy back to the host).
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload kr|ne|he|batch|scf]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload kr|ne|he|batch|scf|be_tc]
                   [--precision bf16x3|fp64|tf32]
 
 Under torchrun (N > 1) every rank runs an independent replica (the Fock build does not shard in
@@ -89,14 +89,13 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def scf_guess_density(basis, Z: int, nocc: int):
+def guess_from(S, h, basis, nocc: int):
     """Core-Hamiltonian guess (the reference's first iteration: zero density -> F = h), solved in the
     real-harmonic basis with canonical orthogonalisation (the even-tempered overlap is
-    ill-conditioned), so the closed-shell density is real there; returned in the reference basis."""
-    from tcscf_b200 import api
+    ill-conditioned), so the closed-shell density is real there; returned in the reference basis.
+    numpy only: both bench arms take their density from here."""
     from tcscf_b200.basis import real_harmonic_unitary
 
-    S, h = api.overlap_core(basis, Z)
     U = real_harmonic_unitary(basis)
     SR = np.real(U.conj() @ S @ U.T)
     hR = np.real(U.conj() @ h @ U.T)
@@ -107,7 +106,15 @@ def scf_guess_density(basis, Z: int, nocc: int):
     CR = X @ Cp[:, :nocc]
     DR = CR @ CR.T
     D = U.T @ DR @ U.conj()
-    return np.ascontiguousarray(D.astype(np.complex128)), h
+    return np.ascontiguousarray(D.astype(np.complex128))
+
+
+def scf_guess_density(basis, Z: int, nocc: int):
+    """The guess density of the GPU arm, from the library's analytic S and h."""
+    from tcscf_b200 import api
+
+    S, h = api.overlap_core(basis, Z)
+    return guess_from(S, h, basis, nocc), h
 
 
 def workload(name: str):
@@ -116,44 +123,114 @@ def workload(name: str):
     return {"kr": wl.kr, "ne": wl.ne, "he": wl.he}[name]()
 
 
-def cpu_reference(w, grid, D, h, budget_s: float, threads: int | None = None) -> dict:
-    """The reference algorithm (precomputeIntegrand + computeF once, then calculateIaa / calculateFai /
-    assembly per iteration) timed on the host cores through the oracle port on a sample of r1 rows
-    with the full r2 grid, extrapolated linearly to all rows (rows are independent and of equal cost)."""
+def workload_config(w, n_points: int, dropped: int, near: int) -> dict:
+    """The `config` object of a direct-form workload, identical in both arms."""
+    return {"workload": f"{w.name} RCS Fock build", "Z": w.Z, "n_points": n_points, "n_basis": w.nb, "n_occ": w.n_up,
+            "grid": f"{w.nrad} radial (Gauss-Chebyshev, r=(1+x)/(1-x)) x Lebedev order {w.order}",
+            "density": "core-Hamiltonian guess (canonical orthogonalisation)",
+            "l2": "GPU arm: flushed (256 MB write) between timed steps",
+            "dropped_pairs": dropped, "near_coincident_pairs": near}
+
+
+def host_cpu() -> dict:
+    """lscpu's model name, sockets, cores per socket and threads per core of the host."""
+    out = {}
+    try:
+        txt = subprocess.run(["lscpu"], capture_output=True, text=True, timeout=10).stdout
+    except Exception:
+        return out
+    keys = {"Model name": "model", "Socket(s)": "sockets", "Core(s) per socket": "cores_per_socket",
+            "Thread(s) per core": "threads_per_core", "CPU(s)": "cpus"}
+    for line in txt.splitlines():
+        k, _, v = line.partition(":")
+        if k.strip() in keys and keys[k.strip()] not in out:
+            out[keys[k.strip()]] = v.strip()
+    return out
+
+
+def stratified_rows(n: int, k: int) -> np.ndarray:
+    """k row indices spread evenly over the n points (the product grid orders them radial shell by
+    radial shell, so the sample covers every radial range and angular position)."""
+    k = max(1, min(n, k))
+    return np.unique((np.arange(k) * (n / k) + n / (2 * k)).astype(np.int64).clip(0, n - 1))
+
+
+# FP64 RCS SCF iterations of the Kr configuration from the zero density to |dE| < 1e-8 Eh
+# (`bench.py --workload scf`, fp64_plain): the reference's precompute is amortised over these
+SCF_ITERATIONS_KR = 9
+PER_ITERATION_ROWS = 1024
+
+
+def cpu_reference(w, grid, D, h, budget_s: float, threads: int | None = None, calib: dict | None = None) -> dict:
+    """The reference algorithm timed on the host cores through the oracle port: precomputeIntegrand +
+    computeF (HartreeFock.hpp:23-180) on a stratified sample of r1 rows against the full r2 grid, then
+    the per-iteration calculateIaa / calculateFai / assembly (HartreeFock.cpp:144-213, 817-850) on
+    1,024 stratified rows; both extrapolated linearly to all rows (rows are independent and of equal
+    cost).  `calib` carries the sample size between steps."""
     import oracle
 
     if threads:
         oracle.set_threads(threads)
     cores = oracle.threads()
-    vals2 = oracle.basis_values(grid.points, w.basis)
-    rng = np.random.default_rng(0)
-    # calibrate with one row per thread, then size the sample to the budget
-    rows = cores
-    t_row = None
-    sample_rows = rows
-    for _ in range(2):
-        idx = np.sort(rng.choice(grid.n, sample_rows, replace=False))
-        p1 = np.ascontiguousarray(grid.points[:, idx])
+    if calib is None:
+        calib = {}
+    if "rows" not in calib:
+        # one row per thread times the per-row precompute cost, then the sample is sized to the budget
+        idx = stratified_rows(grid.n, cores)
+        vals2 = oracle.basis_values(grid.points, w.basis)
         t0 = time.perf_counter()
-        F = oracle.compute_F(p1, grid.points, grid.weights, vals2, w.nb)
-        t_pre = time.perf_counter() - t0
-        vals1 = np.ascontiguousarray(vals2[idx])
-        t0 = time.perf_counter()
-        oracle.fock_build(F, vals1, np.ascontiguousarray(grid.weights[idx]), D, h)
-        t_it = time.perf_counter() - t0
-        t_row = (t_pre + t_it) / sample_rows
-        want = int(max(cores, min(grid.n, budget_s / max(t_row, 1e-9))))
-        want = (want // cores) * cores or cores
-        if want <= sample_rows * 1.2:
-            break
-        sample_rows = want
-    scale = grid.n / sample_rows
-    # per SCF iteration the reference rebuilds the Fock matrix from its precomputed F; computeF runs
-    # once per SCF and is reported beside it
-    return {"s_per_iter": t_it * scale, "precompute_s": t_pre * scale, "iteration_s": t_it * scale,
-            "cores": cores, "rows": sample_rows, "sample": f"{sample_rows} of {grid.n} r1 rows x all {grid.n} r2 points: "
-            "per-iteration Fock build (calculateIaa/calculateFai/assembly) from the precomputed F, extrapolated linearly "
-            "to all rows; the one-off computeF precompute is reported as precompute_s"}
+        oracle.compute_F(np.ascontiguousarray(grid.points[:, idx]), grid.points, grid.weights, vals2, w.nb)
+        per_row = (time.perf_counter() - t0) / len(idx)
+        want = int(max(cores, min(grid.n, budget_s / max(per_row, 1e-9))))
+        calib["rows"] = max(cores, (want // cores) * cores)
+        calib["vals2"] = vals2
+    vals2 = calib.get("vals2")
+    if vals2 is None:
+        vals2 = calib["vals2"] = oracle.basis_values(grid.points, w.basis)
+    idx = stratified_rows(grid.n, calib["rows"])
+    t0 = time.perf_counter()
+    F = oracle.compute_F(np.ascontiguousarray(grid.points[:, idx]), grid.points, grid.weights, vals2, w.nb)
+    t_pre = (time.perf_counter() - t0) / len(idx)
+    # per-iteration build on 1,024 stratified rows: their basis values and weights, with the sampled
+    # rows' F repeated (the per-row arithmetic of calculateIaa / calculateFai does not depend on F's values)
+    it_idx = stratified_rows(grid.n, PER_ITERATION_ROWS)
+    reps = -(-len(it_idx) // len(idx))
+    F_it = np.ascontiguousarray(np.concatenate([F] * reps)[: len(it_idx)])
+    vals1 = np.ascontiguousarray(vals2[it_idx])
+    w1 = np.ascontiguousarray(grid.weights[it_idx])
+    t0 = time.perf_counter()
+    oracle.fock_build(F_it, vals1, w1, D, h)
+    t_it = (time.perf_counter() - t0) / len(it_idx)
+    T_pre, T_it = t_pre * grid.n, t_it * grid.n
+    return {"s_per_iter": T_it, "precompute_s": T_pre, "iteration_s": T_it,
+            "amortised_s_per_iter": T_pre / SCF_ITERATIONS_KR + T_it, "amortised_over_iterations": SCF_ITERATIONS_KR,
+            "cores": cores, "rows": len(idx),
+            "sample": f"precompute (precomputeIntegrand + computeF) on {len(idx)} stratified r1 rows x all {grid.n} r2 "
+                      f"points; per-iteration Fock build (calculateIaa/calculateFai/assembly from the precomputed F) on "
+                      f"{len(it_idx)} stratified r1 rows; both extrapolated linearly to all {grid.n} rows; value = the "
+                      f"per-iteration cost, the one-off precompute reported as precompute_s and amortised over "
+                      f"{SCF_ITERATIONS_KR} SCF iterations as amortised_s_per_iter"}
+
+
+def reference_inputs(w):
+    """Grid, guess density and h of the reference arm from the oracle, scipy's Lebedev rule and numpy:
+    the product library is not loaded in that process."""
+    import oracle
+    from tcscf_b200 import ffi
+    from tcscf_b200.grids import QuadratureGrid, lebedev_table
+
+    r, wr = oracle.radial_grid(w.nrad, ffi.MAP_ONE_PLUS_X)
+    pts, wts = oracle.product_grid(r, wr, lebedev_table(w.order))
+    S, h = oracle.overlap_core(w.basis, w.Z)
+    return QuadratureGrid(pts, wts), guess_from(S, h, w.basis, w.n_up), h
+
+
+def product_library_loaded() -> bool:
+    """Whether libtcscf_gpu.so is mapped into this process."""
+    try:
+        return "libtcscf_gpu.so" in Path("/proc/self/maps").read_text()
+    except OSError:
+        return False
 
 
 def run_reference(args, rank: int) -> None:
@@ -164,22 +241,25 @@ def run_reference(args, rank: int) -> None:
     w = workload(args.workload)
     if args.nrad:
         w.nrad = args.nrad
-    g = grids.product_grid(w.nrad, w.order)
-    D, h = scf_guess_density(w.basis, w.Z, w.n_up)
-    vals = []
+    g, D, h = reference_inputs(w)
+    vals, calib = [], {}
     for i in range(args.warmup + args.steps):
-        r = cpu_reference(w, g, D, h, budget_s=args.ref_seconds)
+        r = cpu_reference(w, g, D, h, budget_s=args.ref_seconds, calib=calib)
         if i >= args.warmup:
-            vals.append(r["s_per_iter"])
-    v = statistics.median(vals)
+            vals.append(r)
+    v = statistics.median(x["s_per_iter"] for x in vals)
+    pre = statistics.median(x["precompute_s"] for x in vals)
+    amort = statistics.median(x["amortised_s_per_iter"] for x in vals)
     dropped, near = grids.coincident_pairs(g, g)   # r1 = r2 grid: the diagonal pairs contribute 0
+    if product_library_loaded():
+        raise RuntimeError("the reference arm must not load the product library")
     line = {"metric": METRIC, "value": v, "unit": "s/iter", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "impl": "reference",
-            "config": {"workload": f"{w.name} RCS Fock build", "n_points": g.n, "n_basis": w.nb, "n_occ": w.n_up,
-                       "dropped_pairs": dropped, "near_coincident_pairs": near},
+            "config": workload_config(w, g.n, dropped, near),
             "cpu_baseline": {"value": v, "unit": "s/iter", "cores": r["cores"], "kind": "port", "sample": r["sample"],
-                             "precompute_s": r["precompute_s"]},
+                             "precompute_s": pre, "amortised_s_per_iter": amort,
+                             "amortised_over_iterations": r["amortised_over_iterations"], "lscpu": host_cpu()},
             "e2e": {"value": v, "unit": "s/iter", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -229,17 +309,12 @@ def roofline(prec: int, n: int, nb: int, nocc: int, c_ms: float, peaks: dict, pe
 METRIC = "Fock-build s/iter, mixed vs FP64 GPU at |dE|<=1 uEh; % of roofline"
 
 
-def profiled_traffic(name: str):
-    """DRAM bytes per launch of the tensor contraction kernel for this workload, as recorded in the
-    committed ncu summary (profiles/kflashtc_dram_traffic.md: 'traffic_bytes_per_launch <name> <bytes>')."""
-    path = Path(__file__).resolve().parent / "profiles" / "kflashtc_dram_traffic.md"
-    if not path.exists():
-        return None
-    for line in path.read_text().splitlines():
-        parts = line.strip("` ").split()
-        if len(parts) == 3 and parts[0] == "traffic_bytes_per_launch" and parts[1].lower() == name.lower():
-            return float(parts[2])
-    return None
+# DRAM bytes per launch of the split-BF16 contraction kernel (kFlashTc<128,32,3>) on the Kr workload:
+# ncu's dram__bytes_read.sum + dram__bytes_write.sum of one launch on the 263,900-point Kr grid
+# (130 radial x Lebedev 77) was 11.94 GB + 0.268 GB = 1.221e10 B; a launch re-streams the r2 operands
+# once per (r1 tile, r2 block) unit where L2 misses, so the figure scales with the unit count,
+# 3172 x 6344 at 406,000 points against 2062 x 4124 (x 2.366), to 2.889e10 B
+TRAFFIC_BYTES_PER_LAUNCH = {"Kr": 2.889e10}
 
 
 def run_ours(args, rank: int, world: int) -> None:
@@ -334,28 +409,28 @@ def run_ours(args, rank: int, world: int) -> None:
     n = g.n
     dropped, near = grids.coincident_pairs(g, g)   # r1 = r2 grid: the diagonal pairs contribute 0
     c_ms = statistics.median(cms)
-    roof = roofline(prec, n, w.nb, w.n_up, c_ms, peaks, peak_kind, args.fp64_peak, profiled_traffic(w.name))
+    roof = roofline(prec, n, w.nb, w.n_up, c_ms, peaks, peak_kind, args.fp64_peak,
+                    TRAFFIC_BYTES_PER_LAUNCH.get(w.name) if prec == ffi.PREC_BF16X3 and args.nrad == 0 else None)
     cpu = None
     if not args.skip_cpu:
         r = cpu_reference(w, g, D, h, budget_s=args.cpu_seconds)
         cpu = {"value": r["s_per_iter"], "unit": "s/iter", "cores": r["cores"], "kind": "port", "sample": r["sample"],
-               "precompute_s": r["precompute_s"], "iteration_s": r["iteration_s"]}
+               "precompute_s": r["precompute_s"], "iteration_s": r["iteration_s"],
+               "amortised_s_per_iter": r["amortised_s_per_iter"], "amortised_over_iterations": r["amortised_over_iterations"],
+               "lscpu": host_cpu()}
     line = {"metric": METRIC, "value": s_per_iter, "unit": "s/iter", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": total_ms / args.steps, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
             "dtype": {"fp64": "f64", "bf16x3": "bf16", "tf32": "tf32"}[args.precision],
             "data": "synthetic",
-            "config": {"workload": f"{w.name} RCS Fock build (direct form)", "Z": w.Z, "n_points": n, "n_basis": w.nb,
-                       "n_occ": w.n_up, "grid": f"{w.nrad} radial (Gauss-Chebyshev, r=(1+x)/(1-x)) x Lebedev order {w.order}",
-                       "precision": {"fp64": "fp64",
-                                     "bf16x3": "bf16 fixed-point slices (24-bit factors and kernel tile), exact fp32 "
-                                               "accumulation of the leading slices per 64-point block, double-float across blocks",
-                                     "tf32": "tf32 operands (10-bit mantissa, round to nearest), fp32 accumulation per 64-point "
-                                             "block, double-float across blocks"}[args.precision],
-                       "l2": "flushed (256 MB write) between timed steps",
-                       "density": "core-Hamiltonian guess (canonical orthogonalisation)",
-                       "dropped_pairs": dropped, "near_coincident_pairs": near,
-                       "schedule": "autotuned r2 split (tuned in the warm-up: shapes, batches, measurements = %s)" % (ctx.autotune_stats(),)
-                       if args.autotune else "fixed rule"},
+            "config": workload_config(w, n, dropped, near),
+            "form": "direct (no stored Fji)",
+            "precision": {"fp64": "fp64",
+                          "bf16x3": "bf16 fixed-point slices (24-bit factors and kernel tile), exact fp32 accumulation of "
+                                    "the leading slices per 64-point block, double-float across blocks",
+                          "tf32": "tf32 operands (10-bit mantissa, round to nearest), fp32 accumulation per 64-point block, "
+                                  "double-float across blocks"}[args.precision],
+            "schedule": "autotuned r2 split (tuned in the warm-up: shapes, batches, measurements = %s)" % (ctx.autotune_stats(),)
+            if args.autotune else "fixed rule",
             "energy": E, "contraction_ms": c_ms, "gpu_launches": launches, "roofline": roof, "fp64": fp64,
             "speedup_vs_fp64": (fp64["s_per_iter"] / (total_ms / args.steps / 1e3)) if fp64 else None,
             "e2e": e2e, "cpu_baseline": cpu, "clocks": clk.summary()}
@@ -480,14 +555,132 @@ def run_scf(args, rank: int) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_be_tc(args, rank: int) -> None:
+    """The Be transcorrelated configuration: 24 STOs, three 2^16-point scrambled-Sobol grids, Jastrow
+    u = r12 / (2 (1 + b r12)), b = 1.  Per precision (split BF16 and FP64): the precompute
+    (computeF of the same- and opposite-spin TC scalar kernels on r1 x r2, computeV of grad u on r1 x r3,
+    HartreeFockTest.cpp:261-319), the TC SCF on those tensors to |dE| < 1e-8 Eh (TCHartreeFock,
+    HartreeFock.cpp:1105-1362), and the per-iteration TC Fock build timed on its own.  value = the mixed
+    precompute amortised over the SCF's iterations plus one per-iteration build (s/iter); the FP64
+    figure beside it; device time on the context stream for the precompute, wall time around the
+    synchronous per-iteration call."""
+    import torch
+
+    from tcscf_b200 import api, ffi, grids
+    from tcscf_b200 import basis as wl
+
+    if rank != 0:
+        return
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(local)
+    w = wl.be_tc()
+    n = args.qmc_points or w.qmc_points
+    jd = wl.be_tc_jastrow(w)
+    u = ffi.ochi_struct(jd["a"], jd["a12"], jd["terms"])
+    seed = w.extra["seed"]
+    g = [grids.qmc_grid(3, n, seed + k) for k in range(3)]
+    ctx = api.Context(local)
+    G = [api.QMCGrid(ctx, gk) for gk in g]
+    G[0].setBasisFunctions(w.basis, storeGradients=True)
+    G[1].setBasisFunctions(w.basis)
+    G[2].setBasisFunctions(w.basis)
+    S, h = api.overlap_core(w.basis, w.Z)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=torch.device("cuda", local))
+    peaks, peak_kind = load_peaks()
+    np_ = w.nb * (w.nb + 1) // 2
+
+    def precompute(prec):
+        ts, cms = [], []
+        for kern, fn, grid in ((ffi.K_TC_SCALAR_SAME, api.computeF, G[1]), (ffi.K_TC_SCALAR_OPPO, api.computeF, G[1]),
+                               (ffi.K_GRAD_U_SAME, api.computeV, G[2]), (ffi.K_GRAD_U_OPPO, api.computeV, G[2])):
+            _, t = fn(G[0], grid, kern, u, keep=True, copy=False, precision=prec)
+            ts.append(t)
+            cms.append(ctx.last_timing()[0])
+        return ts, cms
+
+    res = {}
+    with ClockSampler(local) as clk:
+        for name, prec in (("bf16x3", ffi.PREC_BF16X3), ("fp64", ffi.PREC_FP64)):
+            steps = args.steps if prec == ffi.PREC_BF16X3 else max(1, min(args.steps, args.fp64_steps))
+            warm = args.warmup if prec == ffi.PREC_BF16X3 else 1
+            pre_ms, kern_ms, launches = [], [], 0
+            for i in range(warm + steps):
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                l0 = ctx.last_timing()[2]
+                e0.record(stream)
+                ts, cms = precompute(prec)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                if i >= warm:
+                    pre_ms.append(e0.elapsed_time(e1))
+                    kern_ms.append(cms)
+                if i < warm + steps - 1:
+                    for t in ts:
+                        t.close()
+            scf = api.TCHartreeFock(w.n_up, w.n_down)
+            t0 = time.perf_counter()
+            E = scf.compute(S, h, G[0], *ts, tol=1e-8, max_iter=200)
+            scf_s = time.perf_counter() - t0
+            occ = []
+            for s_, nocc in ((0, w.n_up), (1, w.n_down)):
+                # occupied orbitals of the converged density (its leading eigenvectors) for the timed build
+                ev, V = np.linalg.eigh(scf.density[s_])
+                occ.append((V[:, ::-1][:, :nocc] * np.sqrt(np.maximum(ev[::-1][:nocc], 0))).T.copy())
+            it_s = []
+            for i in range(3 + steps):
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                api.tc_fock_build(G[0], *ts, w.n_up, w.n_down, scf.density, occ[0], occ[1], h)
+                torch.cuda.synchronize()
+                if i >= 3:
+                    it_s.append(time.perf_counter() - t0)
+            for t in ts:
+                t.close()
+            T_pre = statistics.median(pre_ms) / 1e3
+            T_it = statistics.median(it_s)
+            res[name] = {"precompute_s": T_pre, "iteration_s": T_it, "scf_iterations": scf.iterations, "scf_wall_s": scf_s,
+                         "energy": E, "s_per_iter": T_pre / scf.iterations + T_it,
+                         "contraction_ms": [statistics.median(k[j] for k in kern_ms) for j in range(4)]}
+    m, f = res["bf16x3"], res["fp64"]
+    # roofline of the dominant kernel (one computeV component launch of kPairTc): algorithmic flops
+    # 2 N1 N2 np per launch (np = nb (nb+1)/2 real basis-pair columns); issued slice products
+    # 6 x 2 x NBtot per pair (NBtot = np rounded up to whole 128-column chunks)
+    NB = 64 if np_ <= 64 else 128
+    nbtot = -(-np_ // NB) * NB
+    c_ms = m["contraction_ms"][2] / 3   # computeV: three component launches
+    alg = 2.0 * n * n * np_ / (c_ms / 1e3) / 1e12
+    issued = 12.0 * nbtot * n * n / (c_ms / 1e3) / 1e12
+    peak = peaks["bf16_tflops"]
+    line = {"metric": "Be-TC Fock-build s/iter (precompute amortised over the TC-SCF iterations), mixed vs FP64 GPU",
+            "value": m["s_per_iter"], "unit": "s/iter", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": m["s_per_iter"] * 1e3, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16", "data": "synthetic",
+            "config": {"workload": "Be transcorrelated HF (precompute form)", "Z": w.Z, "n_basis": w.nb,
+                       "n_up": w.n_up, "n_down": w.n_down, "points_per_grid": n, "grids": "3 scrambled-Sobol sets "
+                       f"(seeds {seed}..{seed + 2}), reference QMC map", "jastrow": "u = r12/(2(1+b r12)), b = 1, "
+                       "c = -a12/2 (opposite), -a12/4 (same)", "scf_tol": 1e-8},
+            "mixed": m, "fp64": f, "dE_mixed_vs_fp64": m["energy"] - f["energy"],
+            "precompute_speedup_vs_fp64": f["precompute_s"] / m["precompute_s"],
+            "speedup_vs_fp64": f["s_per_iter"] / m["s_per_iter"],
+            "roofline": {"bound": "tensor", "achieved": alg, "peak": peak, "unit": "TFLOP/s", "frac": alg / peak, "traffic": None,
+                         "kernel": "kPairTc (computeV component)", "peak_source": f"bf16 dense burst, {peak_kind}",
+                         "issued_tensor_tflops": issued, "issued_frac": issued / peak,
+                         "achieved_numerator": "2 N1 N2 nb(nb+1)/2 flops per launch"},
+            "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="kr", choices=["kr", "ne", "he", "batch", "scf"],
-                    help="scf: full Kr SCF to 1e-8 Eh (split BF16 and FP64, plain iteration and DIIS)")
+    ap.add_argument("--workload", default="kr", choices=["kr", "ne", "he", "batch", "scf", "be_tc"],
+                    help="scf: full Kr SCF to 1e-8 Eh (split BF16 and FP64, plain iteration and DIIS); "
+                         "be_tc: the Be transcorrelated configuration (precompute, TC SCF, per-iteration build)")
+    ap.add_argument("--qmc-points", type=int, default=0, help="override the be_tc points per grid (smaller profiling cases)")
     ap.add_argument("--diis", type=int, default=8, help="DIIS history of --workload scf")
     ap.add_argument("--scf-max-iter", type=int, default=50, help="iteration limit of --workload scf (the reference's RCS limit)")
     ap.add_argument("--precision", default="bf16x3", choices=["bf16x3", "fp64", "tf32"])
@@ -515,6 +708,8 @@ def main() -> None:
             run_batch(args, rank)
         elif args.workload == "scf":
             run_scf(args, rank)
+        elif args.workload == "be_tc":
+            run_be_tc(args, rank)
         else:
             run_ours(args, rank, world)
     finally:

@@ -83,8 +83,8 @@ typedef enum tcscf_kernel {
   TCSCF_K_GRAD_U_OPPO = 4
 } tcscf_kernel;
 
-/* Precision of the r12 contraction (the direct Fock build; the precompute form and the TC tensors
- * are FP64).  FP64: CUDA-core FP64 throughout.  BF16X3: tcgen05 tensor cores on fixed-point BF16
+/* Precision of the r12 contraction (the direct Fock build; computeF / computeV take FP64 and BF16X3).
+ * FP64: CUDA-core FP64 throughout.  BF16X3: tcgen05 tensor cores on fixed-point BF16
  * slices of every operand (24 bits for the orbital factors and the weighted basis, 16 or 24 bits for
  * g * rho; power-of-two scales per row / column / r2 block of 64), so the tensor-core sum of the
  * leading slices is exact; each block is added into double-float (FP32 hi + lo) accumulators.
@@ -112,6 +112,11 @@ typedef struct tcscf_ctx tcscf_ctx;
 int tcscf_ctx_create(int device, tcscf_ctx ** ctx);
 int tcscf_ctx_destroy(tcscf_ctx * ctx);
 const char * tcscf_last_error(tcscf_ctx * ctx);
+/* Self-test of the failure path of the library's bounded device waits (no reference counterpart):
+ * one warp waits, through the same bounded-wait helper as the tensor-core kernels, on an mbarrier that
+ * nothing arrives at, and gives up after limit_ms (1..1000) milliseconds.  Returns TCSCF_ERR_TIMEOUT,
+ * the expected outcome; the context stays usable afterwards. */
+int tcscf_selftest_bounded_wait(tcscf_ctx * ctx, double limit_ms);
 /* the context's cudaStream_t, for callers that time or order work around it */
 int tcscf_ctx_stream(tcscf_ctx * ctx, void ** stream);
 int tcscf_synchronize(tcscf_ctx * ctx);
@@ -174,17 +179,24 @@ int tcscf_overlap_core_quadrature(tcscf_ctx * ctx, int grid, int Z, double * S, 
 /* Same quadrature with no device allocation: the block results use a fixed 2 MiB device array
  * (nb <= 256, else TCSCF_ERR_UNSUPPORTED), for callers that cannot allocate device memory at that
  * point (device memory already handed to their own pool, or no device-wide synchronisation allowed).
- * The first call on a device sets up the array's address and should come before any stream capture;
+ * tcscf_ctx_create looks up the array's address on its device, so calls do no set-up of their own;
  * overlapping calls on one device share the array and race.  No counterpart in the reference. */
 int tcscf_overlap_core_quadrature_static(tcscf_ctx * ctx, int grid, int Z, double * S, double * H);
 
 /* ---- r12 kernel contractions (precompute form) --------------------------------------------- */
 /* precomputeIntegrand + computeF (HartreeFock.hpp:23-180): F written to host memory in the Fji
  * layout (complex for a 3-D r2 grid, real x 2 pi for a 2-D r2 grid).  When keep != 0 the result also
- * stays on the device as handle *fji for tcscf_fock_build_precomputed. */
-int tcscf_compute_F(tcscf_ctx * ctx, int r1, int r2, int kernel, const tcscf_ochi * jastrow, double * F, int keep, int * fji);
-/* precomputeIntegrand + computeV (HartreeFock.hpp:55-83, :185-229), vector kernels only */
-int tcscf_compute_V(tcscf_ctx * ctx, int r1, int r2, int kernel, const tcscf_ochi * jastrow, double * V, int keep, int * vji);
+ * stays on the device as handle *fji for tcscf_fock_build_precomputed / tcscf_tc_fock_build.
+ * precision: TCSCF_PREC_FP64, or TCSCF_PREC_BF16X3 (the r12 kernel-GEMM on the tensor cores in the
+ * split-BF16 scheme of the Fock build, kernel values generated in FP32 from FP32 coordinates; the
+ * Jastrow factor of a TC kernel must depend on r12 alone, every term S[k] = (i, 0, 0), as the
+ * reference's own TC driver uses it, HartreeFockTest.cpp:351-360). */
+int tcscf_compute_F(tcscf_ctx * ctx, int r1, int r2, int kernel, const tcscf_ochi * jastrow, int precision, double * F, int keep,
+                    int * fji);
+/* precomputeIntegrand + computeV (HartreeFock.hpp:55-83, :185-229), vector kernels only; precision as
+ * for tcscf_compute_F */
+int tcscf_compute_V(tcscf_ctx * ctx, int r1, int r2, int kernel, const tcscf_ochi * jastrow, int precision, double * V, int keep,
+                    int * vji);
 int tcscf_tensor_destroy(tcscf_ctx * ctx, int handle);
 
 /* ---- 4- and 6-index tensors (integrateAll.hpp:147-442) --------------------------------------- */

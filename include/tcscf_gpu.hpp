@@ -255,18 +255,19 @@ inline std::pair<std::vector<cplx>, std::vector<cplx>> overlapCoreQuadrature(QMC
 // precomputeIntegrand + computeF (HartreeFock.hpp:23-180): scalar kernels; kept on the device for
 // the precompute-form Fock build and the TC SCF
 inline DeviceTensor computeF(QMCGrid const & r1Grid, QMCGrid const & r2Grid, tcscf_kernel kernel = TCSCF_K_INV_R12,
-                             tcscf_ochi const * jastrow = nullptr)
+                             tcscf_ochi const * jastrow = nullptr, tcscf_precision precision = TCSCF_PREC_FP64)
 {
   int h = 0;
-  check(tcscf_compute_F(r1Grid.context(), r1Grid.id(), r2Grid.id(), kernel, jastrow, nullptr, 1, &h), r1Grid.context());
+  check(tcscf_compute_F(r1Grid.context(), r1Grid.id(), r2Grid.id(), kernel, jastrow, precision, nullptr, 1, &h), r1Grid.context());
   return DeviceTensor(r1Grid.context(), h);
 }
 
 // precomputeIntegrand + computeV (HartreeFock.hpp:55-83, 185-229): vector kernels, on the device
-inline DeviceTensor computeV(QMCGrid const & r1Grid, QMCGrid const & r2Grid, tcscf_kernel kernel, tcscf_ochi const & jastrow)
+inline DeviceTensor computeV(QMCGrid const & r1Grid, QMCGrid const & r2Grid, tcscf_kernel kernel, tcscf_ochi const & jastrow,
+                             tcscf_precision precision = TCSCF_PREC_FP64)
 {
   int h = 0;
-  check(tcscf_compute_V(r1Grid.context(), r1Grid.id(), r2Grid.id(), kernel, &jastrow, nullptr, 1, &h), r1Grid.context());
+  check(tcscf_compute_V(r1Grid.context(), r1Grid.id(), r2Grid.id(), kernel, &jastrow, precision, nullptr, 1, &h), r1Grid.context());
   return DeviceTensor(r1Grid.context(), h);
 }
 

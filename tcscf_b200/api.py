@@ -191,8 +191,10 @@ class DeviceTensor:
 
 
 def computeF(r1Grid: QMCGrid, r2Grid: QMCGrid, kernel: int = ffi.K_INV_R12, jastrow: ffi.Ochi | None = None,
-             keep: bool = False, copy: bool = True):
-    """precomputeIntegrand + computeF: Fji [N1][nb][nb] (complex for a 3-D r2 grid, real x 2 pi for 2-D)."""
+             keep: bool = False, copy: bool = True, precision: int = ffi.PREC_FP64):
+    """precomputeIntegrand + computeF: Fji [N1][nb][nb] (complex for a 3-D r2 grid, real x 2 pi for 2-D).
+    precision: PREC_FP64 or PREC_BF16X3 (tensor-core kernel-GEMM; TC kernels need a Jastrow factor of
+    r12 alone)."""
     ctx = r1Grid.ctx
     n1, nb = r1Grid.nGrid(), r1Grid.nBasis()
     F = None
@@ -200,18 +202,19 @@ def computeF(r1Grid: QMCGrid, r2Grid: QMCGrid, kernel: int = ffi.K_INV_R12, jast
         F = np.empty((n1, nb, nb), dtype=np.complex128 if r2Grid.quadratureGrid.ndim == 3 else np.float64)
     h = C.c_int()
     _raise(ffi.lib().tcscf_compute_F(ctx.handle, r1Grid.id, r2Grid.id, kernel, C.byref(jastrow) if jastrow else None,
-                                     ffi.dptr(F), int(keep), C.byref(h)), ctx.handle)
+                                     int(precision), ffi.dptr(F), int(keep), C.byref(h)), ctx.handle)
     return (F, DeviceTensor(ctx, h.value)) if keep else F
 
 
-def computeV(r1Grid: QMCGrid, r2Grid: QMCGrid, kernel: int, jastrow: ffi.Ochi, keep: bool = False, copy: bool = True):
-    """precomputeIntegrand + computeV: Vji [N1][nb][nb][3] complex."""
+def computeV(r1Grid: QMCGrid, r2Grid: QMCGrid, kernel: int, jastrow: ffi.Ochi, keep: bool = False, copy: bool = True,
+             precision: int = ffi.PREC_FP64):
+    """precomputeIntegrand + computeV: Vji [N1][nb][nb][3] complex (precision as for computeF)."""
     ctx = r1Grid.ctx
     n1, nb = r1Grid.nGrid(), r1Grid.nBasis()
     V = np.empty((n1, nb, nb, 3), dtype=np.complex128) if copy else None
     h = C.c_int()
-    _raise(ffi.lib().tcscf_compute_V(ctx.handle, r1Grid.id, r2Grid.id, kernel, C.byref(jastrow), ffi.dptr(V), int(keep),
-                                     C.byref(h)), ctx.handle)
+    _raise(ffi.lib().tcscf_compute_V(ctx.handle, r1Grid.id, r2Grid.id, kernel, C.byref(jastrow), int(precision), ffi.dptr(V),
+                                     int(keep), C.byref(h)), ctx.handle)
     return (V, DeviceTensor(ctx, h.value)) if keep else V
 
 

@@ -108,10 +108,19 @@ def ne() -> Workload:
 
 
 def be_tc() -> Workload:
-    """Be, Z=4, transcorrelated: 12 s (0.4*1.8^k) + 4 p x 3 (0.4*1.8^k); 2^16 Sobol points per coordinate."""
+    """Be, Z=4, transcorrelated: 12 s (0.4*1.8^k) + 4 p x 3 (0.4*1.8^k); 2^16 Sobol points per coordinate
+    on three independent grids (seeds seed, seed+1, seed+2: r1, r2 for the scalar kernels, r3 for grad u)."""
     basis = expand(0, [0.4 * 1.8 ** k for k in range(12)]) + expand(1, [0.4 * 1.8 ** k for k in range(4)])
     return Workload("Be-TC", 4, basis, n_up=2, n_down=2, qmc_points=1 << 16,
                     extra={"b": 1.0, "seed": 20261203})
+
+
+def be_tc_jastrow(w: Workload) -> dict:
+    """u(r12) = r12 / (2 (1 + b r12)) as an Ochi factor of r12 alone: S = {(1, 0, 0)}, a12 = 1/b, in the
+    sign convention of the reference's TC driver (HartreeFockTest.cpp:351-360): c = -a12/2 for opposite
+    spins and -a12/4 for equal spins.  a (the r1 / r2 scale) does not enter; it is set to a12."""
+    a12 = 1.0 / w.extra["b"]
+    return dict(a=a12, a12=a12, terms=[((1, 0, 0), -a12 / 2, -a12 / 4)])
 
 
 def kr() -> Workload:

@@ -424,8 +424,10 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             y = f2fma(f2mul(y, mHalf), em, y);
             float ya, yb;
             f2unpack(y, ya, yb);
-            ya = r2a > 0.0f ? ya : 0.0f;                // coincident pair contributes 0
-            yb = r2b > 0.0f ? yb : 0.0f;
+            // a coincident pair contributes 0; so does a separation whose square is subnormal, which
+            // rsqrt.approx.ftz flushes to 0 (its estimate +inf would turn the Newton step into NaN)
+            ya = r2a >= kMinNormal ? ya : 0.0f;
+            yb = r2b >= kMinNormal ? yb : 0.0f;
             y = f2pack(ya, yb);
             vsum2 = f2fma(y, f2pack(qb.z, qb.w), vsum2);
             float2 const a2 = sa[pr];
@@ -732,6 +734,27 @@ int packVt(tcscf_ctx * ctx, int64_t n2, int64_t n2pad, int nb, int NB, const dou
 }
 
 }  // namespace
+
+size_t packedVtOperandBytes(int NB, int64_t n2pad) { return packedVtBytes(NB, n2pad); }
+
+int packVtOperand(tcscf_ctx * ctx, int64_t n2, int64_t n2pad, int nb, int NB, const double * V, int ldv, void * out)
+{
+  return packVt(ctx, n2, n2pad, nb, NB, V, ldv, out);
+}
+
+int packPointsFp32(tcscf_ctx * ctx, int64_t n, int64_t npad, const double * pts, float4 * out)
+{
+  tc::kPackCoords<<<gridBlocks(npad, 256), 256, 0, ctx->stream>>>(n, npad, pts, out);
+  TCSCF_LAUNCH(ctx);
+  return TCSCF_OK;
+}
+
+int packPointPairsFp32(tcscf_ctx * ctx, int64_t n, int64_t npad, const double * pts, const double * coul, float4 * out)
+{
+  tc::kPackCoordPairs<<<gridBlocks(npad / 2, 256), 256, 0, ctx->stream>>>(n, npad, pts, coul, out);
+  TCSCF_LAUNCH(ctx);
+  return TCSCF_OK;
+}
 
 int tensorPackedV(tcscf_ctx * ctx, Grid & g2, const double * V, double scale, const void ** packed)
 {
@@ -1128,6 +1151,42 @@ int contractTensor(tcscf_ctx * ctx, Contraction const & c, int precision)
     }
   }
   cudaEventRecord(ctx->ev[3], ctx->stream);
+  return TCSCF_OK;
+}
+
+namespace tc {
+
+// The failure path of the bounded waits: lane 0 of one warp waits through waitBarLimit on an
+// mbarrier that nothing arrives at (its phase 0 never completes); the wait gives up after limitNs,
+// records code 90 in the status word and the kernel returns.
+__global__ void kBoundedWaitSelfTest(unsigned long long limitNs, int * status)
+{
+  __shared__ uint64_t bar;
+  __shared__ int abortWord;
+  if (threadIdx.x == 0) {
+    mbarInit(&bar, 1);
+    abortWord = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncwarp();
+  if (threadIdx.x == 0) waitBarLimit(&bar, 0, &abortWord, status, 90, limitNs);
+  __syncwarp();
+}
+
+}  // namespace tc
+
+int boundedWaitSelfTest(tcscf_ctx * ctx, double limitMs)
+{
+  TCSCF_CHECK(ctx, limitMs >= 1.0 && limitMs <= 1000.0, TCSCF_ERR_INVALID_ARGUMENT, "limit_ms must be in [1, 1000]");
+  int * dStatus = nullptr;
+  TCSCF_TRY(scratch(ctx, "wait_selftest", sizeof(int), reinterpret_cast<void **>(&dStatus)));
+  TCSCF_CUDA(ctx, cudaMemsetAsync(dStatus, 0, sizeof(int), ctx->stream));
+  tc::kBoundedWaitSelfTest<<<1, 32, 0, ctx->stream>>>((unsigned long long)(limitMs * 1e6), dStatus);
+  TCSCF_LAUNCH(ctx);
+  int st = 0;
+  TCSCF_CUDA(ctx, cudaMemcpyAsync(&st, dStatus, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (st != 0) return fail(ctx, TCSCF_ERR_TIMEOUT, "bounded wait expired (code " + std::to_string(st) + ")");
   return TCSCF_OK;
 }
 

@@ -238,7 +238,7 @@ int tcscf_integrate_all_r1r2(tcscf_ctx * ctx, int r1, int r2, int use_gradient, 
   int fid = 0;
   double * B = nullptr;
   if (!use_gradient) {
-    TCSCF_TRY(tcscf_compute_F(ctx, r1, r2, kernel, jastrow, nullptr, 1, &fid));
+    TCSCF_TRY(tcscf_compute_F(ctx, r1, r2, kernel, jastrow, TCSCF_PREC_FP64, nullptr, 1, &fid));
     B = ctx->tensors[fid].d;
   }
   size_t const bytesA = sizeof(double2) * size_t(n1) * nn;
@@ -306,7 +306,7 @@ int tcscf_three_electron_integrals(tcscf_ctx * ctx, int r1, int r2, const tcscf_
   cublasHandle_t h = nullptr;
   TCSCF_TRY(blasHandle(ctx, &h));
   int vid = 0;
-  TCSCF_TRY(tcscf_compute_V(ctx, r1, r2, TCSCF_K_GRAD_U_SAME, jastrow, nullptr, 1, &vid));
+  TCSCF_TRY(tcscf_compute_V(ctx, r1, r2, TCSCF_K_GRAD_U_SAME, jastrow, TCSCF_PREC_FP64, nullptr, 1, &vid));
   const double2 * V = reinterpret_cast<const double2 *>(ctx->tensors[vid].d);
   // r1 chunk so that the (q,t,r,u) operand stays below ~1 GB
   int64_t const chunk = std::max<int64_t>(1, std::min<int64_t>(n1, (int64_t(1) << 26) / n4));

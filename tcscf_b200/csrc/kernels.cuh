@@ -34,12 +34,22 @@ struct Contraction {
 
 int contractFp64(tcscf_ctx * ctx, Contraction const & c);
 
+// one warp waits through the tensor kernels' bounded-wait helper on an mbarrier that nothing arrives
+// at, for limitMs; returns TCSCF_ERR_TIMEOUT when the wait gave up (the expected outcome)
+int boundedWaitSelfTest(tcscf_ctx * ctx, double limitMs);
+
 // the context's cuBLAS handle (created on first use), bound to the context stream
 int blasHandle(tcscf_ctx * ctx, cublasHandle_t * out);
 
 // tensor-core (tcgen05) contraction of the same quantity for g = 1/r12: split-BF16 (flash_tc.cu) or
 // TF32 (flash_tf32.cu)
 int contractTensor(tcscf_ctx * ctx, Contraction const & c, int precision);
+// tensor-core precompute form (flash_pairs.cu): T[r1][p] = sum_r2 g(r1,r2) V[r2][p] with rho == 1
+// (c.R == 0) for the kernel c.kernel (component c.component of a vector kernel), g generated in FP32
+// and contracted in the split-BF16 scheme of the Fock build; TC kernels need a Jastrow factor of r12
+// alone
+bool pairsTensorAvailable(Contraction const & c, int precision, std::string * why);
+int contractPairsTensor(tcscf_ctx * ctx, Contraction const & c, int precision);
 // r2 split counts the autotuner measures for a tensor-path launch over n1 x n2 points on sms SMs:
 // the default rule's count first, then 1, 2, 3, 4, 6 and 8 where every split keeps at least 16
 // r2 blocks of 64 points (effective counts after rounding the blocks per split, no repeats)

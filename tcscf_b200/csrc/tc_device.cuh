@@ -20,6 +20,7 @@ constexpr int NTHREADS = 384;  // warpgroup 0: TMA, MMA, 2 idle warps; warpgroup
 constexpr int kRegsLaunch = 168, kRegsProducer = 56, kRegsCompute = 224;
 static_assert(128 * kRegsProducer + 256 * kRegsCompute <= NTHREADS * kRegsLaunch, "register split exceeds the launch allocation");
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s per wait
+constexpr float kMinNormal = 1.17549435e-38f;                // smallest normal FP32 (2^-126)
 // a waiting thread sleeps in mbarrier.try_wait (woken when the phase completes) instead of spinning
 // on the issue slots the compute warps need
 constexpr uint32_t kSuspendHintNs = 1000000;
@@ -80,21 +81,26 @@ __device__ __forceinline__ bool mbarTryWait(uint64_t * b, uint32_t parity)
   return ok != 0;
 }
 
-// Bounded wait; returns false (after recording the failure) when the limit expires or another role
-// has already aborted.
-__device__ __forceinline__ bool waitBar(uint64_t * b, uint32_t parity, volatile int * abortFlag, int * status, int code)
+// Bounded wait; returns false (after recording the failure) when limitNs of wall-clock time pass or
+// another role has already aborted.
+__device__ __forceinline__ bool waitBarLimit(uint64_t * b, uint32_t parity, volatile int * abortFlag, int * status, int code,
+                                             unsigned long long limitNs)
 {
   if (mbarTryWait(b, parity)) return true;
   unsigned long long const t0 = globalTimer();
   while (true) {
     if (mbarTryWait(b, parity)) return true;
     if (*abortFlag) return false;
-    if (globalTimer() - t0 > kWaitLimitNs) {
+    if (globalTimer() - t0 > limitNs) {
       *abortFlag = 1;
       atomicCAS(status, 0, code);
       return false;
     }
   }
+}
+__device__ __forceinline__ bool waitBar(uint64_t * b, uint32_t parity, volatile int * abortFlag, int * status, int code)
+{
+  return waitBarLimit(b, parity, abortFlag, status, code, kWaitLimitNs);
 }
 
 __device__ __forceinline__ void tmaLoad2d(void * dst, const CUtensorMap * map, int x, int y, uint64_t * bar)
@@ -220,6 +226,16 @@ __device__ __forceinline__ uint32_t sw128(int row, int chunk)
 size_t tf32OperandBytes(int NB, int64_t n1pad, int64_t n2pad);
 int tf32PackOperands(tcscf_ctx * ctx, Contraction const & c, int NB, int64_t n1pad, int64_t n2pad, void * dst, CUtensorMap * maps);
 int launchTf32(tcscf_ctx * ctx, int NB, tc::Params const & P, int grid);
+
+// operand packing shared by the tensor kernels (flash_tc.cu): the transposed fixed-point BF16 slices
+// h / m / l/256 [NB][n2pad] of V [n2][ldv] (nb real columns) followed by the per-(r2 block, column)
+// inverse scales [n2pad/64][NB]; points [3][n] as FP32 float4 {x, y, z, 0} [npad]; points in pairs
+// {x0,x1,y0,y1}{z0,z1,c0,c1} [npad] with the Coulomb source c (0 when coul is null).  Padding points
+// sit far away.
+size_t packedVtOperandBytes(int NB, int64_t n2pad);
+int packVtOperand(tcscf_ctx * ctx, int64_t n2, int64_t n2pad, int nb, int NB, const double * V, int ldv, void * out);
+int packPointsFp32(tcscf_ctx * ctx, int64_t n, int64_t npad, const double * pts, float4 * out);
+int packPointPairsFp32(tcscf_ctx * ctx, int64_t n, int64_t npad, const double * pts, const double * coul, float4 * out);
 
 // cuTensorMapEncodeTiled from the CUDA driver API (null when unavailable)
 using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *, const cuuint64_t *,

@@ -1293,6 +1293,87 @@ int validateBasis(tcscf_ctx * ctx, const tcscf_sto * basis, int nb, std::vector<
   return TCSCF_OK;
 }
 
+// precomputeIntegrand + computeF / computeV (HartreeFock.hpp:23-229): the weighted basis-pair products
+// of the r2 grid (real-harmonic basis, k <= l) contracted with the r12 kernel (ncomp = 1: a scalar
+// kernel; 3: the components of grad_1 u) in the requested precision, then mapped to the reference's
+// complex Fji / Vji layout; written to host memory (out) and / or kept on the device as a handle.
+int precomputeTensor(tcscf_ctx * ctx, int r1, int r2, int kernel, const tcscf_ochi * jastrow, int precision, int ncomp, double * out,
+                     int keep, int * handle)
+{
+  Grid * g1 = findGrid(ctx, r1);
+  Grid * g2 = findGrid(ctx, r2);
+  TCSCF_TRY(checkBasisPair(ctx, g1, g2));
+  TCSCF_CHECK(ctx, !jastrow || (jastrow->nterms >= 0 && jastrow->nterms <= 8), TCSCF_ERR_INVALID_ARGUMENT, "at most 8 Jastrow terms");
+  TCSCF_CHECK(ctx, out || keep, TCSCF_ERR_INVALID_ARGUMENT, "nothing to do");
+  TCSCF_CHECK(ctx, ncomp == 1 || g2->ndim == 3, TCSCF_ERR_INVALID_ARGUMENT, "computeV needs a 3-D r2 grid");
+  TCSCF_CHECK(ctx, precision == TCSCF_PREC_FP64 || precision == TCSCF_PREC_BF16X3, TCSCF_ERR_UNSUPPORTED,
+              "computeF / computeV run in FP64 or BF16X3");
+  int const nb = g1->nb;
+  int const np = nb * (nb + 1) / 2;
+  int64_t const n1 = g1->n, n2 = g2->n;
+  bool const realOut = ncomp == 1 && g2->ndim == 2;
+  double const scale = realOut ? 2 * kPi : 1.0;
+  Contraction c;
+  c.n1 = n1; c.n2 = n2; c.R = 0; c.ncol = np; c.p1 = g1->pts; c.p2 = g2->pts; c.ldv = np; c.ldt = np;
+  c.kernel = kernel; c.jastrow = jastrow;
+  if (precision != TCSCF_PREC_FP64) {
+    std::string why;
+    TCSCF_CHECK(ctx, pairsTensorAvailable(c, precision, &why), TCSCF_ERR_UNSUPPORTED, why);
+  }
+  void * p = nullptr;
+  TCSCF_TRY(scratch(ctx, "computeF", sizeof(double) * (size_t(n2) * np + size_t(n1) * np), &p));
+  double * pairs = static_cast<double *>(p);
+  double * FR = pairs + size_t(n2) * np;
+  size_t const outElems = size_t(n1) * nb * nb * (realOut ? 1 : 2) * ncomp;
+  double * dOut = nullptr;
+  TCSCF_CUDA(ctx, cudaMalloc(&dOut, sizeof(double) * outElems));
+  cudaEventRecord(ctx->ev[0], ctx->stream);
+  int const launch0 = ctx->launchCount;
+  kPairProducts<<<gridBlocks(n2 * np, 256), 256, 0, ctx->stream>>>(n2, nb, g2->phiR, g2->w, scale, pairs);
+  ctx->launchCount++;
+  int st = TCSCF_OK;
+  if (cudaError_t const e = cudaGetLastError(); e != cudaSuccess)   // dOut is released below
+    st = fail(ctx, TCSCF_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+  c.V = pairs;
+  c.T = FR;
+  float contraction = 0;
+  for (int comp = 0; comp < ncomp && st == TCSCF_OK; ++comp) {
+    c.component = comp;
+    // the contraction alone is bracketed by ev[2] / ev[3]; tcscf_last_timing reports the components' sum
+    cudaEventRecord(ctx->ev[2], ctx->stream);
+    st = precision == TCSCF_PREC_FP64 ? contractFp64(ctx, c) : contractPairsTensor(ctx, c, precision);
+    cudaEventRecord(ctx->ev[3], ctx->stream);
+    if (st == TCSCF_OK) {
+      kPairsToReference<<<gridBlocks(n1 * nb * nb, 256), 256, 0, ctx->stream>>>(n1, nb, g1->dsto, FR, ncomp, comp, realOut ? 1 : 0, dOut);
+      ctx->launchCount++;
+      cudaError_t const e = cudaGetLastError();
+      if (e != cudaSuccess) st = fail(ctx, TCSCF_ERR_CUDA, cudaGetErrorString(e));
+    }
+    cudaStreamSynchronize(ctx->stream);
+    float a = 0;
+    cudaEventElapsedTime(&a, ctx->ev[2], ctx->ev[3]);
+    contraction += a;
+  }
+  if (st == TCSCF_OK && out) {
+    cudaError_t const e = cudaMemcpyAsync(out, dOut, sizeof(double) * outElems, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e != cudaSuccess) st = fail(ctx, TCSCF_ERR_CUDA, cudaGetErrorString(e));
+  }
+  cudaEventRecord(ctx->ev[1], ctx->stream);
+  cudaStreamSynchronize(ctx->stream);
+  float b = 0;
+  cudaEventElapsedTime(&b, ctx->ev[0], ctx->ev[1]);
+  ctx->lastContractionMs = contraction;
+  ctx->lastTotalMs = b;
+  ctx->lastLaunches = ctx->launchCount - launch0;
+  if (st != TCSCF_OK || !keep) { cudaFree(dOut); return st; }
+  Tensor t;
+  t.d = dOut; t.n1 = n1; t.nb = nb; t.isComplex = realOut ? 0 : 1; t.vec = ncomp == 3 ? 1 : 0;
+  int const id = ctx->nextId++;
+  ctx->tensors[id] = t;
+  if (handle) *handle = id;
+  return TCSCF_OK;
+}
+
 }  // namespace
 }  // namespace tcscf
 
@@ -1336,6 +1417,14 @@ int tcscf_ctx_create(int device, tcscf_ctx ** out)
     return TCSCF_ERR_CUDA;
   }
   cusolverDnSetStream(ctx->solver, ctx->stream);
+  // the fixed array of tcscf_overlap_core_quadrature_static: its address is looked up here, where
+  // allocation is allowed anyway (a lazily loaded module may allocate its globals on first use), so
+  // the entry point itself never does set-up work
+  double2 * fixedScratch = nullptr;
+  if (quadStaticScratch(ctx, &fixedScratch) != TCSCF_OK) {
+    tcscf_ctx_destroy(ctx);
+    return TCSCF_ERR_CUDA;
+  }
   *out = ctx;
   return TCSCF_OK;
 }
@@ -1396,6 +1485,13 @@ int tcscf_autotune_split_candidates(int64_t n1, int64_t n2, int sms, int * split
   for (int i = 0; i < n; ++i) splits[i] = c[i];
   *count = n;
   return TCSCF_OK;
+}
+
+int tcscf_selftest_bounded_wait(tcscf_ctx * ctx, double limit_ms)
+{
+  if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
+  TCSCF_CUDA(ctx, cudaSetDevice(ctx->device));
+  return boundedWaitSelfTest(ctx, limit_ms);
 }
 
 int tcscf_ctx_stream(tcscf_ctx * ctx, void ** stream)
@@ -1543,8 +1639,8 @@ int tcscf_overlap_core_quadrature(tcscf_ctx * ctx, int grid, int Z, double * S, 
 // synchronisation that cudaFree implies while its other streams are running.
 //   * Limit: nb <= kQuadStaticMaxNb (256), i.e. 2 x 256 x 256 complex doubles = 2 MiB per device;
 //     larger bases are rejected with TCSCF_ERR_UNSUPPORTED.
-//   * Set-up: the first call on a device looks up the array's device address with that device
-//     current (cudaGetSymbolAddress); make that first call before any stream capture.
+//   * Set-up: tcscf_ctx_create looks up the array's device address (cudaGetSymbolAddress, with the
+//     context's device current), so a call of this entry point does no set-up of its own.
 //   * Sharing: every call on a device uses the same array, so overlapping calls on one device (other
 //     streams or other contexts) race; callers serialise them.  Nothing in the array needs to start
 //     at zero: kQuadOverlapCore writes every element it returns (one block per (i, j)).
@@ -1628,136 +1724,26 @@ int tcscf_fock_build_device(tcscf_ctx * ctx, int r1, int r2, int nspin, const do
   return TCSCF_OK;
 }
 
-int tcscf_compute_F(tcscf_ctx * ctx, int r1, int r2, int kernel, const tcscf_ochi * jastrow, double * F, int keep, int * fji)
+int tcscf_compute_F(tcscf_ctx * ctx, int r1, int r2, int kernel, const tcscf_ochi * jastrow, int precision, double * F, int keep,
+                    int * fji)
 {
   TCSCF_NVTX();
   if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
   cudaSetDevice(ctx->device);
-  Grid * g1 = findGrid(ctx, r1);
-  Grid * g2 = findGrid(ctx, r2);
-  TCSCF_TRY(checkBasisPair(ctx, g1, g2));
   TCSCF_CHECK(ctx, kernel >= TCSCF_K_INV_R12 && kernel <= TCSCF_K_TC_SCALAR_OPPO, TCSCF_ERR_INVALID_ARGUMENT, "computeF takes a scalar kernel");
   TCSCF_CHECK(ctx, kernel == TCSCF_K_INV_R12 || jastrow, TCSCF_ERR_INVALID_ARGUMENT, "TC kernels need the Jastrow parameters");
-  TCSCF_CHECK(ctx, !jastrow || (jastrow->nterms >= 0 && jastrow->nterms <= 8), TCSCF_ERR_INVALID_ARGUMENT, "at most 8 Jastrow terms");
-  TCSCF_CHECK(ctx, F || keep, TCSCF_ERR_INVALID_ARGUMENT, "nothing to do");
-  int const nb = g1->nb;
-  int const np = nb * (nb + 1) / 2;
-  int64_t const n1 = g1->n, n2 = g2->n;
-  bool const realOut = g2->ndim == 2;
-  double const scale = realOut ? 2 * kPi : 1.0;
-  void * p = nullptr;
-  TCSCF_TRY(scratch(ctx, "computeF", sizeof(double) * (size_t(n2) * np + size_t(n1) * np), &p));
-  double * pairs = static_cast<double *>(p);
-  double * FR = pairs + size_t(n2) * np;
-  size_t const outElems = size_t(n1) * nb * nb * (realOut ? 1 : 2);
-  double * dOut = nullptr;
-  TCSCF_CUDA(ctx, cudaMalloc(&dOut, sizeof(double) * outElems));
-  cudaEventRecord(ctx->ev[0], ctx->stream);
-  int const launch0 = ctx->launchCount;
-  kPairProducts<<<gridBlocks(n2 * np, 256), 256, 0, ctx->stream>>>(n2, nb, g2->phiR, g2->w, scale, pairs);
-  ctx->launchCount++;
-  int st = TCSCF_OK;
-  if (cudaError_t const e = cudaGetLastError(); e != cudaSuccess)   // dOut is released below
-    st = fail(ctx, TCSCF_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
-  Contraction c;
-  c.n1 = n1; c.n2 = n2; c.R = 0; c.ncol = np; c.p1 = g1->pts; c.p2 = g2->pts; c.V = pairs; c.ldv = np; c.T = FR; c.ldt = np;
-  c.kernel = kernel; c.jastrow = jastrow;
-  cudaEventRecord(ctx->ev[2], ctx->stream);
-  if (st == TCSCF_OK) st = contractFp64(ctx, c);
-  cudaEventRecord(ctx->ev[3], ctx->stream);
-  if (st == TCSCF_OK) {
-    kPairsToReference<<<gridBlocks(n1 * nb * nb, 256), 256, 0, ctx->stream>>>(n1, nb, g1->dsto, FR, 1, 0, realOut ? 1 : 0, dOut);
-    cudaError_t const e = cudaGetLastError();
-    if (e != cudaSuccess) st = fail(ctx, TCSCF_ERR_CUDA, cudaGetErrorString(e));
-    ctx->launchCount++;
-  }
-  if (st == TCSCF_OK && F) {
-    cudaError_t const e = cudaMemcpyAsync(F, dOut, sizeof(double) * outElems, cudaMemcpyDeviceToHost, ctx->stream);
-    if (e != cudaSuccess) st = fail(ctx, TCSCF_ERR_CUDA, cudaGetErrorString(e));
-  }
-  cudaEventRecord(ctx->ev[1], ctx->stream);
-  cudaStreamSynchronize(ctx->stream);
-  float a = 0, b = 0;
-  cudaEventElapsedTime(&a, ctx->ev[2], ctx->ev[3]);
-  cudaEventElapsedTime(&b, ctx->ev[0], ctx->ev[1]);
-  ctx->lastContractionMs = a;
-  ctx->lastTotalMs = b;
-  ctx->lastLaunches = ctx->launchCount - launch0;
-  if (st != TCSCF_OK || !keep) { cudaFree(dOut); return st; }
-  Tensor t;
-  t.d = dOut; t.n1 = n1; t.nb = nb; t.isComplex = realOut ? 0 : 1; t.vec = 0;
-  int const id = ctx->nextId++;
-  ctx->tensors[id] = t;
-  if (fji) *fji = id;
-  return TCSCF_OK;
+  return precomputeTensor(ctx, r1, r2, kernel, jastrow, precision, 1, F, keep, fji);
 }
 
-int tcscf_compute_V(tcscf_ctx * ctx, int r1, int r2, int kernel, const tcscf_ochi * jastrow, double * V, int keep, int * vji)
+int tcscf_compute_V(tcscf_ctx * ctx, int r1, int r2, int kernel, const tcscf_ochi * jastrow, int precision, double * V, int keep,
+                    int * vji)
 {
   TCSCF_NVTX();
   if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
   cudaSetDevice(ctx->device);
-  Grid * g1 = findGrid(ctx, r1);
-  Grid * g2 = findGrid(ctx, r2);
-  TCSCF_TRY(checkBasisPair(ctx, g1, g2));
-  TCSCF_CHECK(ctx, g2->ndim == 3, TCSCF_ERR_INVALID_ARGUMENT, "computeV needs a 3-D r2 grid");
   TCSCF_CHECK(ctx, kernel == TCSCF_K_GRAD_U_SAME || kernel == TCSCF_K_GRAD_U_OPPO, TCSCF_ERR_INVALID_ARGUMENT, "computeV takes a vector kernel");
-  TCSCF_CHECK(ctx, jastrow && jastrow->nterms >= 0 && jastrow->nterms <= 8, TCSCF_ERR_INVALID_ARGUMENT, "Jastrow parameters required");
-  TCSCF_CHECK(ctx, V || keep, TCSCF_ERR_INVALID_ARGUMENT, "nothing to do");
-  int const nb = g1->nb;
-  int const np = nb * (nb + 1) / 2;
-  int64_t const n1 = g1->n, n2 = g2->n;
-  void * p = nullptr;
-  TCSCF_TRY(scratch(ctx, "computeF", sizeof(double) * (size_t(n2) * np + size_t(n1) * np), &p));
-  double * pairs = static_cast<double *>(p);
-  double * FR = pairs + size_t(n2) * np;
-  size_t const outElems = size_t(n1) * nb * nb * 3 * 2;
-  double * dOut = nullptr;
-  TCSCF_CUDA(ctx, cudaMalloc(&dOut, sizeof(double) * outElems));
-  cudaEventRecord(ctx->ev[0], ctx->stream);
-  int const launch0 = ctx->launchCount;
-  kPairProducts<<<gridBlocks(n2 * np, 256), 256, 0, ctx->stream>>>(n2, nb, g2->phiR, g2->w, 1.0, pairs);
-  ctx->launchCount++;
-  int st = TCSCF_OK;
-  if (cudaError_t const e = cudaGetLastError(); e != cudaSuccess)   // dOut is released below
-    st = fail(ctx, TCSCF_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
-  float contraction = 0;
-  for (int comp = 0; comp < 3 && st == TCSCF_OK; ++comp) {
-    Contraction c;
-    c.n1 = n1; c.n2 = n2; c.R = 0; c.ncol = np; c.p1 = g1->pts; c.p2 = g2->pts; c.V = pairs; c.ldv = np; c.T = FR; c.ldt = np;
-    c.kernel = kernel; c.component = comp; c.jastrow = jastrow;
-    cudaEventRecord(ctx->ev[2], ctx->stream);
-    st = contractFp64(ctx, c);
-    cudaEventRecord(ctx->ev[3], ctx->stream);
-    if (st == TCSCF_OK) {
-      kPairsToReference<<<gridBlocks(n1 * nb * nb, 256), 256, 0, ctx->stream>>>(n1, nb, g1->dsto, FR, 3, comp, 0, dOut);
-      ctx->launchCount++;
-      cudaError_t const e = cudaGetLastError();
-      if (e != cudaSuccess) st = fail(ctx, TCSCF_ERR_CUDA, cudaGetErrorString(e));
-    }
-    cudaStreamSynchronize(ctx->stream);
-    float a = 0;
-    cudaEventElapsedTime(&a, ctx->ev[2], ctx->ev[3]);
-    contraction += a;
-  }
-  if (st == TCSCF_OK && V) {
-    cudaError_t const e = cudaMemcpyAsync(V, dOut, sizeof(double) * outElems, cudaMemcpyDeviceToHost, ctx->stream);
-    if (e != cudaSuccess) st = fail(ctx, TCSCF_ERR_CUDA, cudaGetErrorString(e));
-  }
-  cudaEventRecord(ctx->ev[1], ctx->stream);
-  cudaStreamSynchronize(ctx->stream);
-  float b = 0;
-  cudaEventElapsedTime(&b, ctx->ev[0], ctx->ev[1]);
-  ctx->lastContractionMs = contraction;
-  ctx->lastTotalMs = b;
-  ctx->lastLaunches = ctx->launchCount - launch0;
-  if (st != TCSCF_OK || !keep) { cudaFree(dOut); return st; }
-  Tensor t;
-  t.d = dOut; t.n1 = n1; t.nb = nb; t.isComplex = 1; t.vec = 1;
-  int const id = ctx->nextId++;
-  ctx->tensors[id] = t;
-  if (vji) *vji = id;
-  return TCSCF_OK;
+  TCSCF_CHECK(ctx, jastrow, TCSCF_ERR_INVALID_ARGUMENT, "Jastrow parameters required");
+  return precomputeTensor(ctx, r1, r2, kernel, jastrow, precision, 3, V, keep, vji);
 }
 
 int tcscf_tensor_destroy(tcscf_ctx * ctx, int handle)

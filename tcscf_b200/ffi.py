@@ -49,6 +49,7 @@ SIGNATURES: dict[str, tuple] = {
     "tcscf_ctx_destroy": (_I, [_P]),
     "tcscf_last_error": (C.c_char_p, [_P]),
     "tcscf_ctx_stream": (_I, [_P, C.POINTER(_P)]),
+    "tcscf_selftest_bounded_wait": (_I, [_P, C.c_double]),
     "tcscf_synchronize": (_I, [_P]),
     "tcscf_last_timing": (_I, [_P, _D, _D, C.POINTER(_I)]),
     "tcscf_last_potentials": (_I, [_P, _D, _D]),
@@ -76,8 +77,8 @@ SIGNATURES: dict[str, tuple] = {
     "tcscf_tc_compute_q": (_I, [_P, _I, _I, _I, _D, _D, _D]),
     "tcscf_tc_assemble_g": (_I, [_P, _I, _D, _D, _D, _D, _D]),
     "tcscf_tc_scf": (_I, [_P, _I, _I, _I, _I, _I, _D, _D, _I, _I, _I, C.c_double, _I, _D, C.POINTER(_I), _D, _D]),
-    "tcscf_compute_F": (_I, [_P, _I, _I, _I, C.POINTER(Ochi), _D, _I, C.POINTER(_I)]),
-    "tcscf_compute_V": (_I, [_P, _I, _I, _I, C.POINTER(Ochi), _D, _I, C.POINTER(_I)]),
+    "tcscf_compute_F": (_I, [_P, _I, _I, _I, C.POINTER(Ochi), _I, _D, _I, C.POINTER(_I)]),
+    "tcscf_compute_V": (_I, [_P, _I, _I, _I, C.POINTER(Ochi), _I, _D, _I, C.POINTER(_I)]),
     "tcscf_tensor_destroy": (_I, [_P, _I]),
     "tcscf_fock_build": (_I, [_P, _I, _I, _I, _D, _D, _I, _I, _D, _D, _D]),
     "tcscf_fock_build_device": (_I, [_P, _I, _I, _I, _P, _P, _I, _I, _P, _P, _P]),

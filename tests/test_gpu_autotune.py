@@ -7,7 +7,7 @@ the r2 block sums (each split's double-float partial sums are added in FP64 afte
 against the default schedule is 1e-10 relative in the energy and 1e-9 of the largest |Fock| element,
 far below the mixed path's own error against FP64 (about 1e-8 relative).  A fixed schedule is
 deterministic: the same split gives bit-identical results, and turning the tuner off returns the
-default schedule's results exactly.  The file name puts these tests after the other GPU files.
+default schedule's results exactly. 
 """
 import numpy as np
 import pytest

@@ -1,11 +1,14 @@
 """Fixed-scratch S/H quadrature (tcscf_overlap_core_quadrature_static) through the C ABI.
 
 The entry point allocates nothing: its block results live in a 2 MiB device array shared by every
-call on the device.  It must return what the allocating entry point returns, on consecutive calls
-(the shared array is reused) and after whatever the other test files left on the device.
+call on the device, whose address the context looked up when it was created.  It must return what
+the allocating entry point returns, on consecutive calls (the shared array is reused) and after
+whatever the other test files left on the device, and the device's free memory must not drop
+across its calls.
 """
 import numpy as np
 import pytest
+import torch
 
 from tcscf_b200 import api, ffi, grids
 from tcscf_b200 import basis as wl
@@ -49,14 +52,17 @@ def test_static_scratch_matches_allocating_entry_point(ctx):
     S0, H0 = _allocating(lib, ctx, G, w.Z, w.nb)
     assert np.isfinite(S0).all() and np.isfinite(H0).all()
     scale_s, scale_h = np.abs(S0).max(), np.abs(H0).max()
+    free0 = torch.cuda.mem_get_info(0)[0]
     for _ in range(2):  # two calls in a row share the fixed array
         S1, H1 = _static(lib, ctx, G, w.Z, w.nb)
         assert np.abs(S1 - S0).max() <= TOL * scale_s
         assert np.abs(H1 - H0).max() <= TOL * scale_h
+    # no device allocation: free memory cannot have dropped (a pool may only have returned memory)
+    assert torch.cuda.mem_get_info(0)[0] >= free0
 
 
 def test_static_scratch_smaller_basis_then_s_only(ctx):
-    # a second grid and basis size reuse the same array; an S-only call leaves H untouched
+    # a second grid and basis size reuse the same array; an S-only call (H NULL) returns the same S
     lib = ffi.lib()
     w = wl.he()
     g = _rotated_grid(w.nrad, w.order)
@@ -66,8 +72,11 @@ def test_static_scratch_smaller_basis_then_s_only(ctx):
     S1, H1 = _static(lib, ctx, G, w.Z, w.nb)
     assert np.abs(S1 - S0).max() <= TOL * np.abs(S0).max()
     assert np.abs(H1 - H0).max() <= TOL * np.abs(H0).max()
-    S2, _ = _static(lib, ctx, G, w.Z, w.nb, with_h=False)
+    free0 = torch.cuda.mem_get_info(0)[0]
+    S2, H2 = _static(lib, ctx, G, w.Z, w.nb, with_h=False)
+    assert H2 is None
     assert np.abs(S2 - S0).max() <= TOL * np.abs(S0).max()
+    assert torch.cuda.mem_get_info(0)[0] >= free0
 
 
 def test_static_scratch_rejects_basis_beyond_limit(ctx):
