@@ -264,34 +264,75 @@ def run_reference(args, rank: int) -> None:
     print(json.dumps(line), flush=True)
 
 
-def roofline(prec: int, n: int, nb: int, nocc: int, c_ms: float, peaks: dict, peak_kind: str, fp64_peak: float, traffic) -> dict:
+def measure_matmul_peaks(dev, n: int = 8192, reps: int = 10) -> dict:
+    """Dense FP64 and TF32 matmul rates of this GPU, measured the way the BF16 peak of the peaks file
+    is (torch.matmul of n x n operands, best of reps, CUDA events): the denominators of the FP64 and
+    TF32 rooflines."""
+    import torch
+
+    out = {}
+    saved = torch.backends.cuda.matmul.allow_tf32
+    try:
+        for name, dtype, tf32 in (("fp64_tflops", torch.float64, False), ("tf32_tflops", torch.float32, True)):
+            torch.backends.cuda.matmul.allow_tf32 = tf32
+            g = torch.Generator(device=dev).manual_seed(0)
+            a = torch.randn(n, n, dtype=dtype, device=dev, generator=g)
+            b = torch.randn(n, n, dtype=dtype, device=dev, generator=g)
+            torch.matmul(a, b)
+            torch.cuda.synchronize()
+            best = float("inf")
+            for _ in range(reps):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                torch.matmul(a, b)
+                e1.record()
+                torch.cuda.synchronize()
+                best = min(best, e0.elapsed_time(e1))
+            out[name] = 2.0 * n ** 3 / (best / 1e3) / 1e12
+            del a, b
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = saved
+    torch.cuda.empty_cache()
+    return out
+
+
+def roofline(prec: int, n: int, nb: int, nocc: int, c_ms: float, peaks: dict, peak_kind: str, traffic) -> dict:
     """The line's roofline object for one Fock build of n points (r1 = r2 grid) whose contraction
-    kernel took c_ms milliseconds."""
+    kernel took c_ms milliseconds.  peaks: the BF16 peak (bf16_tflops) and the FP64 / TF32 matmul rates
+    (fp64_tflops, tf32_tflops) when measured."""
     from tcscf_b200 import ffi
 
     # algorithmic work per Fock build: F_alg = 2 N^2 (nb nocc + 1), the pair-density count of the direct
-    # build (nb nocc exchange pair densities and the Coulomb density per (r1, r2) pair); this kernel
-    # contracts the same sum in factored form, 2 N^2 (nocc + nb + 1) flops (rho GEMM, exchange GEMM,
+    # build (nb nocc exchange pair densities and the Coulomb density per (r1, r2) pair); the kernels
+    # contract the same sum in factored form, 2 N^2 (nocc + nb + 1) flops (rho GEMM, exchange GEMM,
     # Coulomb), reported beside it as kernel_algorithm_tflops
     flops = 2.0 * n * n * (nb * nocc + 1)
     kernel_flops = 2.0 * n * n * (nocc + nb + 1)
     achieved = flops / (c_ms / 1e3) / 1e12
     kernel_achieved = kernel_flops / (c_ms / 1e3) / 1e12
     numerator = {"achieved_numerator": "F_alg = 2 N^2 (nb nocc + 1) flops per build (pair-density count)",
-                 "kernel_algorithm_tflops": kernel_achieved}
+                 "kernel_algorithm_tflops": kernel_achieved,
+                 "frac_note": "frac counts F_alg, the pair-density work the factored form avoids; issued_frac (the "
+                              "slice products the tensor pipe executes) and ncu's tensor-pipe activity measure the hardware"}
     if prec == ffi.PREC_FP64:
-        roof = {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s", "frac": achieved / fp64_peak,
-                "traffic": None, "peak_source": "nominal B200 FP64 dense rate (--fp64-peak or TCSCF_FP64_PEAK_TFLOPS overrides)",
-                **numerator}
+        # the FP64 kernel runs on the FP64 pipe: its roofline counts the flops it performs
+        peak = peaks.get("fp64_tflops", 37.0)
+        src = "fp64 dense matmul (torch, 8192^3), measured in this run" if "fp64_tflops" in peaks else "nominal B200 FP64 rate"
+        roof = {"bound": "fp64", "achieved": kernel_achieved, "peak": peak, "unit": "TFLOP/s", "frac": kernel_achieved / peak,
+                "traffic": None, "peak_source": src,
+                "achieved_numerator": "2 N^2 (nocc + nb + 1) flops per build (the factored contraction the kernel performs)",
+                "effective_tflops": achieved}
     elif prec == ffi.PREC_TF32:
-        # TF32 dense rate is half the BF16 rate (nominal 1.1 vs 2.25 PFLOP/s): half the measured BF16 burst
-        peak = peaks["bf16_tflops"] / 2
+        if "tf32_tflops" in peaks:
+            peak, src = peaks["tf32_tflops"], "tf32 dense matmul (torch, 8192^3), measured in this run"
+        else:
+            peak, src = peaks["bf16_tflops"] / 2, f"tf32 dense = half the bf16 dense burst, {peak_kind}"
         RP = 32                            # TF32 launches hold rank 32 (larger ranks run in chunks)
         NB = 64 if nb <= 64 else 128
         chunks = -(-nocc // RP)
         issued = n * n * chunks * (2.0 * RP + 2.0 * NB) / (c_ms / 1e3) / 1e12
         roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                "traffic": None, "peak_source": f"tf32 dense = half the bf16 dense burst, {peak_kind}",
+                "traffic": None, "peak_source": src,
                 "issued_tensor_tflops": issued, "issued_frac": issued / peak, **numerator}
     else:
         peak = peaks["bf16_tflops"]
@@ -406,11 +447,16 @@ def run_ours(args, rank: int, world: int) -> None:
 
     if rank != 0:
         return
+    # FP64 / TF32 matmul rates of this GPU (untimed region): the FP64 and TF32 roofline denominators
+    mm_peaks = {} if args.skip_peaks else measure_matmul_peaks(dev)
     n = g.n
     dropped, near = grids.coincident_pairs(g, g)   # r1 = r2 grid: the diagonal pairs contribute 0
     c_ms = statistics.median(cms)
-    roof = roofline(prec, n, w.nb, w.n_up, c_ms, peaks, peak_kind, args.fp64_peak,
+    allpeaks = dict(peaks, **mm_peaks)
+    roof = roofline(prec, n, w.nb, w.n_up, c_ms, allpeaks, peak_kind,
                     TRAFFIC_BYTES_PER_LAUNCH.get(w.name) if prec == ffi.PREC_BF16X3 and args.nrad == 0 else None)
+    if fp64 is not None:
+        fp64["roofline"] = roofline(ffi.PREC_FP64, n, w.nb, w.n_up, fp64["contraction_ms"], allpeaks, peak_kind, None)
     cpu = None
     if not args.skip_cpu:
         r = cpu_reference(w, g, D, h, budget_s=args.cpu_seconds)
@@ -502,11 +548,12 @@ def run_batch(args, rank: int) -> None:
 
 def run_scf(args, rank: int) -> None:
     """Full RCS SCF of the Kr configuration to |dE| < 1e-8 Eh: split-BF16 and FP64 Fock builds in the plain
-    Roothaan iteration of the reference (at most --scf-max-iter iterations), split BF16 with Pulay DIIS
-    (history --diis), and the FP64 SCF converged to 1e-10 Eh as the energy reference; all with the
-    real-harmonic eigen-solve (real densities throughout, one contraction per build).  Each SCF starts
-    from the zero density (core-Hamiltonian first step, as the reference); wall time around the public
-    call."""
+    Roothaan iteration of the reference (at most --scf-max-iter iterations), each as the device loop in
+    one CUDA graph (tcscf_scf_graph) and as the host-driven loop (tcscf_scf), optionally split BF16 with
+    Pulay DIIS (--diis), and the FP64 device loop converged to 1e-10 Eh as the energy reference; all
+    with the real-harmonic eigen-solve (real densities throughout, one contraction per build).  Each SCF
+    starts from the zero density (core-Hamiltonian first step, as the reference); wall time around the
+    public call."""
     import torch
 
     from tcscf_b200 import api, ffi, grids
@@ -524,34 +571,43 @@ def run_scf(args, rank: int) -> None:
     S, h = api.overlap_core(w.basis, w.Z)
     # the 1e-8 runs time the configuration; the mixed-precision energy is compared with the FP64 SCF
     # converged to 1e-10 (the split-BF16 energy settles to its own precision, ~1e-9 Eh per build, so it
-    # is not itself run to 1e-10)
-    runs = [("bf16x3_plain", ffi.PREC_BF16X3, 0, 1e-8), ("bf16x3_diis", ffi.PREC_BF16X3, args.diis, 1e-8),
-            ("fp64_plain", ffi.PREC_FP64, 0, 1e-8), ("fp64_plain_1e-10", ffi.PREC_FP64, 0, 1e-10)]
+    # is not itself run to 1e-10).  "graph": the whole loop on the device as one CUDA graph launch
+    # (tcscf_scf_graph); "host": the host-driven loop (tcscf_scf, real-harmonic eigen-solve)
+    runs = [("bf16x3_graph", ffi.PREC_BF16X3, "graph", 0, 1e-8), ("fp64_graph", ffi.PREC_FP64, "graph", 0, 1e-8),
+            ("bf16x3_host", ffi.PREC_BF16X3, "host", 0, 1e-8), ("fp64_host", ffi.PREC_FP64, "host", 0, 1e-8),
+            ("fp64_graph_1e-10", ffi.PREC_FP64, "graph", 0, 1e-10)]
+    if args.diis:
+        runs.append(("bf16x3_host_diis", ffi.PREC_BF16X3, "host", args.diis, 1e-8))
     res = {}
     with ClockSampler(int(os.environ.get("LOCAL_RANK", 0))) as clk:
-        for name, prec, nd, tol in runs:
+        for name, prec, mode, nd, tol in runs:
             hf = api.RCSHartreeFock(w.n_up, w.n_down, w.nb)
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             try:
-                E, ok = hf.compute(S, h, G, G, precision=prec, tol=tol, max_iter=args.scf_max_iter, diis=nd,
-                                   real_eigensolve=True), True
+                if mode == "graph":
+                    E = hf.computeOnDevice(S, h, G, G, precision=prec, tol=tol, max_iter=args.scf_max_iter, capture=True)
+                else:
+                    E = hf.compute(S, h, G, G, precision=prec, tol=tol, max_iter=args.scf_max_iter, diis=nd, real_eigensolve=True)
+                ok = True
             except ffi.TcscfError as e:
                 if e.code != ffi.ERR_NOT_CONVERGED:
                     raise
                 E, ok = None, False
             torch.cuda.synchronize()
             res[name] = {"converged": ok, "energy": E, "iterations": hf.numberOfConvergenceLoops(),
-                         "seconds": time.perf_counter() - t0, "diis": nd, "tol": tol}
-    m, f, ft = res["bf16x3_plain"], res["fp64_plain"], res["fp64_plain_1e-10"]
-    line = {"metric": "Kr RCS SCF to |dE| < 1e-8 Eh, wall s (split-BF16 Fock builds)", "value": m["seconds"], "unit": "s",
+                         "seconds": time.perf_counter() - t0, "loop": mode, "diis": nd, "tol": tol}
+    m, f, ft = res["bf16x3_graph"], res["fp64_graph"], res["fp64_graph_1e-10"]
+    line = {"metric": "Kr RCS SCF to |dE| < 1e-8 Eh, wall s (split-BF16 Fock builds, device loop in one CUDA graph)",
+            "value": m["seconds"], "unit": "s",
             "n_gpus": 1, "steps": 1, "warmup": 0, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
             "dtype": "bf16", "data": "synthetic",
             "config": {"workload": f"Kr RCS SCF (direct-form Fock builds), {w.nrad} radial x Lebedev order {w.order}",
                        "n_points": g.n, "n_basis": w.nb, "n_occ": w.n_up, "start": "zero density (core-Hamiltonian step)"},
             "runs": res,
             "dE_mixed_vs_fp64_converged": (m["energy"] - ft["energy"]) if m["converged"] and ft["converged"] else None,
-            "speedup_vs_fp64": f["seconds"] / m["seconds"], "clocks": clk.summary()}
+            "speedup_vs_fp64": f["seconds"] / m["seconds"],
+            "speedup_vs_fp64_host_loop": res["fp64_host"]["seconds"] / m["seconds"], "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
 
 
@@ -681,12 +737,12 @@ def main() -> None:
                     help="scf: full Kr SCF to 1e-8 Eh (split BF16 and FP64, plain iteration and DIIS); "
                          "be_tc: the Be transcorrelated configuration (precompute, TC SCF, per-iteration build)")
     ap.add_argument("--qmc-points", type=int, default=0, help="override the be_tc points per grid (smaller profiling cases)")
-    ap.add_argument("--diis", type=int, default=8, help="DIIS history of --workload scf")
+    ap.add_argument("--diis", type=int, default=0, help="add a split-BF16 host-loop run with this DIIS history to --workload scf")
     ap.add_argument("--scf-max-iter", type=int, default=50, help="iteration limit of --workload scf (the reference's RCS limit)")
     ap.add_argument("--precision", default="bf16x3", choices=["bf16x3", "fp64", "tf32"])
     ap.add_argument("--nrad", type=int, default=0, help="override the workload's radial points (smaller profiling cases)")
     ap.add_argument("--fp64-steps", type=int, default=2)
-    ap.add_argument("--fp64-peak", type=float, default=float(os.environ.get("TCSCF_FP64_PEAK_TFLOPS", "37.0")))
+    ap.add_argument("--skip-peaks", action="store_true", help="do not measure the FP64 / TF32 matmul rates")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--ref-seconds", type=float, default=10.0)

@@ -277,6 +277,25 @@ int tcscf_scf(tcscf_ctx * ctx, int r1, int r2, int nspin, int n_up, int n_down, 
               int respect_symmetry, int precision, double tol, int max_iter, double * energy, int * iterations,
               double * density, double * eigenvalues);
 
+/* RCSHartreeFock::compute (HartreeFock.cpp:785-882) with the whole loop on the device (no reference
+ * counterpart to the mechanism): from the zero density, every iteration builds the Fock matrix at
+ * `precision` from the occupied coefficients (the density's factor D = C C^T, rank n_up), assembles
+ * G, F and the energy as tcscf_scf does, tests |dE| < tol on the device, and takes the next C from
+ * the Fock matrix in the real-harmonic basis: canonical orthogonalisation of S (eigenvalues of S
+ * above 1e-12 of the largest kept; computed once), a device Jacobi eigen-solve, the n_up lowest
+ * eigenvectors.  With capture != 0 the iterations after the first run as one CUDA graph launch whose
+ * conditional WHILE node repeats the iteration until the device-side test ends the loop, so the host
+ * reads nothing per iteration; with capture == 0 the same launches are issued per iteration and the
+ * host reads the loop state after each (results bit-identical to the captured run).  Restricted closed
+ * shell (n_up == n_down), nb <= 128, a density that is real in the real-harmonic basis (the real
+ * eigen-solve of tcscf_set_scf_options); the tensor-core precisions need n_up within one launch's
+ * rank (32 for nb > 64, else 64).  Outputs as tcscf_scf (eigenvalues: the orthogonalised problem's,
+ * ascending; NaN beyond their count) and graph_launches (1 when the loop ran as a graph, may be NULL).
+ * Returns TCSCF_ERR_NOT_CONVERGED after max_iter. */
+int tcscf_scf_graph(tcscf_ctx * ctx, int r1, int r2, int n_up, int n_down, const double * S, const double * h, int respect_symmetry,
+                    int precision, double tol, int max_iter, int capture, double * energy, int * iterations, double * density,
+                    double * eigenvalues, int * graph_launches);
+
 /* ---- transcorrelated Fock build and SCF (TCHartreeFock, HartreeFock.cpp:102-609, :1007-1362) ---- */
 /* One TC Fock build from device-resident tensors: Fji same / opposite spin (computeF with
  * TCSCF_K_TC_SCALAR_SAME / _OPPO) and Vji same / opposite (computeV with TCSCF_K_GRAD_U_SAME / _OPPO),

@@ -369,6 +369,30 @@ class RCSHartreeFock : public HartreeFockBase {
     : HartreeFockBase(1, numSpinUp, numSpinDown, numBasisFunctions, 50)
   {}
   double highestOccupiedOrbitalEnergy() const { return eigenvalues_[(nUp_ + nDown_) / 2 - 1]; }
+
+  // compute() with the whole loop on the device (tcscf_scf_graph): with capture, the iterations after
+  // the first are one CUDA graph launch whose device-side WHILE node ends the loop
+  template <class S, class H>
+  double computeOnDevice(S const & overlap, H const & oneElectronTerms, QMCGrid const & r1Grid, QMCGrid const & r2Grid,
+                         bool respectOneElectronSymmetry = true, tcscf_precision precision = TCSCF_PREC_FP64, double tol = 1e-5,
+                         int maxIter = 0, bool capture = true)
+  {
+    std::size_t const nn = std::size_t(nb_) * nb_;
+    if (r1Grid.nBasis() != nb_) throw Error(TCSCF_ERR_INVALID_ARGUMENT, "grid basis size differs from numBasisFunctions");
+    detail::requireSize(overlap, nn, "overlap");
+    detail::requireSize(oneElectronTerms, nn, "oneElectronTerms");
+    tcscf_ctx * ctx = r1Grid.context();
+    double energy = 0.0;
+    check(tcscf_scf_graph(ctx, r1Grid.id(), r2Grid.id(), nUp_, nDown_, overlap.data(), oneElectronTerms.data(),
+                          respectOneElectronSymmetry ? 1 : 0, precision, tol, maxIter > 0 ? maxIter : maxIter_, capture ? 1 : 0, &energy,
+                          &iterations_, detail::real(density_.data()), eigenvalues_.data(), &graphLaunches_),
+          ctx);
+    return energy;
+  }
+  int graphLaunches() const { return graphLaunches_; }
+
+ private:
+  int graphLaunches_ = 0;
 };
 
 // unrestricted open shell, at most 100 iterations (HartreeFock.cpp:923)

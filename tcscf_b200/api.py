@@ -415,6 +415,29 @@ class RCSHartreeFock(_SCF):
     def highestOccupiedOrbitalEnergy(self) -> float:
         return float(self.eigenvalues[0, sum(self.nElectrons) // 2 - 1])
 
+    def computeOnDevice(self, overlap: np.ndarray, oneElectronTerms: np.ndarray, r1Grid: QMCGrid, r2Grid: QMCGrid,
+                        respectOneElectronSymmetry: bool = True, precision: int = ffi.PREC_FP64, tol: float = 1e-5,
+                        max_iter: int | None = None, capture: bool = True) -> float:
+        """compute() with the whole loop on the device (tcscf_scf_graph): from the zero density, every
+        iteration builds, assembles, tests |dE| < tol and diagonalises (real-harmonic basis, canonical
+        orthogonalisation, device Jacobi) on the device; with capture the iterations after the first are
+        one CUDA graph launch with a device-side WHILE loop (self.graphLaunches == 1)."""
+        ctx = r1Grid.ctx
+        S = np.ascontiguousarray(np.real(overlap), dtype=np.float64)
+        hh = np.ascontiguousarray(oneElectronTerms, dtype=np.float64)
+        nb = r1Grid.nBasis()
+        if S.shape != (nb, nb) or hh.shape != (nb, nb) or nb != self.basisSize:
+            raise ffi.TcscfError(ffi.ERR_INVALID_ARGUMENT, "overlap / oneElectronTerms do not match nBasis")
+        e, it, gl = C.c_double(), C.c_int(), C.c_int()
+        code = ffi.lib().tcscf_scf_graph(ctx.handle, r1Grid.id, r2Grid.id, self.nElectrons[0], self.nElectrons[1], ffi.dptr(S),
+                                         ffi.dptr(hh), int(respectOneElectronSymmetry), precision, tol, max_iter or self.max_iter,
+                                         int(capture), C.byref(e), C.byref(it), ffi.dptr(self.density[0]),
+                                         ffi.dptr(self.eigenvalues[0]), C.byref(gl))
+        self._iter = it.value
+        self.graphLaunches = gl.value
+        _raise(code, ctx.handle)
+        return e.value
+
 
 class UOSHartreeFock(_SCF):
     """UOSHartreeFock (HartreeFock.hpp:297-349): unrestricted open shell, at most 100 iterations."""

@@ -84,6 +84,9 @@ struct tcscf_ctx {
   std::vector<uint64_t> tensorGraphKey;
   int graphCaptures = 0, graphReplays = 0;
   int realEigen = 0;  // tcscf_scf solves a Fock matrix that is real in the real-harmonic basis there
+  // set while a conditional graph body is captured: the contraction routines then record no timing
+  // events (event nodes are not allowed inside a conditional body)
+  int capturing = 0;
   // autotuner (tcscf_set_autotune): the measured r2 split count of the tensor-path launch per shape
   // {n1, n2, padded nb, padded rank, precision}, the split policy per batch signature, the policy
   // the batch build applies (1: the default rule, 0: no split, k > 1: k x the default split),

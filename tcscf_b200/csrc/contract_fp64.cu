@@ -462,9 +462,9 @@ int contractFp64(tcscf_ctx * ctx, Contraction const & c)
   size_t const smem = sizeof(double) * (size_t(c.R) * BM + 3 * BM + BK * BM + 2 * (size_t(BK) * bn + 4 * BK + size_t(c.R) * BK));
   int const kind = c.kernel == TCSCF_K_INV_R12 ? 0 : (c.kernel <= TCSCF_K_TC_SCALAR_OPPO ? 1 : 2);
   // the contraction kernel alone is bracketed by the context's timing events (tcscf_last_timing)
-  cudaEventRecord(ctx->ev[2], ctx->stream);
+  if (!ctx->capturing) cudaEventRecord(ctx->ev[2], ctx->stream);
   TCSCF_TRY(launchContract(ctx, kind, bn, a, unsigned(tiles), unsigned(nsplit), smem));
-  cudaEventRecord(ctx->ev[3], ctx->stream);
+  if (!ctx->capturing) cudaEventRecord(ctx->ev[3], ctx->stream);
   if (nsplit > 1) {
     int64_t const n = c.n1 * c.ncol;
     kSumSplits<<<gridBlocks(n, 256), 256, 0, ctx->stream>>>(n, int(nsplit), c.n1 * c.ldt, Tpart, c.T, c.n1, c.ncol, c.ldt, c.ldt);

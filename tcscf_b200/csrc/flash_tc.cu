@@ -1055,6 +1055,48 @@ int tensorRun(tcscf_ctx * ctx, TensorPrep * const * preps, int count, bool recor
   return TCSCF_OK;
 }
 
+int tensorPlanUpload(tcscf_ctx * ctx, TensorPrep & tp, char const * scratchName, TensorPlan & plan)
+{
+  size_t const instBytes = align256(sizeof(tc::Instance));
+  size_t const mapBytes = align256(sizeof(CUtensorMap) * tc::kMapsPerInstance);
+  void * p = nullptr;
+  TCSCF_TRY(scratch(ctx, scratchName, instBytes + mapBytes + 256, &p));
+  auto * dInst = static_cast<tc::Instance *>(p);
+  auto * dMaps = reinterpret_cast<CUtensorMap *>(static_cast<char *>(p) + instBytes);
+  int * dStatus = reinterpret_cast<int *>(static_cast<char *>(p) + instBytes + mapBytes);
+  tc::Instance hInst = tp.inst;
+  hInst.maps = dMaps;
+  TCSCF_CUDA(ctx, cudaMemcpyAsync(dInst, &hInst, sizeof(tc::Instance), cudaMemcpyHostToDevice, ctx->stream));
+  TCSCF_CUDA(ctx, cudaMemcpyAsync(dMaps, tp.maps, sizeof(CUtensorMap) * tc::kMapsPerInstance, cudaMemcpyHostToDevice, ctx->stream));
+  TCSCF_CUDA(ctx, cudaMemsetAsync(dStatus, 0, sizeof(int), ctx->stream));
+  TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));   // the host copies are consumed before they go out of scope
+  plan.NB = tp.NB; plan.RP = tp.RP; plan.XS = tp.XS;
+  plan.nItems = tp.inst.nTiles * tp.inst.nSplit;
+  plan.grid = std::min(plan.nItems, smCount());
+  plan.inst = dInst;
+  plan.status = dStatus;
+  plan.prep = &tp;
+  return TCSCF_OK;
+}
+
+int tensorPlanLaunch(tcscf_ctx * ctx, TensorPlan const & plan)
+{
+  tc::Params P{};
+  P.nItems = plan.nItems;
+  P.items = nullptr;   // one instance: item = tile * nSplit + split
+  P.inst = static_cast<tc::Instance const *>(plan.inst);
+  P.status = plan.status;
+  TCSCF_TRY(launchClass(ctx, plan.NB, plan.RP, plan.XS, P, plan.grid));
+  tc::Instance const & I = plan.prep->inst;
+  Contraction const & c = plan.prep->c;
+  if (I.nSplit > 1) {
+    int64_t const n = int64_t(c.n1) * c.ncol;
+    TCSCF_TRY(sumSplitsLaunch(ctx, n, I.nSplit, int64_t(c.n1) * c.ldt, I.T, c.T, c.n1, c.ncol, c.ldt, c.ldt));
+    if (c.VH) TCSCF_TRY(sumSplitsLaunch(ctx, c.n1, I.nSplit, c.n1, I.VH, c.VH, c.n1, 1, 1, 1));
+  }
+  return TCSCF_OK;
+}
+
 namespace {
 
 // T[r][j] += A[r][j] for j < ncol (leading dimension ld)

@@ -106,6 +106,21 @@ size_t tensorArenaBytes(Contraction const & c, int precision = TCSCF_PREC_BF16X3
 int tensorPrepare(tcscf_ctx * ctx, Contraction const & c, int precision, void * arena, size_t arenaBytes, TensorPrep & tp);
 int tensorRun(tcscf_ctx * ctx, TensorPrep * const * preps, int count, bool recordStart = true);
 
+// A single prepared contraction whose device tables (instance, tensor maps) and status word are
+// uploaded once (tensorPlanUpload, which synchronises); tensorPlanLaunch then issues the persistent
+// launch and the split sums with no host synchronisation and no host memory read, so a CUDA graph can
+// capture it and replay it while the prepared operands keep their addresses (re-packed in place by
+// tensorPrepare on the same arena).  The status word accumulates over launches (0 = every bounded
+// wait completed).
+struct TensorPlan {
+  int NB = 0, RP = 0, XS = 0, grid = 0, nItems = 0;
+  const void * inst = nullptr;
+  int * status = nullptr;
+  TensorPrep * prep = nullptr;
+};
+int tensorPlanUpload(tcscf_ctx * ctx, TensorPrep & tp, char const * scratchName, TensorPlan & plan);
+int tensorPlanLaunch(tcscf_ctx * ctx, TensorPlan const & plan);
+
 // out[r][c] = sum_s part[s*stride + r*ldPart + c] for r < rows, c < cols (deterministic split sum)
 int sumSplitsLaunch(tcscf_ctx * ctx, int64_t n, int nsplit, int64_t stride, const double * part, double * out, int64_t rows, int cols,
                     int ldOut, int ldPart);

@@ -1374,6 +1374,407 @@ int precomputeTensor(tcscf_ctx * ctx, int r1, int r2, int kernel, const tcscf_oc
   return TCSCF_OK;
 }
 
+// ---- SCF as one CUDA graph (tcscf_scf_graph) ------------------------------------------------------
+// C = op(A) B for small dense row-major matrices (op(A) = A [M][K] or A^T with A [K][M]); one thread
+// per output element
+__global__ void kSmallGemm(int M, int N, int K, const double * A, int lda, int transA, const double * B, int ldb, double * C, int ldc)
+{
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < M * N; idx += gridDim.x * blockDim.x) {
+    int const i = idx / N, j = idx % N;
+    double s = 0;
+    for (int k = 0; k < K; ++k) s = fma(transA ? A[k * lda + i] : A[i * lda + k], B[k * ldb + j], s);
+    C[i * ldc + j] = s;
+  }
+}
+
+// Two-sided cyclic Jacobi eigen-solver of the symmetric m x m matrix A (row-major) in one CTA
+// (Golub & Van Loan, Matrix Computations, sym.schur2 rotations in the round-robin parallel ordering:
+// m (rounded up to even, the padding index carries a zero row) indices are paired into m/2 disjoint
+// rotations per step, m - 1 steps per sweep).  A lives in shared memory, the eigenvectors V (columns,
+// row-major [m][m]) in global memory.  A rotation is skipped when |a_pq| <= eps sqrt|a_pp a_qq|; the
+// sweeps stop when one performs no rotation (at most 40).  Out: W[m] the eigenvalues (A's diagonal,
+// unsorted) and V.
+constexpr int kJacobiThreads = 512;
+__global__ void __launch_bounds__(kJacobiThreads) kJacobiSym(int m, const double * Ain, double * W, double * V)
+{
+  extern __shared__ double sJ[];
+  __shared__ double cs[64], sn[64];
+  __shared__ int pp[64], qq[64];
+  __shared__ int rotated;
+  int const mp = m + (m & 1);
+  int const half = mp / 2;
+  int const tid = threadIdx.x;
+  for (int idx = tid; idx < mp * mp; idx += blockDim.x) {
+    int const i = idx / mp, j = idx % mp;
+    sJ[idx] = (i < m && j < m) ? 0.5 * (Ain[i * m + j] + Ain[j * m + i]) : 0.0;
+  }
+  for (int idx = tid; idx < m * m; idx += blockDim.x) V[idx] = (idx / m == idx % m) ? 1.0 : 0.0;
+  __syncthreads();
+  for (int sweep = 0; sweep < 40; ++sweep) {
+    if (tid == 0) rotated = 0;
+    __syncthreads();
+    for (int step = 0; step < mp - 1; ++step) {
+      if (tid < half) {
+        // round-robin pairing: index mp - 1 stays, the others rotate by one each step
+        int p = tid == 0 ? mp - 1 : (step + tid) % (mp - 1);
+        int q = (step + mp - 1 - tid) % (mp - 1);
+        if (tid == 0) q = step % (mp - 1);
+        if (p > q) { int const t = p; p = q; q = t; }
+        double const apq = sJ[p * mp + q], app = sJ[p * mp + p], aqq = sJ[q * mp + q];
+        double c = 1.0, s = 0.0;
+        if (apq != 0.0 && fabs(apq) > 2.2204460492503131e-16 * sqrt(fabs(app * aqq))) {
+          double const tau = (aqq - app) / (2.0 * apq);
+          double const t = (tau >= 0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+          c = 1.0 / sqrt(1.0 + t * t);
+          s = t * c;
+          rotated = 1;
+        }
+        pp[tid] = p; qq[tid] = q; cs[tid] = c; sn[tid] = s;
+      }
+      __syncthreads();
+      // rows: A <- J^T A
+      for (int idx = tid; idx < half * mp; idx += blockDim.x) {
+        int const k = idx / mp, j = idx % mp;
+        if (sn[k] == 0.0) continue;
+        int const p = pp[k], q = qq[k];
+        double const c = cs[k], s = sn[k];
+        double const ap = sJ[p * mp + j], aq = sJ[q * mp + j];
+        sJ[p * mp + j] = c * ap - s * aq;
+        sJ[q * mp + j] = s * ap + c * aq;
+      }
+      __syncthreads();
+      // columns: A <- A J, V <- V J
+      for (int idx = tid; idx < half * mp; idx += blockDim.x) {
+        int const k = idx / mp, i = idx % mp;
+        if (sn[k] == 0.0) continue;
+        int const p = pp[k], q = qq[k];
+        double const c = cs[k], s = sn[k];
+        double const ap = sJ[i * mp + p], aq = sJ[i * mp + q];
+        sJ[i * mp + p] = c * ap - s * aq;
+        sJ[i * mp + q] = s * ap + c * aq;
+        if (i < m && q < m) {
+          double const vp = V[i * m + p], vq = V[i * m + q];
+          V[i * m + p] = c * vp - s * vq;
+          V[i * m + q] = s * vp + c * vq;
+        }
+      }
+      __syncthreads();
+    }
+    if (!rotated) break;
+    __syncthreads();
+  }
+  for (int i = tid; i < m; i += blockDim.x) W[i] = sJ[i * mp + i];
+}
+
+// Eigenvalues in ascending order (ties by index): Ws[m], and the indices of the nocc lowest; then
+// the occupied coefficients C[k][a] = sum_j Xc[k][j] V[j][idx[a]] ([nb][nocc], real-harmonic basis)
+// and the density DR = C C^T.  One block.
+__global__ void kOccupiedOrbitals(int nb, int m, int nocc, const double * W, const double * V, const double * Xc, double * Ws, double * C,
+                                  double * DR)
+{
+  __shared__ int idx[128];
+  for (int t = threadIdx.x; t < m; t += blockDim.x) {
+    double const wt = W[t];
+    int r = 0;
+    for (int j = 0; j < m; ++j) r += (W[j] < wt || (W[j] == wt && j < t)) ? 1 : 0;
+    Ws[r] = wt;
+    if (r < nocc) idx[r] = t;
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < nb * nocc; e += blockDim.x) {
+    int const k = e / nocc, a = e % nocc;
+    double s = 0;
+    for (int j = 0; j < m; ++j) s = fma(Xc[k * m + j], V[j * m + idx[a]], s);
+    C[e] = s;
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
+    int const u = e / nb, v = e % nb;
+    double s = 0;
+    for (int a = 0; a < nocc; ++a) s = fma(C[u * nocc + a], C[v * nocc + a], s);
+    DR[e] = s;
+  }
+}
+
+// The convergence test of the SCF loop (RCSHartreeFock::compute, HartreeFock.cpp:857): the energy of
+// this iteration's build against the previous one; on convergence, a non-finite energy, an expired
+// bounded wait of the tensor kernel or the iteration limit, the loop ends (the graph's WHILE
+// condition is cleared) with the density and eigenvalues this build used saved.
+struct ScfGraphState {
+  double eprev, eres;
+  int iter, done, code, pad;
+};
+__global__ void kScfCheck(ScfGraphState * st, const double * E, const int * tstatus, int maxIter, double tol, int nD, const double2 * D,
+                          double2 * Dres, int nW, const double * Wcur, double * Wres, cudaGraphConditionalHandle handle, int useHandle)
+{
+  __shared__ int stop;
+  if (threadIdx.x == 0) {
+    double const e = *E;
+    int const it = st->iter + 1;
+    st->iter = it;
+    int code = TCSCF_OK;
+    bool s = true;
+    if (tstatus && *tstatus != 0) code = TCSCF_ERR_TIMEOUT;
+    else if (!isfinite(e)) code = TCSCF_ERR_NONFINITE;
+    else if (fabs(e - st->eprev) < tol) code = TCSCF_OK;
+    else if (it >= maxIter) code = TCSCF_ERR_NOT_CONVERGED;
+    else s = false;
+    st->eprev = e;
+    if (s) { st->done = 1; st->code = code; st->eres = e; }
+    stop = s ? 1 : 0;
+  }
+  __syncthreads();
+  if (stop) {
+    for (int i = threadIdx.x; i < nD; i += blockDim.x) Dres[i] = D[i];
+    for (int i = threadIdx.x; i < nW; i += blockDim.x) Wres[i] = Wcur[i];
+  }
+  if (useHandle && threadIdx.x == 0) cudaGraphSetConditional(handle, stop ? 0u : 1u);
+}
+
+// One RCS SCF on the device (tcscf_scf_graph).  Every iteration is the same launch sequence on fixed
+// buffers: orbitals of the current occupied coefficients C on both grids, the Coulomb source, the r12
+// contraction (FP64 or tensor cores) from those factors (D = C C^T, rank nocc), the real Fock
+// reduction, the reference-basis G, F and energy (kFinalize), the convergence test, then the new C from
+// the Fock matrix: real-harmonic F, Xc^T F Xc with the canonical orthogonaliser Xc of S, Jacobi, the
+// nocc lowest eigenvectors.  The first iteration (zero density: F = h) runs directly and allocates
+// every buffer; with capture the rest run as one graph launch whose conditional WHILE node repeats the
+// body until the device-side test clears it, so the host neither reads nor waits per iteration.
+int scfGraph(tcscf_ctx * ctx, Grid & g1, Grid & g2, int nocc, const double * S, const double * h, int respectSym, int precision, double tol,
+             int maxIter, int capture, double * energy, int * iterations, double * density, double * eigenvalues, int * graphLaunches)
+{
+  int const nb = g1.nb;
+  int64_t const n1 = g1.n, n2 = g2.n;
+  size_t const nn = size_t(nb) * nb;
+  double const scale = g2.ndim == 2 ? 2 * kPi : 1.0;
+  TCSCF_CHECK(ctx, nb <= 128, TCSCF_ERR_UNSUPPORTED, "the graph SCF's device eigen-solver takes nb <= 128");
+  TCSCF_CHECK(ctx, nocc >= 1 && nocc <= nb, TCSCF_ERR_INVALID_ARGUMENT, "occupied orbitals out of range");
+  // ---- small buffers
+  void * p = nullptr;
+  size_t const smallBytes = sizeof(double2) * nn * 7 + sizeof(double) * (nn * 8 + size_t(nb) * nocc + 4 * nb + 64) + sizeof(ScfGraphState) + 4096;
+  TCSCF_TRY(scratch(ctx, "scf_graph_small", smallBytes, &p));
+  char * q = static_cast<char *>(p);
+  auto take = [&](size_t n) { char * r = q; q += (n + 255) & ~size_t(255); return r; };
+  auto * dD = reinterpret_cast<double2 *>(take(sizeof(double2) * nn));
+  auto * dG = reinterpret_cast<double2 *>(take(sizeof(double2) * nn));
+  auto * dF = reinterpret_cast<double2 *>(take(sizeof(double2) * nn));
+  auto * FRc = reinterpret_cast<double2 *>(take(sizeof(double2) * nn));
+  auto * Sc = reinterpret_cast<double2 *>(take(sizeof(double2) * nn));
+  auto * SRc = reinterpret_cast<double2 *>(take(sizeof(double2) * nn));
+  auto * Dres = reinterpret_cast<double2 *>(take(sizeof(double2) * nn));
+  double * dH = reinterpret_cast<double *>(take(sizeof(double) * nn));
+  double * FR = reinterpret_cast<double *>(take(sizeof(double) * nn));
+  double * SR = reinterpret_cast<double *>(take(sizeof(double) * nn));
+  double * Xc = reinterpret_cast<double *>(take(sizeof(double) * nn));
+  double * Tm = reinterpret_cast<double *>(take(sizeof(double) * nn));
+  double * Fp = reinterpret_cast<double *>(take(sizeof(double) * nn));
+  double * Vm = reinterpret_cast<double *>(take(sizeof(double) * nn));
+  double * DR = reinterpret_cast<double *>(take(sizeof(double) * nn));
+  double * C = reinterpret_cast<double *>(take(sizeof(double) * nb * nocc));
+  double * W = reinterpret_cast<double *>(take(sizeof(double) * nb));
+  double * Ws = reinterpret_cast<double *>(take(sizeof(double) * nb));
+  double * Wres = reinterpret_cast<double *>(take(sizeof(double) * nb));
+  double * fmaxv = reinterpret_cast<double *>(take(sizeof(double) * 4));
+  double * dE = reinterpret_cast<double *>(take(sizeof(double) * 4));
+  auto * st = reinterpret_cast<ScfGraphState *>(take(sizeof(ScfGraphState)));
+  // ---- grid-sized buffers of the build
+  int const ldpsi = nocc;
+  size_t const bigBytes = sizeof(double) * (size_t(n2) * nb + size_t(n1) * ldpsi + size_t(n2) * ldpsi + n2 + size_t(n1) * nb + n1) + 8 * 256;
+  TCSCF_TRY(scratch(ctx, "scf_graph_build", bigBytes, &p));
+  q = static_cast<char *>(p);
+  double * Vw = reinterpret_cast<double *>(take(sizeof(double) * n2 * nb));
+  double * psi1 = reinterpret_cast<double *>(take(sizeof(double) * n1 * ldpsi));
+  double * psi2 = reinterpret_cast<double *>(take(sizeof(double) * n2 * ldpsi));
+  double * coul = reinterpret_cast<double *>(take(sizeof(double) * n2));
+  double * Tb = reinterpret_cast<double *>(take(sizeof(double) * n1 * nb));
+  double * VH = reinterpret_cast<double *>(take(sizeof(double) * n1));
+
+  // ---- canonical orthogonaliser Xc = U s^-1/2 of the real-harmonic overlap (eigenvalues above 1e-12
+  // of the largest kept)
+  TCSCF_CUDA(ctx, cudaMemcpyAsync(SR, S, sizeof(double) * nn, cudaMemcpyHostToDevice, ctx->stream));
+  TCSCF_CUDA(ctx, cudaMemcpyAsync(dH, h, sizeof(double) * nn, cudaMemcpyHostToDevice, ctx->stream));
+  kRealToComplex<<<gridBlocks(int64_t(nn), 256), 256, 0, ctx->stream>>>(int64_t(nn), SR, Sc);
+  TCSCF_LAUNCH(ctx);
+  kDensityToReal<<<gridBlocks(nn, 256), 256, 0, ctx->stream>>>(1, nb, g1.dsto, Sc, SRc);
+  TCSCF_LAUNCH(ctx);
+  kSplitDensity<<<1, 256, 0, ctx->stream>>>(nb, SRc, SR, fmaxv);
+  TCSCF_LAUNCH(ctx);
+  int m = 0;
+  {
+    int lwork = 0;
+    if (cusolverDnDsyevd_bufferSize(ctx->solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, nb, SR, nb, W, &lwork) != CUSOLVER_STATUS_SUCCESS)
+      return fail(ctx, TCSCF_ERR_LINALG, "cusolverDnDsyevd_bufferSize failed");
+    void * wk = nullptr;
+    TCSCF_TRY(scratch(ctx, "scf_graph_syevd", sizeof(double) * size_t(lwork) + 64 + sizeof(int) * 4, &wk));
+    int * info = reinterpret_cast<int *>(static_cast<double *>(wk) + lwork);
+    if (cusolverDnDsyevd(ctx->solver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, nb, SR, nb, W, static_cast<double *>(wk), lwork, info) !=
+        CUSOLVER_STATUS_SUCCESS)
+      return fail(ctx, TCSCF_ERR_LINALG, "cusolverDnDsyevd failed");
+    std::vector<double> hs(nb), hv(nn);
+    int hinfo = 0;
+    TCSCF_CUDA(ctx, cudaMemcpyAsync(hs.data(), W, sizeof(double) * nb, cudaMemcpyDeviceToHost, ctx->stream));
+    TCSCF_CUDA(ctx, cudaMemcpyAsync(hv.data(), SR, sizeof(double) * nn, cudaMemcpyDeviceToHost, ctx->stream));
+    TCSCF_CUDA(ctx, cudaMemcpyAsync(&hinfo, info, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    TCSCF_CHECK(ctx, hinfo == 0 && hs[nb - 1] > 0 && std::isfinite(hs[nb - 1]), TCSCF_ERR_LINALG, "overlap matrix is not positive definite");
+    std::vector<int> keep;
+    for (int j = 0; j < nb; ++j)
+      if (hs[j] > 1e-12 * hs[nb - 1]) keep.push_back(j);
+    m = int(keep.size());
+    TCSCF_CHECK(ctx, m >= nocc, TCSCF_ERR_LINALG, "overlap matrix has fewer independent functions than occupied orbitals");
+    std::vector<double> hx(size_t(nb) * m);
+    for (int k = 0; k < nb; ++k)   // cuSOLVER's eigenvectors are the columns of a column-major array
+      for (int c = 0; c < m; ++c) hx[size_t(k) * m + c] = hv[size_t(keep[c]) * nb + k] / std::sqrt(hs[keep[c]]);
+    TCSCF_CUDA(ctx, cudaMemcpyAsync(Xc, hx.data(), sizeof(double) * hx.size(), cudaMemcpyHostToDevice, ctx->stream));
+    TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+  // ---- static operands and the zero start (D = 0: the first build gives F = h, E = 0)
+  TCSCF_CUDA(ctx, cudaMemsetAsync(C, 0, sizeof(double) * nb * nocc, ctx->stream));
+  TCSCF_CUDA(ctx, cudaMemsetAsync(dD, 0, sizeof(double2) * nn, ctx->stream));
+  TCSCF_CUDA(ctx, cudaMemsetAsync(W, 0, sizeof(double) * nb, ctx->stream));
+  TCSCF_CUDA(ctx, cudaMemsetAsync(Ws, 0, sizeof(double) * nb, ctx->stream));
+  ScfGraphState st0{std::numeric_limits<double>::max(), 0.0, 0, 0, TCSCF_OK, 0};
+  TCSCF_CUDA(ctx, cudaMemcpyAsync(st, &st0, sizeof(st0), cudaMemcpyHostToDevice, ctx->stream));
+  kWeightedBasis<<<gridBlocks(n2 * nb, 256), 256, 0, ctx->stream>>>(n2, nb, g2.phiR, g2.w, scale, Vw);
+  TCSCF_LAUNCH(ctx);
+  Contraction c;
+  c.n1 = n1; c.n2 = n2; c.R = nocc; c.ncol = nb;
+  c.p1 = g1.pts; c.p2 = g2.pts; c.psi1 = psi1; c.psi2 = psi2; c.ldpsi = ldpsi;
+  c.V = Vw; c.ldv = nb; c.T = Tb; c.ldt = nb; c.coul = coul; c.VH = VH;
+  bool const tensor = precision != TCSCF_PREC_FP64;
+  TensorPrep tp;
+  TensorPlan plan;
+  void * arena = nullptr;
+  size_t arenaBytes = 0;
+  if (tensor) {
+    TCSCF_TRY(tensorPackedV(ctx, g2, Vw, scale, &c.vtPacked));
+    std::string why;
+    TCSCF_CHECK(ctx, tensorPathAvailable(c, precision, &why), TCSCF_ERR_UNSUPPORTED, "graph SCF tensor path: " + why);
+    arenaBytes = tensorArenaBytes(c, precision);
+    TCSCF_TRY(scratch(ctx, "scf_graph_tensor", arenaBytes, &arena));
+    TCSCF_TRY(tensorPrepare(ctx, c, precision, arena, arenaBytes, tp));
+    TCSCF_TRY(tensorPlanUpload(ctx, tp, "scf_graph_plan", plan));
+  }
+  size_t const jacobiSmem = sizeof(double) * size_t(m + (m & 1)) * (m + (m & 1));
+  TCSCF_CUDA(ctx, cudaFuncSetAttribute(kJacobiSym, cudaFuncAttributeMaxDynamicSharedMemorySize, int(jacobiSmem)));
+
+  auto body = [&](cudaGraphConditionalHandle handle, int useHandle) -> int {
+    size_t const sm = sizeof(double) * size_t(nb) * nocc;
+    kOrbitals<<<gridBlocks(n1 * nocc, 256), 256, sm, ctx->stream>>>(n1, nb, nocc, g1.phiR, C, nocc, psi1, ldpsi);
+    TCSCF_LAUNCH(ctx);
+    kOrbitals<<<gridBlocks(n2 * nocc, 256), 256, sm, ctx->stream>>>(n2, nb, nocc, g2.phiR, C, nocc, psi2, ldpsi);
+    TCSCF_LAUNCH(ctx);
+    kCoulombSource<<<gridBlocks(n2, 256), 256, 0, ctx->stream>>>(n2, nocc, psi2, psi2, ldpsi, g2.w, scale, coul);
+    TCSCF_LAUNCH(ctx);
+    if (tensor) {
+      TCSCF_TRY(tensorPrepare(ctx, c, precision, arena, arenaBytes, tp));
+      TCSCF_TRY(tensorPlanLaunch(ctx, plan));
+    } else {
+      TCSCF_TRY(contractFp64(ctx, c));
+    }
+    TCSCF_CUDA(ctx, cudaMemsetAsync(FR, 0, sizeof(double) * nn, ctx->stream));
+    TCSCF_TRY(reduceFockReal(ctx, n1, nb, g1.phiR, g1.w, VH, 2.0, Tb, nb, 1.0, FR));
+    kRealToReference<<<gridBlocks(int64_t(nn), 256), 256, 0, ctx->stream>>>(1, nb, g1.dsto, FR, nullptr, dG);
+    TCSCF_LAUNCH(ctx);
+    kFinalize<<<1, 512, 0, ctx->stream>>>(1, nb, dH, dG, nullptr, dD, respectSym, 2.0, dF, dE);
+    TCSCF_LAUNCH(ctx);
+    kScfCheck<<<1, 256, 0, ctx->stream>>>(st, dE, tensor ? plan.status : nullptr, maxIter, tol, int(nn), dD, Dres, nb, Ws, Wres, handle,
+                                          useHandle);
+    TCSCF_LAUNCH(ctx);
+    // the next density from this Fock matrix (real in the real-harmonic basis)
+    kDensityToReal<<<gridBlocks(nn, 256), 256, 0, ctx->stream>>>(1, nb, g1.dsto, dF, FRc);
+    TCSCF_LAUNCH(ctx);
+    kSplitDensity<<<1, 256, 0, ctx->stream>>>(nb, FRc, FR, fmaxv);
+    TCSCF_LAUNCH(ctx);
+    kSmallGemm<<<gridBlocks(int64_t(nb) * m, 256), 256, 0, ctx->stream>>>(nb, m, nb, FR, nb, 0, Xc, m, Tm, m);
+    TCSCF_LAUNCH(ctx);
+    kSmallGemm<<<gridBlocks(int64_t(m) * m, 256), 256, 0, ctx->stream>>>(m, m, nb, Xc, m, 1, Tm, m, Fp, m);
+    TCSCF_LAUNCH(ctx);
+    kJacobiSym<<<1, kJacobiThreads, jacobiSmem, ctx->stream>>>(m, Fp, W, Vm);
+    TCSCF_LAUNCH(ctx);
+    kOccupiedOrbitals<<<1, 256, 0, ctx->stream>>>(nb, m, nocc, W, Vm, Xc, Ws, C, DR);
+    TCSCF_LAUNCH(ctx);
+    kRealToReference<<<gridBlocks(int64_t(nn), 256), 256, 0, ctx->stream>>>(1, nb, g1.dsto, DR, nullptr, dD);
+    TCSCF_LAUNCH(ctx);
+    return TCSCF_OK;
+  };
+
+  ScfGraphState hst{};
+  // first iteration directly (allocates every scratch buffer the body uses)
+  TCSCF_TRY(body(0, 0));
+  TCSCF_CUDA(ctx, cudaMemcpyAsync(&hst, st, sizeof(hst), cudaMemcpyDeviceToHost, ctx->stream));
+  TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  *graphLaunches = 0;
+  if (!hst.done) {
+    if (capture) {
+      cudaGraph_t graph = nullptr;
+      TCSCF_CUDA(ctx, cudaGraphCreate(&graph, 0));
+      cudaGraphConditionalHandle handle;
+      cudaGraphNode_t node;
+      cudaGraphNodeParams cp = {};
+      cudaError_t e = cudaGraphConditionalHandleCreate(&handle, graph, 1, cudaGraphCondAssignDefault);
+      if (e == cudaSuccess) {
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = handle;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        e = cudaGraphAddNode(&node, graph, nullptr, 0, &cp);
+      }
+      if (e != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        return fail(ctx, TCSCF_ERR_CUDA, std::string("conditional graph node: ") + cudaGetErrorString(e));
+      }
+      cudaGraph_t bodyGraph = cp.conditional.phGraph_out[0];
+      e = cudaStreamBeginCaptureToGraph(ctx->stream, bodyGraph, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed);
+      if (e != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        return fail(ctx, TCSCF_ERR_CUDA, std::string("begin capture: ") + cudaGetErrorString(e));
+      }
+      ctx->capturing = 1;
+      int const bst = body(handle, 1);
+      ctx->capturing = 0;
+      cudaGraph_t captured = nullptr;
+      e = cudaStreamEndCapture(ctx->stream, &captured);
+      if (bst != TCSCF_OK || e != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        if (bst != TCSCF_OK) return bst;
+        return fail(ctx, TCSCF_ERR_CUDA, std::string("end capture: ") + cudaGetErrorString(e));
+      }
+      cudaGraphExec_t exec = nullptr;
+      e = cudaGraphInstantiate(&exec, graph, 0);
+      cudaGraphDestroy(graph);
+      TCSCF_CHECK(ctx, e == cudaSuccess, TCSCF_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+      e = cudaGraphLaunch(exec, ctx->stream);
+      cudaError_t const e2 = cudaStreamSynchronize(ctx->stream);
+      cudaGraphExecDestroy(exec);
+      TCSCF_CHECK(ctx, e == cudaSuccess && e2 == cudaSuccess, TCSCF_ERR_CUDA,
+                  std::string("graph launch: ") + cudaGetErrorString(e != cudaSuccess ? e : e2));
+      *graphLaunches = 1;
+    } else {
+      // the same body launched per iteration, with the host reading the loop state after each
+      for (int it = 1; it < maxIter && !hst.done; ++it) {
+        TCSCF_TRY(body(0, 0));
+        TCSCF_CUDA(ctx, cudaMemcpyAsync(&hst, st, sizeof(hst), cudaMemcpyDeviceToHost, ctx->stream));
+        TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+      }
+    }
+    TCSCF_CUDA(ctx, cudaMemcpyAsync(&hst, st, sizeof(hst), cudaMemcpyDeviceToHost, ctx->stream));
+    TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+  if (iterations) *iterations = hst.iter;
+  if (energy) *energy = hst.eres;
+  if (density) TCSCF_CUDA(ctx, cudaMemcpy(density, Dres, sizeof(double2) * nn, cudaMemcpyDeviceToHost));
+  if (eigenvalues) {
+    std::vector<double> hw(nb, std::numeric_limits<double>::quiet_NaN());
+    TCSCF_CUDA(ctx, cudaMemcpy(hw.data(), Wres, sizeof(double) * m, cudaMemcpyDeviceToHost));
+    std::copy(hw.begin(), hw.end(), eigenvalues);
+  }
+  if (hst.code == TCSCF_ERR_TIMEOUT) return fail(ctx, TCSCF_ERR_TIMEOUT, "graph SCF: a bounded wait of the tensor kernel expired");
+  if (hst.code == TCSCF_ERR_NONFINITE) return fail(ctx, TCSCF_ERR_NONFINITE, "non-finite energy");
+  if (hst.code == TCSCF_ERR_NOT_CONVERGED || !hst.done)
+    return fail(ctx, TCSCF_ERR_NOT_CONVERGED, "SCF did not converge in " + std::to_string(maxIter) + " iterations");
+  return TCSCF_OK;
+}
+
 }  // namespace
 }  // namespace tcscf
 
@@ -2101,6 +2502,26 @@ int tcscf_scf(tcscf_ctx * ctx, int r1, int r2, int nspin, int n_up, int n_down, 
   if (density) TCSCF_CUDA(ctx, cudaMemcpy(density, dD, sizeof(double2) * nn * nspin, cudaMemcpyDeviceToHost));
   if (eigenvalues) TCSCF_CUDA(ctx, cudaMemcpy(eigenvalues, W, sizeof(double) * nb * nspin, cudaMemcpyDeviceToHost));
   return fail(ctx, TCSCF_ERR_NOT_CONVERGED, "Did not converge.");
+}
+
+int tcscf_scf_graph(tcscf_ctx * ctx, int r1, int r2, int n_up, int n_down, const double * S, const double * h, int respect_symmetry,
+                    int precision, double tol, int max_iter, int capture, double * energy, int * iterations, double * density,
+                    double * eigenvalues, int * graph_launches)
+{
+  TCSCF_NVTX();
+  if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  Grid * g1 = findGrid(ctx, r1);
+  Grid * g2 = findGrid(ctx, r2);
+  TCSCF_TRY(checkBasisPair(ctx, g1, g2));
+  TCSCF_CHECK(ctx, S && h && max_iter > 0, TCSCF_ERR_INVALID_ARGUMENT, "S, h and max_iter are required");
+  TCSCF_CHECK(ctx, (n_up + n_down) % 2 == 0 && n_up == n_down, TCSCF_ERR_INVALID_ARGUMENT, "the graph SCF is restricted closed shell");
+  TCSCF_CHECK(ctx, precision >= TCSCF_PREC_FP64 && precision <= TCSCF_PREC_TF32, TCSCF_ERR_INVALID_ARGUMENT, "unknown precision");
+  int launches = 0;
+  int const st = scfGraph(ctx, *g1, *g2, (n_up + n_down) / 2, S, h, respect_symmetry, precision, tol, max_iter, capture, energy, iterations,
+                          density, eigenvalues, &launches);
+  if (graph_launches) *graph_launches = launches;
+  return st;
 }
 
 }  // extern "C"

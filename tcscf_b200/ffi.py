@@ -84,6 +84,7 @@ SIGNATURES: dict[str, tuple] = {
     "tcscf_fock_build_device": (_I, [_P, _I, _I, _I, _P, _P, _I, _I, _P, _P, _P]),
     "tcscf_fock_build_precomputed": (_I, [_P, _I, _I, _I, _D, _D, _I, _D, _D, _D]),
     "tcscf_scf": (_I, [_P, _I, _I, _I, _I, _I, _D, _D, _I, _I, C.c_double, _I, _D, C.POINTER(_I), _D, _D]),
+    "tcscf_scf_graph": (_I, [_P, _I, _I, _I, _I, _D, _D, _I, _I, C.c_double, _I, _I, _D, C.POINTER(_I), _D, _D, C.POINTER(_I)]),
 }
 
 _lib: C.CDLL | None = None

@@ -2,8 +2,8 @@
 //
 // Runs without a device: grids, basis-set loading, analytic overlap / core matrices and the error
 // mapping.  The device paths (QMCGrid, fockBuild, the SCF classes, computeF / computeV, the 4- and
-// 6-index tensors) are compiled here, so every template of the header is instantiated, and run only
-// when a context can be created.
+// 6-index tensors) are compiled here, so every template of the header is instantiated, and run when a
+// context can be created (tests/test_gpu_cpp_shim.py on a B200).
 //
 //   shim_host <basis-set directory holding TZ3P/He>
 #include <cmath>
@@ -40,7 +40,8 @@ tcscf::gpu::QMCGrid upload(tcscf::gpu::Context & ctx, tcscf::gpu::QuadratureGrid
   return d;
 }
 
-// device paths: one He core-guess SCF and one Fock build through every class of the header
+// device paths: He through every class of the header; the energies are printed as "key value" lines
+// for tests/test_gpu_cpp_shim.py, which checks them against the oracle
 void deviceRun(tcscf::gpu::Context & ctx)
 {
   using namespace tcscf::gpu;
@@ -49,29 +50,44 @@ void deviceRun(tcscf::gpu::Context & ctx)
   auto const [r, wr] = radialGrid(40, TCSCF_MAP_ONE_PLUS_X);
   QuadratureGrid const g = productGrid(r, wr, octahedron());
   QMCGrid G(ctx, g);
-  G.setBasisFunctions(basis);
+  G.setBasisFunctions(basis, true);
   auto const [S, H] = overlapCore(basis, 2);
   RCSHartreeFock hf(1, 1, static_cast<int>(basis.size()));
-  double const E = hf.compute(S, H, G, G, true, TCSCF_PREC_FP64, 1e-8);
+  double const E = hf.compute(S, H, G, G, true, TCSCF_PREC_FP64, 1e-10);
   std::vector<cplx> D(hf.density());
+  FockBuild const f64 = fockBuild(G, G, D, H, true, TCSCF_PREC_FP64);
   FockBuild const fb = fockBuild(G, G, D, H, true, TCSCF_PREC_BF16X3);
-  std::printf("device: He SCF %.8f in %d iterations, split-BF16 rebuild %.8f\n", E, hf.numberOfConvergenceLoops(), fb.energy);
+  std::printf("E_SCF %.15f\nITER %d\nE_FOCK_FP64 %.15f\nE_FOCK_BF16X3 %.15f\n", E, hf.numberOfConvergenceLoops(), f64.energy, fb.energy);
+  expect(std::abs(f64.energy - E) < 1e-10, "FP64 Fock build at the converged density reproduces the SCF energy");
   expect(std::abs(fb.energy - E) < 1e-6, "split-BF16 Fock build at the converged density reproduces the SCF energy");
+  RCSHartreeFock dev(1, 1, static_cast<int>(basis.size()));
+  double const Eg = dev.computeOnDevice(S, H, G, G, true, TCSCF_PREC_FP64, 1e-10);
+  std::printf("E_GRAPH %.15f\n", Eg);
+  expect(dev.graphLaunches() == 1 && std::abs(Eg - E) < 1e-8, "device-loop SCF (one graph launch) reproduces the SCF energy");
+  UOSHartreeFock uos(1, 1, static_cast<int>(basis.size()));
+  double const Eu = uos.compute(S, H, G, G, true, TCSCF_PREC_FP64, 1e-10);
+  std::printf("E_UOS %.15f\n", Eu);
+  expect(std::abs(Eu - E) < 1e-8, "UOS SCF of the closed-shell atom equals the RCS energy");
   DeviceTensor F = computeF(G, G);
   expect(F.handle() != 0, "computeF keeps a device tensor");
+  DeviceTensor Fm = computeF(G, G, TCSCF_K_INV_R12, nullptr, TCSCF_PREC_BF16X3);
+  expect(Fm.handle() != 0, "computeF in split BF16 keeps a device tensor");
   std::vector<cplx> const vals = G.basisValues();
   expect(vals.size() == std::size_t(g.size()) * basis.size(), "basisValues is [N][nb]");
+  auto const [Sq, Hq] = overlapCoreQuadrature(G, 2);
+  double ds = 0;
+  for (std::size_t i = 0; i < Sq.size(); ++i) ds = std::max(ds, std::abs(Sq[i] - S[i]));
+  std::printf("S_QUAD_ERR %.3e\n", ds);
+  tcscf_ochi u{};
+  u.a = 1.0; u.a12 = 1.0; u.nterms = 1; u.S[0][0] = 1; u.c[0][0] = -0.5; u.c[0][1] = -0.25;
+  DeviceTensor V = computeV(G, G, TCSCF_K_GRAD_U_SAME, u);
+  expect(V.handle() != 0, "computeV keeps a device tensor");
   if (false) {  // instantiated, not run: the remaining device entry points of the header
-    tcscf_ochi u{};
     QMCGrid G2 = upload(ctx, qmcGrid(2, sobol(2, 64, 1)), basis);
-    (void)computeV(G, G, TCSCF_K_GRAD_U_SAME, u);
     (void)integrateAllR1R2(G, G2, false, TCSCF_K_INV_R12);
     (void)threeElectronIntegrals(G, G, u);
-    (void)overlapCoreQuadrature(G, 2);
-    UOSHartreeFock uos(1, 1, 6);
-    (void)uos.compute(S, H, G, G);
     TCHartreeFock tc(1, 1, 6);
-    (void)tc.compute(S, H, G, F, F, F, F);
+    (void)tc.compute(S, H, G, F, F, V, V);
     double a = 0, b = 0;
     int n = 0;
     ctx.lastTiming(a, b, n);

@@ -14,7 +14,7 @@ KR = dict(n=406_000, nb=120, nocc=18)
 
 
 def test_split_bf16_roofline_at_kr():
-    r = bench.roofline(ffi.PREC_BF16X3, KR["n"], KR["nb"], KR["nocc"], 458.2, bench.PEAKS_FALLBACK, "fallback", 37.0, 2.889e10)
+    r = bench.roofline(ffi.PREC_BF16X3, KR["n"], KR["nb"], KR["nocc"], 458.2, bench.PEAKS_FALLBACK, "fallback", 2.889e10)
     n2 = KR["n"] ** 2
     assert r["bound"] == "tensor" and r["unit"] == "TFLOP/s" and r["peak"] == 1590.0
     assert r["achieved"] == pytest.approx(2 * n2 * (120 * 18 + 1) / 0.4582 / 1e12)
@@ -27,13 +27,21 @@ def test_split_bf16_roofline_at_kr():
 
 
 def test_tf32_and_fp64_rooflines():
-    t = bench.roofline(ffi.PREC_TF32, KR["n"], KR["nb"], KR["nocc"], 312.0, bench.PEAKS_FALLBACK, "fallback", 37.0, None)
+    t = bench.roofline(ffi.PREC_TF32, KR["n"], KR["nb"], KR["nocc"], 312.0, bench.PEAKS_FALLBACK, "fallback", None)
     assert t["peak"] == 795.0 and t["frac"] == pytest.approx(t["achieved"] / 795.0)
     # one rank chunk of 32: GEMM1 2 x 32 and GEMM2 2 x 128 flops per pair
     assert t["issued_tensor_tflops"] == pytest.approx(KR["n"] ** 2 * (64 + 256) / 0.312 / 1e12)
-    f = bench.roofline(ffi.PREC_FP64, KR["n"], KR["nb"], KR["nocc"], 3770.0, bench.PEAKS_FALLBACK, "fallback", 37.0, None)
+    f = bench.roofline(ffi.PREC_FP64, KR["n"], KR["nb"], KR["nocc"], 3770.0, bench.PEAKS_FALLBACK, "fallback", None)
     assert f["bound"] == "fp64" and f["peak"] == 37.0 and "issued_tensor_tflops" not in f
-    assert f["achieved"] == pytest.approx(2 * KR["n"] ** 2 * 2161 / 3.77 / 1e12)
+    # the FP64 kernel's roofline counts the factored flops it performs; F_alg is its effective rate
+    assert f["achieved"] == pytest.approx(2 * KR["n"] ** 2 * (18 + 120 + 1) / 3.77 / 1e12)
+    assert f["effective_tflops"] == pytest.approx(2 * KR["n"] ** 2 * 2161 / 3.77 / 1e12)
+    # measured matmul rates take precedence over the nominal FP64 figure and the half-BF16 TF32 rule
+    m = dict(bench.PEAKS_FALLBACK, fp64_tflops=35.5, tf32_tflops=820.0)
+    f = bench.roofline(ffi.PREC_FP64, KR["n"], KR["nb"], KR["nocc"], 3770.0, m, "fallback", None)
+    assert f["peak"] == 35.5 and "measured" in f["peak_source"]
+    t = bench.roofline(ffi.PREC_TF32, KR["n"], KR["nb"], KR["nocc"], 312.0, m, "fallback", None)
+    assert t["peak"] == 820.0 and "measured" in t["peak_source"]
 
 
 def test_measured_peaks_take_precedence(tmp_path, monkeypatch):

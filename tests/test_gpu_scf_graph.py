@@ -1,0 +1,77 @@
+"""The SCF loop on the device (tcscf_scf_graph): RCSHartreeFock::compute (HartreeFock.cpp:785-882) with
+every iteration's build, assembly, convergence test and eigen-solve on the device.
+
+* The captured run (one CUDA graph launch whose conditional WHILE node repeats the iteration) and the
+  uncaptured run (the same launches per iteration, the host reading the loop state) give bit-identical
+  energies, densities and eigenvalues, and the captured run reports its single graph launch.
+* Against the host-driven loop (tcscf_scf with the real-harmonic eigen-solve, cuSOLVER dsygvd) and the
+  oracle's SCF: the converged energies within 1e-8 Eh (different eigen-solvers, |dE| < 1e-10).
+* The split-BF16 build inside the graph loop converges to the FP64 energy within 1 uEh.
+* An iteration limit that is too small gives TCSCF_ERR_NOT_CONVERGED from the device-side test.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from tcscf_b200 import api, ffi, grids
+from tcscf_b200 import basis as wl
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ne_case(ctx):
+    w = wl.ne()
+    g = grids.product_grid(40, 17)
+    G = api.QMCGrid(ctx, g)
+    G.setBasisFunctions(w.basis)
+    S, h = api.overlap_core(w.basis, w.Z)
+    yield w, g, G, S, h
+    G.close()
+
+
+def _graph(w, G, S, h, precision, capture, tol=1e-10, max_iter=60):
+    hf = api.RCSHartreeFock(w.n_up, w.n_down, w.nb)
+    E = hf.computeOnDevice(S, h, G, G, precision=precision, tol=tol, max_iter=max_iter, capture=capture)
+    return E, hf
+
+
+def test_captured_and_uncaptured_device_loops_are_bit_identical(ctx, ne_case):
+    w, g, G, S, h = ne_case
+    for prec in (ffi.PREC_FP64, ffi.PREC_BF16X3):
+        Ec, hc = _graph(w, G, S, h, prec, True)
+        Eu, hu = _graph(w, G, S, h, prec, False)
+        assert hc.graphLaunches == 1 and hu.graphLaunches == 0
+        assert Ec == Eu, (prec, Ec, Eu)
+        assert hc.numberOfConvergenceLoops() == hu.numberOfConvergenceLoops()
+        np.testing.assert_array_equal(hc.density, hu.density)
+        np.testing.assert_array_equal(hc.eigenvalues, hu.eigenvalues)
+
+
+def test_device_loop_matches_host_loop_and_oracle(ctx, ne_case):
+    w, g, G, S, h = ne_case
+    Eg, hg = _graph(w, G, S, h, ffi.PREC_FP64, True)
+    hf = api.RCSHartreeFock(w.n_up, w.n_down, w.nb)
+    Eh = hf.compute(S, h, G, G, precision=ffi.PREC_FP64, tol=1e-10, max_iter=60, real_eigensolve=True)
+    assert abs(Eg - Eh) < 1e-8, (Eg, Eh, hg.numberOfConvergenceLoops(), hf.numberOfConvergenceLoops())
+    np.testing.assert_allclose(hg.eigenvalues[0, : w.n_up], hf.eigenvalues[0, : w.n_up], rtol=0, atol=1e-7)
+    vals = oracle.basis_values(g.points, w.basis)
+    F = oracle.compute_F(g.points, g.points, g.weights, vals, w.nb)
+    st, Eo, it, D, eig = oracle.scf(1, w.n_up, w.n_down, F, vals, g.weights, S, h, tol=1e-10, max_iter=60)
+    assert st == 0
+    assert abs(Eg - Eo) < 1e-8, (Eg, Eo)
+
+
+def test_device_loop_split_bf16_within_one_microhartree(ctx, ne_case):
+    w, g, G, S, h = ne_case
+    E64, _ = _graph(w, G, S, h, ffi.PREC_FP64, True, tol=1e-9)
+    Em, hm = _graph(w, G, S, h, ffi.PREC_BF16X3, True, tol=1e-9)
+    assert abs(Em - E64) <= 1e-6, (Em, E64, hm.numberOfConvergenceLoops())
+
+
+def test_device_loop_iteration_limit(ctx, ne_case):
+    w, g, G, S, h = ne_case
+    hf = api.RCSHartreeFock(w.n_up, w.n_down, w.nb)
+    with pytest.raises(api.ConvergenceError):
+        hf.computeOnDevice(S, h, G, G, precision=ffi.PREC_FP64, tol=1e-14, max_iter=3, capture=True)
+    assert hf.numberOfConvergenceLoops() == 3
