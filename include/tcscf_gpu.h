@@ -173,6 +173,14 @@ int tcscf_grid_set_basis(tcscf_ctx * ctx, int grid, const tcscf_sto * basis, int
 /* copies QMCGrid::basisValues / basisGradients to host buffers (either may be NULL) */
 int tcscf_grid_basis_values(tcscf_ctx * ctx, int grid, double * values, double * gradients);
 
+/* Near-coincident pairs of two grids (no reference counterpart): the r1 / r2 point pairs that are
+ * closer than 2^-16 |r1| (below what FP32 coordinates resolve) without being identical.  The
+ * tensor-core paths leave these pairs out of their FP32 kernel generation and add them back evaluated
+ * in FP64, so every precision follows the reference's rule that only an exactly coincident pair
+ * contributes 0 (IntegrationTest.cpp:298-309).  The list is found on the first use of the grid pair
+ * (here or in a tensor-core build) and kept until either grid is destroyed. */
+int tcscf_near_coincident_pairs(tcscf_ctx * ctx, int r1, int r2, int * count);
+
 /* quadrature S_ij = sum_g w phi_i^* phi_j and H_ij = sum_g w (1/2 grad phi_i^* . grad phi_j - Z phi_i^* phi_j / r)
  * on a 3-D grid with gradients; S, H complex [nb][nb] */
 int tcscf_overlap_core_quadrature(tcscf_ctx * ctx, int grid, int Z, double * S, double * H);

@@ -151,6 +151,13 @@ class QMCGrid:
             ffi.lib().tcscf_grid_destroy(self.ctx.handle, self.id)
             self._id = C.c_int()
 
+    def nearCoincidentPairs(self, r2Grid: "QMCGrid") -> int:
+        """Pairs with this grid as r1 and r2Grid as r2 that are closer than 2^-16 |r1| without being
+        identical (tcscf_near_coincident_pairs): the tensor-core paths evaluate them in FP64."""
+        n = C.c_int()
+        _raise(ffi.lib().tcscf_near_coincident_pairs(self.ctx.handle, self.id, r2Grid.id, C.byref(n)), self.ctx.handle)
+        return n.value
+
 
 def loadSTO(directory: str, basisSet: str, element: str, maxL: int) -> list:
     """loadSTO (SlaterTypeOrbital.cpp:24-75): the (alpha, n, l, m) Slater-type orbitals of `element`

@@ -58,6 +58,13 @@ struct Scratch {
   size_t bytes = 0;
 };
 
+// pairs (r1 index, r2 index) of two grids that the tensor-core kernels drop for FP32 resolution but
+// that are not exactly coincident in FP64 (near_pairs.cu); d is device memory, null when count is 0
+struct NearList {
+  int2 * d = nullptr;
+  int count = 0;
+};
+
 }  // namespace tcscf
 
 struct tcscf_ctx {
@@ -98,6 +105,8 @@ struct tcscf_ctx {
   int tuneMeasurements = 0;
   cudaEvent_t tuneEv[2] = {nullptr, nullptr};
   std::map<std::string, tcscf::Scratch> scratch;
+  // near-coincident pair lists per (r1 grid, r2 grid), found on the first tensor-core use of the pair
+  std::map<std::pair<const void *, const void *>, tcscf::NearList> nearPairs;
   // device buffers of the most recent direct Fock build (for tcscf_last_potentials)
   const double * lastVH = nullptr;
   const double * lastT = nullptr;

@@ -13,7 +13,8 @@
 // then grad_1 u(r1,r2) = u'(r12) (r1 - r2) / r12 = -grad_1 u(r2,r1), so the TC scalar kernel is
 // 2 / r12 - 2 u'^2, with u'(r12) = t^2 P(r12 t), t = 1 / (r12 + a12), P(z) = sum_n p_n z^n and
 // p_n = a12 sum_{k: i_k = n + 1} i_k c_k.  An exactly coincident pair (and a separation whose square is
-// below the smallest normal FP32) contributes 0 in every kind, as in the FP64 path.
+// below nearThreshold, the FP32 resolution of r1) contributes 0 here; the near-pair correction adds the
+// pairs that are not exactly coincident back in FP64, so every kind follows the FP64 path's rule.
 //
 // The kernel values are generated in FP32 from FP32 coordinates (rsqrt and reciprocal estimates each
 // refined by one Newton step) and enter the tensor cores as 24-bit fixed-point BF16 slices (four
@@ -54,7 +55,7 @@ struct PairParams {
   int kind, comp, same, npoly;
   float a12;
   float poly[kMaxPoly];             // p_n of u'(r12) = t^2 sum_n p_n (r12 t)^n
-  const float4 * r1xyz;             // [n1pad] {x, y, z, 0}
+  const float4 * r1xyz;             // [n1pad] {x, y, z, nearThreshold}
   const float4 * r2pairs;           // [n2pad] pair layout {x0,x1,y0,y1}{z0,z1,0,0}
   const float * cinv;               // [nBlocks][NBtot] inverse column scales of Vp
   int NBtot;
@@ -97,7 +98,7 @@ __device__ __forceinline__ uint64_t f2rcp(uint64_t s)
 
 // Kernel values of two pairs (packed): d = r1 - r2 components, r2sq = |d|^2.
 template <int KIND>
-__device__ __forceinline__ uint64_t pairKernel(PairParams const & P, uint64_t dx, uint64_t dy, uint64_t dz, uint64_t r2sq)
+__device__ __forceinline__ uint64_t pairKernel(PairParams const & P, uint64_t dx, uint64_t dy, uint64_t dz, uint64_t r2sq, float thr)
 {
   float r2a, r2b;
   f2unpack(r2sq, r2a, r2b);
@@ -124,8 +125,8 @@ __device__ __forceinline__ uint64_t pairKernel(PairParams const & P, uint64_t dx
   }
   float ga, gb;
   f2unpack(g, ga, gb);
-  ga = r2a >= kMinNormal ? ga : 0.0f;
-  gb = r2b >= kMinNormal ? gb : 0.0f;
+  ga = r2a >= thr ? ga : 0.0f;
+  gb = r2b >= thr ? gb : 0.0f;
   return f2pack(ga, gb);
 }
 
@@ -370,7 +371,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           uint64_t const dy = f2sub(p1y, f2pack(qa.z, qa.w));
           uint64_t const dz = f2sub(p1z, f2pack(qb.x, qb.y));
           uint64_t const r2 = f2fma(dx, dx, f2fma(dy, dy, f2mul(dz, dz)));
-          xv[pr] = pairKernel<KIND>(P, dx, dy, dz, r2);
+          xv[pr] = pairKernel<KIND>(P, dx, dy, dz, r2, p1.w);
         }
         // row maximum of |X| over the block's 64 r2 points: this warp's 32 and the other half's
         float mx = 0.0f;
@@ -567,7 +568,7 @@ int contractPairsTensor(tcscf_ctx * ctx, Contraction const & c, int precision)
   TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   if (hs != 0) return fail(ctx, TCSCF_ERR_TIMEOUT, "tensor-core precompute contraction: bounded wait expired (code " + std::to_string(hs) + ")");
   if (nSplit > 1) TCSCF_TRY(sumSplitsLaunch(ctx, int64_t(c.n1) * c.ncol, nSplit, int64_t(c.n1) * c.ldt, part, c.T, c.n1, c.ncol, c.ldt, c.ldt));
-  return TCSCF_OK;
+  return nearCorrect(ctx, c);
 }
 
 }  // namespace tcscf

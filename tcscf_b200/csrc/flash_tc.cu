@@ -424,10 +424,10 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             y = f2fma(f2mul(y, mHalf), em, y);
             float ya, yb;
             f2unpack(y, ya, yb);
-            // a coincident pair contributes 0; so does a separation whose square is subnormal, which
-            // rsqrt.approx.ftz flushes to 0 (its estimate +inf would turn the Newton step into NaN)
-            ya = r2a >= kMinNormal ? ya : 0.0f;
-            yb = r2b >= kMinNormal ? yb : 0.0f;
+            // pairs below the FP32 resolution of r1 (nearThreshold, packed as r1's w) are dropped here;
+            // the near-pair correction adds those that are not exactly coincident in FP64
+            ya = r2a >= p1.w ? ya : 0.0f;
+            yb = r2b >= p1.w ? yb : 0.0f;
             y = f2pack(ya, yb);
             vsum2 = f2fma(y, f2pack(qb.z, qb.w), vsum2);
             float2 const a2 = sa[pr];
@@ -622,12 +622,12 @@ __global__ void kPackVt(int64_t n, int64_t npad, int nb, int NB, const double * 
   }
 }
 
-// pts [3][n] -> float4 [npad] (x, y, z, 0); padding points sit far away
+// pts [3][n] -> float4 [npad] (x, y, z, nearThreshold(x, y, z)); padding points sit far away
 __global__ void kPackCoords(int64_t n, int64_t npad, const double * pts, float4 * out)
 {
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < npad; i += int64_t(gridDim.x) * blockDim.x) {
-    if (i < n) out[i] = make_float4(float(pts[i]), float(pts[n + i]), float(pts[2 * n + i]), 0.0f);
-    else out[i] = make_float4(1.0e4f, 1.0e4f, 1.0e4f, 0.0f);
+    float const x = i < n ? float(pts[i]) : 1.0e4f, y = i < n ? float(pts[n + i]) : 1.0e4f, z = i < n ? float(pts[2 * n + i]) : 1.0e4f;
+    out[i] = make_float4(x, y, z, nearThreshold(x, y, z));
   }
 }
 
@@ -1174,7 +1174,10 @@ int tensorRankLimit(Contraction const & c, int precision) { return precision == 
 int contractTensor(tcscf_ctx * ctx, Contraction const & c, int precision)
 {
   int const lim = tensorRankLimit(c, precision);
-  if (c.R <= lim) return contractTensorOnce(ctx, c, precision, true);
+  if (c.R <= lim) {
+    TCSCF_TRY(contractTensorOnce(ctx, c, precision, true));
+    return nearCorrect(ctx, c);
+  }
   // rho is linear in the density factor: a rank beyond what one launch's psi tiles hold (32 for TF32
   // or with nb > 64, 64 otherwise) is contracted in column chunks whose T add up (the Coulomb potential,
   // which does not depend on the factor, with the first); ev[2] / ev[3] span all chunks
@@ -1186,6 +1189,7 @@ int contractTensor(tcscf_ctx * ctx, Contraction const & c, int precision)
     ck.psi1 = c.psi1 + r0;
     ck.psi2 = c.psi2 + r0;
     if (r0 > 0) { ck.coul = nullptr; ck.VH = nullptr; ck.T = tmp; }
+    ck.near = nullptr;   // the near-pair correction runs once with the whole factor
     TCSCF_TRY(contractTensorOnce(ctx, ck, precision, r0 == 0));
     if (r0 > 0) {
       kAddTChunk<<<gridBlocks(c.n1 * c.ncol, 256), 256, 0, ctx->stream>>>(c.n1, c.ncol, c.ldt, tmp, c.T);
@@ -1193,7 +1197,7 @@ int contractTensor(tcscf_ctx * ctx, Contraction const & c, int precision)
     }
   }
   cudaEventRecord(ctx->ev[3], ctx->stream);
-  return TCSCF_OK;
+  return nearCorrect(ctx, c);
 }
 
 namespace tc {

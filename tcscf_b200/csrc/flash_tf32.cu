@@ -319,10 +319,10 @@ __global__ void __launch_bounds__(NTHREADS, 1)
             y = f2fma(f2mul(y, mHalf), em, y);
             float ya, yb;
             f2unpack(y, ya, yb);
-            // a coincident pair contributes 0; so does a separation whose square is subnormal, which
-            // rsqrt.approx.ftz flushes to 0 (its estimate +inf would turn the Newton step into NaN)
-            ya = r2a >= kMinNormal ? ya : 0.0f;
-            yb = r2b >= kMinNormal ? yb : 0.0f;
+            // pairs below the FP32 resolution of r1 (nearThreshold, packed as r1's w) are dropped here;
+            // the near-pair correction adds those that are not exactly coincident in FP64
+            ya = r2a >= p1.w ? ya : 0.0f;
+            yb = r2b >= p1.w ? yb : 0.0f;
             y = f2pack(ya, yb);
             vsum2 = f2fma(y, f2pack(qb.z, qb.w), vsum2);
             xv[pr] = f2mul(y, f2pack(rho[pr >> 3][2 * (pr & 7)], rho[pr >> 3][2 * (pr & 7) + 1]));

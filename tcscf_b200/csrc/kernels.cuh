@@ -30,7 +30,15 @@ struct Contraction {
   int component = 0;
   const tcscf_ochi * jastrow = nullptr;
   int nSplit = 0;                  // r2 split count of the tensor-path launch (0: the default rule)
+  const NearList * near = nullptr; // tensor paths: pairs dropped in FP32 that the FP64 rule keeps
 };
+
+// near-coincident pairs (near_pairs.cu): the list of (g1, g2), found once per grid pair and kept on the
+// context; its release when a grid goes away; the FP64 contributions of the listed pairs added to
+// c.T (and c.VH) after a tensor contraction of c (direct form when c.R > 0, else the precompute form)
+int nearPairsFor(tcscf_ctx * ctx, Grid const & g1, Grid const & g2, NearList const ** out);
+void nearPairsForget(tcscf_ctx * ctx, Grid const * g);
+int nearCorrect(tcscf_ctx * ctx, Contraction const & c);
 
 int contractFp64(tcscf_ctx * ctx, Contraction const & c);
 

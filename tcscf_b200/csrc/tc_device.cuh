@@ -21,6 +21,18 @@ constexpr int kRegsLaunch = 168, kRegsProducer = 56, kRegsCompute = 224;
 static_assert(128 * kRegsProducer + 256 * kRegsCompute <= NTHREADS * kRegsLaunch, "register split exceeds the launch allocation");
 constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s per wait
 constexpr float kMinNormal = 1.17549435e-38f;                // smallest normal FP32 (2^-126)
+// Pairs closer than 2^-16 |r1| are below what FP32 coordinates resolve (their rounding, 2^-24 |r| per
+// coordinate, is then more than 1/256 of the separation).  The tensor kernels drop every pair whose FP32
+// squared separation is below nearThreshold(r1) (never below the smallest normal FP32, where the
+// rsqrt estimate turns the Newton step into NaN), and the near-pair correction (near_pairs.cu) adds
+// the pairs that are not exactly coincident back with their FP64 value, so the mixed paths follow the
+// FP64 rule: only an exactly coincident pair contributes 0.  Evaluated with explicit round-to-nearest
+// operations (no contraction), so every kernel that packs or tests a point gets the same bits.
+__device__ __forceinline__ float nearThreshold(float x, float y, float z)
+{
+  float const s = __fadd_rn(__fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y)), __fmul_rn(z, z));
+  return fmaxf(kMinNormal, __fmul_rn(s, 2.3283064365386963e-10f));   // 2^-32 |r1|^2
+}
 // a waiting thread sleeps in mbarrier.try_wait (woken when the phase completes) instead of spinning
 // on the issue slots the compute warps need
 constexpr uint32_t kSuspendHintNs = 1000000;

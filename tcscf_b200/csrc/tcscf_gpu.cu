@@ -1070,6 +1070,7 @@ int fockBuildDevice(tcscf_ctx * ctx, Grid & g1, Grid & g2, int nspin, const doub
       c.p1 = g1.pts; c.p2 = g2.pts; c.psi1 = psi1; c.psi2 = psi2; c.ldpsi = ldpsi;
       c.V = V; c.ldv = nb; c.T = part == 0 ? Ts : Ti; c.ldt = ldt;
       c.vtPacked = vtPacked;
+      if (precision != TCSCF_PREC_FP64) TCSCF_TRY(nearPairsFor(ctx, g1, g2, &c.near));
       if (part == 0) {
         kCoulombSource<<<gridBlocks(n2, 256), 256, 0, ctx->stream>>>(n2, R, psi1at2, psi2, ldpsi, g2.w, scale, coul);
         TCSCF_LAUNCH(ctx);
@@ -1197,8 +1198,14 @@ int fockBuildBatch(tcscf_ctx * ctx, int count, Grid * const * g1s, Grid * const 
     c.T = T; c.VH = VH; c.V = V; c.ldv = nb;
     c.psi1 = psi1; c.psi2 = psi2; c.coul = coul;
     std::string why;
-    bool const eligible = (precision == TCSCF_PREC_BF16X3 || precision == TCSCF_PREC_TF32) && f.R > 0 && !f.complex &&
-                          tensorPathAvailable(c, precision, &why) && tensorArenaBytes(c, precision) <= arenaBytes[k];
+    bool eligible = (precision == TCSCF_PREC_BF16X3 || precision == TCSCF_PREC_TF32) && f.R > 0 && !f.complex &&
+                    tensorPathAvailable(c, precision, &why) && tensorArenaBytes(c, precision) <= arenaBytes[k];
+    if (eligible) {
+      // an instance whose grids hold near-coincident pairs is built on its own (with the FP64 correction)
+      NearList const * nl = nullptr;
+      TCSCF_TRY(nearPairsFor(ctx, g1, g2, &nl));
+      eligible = nl->count == 0;
+    }
     if (!eligible) continue;
     kWeightedBasis<<<gridBlocks(n2 * nb, 256), 256, 0, ctx->stream>>>(n2, nb, g2.phiR, g2.w, scale, V);
     TCSCF_LAUNCH(ctx);
@@ -1319,6 +1326,7 @@ int precomputeTensor(tcscf_ctx * ctx, int r1, int r2, int kernel, const tcscf_oc
   if (precision != TCSCF_PREC_FP64) {
     std::string why;
     TCSCF_CHECK(ctx, pairsTensorAvailable(c, precision, &why), TCSCF_ERR_UNSUPPORTED, why);
+    TCSCF_TRY(nearPairsFor(ctx, *g1, *g2, &c.near));
   }
   void * p = nullptr;
   TCSCF_TRY(scratch(ctx, "computeF", sizeof(double) * (size_t(n2) * np + size_t(n1) * np), &p));
@@ -1647,6 +1655,7 @@ int scfGraph(tcscf_ctx * ctx, Grid & g1, Grid & g2, int nocc, const double * S, 
   size_t arenaBytes = 0;
   if (tensor) {
     TCSCF_TRY(tensorPackedV(ctx, g2, Vw, scale, &c.vtPacked));
+    TCSCF_TRY(nearPairsFor(ctx, g1, g2, &c.near));
     std::string why;
     TCSCF_CHECK(ctx, tensorPathAvailable(c, precision, &why), TCSCF_ERR_UNSUPPORTED, "graph SCF tensor path: " + why);
     arenaBytes = tensorArenaBytes(c, precision);
@@ -1668,6 +1677,7 @@ int scfGraph(tcscf_ctx * ctx, Grid & g1, Grid & g2, int nocc, const double * S, 
     if (tensor) {
       TCSCF_TRY(tensorPrepare(ctx, c, precision, arena, arenaBytes, tp));
       TCSCF_TRY(tensorPlanLaunch(ctx, plan));
+      TCSCF_TRY(nearCorrect(ctx, c));
     } else {
       TCSCF_TRY(contractFp64(ctx, c));
     }
@@ -1840,6 +1850,8 @@ int tcscf_ctx_destroy(tcscf_ctx * ctx)
   if (ctx->gridPool) cudaMemPoolDestroy(ctx->gridPool);
   for (auto & kv : ctx->tensors) cudaFree(kv.second.d);
   for (auto & kv : ctx->scratch) cudaFree(kv.second.p);
+  for (auto & kv : ctx->nearPairs)
+    if (kv.second.d) cudaFree(kv.second.d);
   for (auto & e : ctx->ev) cudaEventDestroy(e);
   for (auto & e : ctx->tuneEv)
     if (e) cudaEventDestroy(e);
@@ -1961,8 +1973,22 @@ int tcscf_grid_destroy(tcscf_ctx * ctx, int grid)
   if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
   Grid * g = findGrid(ctx, grid);
   TCSCF_CHECK(ctx, g, TCSCF_ERR_INVALID_ARGUMENT, "unknown grid handle");
+  nearPairsForget(ctx, g);
   gridReleaseAll(ctx, *g);
   ctx->grids.erase(grid);
+  return TCSCF_OK;
+}
+
+int tcscf_near_coincident_pairs(tcscf_ctx * ctx, int r1, int r2, int * count)
+{
+  if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
+  TCSCF_CUDA(ctx, cudaSetDevice(ctx->device));
+  Grid * g1 = findGrid(ctx, r1);
+  Grid * g2 = findGrid(ctx, r2);
+  TCSCF_CHECK(ctx, g1 && g2 && count, TCSCF_ERR_INVALID_ARGUMENT, "unknown grid handle or null count");
+  NearList const * nl = nullptr;
+  TCSCF_TRY(nearPairsFor(ctx, *g1, *g2, &nl));
+  *count = nl->count;
   return TCSCF_OK;
 }
 

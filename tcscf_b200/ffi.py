@@ -50,6 +50,7 @@ SIGNATURES: dict[str, tuple] = {
     "tcscf_last_error": (C.c_char_p, [_P]),
     "tcscf_ctx_stream": (_I, [_P, C.POINTER(_P)]),
     "tcscf_selftest_bounded_wait": (_I, [_P, C.c_double]),
+    "tcscf_near_coincident_pairs": (_I, [_P, _I, _I, C.POINTER(_I)]),
     "tcscf_synchronize": (_I, [_P]),
     "tcscf_last_timing": (_I, [_P, _D, _D, C.POINTER(_I)]),
     "tcscf_last_potentials": (_I, [_P, _D, _D]),
