@@ -8,6 +8,7 @@
 #include <nvtx3/nvToolsExt.h>
 #include <cmath>
 #include <cstdint>
+#include <array>
 #include <map>
 #include <string>
 #include <vector>
@@ -94,12 +95,12 @@ struct tcscf_ctx {
   // set while a conditional graph body is captured: the contraction routines then record no timing
   // events (event nodes are not allowed inside a conditional body)
   int capturing = 0;
-  // autotuner (tcscf_set_autotune): the measured r2 split count of the tensor-path launch per shape
+  // autotuner (tcscf_set_autotune): the measured schedule (r2 split count, tile class) of the tensor-path launch per shape
   // {n1, n2, padded nb, padded rank, precision}, the split policy per batch signature, the policy
   // the batch build applies (1: the default rule, 0: no split, k > 1: k x the default split),
   // candidate measurements taken, and the two events that time them
   int autotune = 0;
-  std::map<std::vector<int64_t>, int> tunedSplit;
+  std::map<std::vector<int64_t>, std::array<int, 3>> tunedSplit;   // {r2 split, T tile width, TMA stages}
   std::map<std::vector<int64_t>, int> tunedBatchPolicy;
   int batchSplitPolicy = 1;
   int tuneMeasurements = 0;

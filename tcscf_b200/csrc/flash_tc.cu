@@ -35,6 +35,7 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <array>
 #include <vector>
 
 #include "tc_device.cuh"
@@ -42,7 +43,8 @@
 namespace tcscf {
 namespace tc {
 
-// TMA stages: three when the tile shapes leave room in shared memory
+// TMA stages (the default rule): three when the tile shapes leave room in shared memory; the autotuner
+// may also try two for (NB 64, RP 32)
 __host__ __device__ constexpr int stagesFor(int NB, int RP) { return NB == 64 && RP == 32 ? 3 : 2; }
 // X precision: XS = 2 slices (16 bits, u s in [2^15, 2^16)) or XS = 3 (24 bits, stored as the four
 // slices h, m, l/256, m/256); its tile buffers: two (GEMM2 of block g - 1 overlaps the writing of
@@ -61,9 +63,9 @@ constexpr int kMinExp = -100;
 constexpr uint32_t TCOL0 = 256;
 
 // RP: padded rank of rho (GEMM1 K): 32 (64-byte rows, 64B swizzle) or 64 (128-byte rows, 128B swizzle)
-template <int NB, int RP, int XS>
+template <int NB, int RP, int XS, int NS>
 struct __align__(1024) Smem {
-  static constexpr int NSTAGE = stagesFor(NB, RP);
+  static constexpr int NSTAGE = NS;
   uint8_t v[NSTAGE][3][NB * BK * 2];       // Vt block h / m / l/256: SW128 K-major [NB rows][64]
   static constexpr int XBUF = xBuffersFor(NB, RP, XS);
   uint8_t x[XBUF][xSlicesFor(XS)][BM * BK * 2];   // X tile slices per buffer: SW128 K-major [128 rows][64]
@@ -164,13 +166,13 @@ __device__ __forceinline__ bool flushBlock(SmemT & S, uint32_t taddr, uint32_t f
 }
 
 // ---- the kernel ------------------------------------------------------------------------------------
-template <int NB, int RP, int XS>
+template <int NB, int RP, int XS, int NS>
 __global__ void __launch_bounds__(NTHREADS, 1)
     kFlashTc(Params P)
 {
   extern __shared__ uint8_t smemRaw[];
-  Smem<NB, RP, XS> & S = *reinterpret_cast<Smem<NB, RP, XS> *>((reinterpret_cast<uintptr_t>(smemRaw) + 1023) & ~uintptr_t(1023));
-  constexpr int NSTAGE = stagesFor(NB, RP);
+  Smem<NB, RP, XS, NS> & S = *reinterpret_cast<Smem<NB, RP, XS, NS> *>((reinterpret_cast<uintptr_t>(smemRaw) + 1023) & ~uintptr_t(1023));
+  constexpr int NSTAGE = NS;
   constexpr int XBUF = xBuffersFor(NB, RP, XS);
   constexpr int XSL = xSlicesFor(XS);
   constexpr int kXExp = xExpFor(XS);
@@ -688,26 +690,36 @@ bool makeMap(CUtensorMap * m, void * base, uint64_t inner, uint64_t outer, uint3
   return makeMap2d(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, inner, outer, boxInner, boxOuter, sw);
 }
 
-template <int NB, int RP, int XS>
+template <int NB, int RP, int XS, int NS>
 int launchFlash(tcscf_ctx * ctx, tc::Params const & P, int grid)
 {
-  size_t const smem = sizeof(tc::Smem<NB, RP, XS>) + 1024;
-  static_assert(sizeof(tc::Smem<NB, RP, XS>) + 1024 <= 232448, "shared memory per CTA");
-  TCSCF_CUDA(ctx, cudaFuncSetAttribute(tc::kFlashTc<NB, RP, XS>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-  tc::kFlashTc<NB, RP, XS><<<grid, tc::NTHREADS, smem, ctx->stream>>>(P);
+  size_t const smem = sizeof(tc::Smem<NB, RP, XS, NS>) + 1024;
+  static_assert(sizeof(tc::Smem<NB, RP, XS, NS>) + 1024 <= 232448, "shared memory per CTA");
+  TCSCF_CUDA(ctx, cudaFuncSetAttribute(tc::kFlashTc<NB, RP, XS, NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  tc::kFlashTc<NB, RP, XS, NS><<<grid, tc::NTHREADS, smem, ctx->stream>>>(P);
   TCSCF_LAUNCH(ctx);
   return TCSCF_OK;
 }
 
 // tile classes: (NB, RP, XS); XS = 0 is the TF32 kernel
-constexpr int kClasses[7][3] = {{64, 32, 2}, {64, 32, 3}, {64, 64, 2}, {128, 32, 2}, {128, 32, 3}, {64, 32, 0}, {128, 32, 0}};
+// tile classes: (NB, RP, XS, TMA stages); XS = 0 is the TF32 kernel (its stage count is its own)
+constexpr int kClasses[8][4] = {{64, 32, 2, 3}, {64, 32, 3, 3}, {64, 32, 3, 2}, {64, 64, 2, 2},
+                                {128, 32, 2, 2}, {128, 32, 3, 2}, {64, 32, 0, 0}, {128, 32, 0, 0}};
 
-int launchClass(tcscf_ctx * ctx, int NB, int RP, int XS, tc::Params const & P, int grid)
+bool classExists(int NB, int RP, int XS, int NS)
+{
+  for (auto const & cl : kClasses)
+    if (cl[0] == NB && cl[1] == RP && cl[2] == XS && cl[3] == NS) return true;
+  return false;
+}
+
+int launchClass(tcscf_ctx * ctx, int NB, int RP, int XS, int NS, tc::Params const & P, int grid)
 {
   if (XS == 0) return launchTf32(ctx, NB, P, grid);
-  if (NB == 64 && RP == 32) return XS == 3 ? launchFlash<64, 32, 3>(ctx, P, grid) : launchFlash<64, 32, 2>(ctx, P, grid);
-  if (NB == 64 && RP == 64 && XS == 2) return launchFlash<64, 64, 2>(ctx, P, grid);
-  if (NB == 128 && RP == 32) return XS == 3 ? launchFlash<128, 32, 3>(ctx, P, grid) : launchFlash<128, 32, 2>(ctx, P, grid);
+  if (NB == 64 && RP == 32 && XS == 3) return NS == 2 ? launchFlash<64, 32, 3, 2>(ctx, P, grid) : launchFlash<64, 32, 3, 3>(ctx, P, grid);
+  if (NB == 64 && RP == 32 && XS == 2) return launchFlash<64, 32, 2, 3>(ctx, P, grid);
+  if (NB == 64 && RP == 64 && XS == 2) return launchFlash<64, 64, 2, 2>(ctx, P, grid);
+  if (NB == 128 && RP == 32) return XS == 3 ? launchFlash<128, 32, 3, 2>(ctx, P, grid) : launchFlash<128, 32, 2, 2>(ctx, P, grid);
   return fail(ctx, TCSCF_ERR_UNSUPPORTED, "no tensor kernel for this tile class");
 }
 
@@ -807,7 +819,7 @@ int effectiveSplit(int nBlocks, int want)
 int maxTunedSplit(int nBlocks) { return std::max(1, nBlocks / 16); }
 
 struct Shape {
-  int NB, RP, XS;
+  int NB, RP, XS, NS;
   int64_t n1pad, n2pad;
   int nTiles, nBlocks, nSplit, perSplit;
 };
@@ -822,6 +834,10 @@ Shape shapeOf(Contraction const & c, int sms, int precision)
   // 9e-8, for a 9 % slower kernel; the TF32 kernel (XS = 0) has rank padding 32
   if (precision == TCSCF_PREC_TF32) sh.XS = 0;
   else sh.XS = sh.RP == 32 ? 3 : 2;
+  // a class the autotuner asks for (wider T tile, fewer TMA stages): the same arithmetic per column
+  if (c.tileNB > sh.NB && sh.XS != 0) sh.NB = c.tileNB;
+  sh.NS = sh.XS == 0 ? 0 : tc::stagesFor(sh.NB, sh.RP);
+  if (c.stages > 0 && sh.XS != 0 && classExists(sh.NB, sh.RP, sh.XS, c.stages)) sh.NS = c.stages;
   sh.n1pad = (c.n1 + tc::BM - 1) / tc::BM * tc::BM;
   sh.n2pad = (c.n2 + tc::BK - 1) / tc::BK * tc::BK;
   sh.nTiles = int(sh.n1pad / tc::BM);
@@ -921,7 +937,7 @@ int tensorPrepare(tcscf_ctx * ctx, Contraction const & c, int precision, void * 
   I.r1xyz = r1c; I.r2pairs = r2c;
   I.T = Tout; I.VH = VHout;
   I.tStride = int64_t(c.n1) * c.ldt; I.vhStride = c.n1;
-  tp.NB = NB; tp.RP = RP; tp.XS = sh.XS;
+  tp.NB = NB; tp.RP = RP; tp.XS = sh.XS; tp.NS = sh.NS;
   tp.c = c;
   if (tf32) return tf32PackOperands(ctx, c, NB, n1pad, n2pad, tf32Ops, tp.maps);
 
@@ -976,17 +992,17 @@ int tensorRun(tcscf_ctx * ctx, TensorPrep * const * preps, int count, bool recor
 
   // one persistent launch per tile class; within it, work items longest first, dealt round-robin
   struct Launch {
-    int NB, RP, XS, grid;
+    int NB, RP, XS, NS, grid;
     tc::Params P;
   };
   std::vector<Launch> launches;
   size_t offset = 0;
   if (recordStart) cudaEventRecord(ctx->ev[2], ctx->stream);
   for (auto const & cl : kClasses) {
-    int const NB = cl[0], RP = cl[1], XS = cl[2];
+    int const NB = cl[0], RP = cl[1], XS = cl[2], NS = cl[3];
     std::vector<int4> items;
     for (int k = 0; k < count; ++k) {
-      if (preps[k]->NB != NB || preps[k]->RP != RP || preps[k]->XS != XS) continue;
+      if (preps[k]->NB != NB || preps[k]->RP != RP || preps[k]->XS != XS || preps[k]->NS != NS) continue;
       tc::Instance const & I = preps[k]->inst;
       for (int t = 0; t < I.nTiles; ++t)
         for (int sp = 0; sp < I.nSplit; ++sp) items.push_back(make_int4(k, t, sp, std::min(I.nBlocks - sp * I.blocksPerSplit, I.blocksPerSplit)));
@@ -999,18 +1015,18 @@ int tensorRun(tcscf_ctx * ctx, TensorPrep * const * preps, int count, bool recor
     P.items = count == 1 ? nullptr : dItems + offset;
     P.inst = dInst;
     P.status = dStatus;
-    launches.push_back({NB, RP, XS, std::min(int(items.size()), sms), P});
+    launches.push_back({NB, RP, XS, NS, std::min(int(items.size()), sms), P});
     offset += items.size();
   }
   if (count == 1) {
-    for (auto const & l : launches) TCSCF_TRY(launchClass(ctx, l.NB, l.RP, l.XS, l.P, l.grid));
+    for (auto const & l : launches) TCSCF_TRY(launchClass(ctx, l.NB, l.RP, l.XS, l.NS, l.P, l.grid));
   } else {
     // A batch runs as a CUDA graph of its persistent launches, captured once per launch sequence and
     // replayed while the sequence repeats (every SCF iteration of the same instances): the instance
     // table, tensor maps and work items the kernels read are refreshed above, before the replay.
     std::vector<uint64_t> key;
     for (auto const & l : launches) {
-      key.insert(key.end(), {uint64_t(l.NB), uint64_t(l.RP), uint64_t(l.XS), uint64_t(l.grid), uint64_t(l.P.nItems),
+      key.insert(key.end(), {uint64_t(l.NB), uint64_t(l.RP), uint64_t(l.XS), uint64_t(l.NS), uint64_t(l.grid), uint64_t(l.P.nItems),
                              uint64_t(reinterpret_cast<uintptr_t>(l.P.items)), uint64_t(reinterpret_cast<uintptr_t>(l.P.inst)),
                              uint64_t(reinterpret_cast<uintptr_t>(l.P.status))});
     }
@@ -1022,7 +1038,7 @@ int tensorRun(tcscf_ctx * ctx, TensorPrep * const * preps, int count, bool recor
       TCSCF_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed));
       int lst = TCSCF_OK;
       for (auto const & l : launches)
-        if (lst == TCSCF_OK) lst = launchClass(ctx, l.NB, l.RP, l.XS, l.P, l.grid);
+        if (lst == TCSCF_OK) lst = launchClass(ctx, l.NB, l.RP, l.XS, l.NS, l.P, l.grid);
       cudaGraph_t graph = nullptr;
       cudaError_t const ce = cudaStreamEndCapture(ctx->stream, &graph);
       TCSCF_TRY(lst);
@@ -1070,7 +1086,7 @@ int tensorPlanUpload(tcscf_ctx * ctx, TensorPrep & tp, char const * scratchName,
   TCSCF_CUDA(ctx, cudaMemcpyAsync(dMaps, tp.maps, sizeof(CUtensorMap) * tc::kMapsPerInstance, cudaMemcpyHostToDevice, ctx->stream));
   TCSCF_CUDA(ctx, cudaMemsetAsync(dStatus, 0, sizeof(int), ctx->stream));
   TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));   // the host copies are consumed before they go out of scope
-  plan.NB = tp.NB; plan.RP = tp.RP; plan.XS = tp.XS;
+  plan.NB = tp.NB; plan.RP = tp.RP; plan.XS = tp.XS; plan.NS = tp.NS;
   plan.nItems = tp.inst.nTiles * tp.inst.nSplit;
   plan.grid = std::min(plan.nItems, smCount());
   plan.inst = dInst;
@@ -1086,7 +1102,7 @@ int tensorPlanLaunch(tcscf_ctx * ctx, TensorPlan const & plan)
   P.items = nullptr;   // one instance: item = tile * nSplit + split
   P.inst = static_cast<tc::Instance const *>(plan.inst);
   P.status = plan.status;
-  TCSCF_TRY(launchClass(ctx, plan.NB, plan.RP, plan.XS, P, plan.grid));
+  TCSCF_TRY(launchClass(ctx, plan.NB, plan.RP, plan.XS, plan.NS, P, plan.grid));
   tc::Instance const & I = plan.prep->inst;
   Contraction const & c = plan.prep->c;
   if (I.nSplit > 1) {
@@ -1126,26 +1142,67 @@ int runTensorOnce(tcscf_ctx * ctx, Contraction const & c, int precision, bool re
 // split sums, between two events on the context stream; the first candidate, the default rule, runs
 // once untimed before) and returns the fastest.  Each run writes the contraction's outputs in full,
 // so the caller's final run leaves them as an untuned build would, up to the order of the r2 sums.
-int tuneSplit(tcscf_ctx * ctx, Contraction const & c, int precision, int * best)
+// Candidate tile classes of a split-BF16 launch besides the default rule's (same results bit for bit:
+// every column of T is computed alike whatever the tile width and stage count): for a 64-column tile
+// with rank padding 32 and 24-bit X, two TMA stages instead of three and the 128-column tile.
+std::vector<std::pair<int, int>> classCandidates(Contraction const & c, int precision)
 {
-  std::vector<int> const cand = splitCandidates(c.n1, c.n2, smCount());
-  *best = cand[0];
-  if (cand.size() == 1) return TCSCF_OK;
+  Shape const sh = shapeOf(c, smCount(), precision);
+  std::vector<std::pair<int, int>> out{{0, 0}};   // (tileNB, stages) = the rule
+  if (precision == TCSCF_PREC_BF16X3 && sh.NB == 64 && sh.RP == 32 && sh.XS == 3) {
+    out.push_back({64, 2});
+    out.push_back({128, 0});
+  }
+  return out;
+}
+
+// Times a candidate schedule (operand packing, the persistent launch and the split sums, between two
+// events on the context stream, after one untimed run).
+int timeSchedule(tcscf_ctx * ctx, Contraction const & ck, int precision, float * ms)
+{
   for (auto & e : ctx->tuneEv)
     if (!e) TCSCF_CUDA(ctx, cudaEventCreate(&e));
+  TCSCF_TRY(runTensorOnce(ctx, ck, precision, false));
+  TCSCF_CUDA(ctx, cudaEventRecord(ctx->tuneEv[0], ctx->stream));
+  TCSCF_TRY(runTensorOnce(ctx, ck, precision, false));
+  TCSCF_CUDA(ctx, cudaEventRecord(ctx->tuneEv[1], ctx->stream));
+  TCSCF_CUDA(ctx, cudaEventSynchronize(ctx->tuneEv[1]));
+  TCSCF_CUDA(ctx, cudaEventElapsedTime(ms, ctx->tuneEv[0], ctx->tuneEv[1]));
+  ++ctx->tuneMeasurements;
+  return TCSCF_OK;
+}
+
+// The schedule of one contraction shape: first the tile class (at the default split), then the r2
+// split (with that class); returns {split, tileNB, stages}.  Each run writes the contraction's outputs
+// in full, so the caller's final run leaves them as an untuned build would, up to the order of the r2
+// block sums.
+int tuneSchedule(tcscf_ctx * ctx, Contraction const & c, int precision, std::array<int, 3> * best)
+{
+  std::vector<int> const cand = splitCandidates(c.n1, c.n2, smCount());
+  std::vector<std::pair<int, int>> const classes = classCandidates(c, precision);
+  *best = {cand[0], 0, 0};
   float bestMs = 0;
+  for (size_t i = 0; i < classes.size(); ++i) {
+    Contraction ck = c;
+    ck.nSplit = cand[0];
+    ck.tileNB = classes[i].first;
+    ck.stages = classes[i].second;
+    if (ck.tileNB > 0 && ck.tileNB != shapeOf(c, smCount(), precision).NB) ck.vtPacked = nullptr;   // packed at the rule's width
+    if (classes.size() == 1) break;
+    float ms = 0;
+    TCSCF_TRY(timeSchedule(ctx, ck, precision, &ms));
+    if (i == 0 || ms < bestMs) { bestMs = ms; (*best)[1] = ck.tileNB; (*best)[2] = ck.stages; }
+  }
+  if (cand.size() == 1) return TCSCF_OK;
   for (size_t i = 0; i < cand.size(); ++i) {
     Contraction ck = c;
     ck.nSplit = cand[i];
-    if (i == 0) TCSCF_TRY(runTensorOnce(ctx, ck, precision, false));
-    TCSCF_CUDA(ctx, cudaEventRecord(ctx->tuneEv[0], ctx->stream));
-    TCSCF_TRY(runTensorOnce(ctx, ck, precision, false));
-    TCSCF_CUDA(ctx, cudaEventRecord(ctx->tuneEv[1], ctx->stream));
-    TCSCF_CUDA(ctx, cudaEventSynchronize(ctx->tuneEv[1]));
+    ck.tileNB = (*best)[1];
+    ck.stages = (*best)[2];
+    if (ck.tileNB > 0 && ck.tileNB != shapeOf(c, smCount(), precision).NB) ck.vtPacked = nullptr;
     float ms = 0;
-    TCSCF_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->tuneEv[0], ctx->tuneEv[1]));
-    ++ctx->tuneMeasurements;
-    if (i == 0 || ms < bestMs) { bestMs = ms; *best = cand[i]; }
+    TCSCF_TRY(timeSchedule(ctx, ck, precision, &ms));
+    if (i == 0 || ms < bestMs) { bestMs = ms; (*best)[0] = cand[i]; }
   }
   return TCSCF_OK;
 }
@@ -1158,12 +1215,15 @@ int contractTensorOnce(tcscf_ctx * ctx, Contraction const & c, int precision, bo
   std::vector<int64_t> const key{c.n1, c.n2, c.ncol <= 64 ? 64 : 128, c.R <= 32 ? 32 : 64, precision};
   auto it = ctx->tunedSplit.find(key);
   if (it == ctx->tunedSplit.end()) {
-    int best = 0;
-    TCSCF_TRY(tuneSplit(ctx, c, precision, &best));
+    std::array<int, 3> best{};
+    TCSCF_TRY(tuneSchedule(ctx, c, precision, &best));
     it = ctx->tunedSplit.emplace(key, best).first;
   }
   Contraction ck = c;
-  ck.nSplit = it->second;
+  ck.nSplit = it->second[0];
+  ck.tileNB = it->second[1];
+  ck.stages = it->second[2];
+  if (ck.tileNB > 0 && ck.tileNB != shapeOf(c, smCount(), precision).NB) ck.vtPacked = nullptr;
   return runTensorOnce(ctx, ck, precision, recordStart);
 }
 

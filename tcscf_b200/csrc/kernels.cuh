@@ -30,6 +30,8 @@ struct Contraction {
   int component = 0;
   const tcscf_ochi * jastrow = nullptr;
   int nSplit = 0;                  // r2 split count of the tensor-path launch (0: the default rule)
+  int tileNB = 0;                  // T tile width the autotuner asks for (0, or 128 where the rule gives 64)
+  int stages = 0;                  // TMA stage count the autotuner asks for (0: the rule)
   const NearList * near = nullptr; // tensor paths: pairs dropped in FP32 that the FP64 rule keeps
 };
 
@@ -101,6 +103,7 @@ constexpr int kTensorMapsPerInstance = 10;
 // a contraction whose operands are packed (tensorPrepare) and ready for tensorRun
 struct TensorPrep {
   int NB = 0, RP = 0, XS = 2;   // Vt tile columns, rank padding, X slices (2: 16 bits, 3: 24 bits; 0: the TF32 kernel)
+  int NS = 0;                   // TMA stages of the split-BF16 kernel
   Contraction c;
   TensorInstance inst{};
   CUtensorMap maps[kTensorMapsPerInstance];
@@ -121,7 +124,7 @@ int tensorRun(tcscf_ctx * ctx, TensorPrep * const * preps, int count, bool recor
 // tensorPrepare on the same arena).  The status word accumulates over launches (0 = every bounded
 // wait completed).
 struct TensorPlan {
-  int NB = 0, RP = 0, XS = 0, grid = 0, nItems = 0;
+  int NB = 0, RP = 0, XS = 0, NS = 0, grid = 0, nItems = 0;
   const void * inst = nullptr;
   int * status = nullptr;
   TensorPrep * prep = nullptr;
