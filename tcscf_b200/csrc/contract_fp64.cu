@@ -15,7 +15,7 @@
 namespace tcscf {
 namespace {
 
-constexpr int BM = 64;    // r1 rows per block
+constexpr int BM = 64;    // r1 rows per block of the 4 x 8 register tile (16 x 8 threads)
 constexpr int BK = 32;    // r2 points per block step
 constexpr int BN = 128;   // columns per block
 constexpr int NT = 256;
@@ -94,25 +94,30 @@ __device__ __forceinline__ void cpAsync8(double * dst, const double * src, bool 
 __device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cpAsyncWait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
-// Block: BM r1 rows x BN columns, 256 threads.  r2 streamed in BK blocks through a two-stage
-// cp.async pipeline (coordinates, Coulomb source, psi2 and V of block i+1 load while block i
-// computes).  Phase B: each thread generates 8 kernel values g(r1,r2) (and rho) of one row;
-// phase C: register-tiled FP64 GEMM, each thread 4 rows x BN/16 columns, columns interleaved in
-// pairs so that a half-warp reads 16 consecutive 16-byte chunks (conflict-free).
-template <int KIND, int BN>
-__global__ void __launch_bounds__(NT, 2) kContractFp64(KArgs a)
+// Block: BMT = 16 RPT r1 rows x BN columns, 256 threads.  r2 streamed in BK blocks through a
+// two-stage cp.async pipeline (coordinates, Coulomb source, psi2 and V of block i+1 load while block i
+// computes).  Phase B: each thread generates VPT kernel values g(r1,r2) (and rho) of one row;
+// phase C: register-tiled FP64 GEMM, each thread RPT rows x BN/16 columns, columns interleaved in
+// pairs so that a half-warp reads 16 consecutive 16-byte chunks (conflict-free).  RPT = 8 (an 8 x 8
+// register tile: 16 shared-memory doubles per 64 FMAs) keeps the FP64 pipe ahead of shared-memory
+// bandwidth where RPT = 4 (12 per 32) does not; it holds one block per SM.
+template <int KIND, int BN, int RPT>
+__global__ void __launch_bounds__(NT, RPT == 8 ? 1 : 2) kContractFp64(KArgs a)
 {
   constexpr int CPT = BN / 16;            // columns per thread
+  constexpr int BMT = 16 * RPT;           // r1 rows per block
+  constexpr int VPT = BMT * BK / NT;      // phase-B values per thread
+  constexpr int TPR = BK / VPT;           // phase-B threads per row
   extern __shared__ __align__(16) double sm[];
   int const R = a.R;
-  double * sP1 = sm;                              // [R][BM]
-  double * sC1 = sP1 + R * BM;                    // [3][BM]
-  double * sX = sC1 + 3 * BM;                     // [BK][BM]
-  double * stage0 = sX + BK * BM;                 // per stage: sV [BK][BN], sC2 [4][BK], sP2 [R][BK]
+  double * sP1 = sm;                              // [R][BMT]
+  double * sC1 = sP1 + R * BMT;                   // [3][BMT]
+  double * sX = sC1 + 3 * BMT;                    // [BK][BMT]
+  double * stage0 = sX + BK * BMT;                // per stage: sV [BK][BN], sC2 [4][BK], sP2 [R][BK]
   int const stageSize = BK * BN + 4 * BK + R * BK;
 
   int const tid = threadIdx.x;
-  int64_t const r1base = int64_t(blockIdx.x) * BM;
+  int64_t const r1base = int64_t(blockIdx.x) * BMT;
   int const cg = blockIdx.z;
   int64_t const r2begin = int64_t(blockIdx.y) * a.r2PerSplit;
   int64_t const r2end = min(a.n2, r2begin + a.r2PerSplit);
@@ -146,25 +151,25 @@ __global__ void __launch_bounds__(NT, 2) kContractFp64(KArgs a)
   if (nsteps > 0) issue(r2begin, 0);
   cpAsyncCommit();
 
-  for (int idx = tid; idx < R * BM; idx += NT) {
+  for (int idx = tid; idx < R * BMT; idx += NT) {
     int const r = idx / R, b = idx % R;
     int64_t const g = r1base + r;
-    sP1[b * BM + r] = g < a.n1 ? a.psi1[g * a.ldpsi + b] : 0.0;
+    sP1[b * BMT + r] = g < a.n1 ? a.psi1[g * a.ldpsi + b] : 0.0;
   }
-  for (int idx = tid; idx < 3 * BM; idx += NT) {
-    int const d = idx / BM, r = idx % BM;
+  for (int idx = tid; idx < 3 * BMT; idx += NT) {
+    int const d = idx / BMT, r = idx % BMT;
     int64_t const g = r1base + r;
     sC1[idx] = g < a.n1 ? a.p1[d * a.n1 + g] : 1.0e6;
   }
   __syncthreads();
 
-  int const rB = tid >> 2;         // phase-B row
-  int const cB = (tid & 3) * 8;    // phase-B first column
-  double const x1 = sC1[rB], y1 = sC1[BM + rB], z1 = sC1[2 * BM + rB];
+  int const rB = tid / TPR;             // phase-B row
+  int const cB = (tid % TPR) * VPT;     // phase-B first column
+  double const x1 = sC1[rB], y1 = sC1[BMT + rB], z1 = sC1[2 * BMT + rB];
   int const tr = tid >> 4, tc = tid & 15;
-  double acc[4][CPT];
+  double acc[RPT][CPT];
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < RPT; ++i)
 #pragma unroll
     for (int j = 0; j < CPT; ++j) acc[i][j] = 0.0;
   double vh = 0.0;
@@ -181,33 +186,37 @@ __global__ void __launch_bounds__(NT, 2) kContractFp64(KArgs a)
     double const * sC2 = sV + BK * BN;
     double const * sP2 = sC2 + 4 * BK;
     int const kn = int(min(int64_t(BK), r2end - k0));
-    double rho[8];
+    double rho[VPT];
 #pragma unroll
-    for (int j = 0; j < 8; ++j) rho[j] = R > 0 ? 0.0 : 1.0;
+    for (int j = 0; j < VPT; ++j) rho[j] = R > 0 ? 0.0 : 1.0;
     for (int b = 0; b < R; ++b) {
-      // one psi1 value against 8 psi2 values: 5 shared loads for 8 FMAs
-      double const p = sP1[b * BM + rB];
+      // one psi1 value against VPT psi2 values
+      double const p = sP1[b * BMT + rB];
 #pragma unroll
-      for (int j = 0; j < 8; j += 2) {
+      for (int j = 0; j < VPT; j += 2) {
         double2 const q = *reinterpret_cast<double2 const *>(&sP2[b * BK + cB + j]);
         rho[j] = fma(p, q.x, rho[j]);
         rho[j + 1] = fma(p, q.y, rho[j + 1]);
       }
     }
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
+    for (int j = 0; j < VPT; ++j) {
       int const c = cB + j;
       double g = r12Kernel<KIND>(a, x1, y1, z1, sC2[c], sC2[BK + c], sC2[2 * BK + c]);
       g = c < kn ? g : 0.0;
       vh = fma(g, sC2[3 * BK + c], vh);
-      sX[c * BM + rB] = g * rho[j];
+      sX[c * BMT + rB] = g * rho[j];
     }
     __syncthreads();
 #pragma unroll 4
     for (int k = 0; k < BK; ++k) {
-      double2 const a01 = *reinterpret_cast<double2 const *>(&sX[k * BM + tr * 4]);
-      double2 const a23 = *reinterpret_cast<double2 const *>(&sX[k * BM + tr * 4 + 2]);
-      double const av[4] = {a01.x, a01.y, a23.x, a23.y};
+      double av[RPT];
+#pragma unroll
+      for (int q = 0; q < RPT / 2; ++q) {
+        double2 const aa = *reinterpret_cast<double2 const *>(&sX[k * BMT + tr * RPT + 2 * q]);
+        av[2 * q] = aa.x;
+        av[2 * q + 1] = aa.y;
+      }
       double bv[CPT];
 #pragma unroll
       for (int q = 0; q < CPT / 2; ++q) {
@@ -216,7 +225,7 @@ __global__ void __launch_bounds__(NT, 2) kContractFp64(KArgs a)
         bv[2 * q + 1] = bb.y;
       }
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
+      for (int i = 0; i < RPT; ++i)
 #pragma unroll
         for (int j = 0; j < CPT; ++j) acc[i][j] = fma(av[i], bv[j], acc[i][j]);
     }
@@ -224,8 +233,8 @@ __global__ void __launch_bounds__(NT, 2) kContractFp64(KArgs a)
 
   double * T = a.T + blockIdx.y * a.tStrideSplit;
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    int64_t const g = r1base + tr * 4 + i;
+  for (int i = 0; i < RPT; ++i) {
+    int64_t const g = r1base + tr * RPT + i;
     if (g >= a.n1) continue;
 #pragma unroll
     for (int j = 0; j < CPT; ++j) {
@@ -234,10 +243,10 @@ __global__ void __launch_bounds__(NT, 2) kContractFp64(KArgs a)
     }
   }
   if (doCoul) {
-    vh += __shfl_xor_sync(0xffffffffu, vh, 1);
-    vh += __shfl_xor_sync(0xffffffffu, vh, 2);
+#pragma unroll
+    for (int o = 1; o < TPR; o <<= 1) vh += __shfl_xor_sync(0xffffffffu, vh, o);
     int64_t const g = r1base + rB;
-    if ((tid & 3) == 0 && g < a.n1) a.VH[blockIdx.y * a.vhStrideSplit + g] = vh;
+    if ((tid % TPR) == 0 && g < a.n1) a.VH[blockIdx.y * a.vhStrideSplit + g] = vh;
   }
 }
 
@@ -382,33 +391,31 @@ __global__ void __launch_bounds__(NT) kReduceComplex(int64_t n1, int nb, const d
   }
 }
 
-template <int KIND, int BNV>
+template <int KIND, int BNV, int RPT>
 int launchOne(tcscf_ctx * ctx, KArgs const & a, dim3 grid, size_t smem)
 {
-  TCSCF_CUDA(ctx, cudaFuncSetAttribute(kContractFp64<KIND, BNV>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
-  TCSCF_CUDA(ctx, cudaFuncSetAttribute(kContractFp64<KIND, BNV>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
-  kContractFp64<KIND, BNV><<<grid, NT, smem, ctx->stream>>>(a);
+  TCSCF_CUDA(ctx, cudaFuncSetAttribute(kContractFp64<KIND, BNV, RPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  TCSCF_CUDA(ctx, cudaFuncSetAttribute(kContractFp64<KIND, BNV, RPT>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+  kContractFp64<KIND, BNV, RPT><<<grid, NT, smem, ctx->stream>>>(a);
   TCSCF_LAUNCH(ctx);
   return TCSCF_OK;
 }
 
-int launchContract(tcscf_ctx * ctx, int kind, int bn, KArgs const & a, unsigned tiles, unsigned nsplit, size_t smem)
+template <int KIND>
+int launchKind(tcscf_ctx * ctx, int bn, int rpt, KArgs const & a, dim3 grid, size_t smem)
+{
+  if (bn == 32) return launchOne<KIND, 32, 4>(ctx, a, grid, smem);
+  if (bn == 64) return launchOne<KIND, 64, 4>(ctx, a, grid, smem);
+  return rpt == 8 ? launchOne<KIND, 128, 8>(ctx, a, grid, smem) : launchOne<KIND, 128, 4>(ctx, a, grid, smem);
+}
+
+int launchContract(tcscf_ctx * ctx, int kind, int bn, int rpt, KArgs const & a, unsigned tiles, unsigned nsplit, size_t smem)
 {
   unsigned const cgroups = a.ncol <= 128 ? 1u : unsigned((a.ncol + BN - 1) / BN);
   dim3 const grid{tiles, nsplit, cgroups};
-  if (kind == 0) {
-    if (bn == 32) return launchOne<0, 32>(ctx, a, grid, smem);
-    if (bn == 64) return launchOne<0, 64>(ctx, a, grid, smem);
-    return launchOne<0, 128>(ctx, a, grid, smem);
-  }
-  if (kind == 1) {
-    if (bn == 32) return launchOne<1, 32>(ctx, a, grid, smem);
-    if (bn == 64) return launchOne<1, 64>(ctx, a, grid, smem);
-    return launchOne<1, 128>(ctx, a, grid, smem);
-  }
-  if (bn == 32) return launchOne<2, 32>(ctx, a, grid, smem);
-  if (bn == 64) return launchOne<2, 64>(ctx, a, grid, smem);
-  return launchOne<2, 128>(ctx, a, grid, smem);
+  if (kind == 0) return launchKind<0>(ctx, bn, rpt, a, grid, smem);
+  if (kind == 1) return launchKind<1>(ctx, bn, rpt, a, grid, smem);
+  return launchKind<2>(ctx, bn, rpt, a, grid, smem);
 }
 
 }  // namespace
@@ -417,14 +424,19 @@ int contractFp64(tcscf_ctx * ctx, Contraction const & c)
 {
   TCSCF_CHECK(ctx, c.R >= 0 && c.R <= 128, TCSCF_ERR_UNSUPPORTED, "contraction rank must be <= 128");
   TCSCF_CHECK(ctx, c.ncol > 0 && c.n1 > 0 && c.n2 > 0, TCSCF_ERR_INVALID_ARGUMENT, "empty contraction");
-  int64_t const tiles = (c.n1 + BM - 1) / BM;
+  int const bn = c.ncol <= 32 ? 32 : (c.ncol <= 64 ? 64 : 128);
+  // 8 x 8 register tiles (128 r1 rows per block) where the 128-column tile and the rank leave the
+  // shared memory room (R <= 64), else 4 x 8 (64 rows)
+  int const rpt = bn == 128 && c.R <= 64 ? 8 : 4;
+  int const bm = 16 * rpt;
+  int64_t const tiles = (c.n1 + bm - 1) / bm;
   int const cgroups = c.ncol <= 128 ? 1 : (c.ncol + BN - 1) / BN;
   int dev = 0;
   cudaGetDevice(&dev);
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   // split r2 so that small r1 sets still fill the machine (partials are summed deterministically)
-  int64_t const want = int64_t(sms) * 4;
+  int64_t const want = int64_t(sms) * (rpt == 8 ? 2 : 4);
   int64_t nsplit = (want + tiles * cgroups - 1) / (tiles * cgroups);
   nsplit = std::max<int64_t>(1, std::min<int64_t>(nsplit, (c.n2 + 4 * BK - 1) / (4 * BK)));
   nsplit = std::min<int64_t>(nsplit, 65535);
@@ -458,12 +470,11 @@ int contractFp64(tcscf_ctx * ctx, Contraction const & c)
   }
   a.T = Tpart;
   a.VH = VHpart;
-  int const bn = c.ncol <= 32 ? 32 : (c.ncol <= 64 ? 64 : 128);
-  size_t const smem = sizeof(double) * (size_t(c.R) * BM + 3 * BM + BK * BM + 2 * (size_t(BK) * bn + 4 * BK + size_t(c.R) * BK));
+  size_t const smem = sizeof(double) * (size_t(c.R) * bm + 3 * bm + BK * bm + 2 * (size_t(BK) * bn + 4 * BK + size_t(c.R) * BK));
   int const kind = c.kernel == TCSCF_K_INV_R12 ? 0 : (c.kernel <= TCSCF_K_TC_SCALAR_OPPO ? 1 : 2);
   // the contraction kernel alone is bracketed by the context's timing events (tcscf_last_timing)
   if (!ctx->capturing) cudaEventRecord(ctx->ev[2], ctx->stream);
-  TCSCF_TRY(launchContract(ctx, kind, bn, a, unsigned(tiles), unsigned(nsplit), smem));
+  TCSCF_TRY(launchContract(ctx, kind, bn, rpt, a, unsigned(tiles), unsigned(nsplit), smem));
   if (!ctx->capturing) cudaEventRecord(ctx->ev[3], ctx->stream);
   if (nsplit > 1) {
     int64_t const n = c.n1 * c.ncol;
