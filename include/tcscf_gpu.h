@@ -291,7 +291,7 @@ int tcscf_scf(tcscf_ctx * ctx, int r1, int r2, int nspin, int n_up, int n_down, 
  * G, F and the energy as tcscf_scf does, tests |dE| < tol on the device, and takes the next C from
  * the Fock matrix in the real-harmonic basis: canonical orthogonalisation of S (eigenvalues of S
  * above 1e-12 of the largest kept; computed once), a device Jacobi eigen-solve, the n_up lowest
- * eigenvectors.  With capture != 0 the iterations after the first run as one CUDA graph launch whose
+ * eigenvectors.  With capture != 0 the iterations after the first two run as one CUDA graph launch whose
  * conditional WHILE node repeats the iteration until the device-side test ends the loop, so the host
  * reads nothing per iteration; with capture == 0 the same launches are issued per iteration and the
  * host reads the loop state after each (results bit-identical to the captured run).  Restricted closed

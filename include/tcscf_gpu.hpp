@@ -371,7 +371,7 @@ class RCSHartreeFock : public HartreeFockBase {
   double highestOccupiedOrbitalEnergy() const { return eigenvalues_[(nUp_ + nDown_) / 2 - 1]; }
 
   // compute() with the whole loop on the device (tcscf_scf_graph): with capture, the iterations after
-  // the first are one CUDA graph launch whose device-side WHILE node ends the loop
+  // the first two are one CUDA graph launch whose device-side WHILE node ends the loop
   template <class S, class H>
   double computeOnDevice(S const & overlap, H const & oneElectronTerms, QMCGrid const & r1Grid, QMCGrid const & r2Grid,
                          bool respectOneElectronSymmetry = true, tcscf_precision precision = TCSCF_PREC_FP64, double tol = 1e-5,

@@ -80,8 +80,8 @@ class Context:
         return a.value, b.value
 
     def set_autotune(self, enable: bool = True) -> None:
-        """Measure the tensor-path launch schedule (r2 split) per build shape and batch signature on
-        first use and keep the fastest (off by default)."""
+        """Measure the tensor-path launch schedule (tile class, then r2 split) per build shape and the
+        split policy per batch signature on first use and keep the fastest (off by default)."""
         _raise(ffi.lib().tcscf_set_autotune(self._h, int(bool(enable))), self._h)
 
     def autotune_stats(self) -> tuple[int, int, int]:
@@ -427,7 +427,7 @@ class RCSHartreeFock(_SCF):
                         max_iter: int | None = None, capture: bool = True) -> float:
         """compute() with the whole loop on the device (tcscf_scf_graph): from the zero density, every
         iteration builds, assembles, tests |dE| < tol and diagonalises (real-harmonic basis, canonical
-        orthogonalisation, device Jacobi) on the device; with capture the iterations after the first are
+        orthogonalisation, device Jacobi) on the device; with capture the iterations after the first two are
         one CUDA graph launch with a device-side WHILE loop (self.graphLaunches == 1)."""
         ctx = r1Grid.ctx
         S = np.ascontiguousarray(np.real(overlap), dtype=np.float64)

@@ -1544,9 +1544,10 @@ __global__ void kScfCheck(ScfGraphState * st, const double * E, const int * tsta
 // contraction (FP64 or tensor cores) from those factors (D = C C^T, rank nocc), the real Fock
 // reduction, the reference-basis G, F and energy (kFinalize), the convergence test, then the new C from
 // the Fock matrix: real-harmonic F, Xc^T F Xc with the canonical orthogonaliser Xc of S, Jacobi, the
-// nocc lowest eigenvectors.  The first iteration (zero density: F = h) runs directly and allocates
-// every buffer; with capture the rest run as one graph launch whose conditional WHILE node repeats the
-// body until the device-side test clears it, so the host neither reads nor waits per iteration.
+// nocc lowest eigenvectors.  The first two iterations run directly (the zero-density one, F = h, with
+// no contraction; the second allocates every buffer); with capture the rest run as one graph launch
+// whose conditional WHILE node repeats the body until the device-side test clears it, so the host
+// neither reads nor waits per iteration.
 int scfGraph(tcscf_ctx * ctx, Grid & g1, Grid & g2, int nocc, const double * S, const double * h, int respectSym, int precision, double tol,
              int maxIter, int capture, double * energy, int * iterations, double * density, double * eigenvalues, int * graphLaunches)
 {
@@ -1666,8 +1667,14 @@ int scfGraph(tcscf_ctx * ctx, Grid & g1, Grid & g2, int nocc, const double * S, 
   size_t const jacobiSmem = sizeof(double) * size_t(m + (m & 1)) * (m + (m & 1));
   TCSCF_CUDA(ctx, cudaFuncSetAttribute(kJacobiSym, cudaFuncAttributeMaxDynamicSharedMemorySize, int(jacobiSmem)));
 
-  auto body = [&](cudaGraphConditionalHandle handle, int useHandle) -> int {
+  // zeroDensity: the first iteration's density is zero, so its exchange and Coulomb potentials are
+  // zero without a contraction (as tcscf_scf skips a rank-0 factor)
+  auto body = [&](cudaGraphConditionalHandle handle, int useHandle, bool zeroDensity) -> int {
     size_t const sm = sizeof(double) * size_t(nb) * nocc;
+    if (zeroDensity) {
+      TCSCF_CUDA(ctx, cudaMemsetAsync(Tb, 0, sizeof(double) * size_t(n1) * nb, ctx->stream));
+      TCSCF_CUDA(ctx, cudaMemsetAsync(VH, 0, sizeof(double) * size_t(n1), ctx->stream));
+    } else {
     kOrbitals<<<gridBlocks(n1 * nocc, 256), 256, sm, ctx->stream>>>(n1, nb, nocc, g1.phiR, C, nocc, psi1, ldpsi);
     TCSCF_LAUNCH(ctx);
     kOrbitals<<<gridBlocks(n2 * nocc, 256), 256, sm, ctx->stream>>>(n2, nb, nocc, g2.phiR, C, nocc, psi2, ldpsi);
@@ -1680,6 +1687,7 @@ int scfGraph(tcscf_ctx * ctx, Grid & g1, Grid & g2, int nocc, const double * S, 
       TCSCF_TRY(nearCorrect(ctx, c));
     } else {
       TCSCF_TRY(contractFp64(ctx, c));
+    }
     }
     TCSCF_CUDA(ctx, cudaMemsetAsync(FR, 0, sizeof(double) * nn, ctx->stream));
     TCSCF_TRY(reduceFockReal(ctx, n1, nb, g1.phiR, g1.w, VH, 2.0, Tb, nb, 1.0, FR));
@@ -1709,10 +1717,13 @@ int scfGraph(tcscf_ctx * ctx, Grid & g1, Grid & g2, int nocc, const double * S, 
   };
 
   ScfGraphState hst{};
-  // first iteration directly (allocates every scratch buffer the body uses)
-  TCSCF_TRY(body(0, 0));
-  TCSCF_CUDA(ctx, cudaMemcpyAsync(&hst, st, sizeof(hst), cudaMemcpyDeviceToHost, ctx->stream));
-  TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  // the first two iterations directly: the zero-density one, then one that allocates every scratch
+  // buffer the body uses
+  for (int it = 0; it < 2 && it < maxIter && !hst.done; ++it) {
+    TCSCF_TRY(body(0, 0, it == 0));
+    TCSCF_CUDA(ctx, cudaMemcpyAsync(&hst, st, sizeof(hst), cudaMemcpyDeviceToHost, ctx->stream));
+    TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  }
   *graphLaunches = 0;
   if (!hst.done) {
     if (capture) {
@@ -1740,7 +1751,7 @@ int scfGraph(tcscf_ctx * ctx, Grid & g1, Grid & g2, int nocc, const double * S, 
         return fail(ctx, TCSCF_ERR_CUDA, std::string("begin capture: ") + cudaGetErrorString(e));
       }
       ctx->capturing = 1;
-      int const bst = body(handle, 1);
+      int const bst = body(handle, 1, false);
       ctx->capturing = 0;
       cudaGraph_t captured = nullptr;
       e = cudaStreamEndCapture(ctx->stream, &captured);
@@ -1761,8 +1772,8 @@ int scfGraph(tcscf_ctx * ctx, Grid & g1, Grid & g2, int nocc, const double * S, 
       *graphLaunches = 1;
     } else {
       // the same body launched per iteration, with the host reading the loop state after each
-      for (int it = 1; it < maxIter && !hst.done; ++it) {
-        TCSCF_TRY(body(0, 0));
+      for (int it = 2; it < maxIter && !hst.done; ++it) {
+        TCSCF_TRY(body(0, 0, false));
         TCSCF_CUDA(ctx, cudaMemcpyAsync(&hst, st, sizeof(hst), cudaMemcpyDeviceToHost, ctx->stream));
         TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
       }
