@@ -406,7 +406,9 @@ int launchKind(tcscf_ctx * ctx, int bn, int rpt, KArgs const & a, dim3 grid, siz
 {
   if (bn == 32) return launchOne<KIND, 32, 4>(ctx, a, grid, smem);
   if (bn == 64) return launchOne<KIND, 64, 4>(ctx, a, grid, smem);
-  return rpt == 8 ? launchOne<KIND, 128, 8>(ctx, a, grid, smem) : launchOne<KIND, 128, 4>(ctx, a, grid, smem);
+  if constexpr (KIND == 0)
+    if (rpt == 8) return launchOne<KIND, 128, 8>(ctx, a, grid, smem);
+  return launchOne<KIND, 128, 4>(ctx, a, grid, smem);
 }
 
 int launchContract(tcscf_ctx * ctx, int kind, int bn, int rpt, KArgs const & a, unsigned tiles, unsigned nsplit, size_t smem)
@@ -425,9 +427,12 @@ int contractFp64(tcscf_ctx * ctx, Contraction const & c)
   TCSCF_CHECK(ctx, c.R >= 0 && c.R <= 128, TCSCF_ERR_UNSUPPORTED, "contraction rank must be <= 128");
   TCSCF_CHECK(ctx, c.ncol > 0 && c.n1 > 0 && c.n2 > 0, TCSCF_ERR_INVALID_ARGUMENT, "empty contraction");
   int const bn = c.ncol <= 32 ? 32 : (c.ncol <= 64 ? 64 : 128);
-  // 8 x 8 register tiles (128 r1 rows per block) where the 128-column tile and the rank leave the
-  // shared memory room (R <= 64), else 4 x 8 (64 rows)
-  int const rpt = bn == 128 && c.R <= 64 ? 8 : 4;
+  int const kind = c.kernel == TCSCF_K_INV_R12 ? 0 : (c.kernel <= TCSCF_K_TC_SCALAR_OPPO ? 1 : 2);
+  // 8 x 8 register tiles (128 r1 rows per block) for 1/r12 where the 128-column tile and the rank
+  // leave the shared memory room (R <= 64), else 4 x 8 (64 rows).  The transcorrelated kernels spend
+  // more of each block generating g, which the one block per SM of the 8 x 8 tile cannot hide: at Be-TC
+  // (24 STO, 65,536 x 65,536 points) their precompute took 4.37 s with 8 x 8 and 2.68 s with 4 x 8.
+  int const rpt = bn == 128 && c.R <= 64 && kind == 0 ? 8 : 4;
   int const bm = 16 * rpt;
   int64_t const tiles = (c.n1 + bm - 1) / bm;
   int const cgroups = c.ncol <= 128 ? 1 : (c.ncol + BN - 1) / BN;
@@ -471,7 +476,6 @@ int contractFp64(tcscf_ctx * ctx, Contraction const & c)
   a.T = Tpart;
   a.VH = VHpart;
   size_t const smem = sizeof(double) * (size_t(c.R) * bm + 3 * bm + BK * bm + 2 * (size_t(BK) * bn + 4 * BK + size_t(c.R) * BK));
-  int const kind = c.kernel == TCSCF_K_INV_R12 ? 0 : (c.kernel <= TCSCF_K_TC_SCALAR_OPPO ? 1 : 2);
   // the contraction kernel alone is bracketed by the context's timing events (tcscf_last_timing)
   if (!ctx->capturing) cudaEventRecord(ctx->ev[2], ctx->stream);
   TCSCF_TRY(launchContract(ctx, kind, bn, rpt, a, unsigned(tiles), unsigned(nsplit), smem));

@@ -108,3 +108,61 @@ def test_compute_q_and_assemble_g_match_oracle(ctx, tc_setup):
     G3 = api.tc_assemble_g(ctx, *Qr, D)
     G3r = oracle.assemble_g(*Qr, D)
     np.testing.assert_allclose(G3, G3r, rtol=0, atol=1e-12 * np.abs(G3r).max())
+
+
+# (basis, n_up, n_down, r2 grid dimension of the Fji tensors): the fused per-point build covers nb <= 32
+# (when its shared-memory layout fits) with complex Fji (3-D r2) or real Fji (2-D r2, nb even); real
+# Fji at odd nb and nb > 32 take the per-intermediate kernels.  Unequal spin counts leave the C columns of the smaller spin partly zero.
+_SHAPES = {
+    "nb7-2-1-complex": (BASIS, 2, 1, 3),
+    "nb8-2-2-real": (wl.expand(0, [0.6, 1.5, 3.6, 8.5, 20.0]) + wl.expand(1, [1.2]), 2, 2, 2),
+    "nb7-2-2-real-odd": (BASIS, 2, 2, 2),
+    "nb32-2-1-complex": (wl.expand(0, [0.5 * 1.7 ** k for k in range(9)]) + wl.expand(1, [0.8 * 1.8 ** k for k in range(4)])
+                         + wl.expand(2, [1.0, 2.6]) + wl.expand(0, [30.0]), 2, 1, 3),
+    "nb33-3-2-complex": (wl.expand(0, [0.5 * 1.7 ** k for k in range(11)]) + wl.expand(1, [0.8 * 1.8 ** k for k in range(4)])
+                         + wl.expand(2, [1.0, 2.6]), 3, 2, 3),
+}
+
+
+@pytest.mark.parametrize("case", sorted(_SHAPES))
+def test_tc_fock_build_shapes(ctx, case):
+    basis, nup, ndown, dim2 = _SHAPES[case]
+    nb = len(basis)
+    assert nb == int(case[2:].split("-")[0])
+    g1 = grids.qmc_grid(3, 128, 61)
+    g2 = grids.qmc_grid(dim2, 512, 62)
+    g3 = grids.qmc_grid(3, 512, 63)
+    G1 = api.QMCGrid(ctx, g1)
+    G1.setBasisFunctions(basis, storeGradients=True)
+    G2 = api.QMCGrid(ctx, g2)
+    G2.setBasisFunctions(basis)
+    G3 = api.QMCGrid(ctx, g3)
+    G3.setBasisFunctions(basis)
+    u = ffi.ochi_struct(U["a"], U["a12"], U["terms"])
+    uo = oracle.ochi(U["a"], U["a12"], U["terms"])
+    t = dict(Fs=api.computeF(G1, G2, ffi.K_TC_SCALAR_SAME, u, keep=True, copy=False)[1],
+             Fo=api.computeF(G1, G2, ffi.K_TC_SCALAR_OPPO, u, keep=True, copy=False)[1],
+             Vs=api.computeV(G1, G3, ffi.K_GRAD_U_SAME, u, keep=True, copy=False)[1],
+             Vo=api.computeV(G1, G3, ffi.K_GRAD_U_OPPO, u, keep=True, copy=False)[1])
+    vals2 = oracle.basis_values(g2.points, basis)
+    vals3 = oracle.basis_values(g3.points, basis)
+    vals1, grads1 = oracle.basis_values(g1.points, basis, gradients=True)
+    o = dict(Fs=oracle.compute_F(g1.points, g2.points, g2.weights, vals2, nb, ffi.K_TC_SCALAR_SAME, uo),
+             Fo=oracle.compute_F(g1.points, g2.points, g2.weights, vals2, nb, ffi.K_TC_SCALAR_OPPO, uo),
+             Vs=oracle.compute_V(g1.points, g3.points, g3.weights, vals3, nb, ffi.K_GRAD_U_SAME, uo),
+             Vo=oracle.compute_V(g1.points, g3.points, g3.weights, vals3, nb, ffi.K_GRAD_U_OPPO, uo))
+    assert (o["Fs"].dtype == np.float64) == (dim2 == 2)
+    _, h = api.overlap_core(basis, Z)
+    rng = np.random.default_rng(nb)
+    occ = [_random_orbitals(nb, nup, rng), _random_orbitals(nb, ndown, rng)]
+    D = np.stack([c.T @ c.conj() for c in occ])
+    try:
+        G2g, G3g, Fg, Eg = api.tc_fock_build(G1, t["Fs"], t["Fo"], t["Vs"], t["Vo"], nup, ndown, D, occ[0], occ[1], h, False)
+        G2r, G3r, Fr, Er = oracle.tc_fock_build(o["Fs"], o["Fo"], o["Vs"], o["Vo"], vals1, grads1, g1.weights, D, nup, ndown,
+                                                occ[0], occ[1], h, False)
+        for a, b in ((G2g, G2r), (G3g, G3r), (Fg, Fr)):
+            np.testing.assert_allclose(a, b, rtol=0, atol=1e-10 * max(1.0, np.abs(b).max()))
+        assert abs(Eg - Er) < 1e-10 * max(1.0, abs(Er)), (Eg, Er)
+    finally:
+        for d in t.values():
+            d.close()
