@@ -296,32 +296,54 @@ def measure_matmul_peaks(dev, n: int = 8192, reps: int = 10) -> dict:
     return out
 
 
-def roofline(prec: int, n: int, nb: int, nocc: int, c_ms: float, peaks: dict, peak_kind: str, traffic) -> dict:
+def symmetric_pairs(n: int, fp64: bool = False) -> int:
+    """(r1, r2) pairs the symmetric contraction computes on an n-point grid used as both r1 and r2:
+    each 128-point r1 tile takes the r2 points from its own first row on (its diagonal tile in full, at
+    half weight).  Split BF16 works in 64-point r2 blocks over the padded grid, sum_p 128 * 64 (nBlocks
+    - 2 p); the FP64 kernel (128-row tiles, 8 x 8 register tiles) stops at the last point, sum_p 128
+    (n - 128 p)."""
+    tiles, blocks = -(-n // 128), -(-n // 64)
+    if fp64:
+        return sum(128 * (n - 128 * p) for p in range(tiles))
+    return sum(128 * 64 * (blocks - 2 * p) for p in range(tiles))
+
+
+def roofline(prec: int, n: int, nb: int, nocc: int, c_ms: float, peaks: dict, peak_kind: str, traffic, sym: bool = False) -> dict:
     """The line's roofline object for one Fock build of n points (r1 = r2 grid) whose contraction
     kernel took c_ms milliseconds.  peaks: the BF16 peak (bf16_tflops) and the FP64 / TF32 matmul rates
-    (fp64_tflops, tf32_tflops) when measured."""
+    (fp64_tflops, tf32_tflops) when measured.  sym: the split-BF16 kernel computed only the pairs on and
+    above the diagonal tiles (X = g rho is symmetric when r1 = r2 and psi1 = psi2); its work counts those
+    pairs, and traffic (given for a full launch) scales with them."""
     from tcscf_b200 import ffi
 
-    # algorithmic work per Fock build: F_alg = 2 N^2 (nb nocc + 1), the pair-density count of the direct
-    # build (nb nocc exchange pair densities and the Coulomb density per (r1, r2) pair); the kernels
-    # contract the same sum in factored form, 2 N^2 (nocc + nb + 1) flops (rho GEMM, exchange GEMM,
-    # Coulomb), reported beside it as kernel_algorithm_tflops
-    flops = 2.0 * n * n * (nb * nocc + 1)
-    kernel_flops = 2.0 * n * n * (nocc + nb + 1)
+    # algorithmic work per Fock build: F_alg = 2 P (nb nocc + 1), the pair-density count of the direct
+    # build (nb nocc exchange pair densities and the Coulomb density per (r1, r2) pair) over the P pairs
+    # the build needs: N^2, or with the symmetric contraction each unordered pair once (the diagonal
+    # tiles in full); the kernels contract the same sum in factored form, 2 P (nocc + nb + 1) flops
+    # (rho GEMM, exchange GEMM, Coulomb), reported beside it as kernel_algorithm_tflops
+    sym = sym and prec in (ffi.PREC_BF16X3, ffi.PREC_FP64)
+    pairs = float(symmetric_pairs(n, fp64=prec == ffi.PREC_FP64)) if sym else float(n) * n
+    flops = 2.0 * pairs * (nb * nocc + 1)
+    kernel_flops = 2.0 * pairs * (nocc + nb + 1)
     achieved = flops / (c_ms / 1e3) / 1e12
     kernel_achieved = kernel_flops / (c_ms / 1e3) / 1e12
-    numerator = {"achieved_numerator": "F_alg = 2 N^2 (nb nocc + 1) flops per build (pair-density count)",
+    numerator = {"achieved_numerator": "F_alg = 2 P (nb nocc + 1) flops per build (pair-density count over the P pairs computed)",
+                 "pairs": pairs, "symmetric": bool(sym),
+                 "full_pairs_tflops": 2.0 * n * n * (nb * nocc + 1) / (c_ms / 1e3) / 1e12,
                  "kernel_algorithm_tflops": kernel_achieved,
                  "frac_note": "frac counts F_alg, the pair-density work the factored form avoids; issued_frac (the "
                               "slice products the tensor pipe executes) and ncu's tensor-pipe activity measure the hardware"}
+    if traffic is not None and sym and prec == ffi.PREC_BF16X3:   # the full-launch figure, scaled by the units
+        traffic = traffic * pairs / (float(-(-n // 128) * 128) * (-(-n // 64) * 64))
     if prec == ffi.PREC_FP64:
         # the FP64 kernel runs on the FP64 pipe: its roofline counts the flops it performs
         peak = peaks.get("fp64_tflops", 37.0)
         src = "fp64 dense matmul (torch, 8192^3), measured in this run" if "fp64_tflops" in peaks else "nominal B200 FP64 rate"
         roof = {"bound": "fp64", "achieved": kernel_achieved, "peak": peak, "unit": "TFLOP/s", "frac": kernel_achieved / peak,
                 "traffic": None, "peak_source": src,
-                "achieved_numerator": "2 N^2 (nocc + nb + 1) flops per build (the factored contraction the kernel performs)",
-                "effective_tflops": achieved}
+                "achieved_numerator": "2 P (nocc + nb + 1) flops per build (the factored contraction the kernel performs over "
+                                      "the P pairs it computes)",
+                "pairs": pairs, "symmetric": bool(sym), "effective_tflops": achieved}
     elif prec == ffi.PREC_TF32:
         if "tf32_tflops" in peaks:
             peak, src = peaks["tf32_tflops"], "tf32 dense matmul (torch, 8192^3), measured in this run"
@@ -340,7 +362,7 @@ def roofline(prec: int, n: int, nb: int, nocc: int, c_ms: float, peaks: dict, pe
         # N = NB with 24-bit X (rank padding 32), 4 with 16-bit X (rank padding 64)
         RP = 32 if nocc <= 32 else 64   # real closed-shell guess density: factor rank = n_occ
         NB = 64 if nb <= 64 else 128
-        issued = n * n * (2.0 * 6 * RP + 2.0 * (6 if RP == 32 else 4) * NB) / (c_ms / 1e3) / 1e12
+        issued = pairs * (2.0 * 6 * RP + 2.0 * (6 if RP == 32 else 4) * NB) / (c_ms / 1e3) / 1e12
         roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                 "traffic": traffic, "peak_source": f"bf16 dense burst, {peak_kind}",
                 "issued_tensor_tflops": issued, "issued_frac": issued / peak, **numerator}
@@ -453,10 +475,12 @@ def run_ours(args, rank: int, world: int) -> None:
     dropped, near = grids.coincident_pairs(g, g)   # r1 = r2 grid: the diagonal pairs contribute 0
     c_ms = statistics.median(cms)
     allpeaks = dict(peaks, **mm_peaks)
+    # one grid object serves as r1 and r2, so the split-BF16 build takes the symmetric contraction
     roof = roofline(prec, n, w.nb, w.n_up, c_ms, allpeaks, peak_kind,
-                    TRAFFIC_BYTES_PER_LAUNCH.get(w.name) if prec == ffi.PREC_BF16X3 and args.nrad == 0 else None)
+                    TRAFFIC_BYTES_PER_LAUNCH.get(w.name) if prec == ffi.PREC_BF16X3 and args.nrad == 0 else None,
+                    sym=prec == ffi.PREC_BF16X3)
     if fp64 is not None:
-        fp64["roofline"] = roofline(ffi.PREC_FP64, n, w.nb, w.n_up, fp64["contraction_ms"], allpeaks, peak_kind, None)
+        fp64["roofline"] = roofline(ffi.PREC_FP64, n, w.nb, w.n_up, fp64["contraction_ms"], allpeaks, peak_kind, None, sym=True)
     cpu = None
     if not args.skip_cpu:
         r = cpu_reference(w, g, D, h, budget_s=args.cpu_seconds)

@@ -124,7 +124,10 @@ int tcscf_synchronize(tcscf_ctx * ctx);
  * computeF call, measured with CUDA events on the context stream; launches = kernels launched */
 int tcscf_last_timing(tcscf_ctx * ctx, double * contraction_ms, double * total_ms, int * launches);
 /* diagnostics: the Coulomb potential VH[N1] (both spins) and the first spin's exchange potential
- * T[N1][nb] (real-harmonic basis) of the most recent direct Fock build on this context */
+ * T[N1][nb] (real-harmonic basis) of the most recent direct Fock build on this context.  A split-BF16
+ * build with one grid as r1 and r2 and a positive semi-definite real density contracts only the pairs
+ * on and above each 128-point r1 tile's diagonal (the diagonal tile at half weight): T is then that
+ * half, whose r1 quadrature plus its transpose is the exchange matrix; VH is complete either way */
 int tcscf_last_potentials(tcscf_ctx * ctx, double * VH, double * T);
 
 /* ---- host-side grid generation (replaces ChebyshevGauss/changeOfVariables/createGrid,

@@ -15,7 +15,6 @@
 namespace tcscf {
 namespace {
 
-constexpr int BM = 64;    // r1 rows per block of the 4 x 8 register tile (16 x 8 threads)
 constexpr int BK = 32;    // r2 points per block step
 constexpr int BN = 128;   // columns per block
 constexpr int NT = 256;
@@ -33,6 +32,7 @@ struct KArgs {
   double * VH;
   int64_t tStrideSplit;   // elements between split partials of T (0 when not split)
   int64_t vhStrideSplit;
+  int sym;                // r1 = r2 points and psi1 = psi2: only r2 >= the block's first row, its own rows at half weight
   OchiDev u;
 };
 
@@ -119,8 +119,12 @@ __global__ void __launch_bounds__(NT, RPT == 8 ? 1 : 2) kContractFp64(KArgs a)
   int const tid = threadIdx.x;
   int64_t const r1base = int64_t(blockIdx.x) * BMT;
   int const cg = blockIdx.z;
-  int64_t const r2begin = int64_t(blockIdx.y) * a.r2PerSplit;
-  int64_t const r2end = min(a.n2, r2begin + a.r2PerSplit);
+  // a symmetric contraction takes the r2 points from this block's own rows on (its own BMT x BMT
+  // square at half weight in T); the Coulomb sums over the points before them come from kCoulombLowerFp64
+  int64_t const r2split = int64_t(blockIdx.y) * a.r2PerSplit;
+  int64_t const r2begin = a.sym ? max(r2split, r1base) : r2split;
+  int64_t const r2end = min(a.n2, r2split + a.r2PerSplit);
+  int64_t const r2half = a.sym ? r1base + BMT : 0;   // r2 below this (and >= r2begin) at half weight
   bool const doCoul = a.coul != nullptr && cg == 0;
 
   auto issue = [&](int64_t k0, int st) {
@@ -147,7 +151,7 @@ __global__ void __launch_bounds__(NT, RPT == 8 ? 1 : 2) kContractFp64(KArgs a)
     }
   };
 
-  int64_t const nsteps = (r2end - r2begin + BK - 1) / BK;
+  int64_t const nsteps = r2end > r2begin ? (r2end - r2begin + BK - 1) / BK : 0;
   if (nsteps > 0) issue(r2begin, 0);
   cpAsyncCommit();
 
@@ -205,7 +209,7 @@ __global__ void __launch_bounds__(NT, RPT == 8 ? 1 : 2) kContractFp64(KArgs a)
       double g = r12Kernel<KIND>(a, x1, y1, z1, sC2[c], sC2[BK + c], sC2[2 * BK + c]);
       g = c < kn ? g : 0.0;
       vh = fma(g, sC2[3 * BK + c], vh);
-      sX[c * BMT + rB] = g * rho[j];
+      sX[c * BMT + rB] = (k0 + c < r2half ? 0.5 * g : g) * rho[j];
     }
     __syncthreads();
 #pragma unroll 4
@@ -248,6 +252,30 @@ __global__ void __launch_bounds__(NT, RPT == 8 ? 1 : 2) kContractFp64(KArgs a)
     int64_t const g = r1base + rB;
     if ((tid % TPR) == 0 && g < a.n1) a.VH[blockIdx.y * a.vhStrideSplit + g] = vh;
   }
+}
+
+// Symmetric contractions: the Coulomb row sums over the r2 points before each block's first row (the
+// pairs kContractFp64 skips), added to the potential: VH[r] += sum_{j < bm floor(r / bm)} g(r, j) c(j),
+// FP64 with the exact-coincidence rule.  One thread per r1 point; the r2 points are read by all threads
+// of a block at once (broadcast).
+__global__ void __launch_bounds__(128) kCoulombLowerFp64(int64_t n, int bm, const double * __restrict__ p, const double * __restrict__ coul,
+                                                        double * VH)
+{
+  int64_t const r = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  int64_t const rr = r < n ? r : n - 1;   // rows past n repeat the last one (nothing is written for them)
+  double const x = p[rr], y = p[n + rr], z = p[2 * n + rr];
+  int64_t const jend = (rr / bm) * bm;   // a multiple of 64
+  double vh = 0.0;
+  for (int64_t j0 = 0; j0 < jend; j0 += 64) {
+    double part = 0.0;   // sums of 64 terms added into the total (shorter rounding chains)
+    for (int64_t j = j0; j < j0 + 64; ++j) {
+      double const dx = x - p[j], dy = y - p[n + j], dz = z - p[2 * n + j];
+      double const q = fma(dx, dx, fma(dy, dy, dz * dz));
+      if (q != 0.0) part = fma(rsqrt_fp64(q), coul[j], part);
+    }
+    vh += part;
+  }
+  if (r < n) VH[r] += vh;
 }
 
 // deterministic sum of split partials: out[i] = sum_s part[s*stride + i]
@@ -475,6 +503,9 @@ int contractFp64(tcscf_ctx * ctx, Contraction const & c)
   }
   a.T = Tpart;
   a.VH = VHpart;
+  TCSCF_CHECK(ctx, !c.sym || (c.p1 == c.p2 && c.n1 == c.n2 && c.psi1 == c.psi2 && c.R > 0 && (c.VH != nullptr) == (c.coul != nullptr)),
+              TCSCF_ERR_INVALID_ARGUMENT, "internal: a symmetric contraction needs r1 = r2 and psi1 = psi2");
+  a.sym = c.sym ? 1 : 0;
   size_t const smem = sizeof(double) * (size_t(c.R) * bm + 3 * bm + BK * bm + 2 * (size_t(BK) * bn + 4 * BK + size_t(c.R) * BK));
   // the contraction kernel alone is bracketed by the context's timing events (tcscf_last_timing)
   if (!ctx->capturing) cudaEventRecord(ctx->ev[2], ctx->stream);
@@ -488,6 +519,10 @@ int contractFp64(tcscf_ctx * ctx, Contraction const & c)
       kSumSplits<<<gridBlocks(c.n1, 256), 256, 0, ctx->stream>>>(c.n1, int(nsplit), c.n1, VHpart, c.VH, c.n1, 1, 1, 1);
       TCSCF_LAUNCH(ctx);
     }
+  }
+  if (c.sym && c.coul && tiles > 1) {
+    kCoulombLowerFp64<<<unsigned((c.n1 + 127) / 128), 128, 0, ctx->stream>>>(c.n1, bm, c.p1, c.coul, c.VH);
+    TCSCF_LAUNCH(ctx);
   }
   return TCSCF_OK;
 }

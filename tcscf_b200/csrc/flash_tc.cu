@@ -219,8 +219,9 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         decodeItem(P, item, ii, tile, split);
         Instance const * I = P.inst + ii;
         CUtensorMap const * maps = I->maps;
-        int const jb = split * I->blocksPerSplit;
-        int const je = min(I->nBlocks, jb + I->blocksPerSplit);
+        int jb, je;
+        itemBlocks(*I, tile, split, jb, je);
+        if (je == jb) continue;   // an empty item of a symmetric instance: the MMA issuer skips it too
         if (p1Use > 0 && !(ok = waitBar(&S.p1free, (p1Use - 1) & 1, abortFlag, P.status, 11))) break;
         mbarArriveTx(&S.p1full, kPsi1Bytes);
         for (int k = 0; k < 4; ++k) tmaLoad2d(S.psi1[k], maps + k, 0, tile * BM, &S.p1full);
@@ -265,9 +266,10 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         int ii, tile, split;
         decodeItem(P, item, ii, tile, split);
         Instance const * I = P.inst + ii;
-        int const jb = split * I->blocksPerSplit;
-        int const je = min(I->nBlocks, jb + I->blocksPerSplit);
+        int jb, je;
+        itemBlocks(*I, tile, split, jb, je);
         int const nblk = je - jb;
+        if (nblk == 0) continue;   // nothing loaded for an empty item
         if (!(ok = waitBar(&S.p1full, p1Use & 1, abortFlag, P.status, 21))) break;
         ++p1Use;
         fenceAfterSync();
@@ -369,9 +371,12 @@ __global__ void __launch_bounds__(NTHREADS, 1)
       int ii, tile, split;
       decodeItem(P, item, ii, tile, split);
       Instance const * I = P.inst + ii;
-      int const jb = split * I->blocksPerSplit;
-      int const je = min(I->nBlocks, jb + I->blocksPerSplit);
-      int const nblk = je - jb;
+      int jb, je;
+      itemBlocks(*I, tile, split, jb, je);
+      int const nblk = je - jb;   // 0 for an empty item: its T rows and VH are written as zeros
+      // a symmetric instance counts the pairs of its diagonal tile (blocks jDiag - 2, jDiag - 1) at half
+      // weight in T; their Coulomb row sums stay whole
+      int const jDiag = I->sym ? (tile + 1) * (BM / BK) : 0;
       int const r1 = tile * BM + row;
       float4 const p1 = I->r1xyz[r1];
       // rho = 2^24 a1inv a2inv (256 A + B), X' = g a2inv (256 A + B) = X / (2^24 a1inv), and a block's
@@ -454,7 +459,8 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         int const E = max(int((__float_as_uint(mx) >> 23) & 0xFF) - 127, kMinExp);
         float const bs = __uint_as_float(uint32_t(127 + kXExp - E) << 23);
         float const binv = __uint_as_float(uint32_t(127 + E - kXExp) << 23);   // 2^(E - kXExp), E >= -100
-        float const fac = rowA * binv;   // a power of two (0 when below FP32 range: those blocks add nothing measurable)
+        float fac = rowA * binv;   // a power of two (0 when below FP32 range: those blocks add nothing measurable)
+        if (jb + jj < jDiag) fac *= 0.5f;
         // X buffer xb is free once GEMM2 of block g - XBUF completed
         int const xb = g % XBUF;
         if (g >= uint32_t(XBUF) && !(ok = waitBar(&S.xfree[xb], ((g / XBUF) - 1) & 1, abortFlag, P.status, 34))) break;
@@ -650,6 +656,49 @@ __global__ void kPackCoordPairs(int64_t n, int64_t npad, const double * pts, con
     out[2 * p] = make_float4(v[0][0], v[1][0], v[0][1], v[1][1]);
     out[2 * p + 1] = make_float4(v[0][2], v[1][2], v[0][3], v[1][3]);
   }
+}
+
+// Symmetric instances (r1 and r2 the same points): the Coulomb row sums over the r2 blocks before each
+// r1 tile's diagonal, which the tensor kernel skips, added to the potential:
+//   VH[r] += sum_{j < BM tile(r)} g(r, j) c(j)
+// with the tensor kernel's FP32 arithmetic on the same packed points (its drop rule and its
+// Newton-refined rsqrt), FP32 sums per 64-point block added in FP64.  One thread per r1 point, one
+// block per r1 tile, the tiles with the most pairs first.
+__global__ void __launch_bounds__(BM) kCoulombLower(int nTiles, int64_t n1, const float4 * __restrict__ r1xyz,
+                                                   const float4 * __restrict__ r2pairs, double * VH)
+{
+  int const tile = nTiles - 1 - int(blockIdx.x);
+  int64_t const r = int64_t(tile) * BM + threadIdx.x;
+  float4 const p1 = r1xyz[r];
+  uint64_t const p1x = f2pack(p1.x, p1.x), p1y = f2pack(p1.y, p1.y), p1z = f2pack(p1.z, p1.z);
+  uint64_t const mOne = f2pack(-1.0f, -1.0f), mHalf = f2pack(-0.5f, -0.5f);
+  double vh = 0.0;
+  int64_t const nPairs = int64_t(tile) * (BM / 2);   // the points [0, BM tile) in pairs
+  for (int64_t b = 0; b < nPairs; b += BK / 2) {
+    uint64_t vs = 0;
+#pragma unroll 8
+    for (int e = 0; e < BK / 2; ++e) {
+      float4 const qa = r2pairs[2 * (b + e)], qb = r2pairs[2 * (b + e) + 1];
+      uint64_t const dx = f2sub(p1x, f2pack(qa.x, qa.y));
+      uint64_t const dy = f2sub(p1y, f2pack(qa.z, qa.w));
+      uint64_t const dz = f2sub(p1z, f2pack(qb.x, qb.y));
+      uint64_t const r2 = f2fma(dx, dx, f2fma(dy, dy, f2mul(dz, dz)));
+      float r2a, r2b;
+      f2unpack(r2, r2a, r2b);
+      uint64_t y = f2pack(rsqrtApprox(r2a), rsqrtApprox(r2b));
+      uint64_t const em = f2fma(f2mul(r2, y), y, mOne);
+      y = f2fma(f2mul(y, mHalf), em, y);
+      float ya, yb;
+      f2unpack(y, ya, yb);
+      ya = r2a >= p1.w ? ya : 0.0f;
+      yb = r2b >= p1.w ? yb : 0.0f;
+      vs = f2fma(f2pack(ya, yb), f2pack(qb.z, qb.w), vs);
+    }
+    float v0, v1;
+    f2unpack(vs, v0, v1);
+    vh += double(v0 + v1);
+  }
+  if (r < n1) VH[r] += vh;
 }
 
 }  // namespace tc
@@ -896,6 +945,8 @@ int tensorPrepare(tcscf_ctx * ctx, Contraction const & c, int precision, void * 
   std::string why;
   if (!tensorPathAvailable(c, precision, &why)) return fail(ctx, TCSCF_ERR_UNSUPPORTED, why);
   TCSCF_CHECK(ctx, arenaBytes >= tensorArenaBytes(c, precision), TCSCF_ERR_INVALID_ARGUMENT, "internal: tensor arena too small");
+  TCSCF_CHECK(ctx, !c.sym || (c.p1 == c.p2 && c.n1 == c.n2 && c.psi1 == c.psi2 && c.R > 0 && (c.VH != nullptr) == (c.coul != nullptr)),
+              TCSCF_ERR_INVALID_ARGUMENT, "internal: a symmetric contraction needs r1 = r2 and psi1 = psi2");
   Shape const sh = shapeOf(c, smCount(), precision);
   int const NB = sh.NB, RP = sh.RP;
   bool const tf32 = precision == TCSCF_PREC_TF32;
@@ -933,6 +984,7 @@ int tensorPrepare(tcscf_ctx * ctx, Contraction const & c, int precision, void * 
   tc::Instance & I = tp.inst;
   I = tc::Instance{};
   I.nTiles = sh.nTiles; I.nSplit = sh.nSplit; I.blocksPerSplit = sh.perSplit; I.nBlocks = sh.nBlocks;
+  I.sym = c.sym && !tf32 ? 1 : 0;
   I.n1 = int(c.n1); I.nb = c.ncol; I.ldt = c.ldt;
   I.r1xyz = r1c; I.r2pairs = r2c;
   I.T = Tout; I.VH = VHout;
@@ -964,6 +1016,17 @@ int tensorPrepare(tcscf_ctx * ctx, Contraction const & c, int precision, void * 
   I.a1inv = a1inv; I.a2inv = a2inv; I.cinv = cinv;
   return TCSCF_OK;
 }
+
+namespace {
+// the Coulomb row sums a symmetric instance skipped (kCoulombLower), once c.VH holds the rest
+int coulombLower(tcscf_ctx * ctx, tc::Instance const & I, Contraction const & c)
+{
+  if (!I.sym || !c.VH || I.nTiles < 2) return TCSCF_OK;
+  tc::kCoulombLower<<<unsigned(I.nTiles), tc::BM, 0, ctx->stream>>>(I.nTiles, c.n1, I.r1xyz, I.r2pairs, c.VH);
+  TCSCF_LAUNCH(ctx);
+  return TCSCF_OK;
+}
+}  // namespace
 
 int tensorRun(tcscf_ctx * ctx, TensorPrep * const * preps, int count, bool recordStart)
 {
@@ -1067,6 +1130,7 @@ int tensorRun(tcscf_ctx * ctx, TensorPrep * const * preps, int count, bool recor
       TCSCF_TRY(sumSplitsLaunch(ctx, n, I.nSplit, int64_t(c.n1) * c.ldt, I.T, c.T, c.n1, c.ncol, c.ldt, c.ldt));
       if (c.VH) TCSCF_TRY(sumSplitsLaunch(ctx, c.n1, I.nSplit, c.n1, I.VH, c.VH, c.n1, 1, 1, 1));
     }
+    TCSCF_TRY(coulombLower(ctx, I, c));
   }
   return TCSCF_OK;
 }
@@ -1110,7 +1174,7 @@ int tensorPlanLaunch(tcscf_ctx * ctx, TensorPlan const & plan)
     TCSCF_TRY(sumSplitsLaunch(ctx, n, I.nSplit, int64_t(c.n1) * c.ldt, I.T, c.T, c.n1, c.ncol, c.ldt, c.ldt));
     if (c.VH) TCSCF_TRY(sumSplitsLaunch(ctx, c.n1, I.nSplit, c.n1, I.VH, c.VH, c.n1, 1, 1, 1));
   }
-  return TCSCF_OK;
+  return coulombLower(ctx, I, c);
 }
 
 namespace {
@@ -1212,7 +1276,7 @@ int contractTensorOnce(tcscf_ctx * ctx, Contraction const & c, int precision, bo
   if (!ctx->autotune || c.nSplit > 0) return runTensorOnce(ctx, c, precision, recordStart);
   std::string why;
   if (!tensorPathAvailable(c, precision, &why)) return fail(ctx, TCSCF_ERR_UNSUPPORTED, why);
-  std::vector<int64_t> const key{c.n1, c.n2, c.ncol <= 64 ? 64 : 128, c.R <= 32 ? 32 : 64, precision};
+  std::vector<int64_t> const key{c.n1, c.n2, c.ncol <= 64 ? 64 : 128, c.R <= 32 ? 32 : 64, precision, c.sym};
   auto it = ctx->tunedSplit.find(key);
   if (it == ctx->tunedSplit.end()) {
     std::array<int, 3> best{};

@@ -32,6 +32,11 @@ struct Contraction {
   int nSplit = 0;                  // r2 split count of the tensor-path launch (0: the default rule)
   int tileNB = 0;                  // T tile width the autotuner asks for (0, or 128 where the rule gives 64)
   int stages = 0;                  // TMA stage count the autotuner asks for (0: the rule)
+  // split-BF16 direct form with r1 and r2 the same points (p1 == p2) and psi1 == psi2: compute only the
+  // r2 blocks on and above each r1 tile's diagonal (the diagonal tile at half weight); T then holds
+  // T' with sum_r1 W T + (sum_r1 W T)^T the full result, and VH is complete (its lower part from
+  // the Coulomb row sums over the skipped blocks)
+  int sym = 0;
   const NearList * near = nullptr; // tensor paths: pairs dropped in FP32 that the FP64 rule keeps
 };
 
@@ -88,6 +93,10 @@ struct TensorInstance {
   int n1;                                          // real r1 rows
   int nb;                                          // real columns of T
   int ldt, pad;
+  // symmetric instance: r1 and r2 are the same points and rho(r1, r2) = rho(r2, r1) (psi1 = psi2), so
+  // X is symmetric; a tile then takes only the r2 blocks from its own diagonal on, the diagonal
+  // tile at half weight, and the caller adds the transpose of the result
+  int sym, symPad;
   const float4 * r1xyz;                            // [n1pad] x, y, z, 0
   const float4 * r2pairs;                          // [nBlocks*64] r2 points in pair layout
   const float * a1inv;                             // [n1pad] 1 / psi1 row scale

@@ -78,11 +78,14 @@ __global__ void __launch_bounds__(kFindThreads) kFindNearPairs(int64_t n1, const
   }
 }
 
-// Direct Fock build: T[i][c] += g rho V[j][c] and VH[i] += g coul[j] for each listed pair, with
-// g = 1/r12 and rho = sum_a psi1[i][a] psi2[j][a] in FP64.  One warp per pair.
+// Direct Fock build: T[i][c] += s g rho V[j][c] and VH[i] += g coul[j] for each listed pair, with
+// g = 1/r12 and rho = sum_a psi1[i][a] psi2[j][a] in FP64.  s = 1, or for a symmetric contraction
+// (T holds the blocks on and above each r1 tile's diagonal, the diagonal tile at half weight) the
+// weight the tensor kernel gives the pair's block: 0 below the diagonal tile, 1/2 in it, 1 above.
+// One warp per pair.
 __global__ void kNearDirect(int count, const int2 * list, int64_t n1, const double * p1, int64_t n2, const double * p2, int R,
                             const double * psi1, const double * psi2, int ldpsi, int ncol, const double * V, int ldv, const double * coul,
-                            double * T, int ldt, double * VH)
+                            double * T, int ldt, double * VH, int sym)
 {
   int const lane = threadIdx.x & 31;
   for (int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; k < count; k += (gridDim.x * blockDim.x) >> 5) {
@@ -94,7 +97,13 @@ __global__ void kNearDirect(int count, const int2 * list, int64_t n1, const doub
     for (int a = lane; a < R; a += 32) rho += psi1[i * ldpsi + a] * psi2[j * ldpsi + a];
     for (int o = 16; o > 0; o >>= 1) rho += __shfl_xor_sync(0xffffffffu, rho, o);
     if (lane == 0 && coul && VH) atomicAdd(&VH[i], g * coul[j]);
-    for (int c = lane; c < ncol; c += 32) atomicAdd(&T[i * ldt + c], g * rho * V[j * ldv + c]);
+    double s = 1.0;
+    if (sym) {
+      int64_t const jd = (i / tc::BM) * (tc::BM / tc::BK), jb = j / tc::BK;   // the tile's diagonal block, the pair's block
+      s = jb < jd ? 0.0 : (jb < jd + tc::BM / tc::BK ? 0.5 : 1.0);
+    }
+    if (s != 0.0)
+      for (int c = lane; c < ncol; c += 32) atomicAdd(&T[i * ldt + c], s * g * rho * V[j * ldv + c]);
   }
 }
 
@@ -219,7 +228,7 @@ int nearCorrect(tcscf_ctx * ctx, Contraction const & c)
   unsigned const blocks = gridBlocks(int64_t(count) * 32, 256);
   if (c.R > 0) {
     kNearDirect<<<blocks, 256, 0, ctx->stream>>>(count, c.near->d, c.n1, c.p1, c.n2, c.p2, c.R, c.psi1, c.psi2, c.ldpsi, c.ncol, c.V, c.ldv,
-                                                 c.coul, c.T, c.ldt, c.VH);
+                                                 c.coul, c.T, c.ldt, c.VH, c.sym);
     TCSCF_LAUNCH(ctx);
     return TCSCF_OK;
   }

@@ -47,6 +47,15 @@ struct Params {
   int * status;             // device status word (0 = ok)
 };
 
+// the r2 blocks [jb, je) of work item (tile, split): all blocks, or for a symmetric instance those from
+// the tile's own diagonal block (BM / BK blocks per tile) on; empty (je == jb) past the last block
+__host__ __device__ __forceinline__ void itemBlocks(Instance const & I, int tile, int split, int & jb, int & je)
+{
+  jb = (I.sym ? tile * (BM / BK) : 0) + split * I.blocksPerSplit;
+  je = jb + I.blocksPerSplit < I.nBlocks ? jb + I.blocksPerSplit : I.nBlocks;
+  if (je < jb) je = jb;
+}
+
 __device__ __forceinline__ void decodeItem(Params const & P, int item, int & inst, int & tile, int & split)
 {
   if (P.items) {

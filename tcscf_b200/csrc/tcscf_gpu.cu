@@ -697,6 +697,12 @@ __global__ void kAddInto(int64_t n, const double * a, double * out)
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) out[i] += a[i];
 }
 
+// out[i][j] += a[j][i] (nb x nb, row-major)
+__global__ void kAddTransposed(int nb, const double * a, double * out)
+{
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < nb * nb; idx += gridDim.x * blockDim.x) out[idx] += a[(idx % nb) * nb + idx / nb];
+}
+
 // column-major complex copy of the row-major (j,i) Fock matrix, and of a real row-major S
 __global__ void kToColumnMajor(int nb, const double2 * fockRow, const double * S, double2 * A, double2 * B)
 {
@@ -837,6 +843,7 @@ namespace {
 struct Factor {
   int R = 0;          // columns of the factor matrices
   bool complex = false;
+  bool same = false;  // X1 == X2 (the pivoted Cholesky factor of a positive semi-definite real density)
   double * X1 = nullptr, * X1im = nullptr, * X2 = nullptr;   // device [nb][ldx]
   int ldx = 0;
 };
@@ -917,7 +924,7 @@ int factorFinish(tcscf_ctx * ctx, Grid & g, FactorBufs const & b, FactorStatus c
   // eigen-solver carry ~1e-12): the density is factored as real, dropping it
   f.complex = hmax[1] > 1e-10 * std::max(hmax[0], 1e-300);
   if (hmax[0] == 0 && hmax[1] == 0) { f.R = 0; return TCSCF_OK; }
-  if (!f.complex && !st.indefinite) { f.R = st.rank; return TCSCF_OK; }
+  if (!f.complex && !st.indefinite) { f.R = st.rank; f.same = true; return TCSCF_OK; }
 
   void * p = nullptr;
   TCSCF_TRY(scratch(ctx, "fac_eig", nn * sizeof(double2) * 2 + nn * sizeof(double) + 64 * sizeof(double) + nb * sizeof(int) + 1024, &p));
@@ -1040,6 +1047,7 @@ int fockBuildDevice(tcscf_ctx * ctx, Grid & g1, Grid & g2, int nspin, const doub
   TCSCF_CUDA(ctx, cudaMemsetAsync(VH, 0, sizeof(double) * (size_t(nspin) * n1 + n1), ctx->stream));
   TCSCF_CUDA(ctx, cudaMemsetAsync(GRre, 0, sizeof(double) * size_t(nspin) * nb * nb * 2, ctx->stream));
   bool anyComplex = false;
+  bool symSpin[2] = {false, false};
   double contractionMs = 0;
   const void * vtPacked = nullptr;
   if (precision == TCSCF_PREC_BF16X3) TCSCF_TRY(tensorPackedV(ctx, g2, V, scale, &vtPacked));
@@ -1053,26 +1061,33 @@ int fockBuildDevice(tcscf_ctx * ctx, Grid & g1, Grid & g2, int nspin, const doub
       continue;
     }
     int const R = f.R;
+    // one grid on both sides and X1 = X2: psi1 = psi2 and X = g rho is symmetric, so the split-BF16 and
+    // FP64 contractions compute only the pairs on and above each r1 tile's diagonal (T'), and the
+    // exchange matrix is sum W T' plus its transpose
+    bool const sym = (precision == TCSCF_PREC_BF16X3 || precision == TCSCF_PREC_FP64) && &g1 == &g2 && f.same;
+    symSpin[s] = sym;
     for (int part = 0; part < (f.complex ? 2 : 1); ++part) {
       double const * X1 = part == 0 ? f.X1 : f.X1im;
       size_t const sm = sizeof(double) * size_t(nb) * R;
       kOrbitals<<<gridBlocks(n1 * R, 256), 256, sm, ctx->stream>>>(n1, nb, R, g1.phiR, X1, f.ldx, psi1, ldpsi);
       TCSCF_LAUNCH(ctx);
-      if (part == 0) {
+      if (part == 0 && !sym) {
         kOrbitals<<<gridBlocks(n2 * R, 256), 256, sm, ctx->stream>>>(n2, nb, R, g2.phiR, f.X2, f.ldx, psi2, ldpsi);
         TCSCF_LAUNCH(ctx);
         // rho(r2, r2) needs the r1-side factor evaluated on the r2 points
         kOrbitals<<<gridBlocks(n2 * R, 256), 256, sm, ctx->stream>>>(n2, nb, R, g2.phiR, f.X1, f.ldx, psi1at2, ldpsi);
         TCSCF_LAUNCH(ctx);
       }
+      double const * p2side = sym ? psi1 : psi2;
       Contraction c;
       c.n1 = n1; c.n2 = n2; c.R = R; c.ncol = nb;
-      c.p1 = g1.pts; c.p2 = g2.pts; c.psi1 = psi1; c.psi2 = psi2; c.ldpsi = ldpsi;
+      c.p1 = g1.pts; c.p2 = g2.pts; c.psi1 = psi1; c.psi2 = p2side; c.ldpsi = ldpsi;
       c.V = V; c.ldv = nb; c.T = part == 0 ? Ts : Ti; c.ldt = ldt;
       c.vtPacked = vtPacked;
+      c.sym = sym ? 1 : 0;
       if (precision != TCSCF_PREC_FP64) TCSCF_TRY(nearPairsFor(ctx, g1, g2, &c.near));
       if (part == 0) {
-        kCoulombSource<<<gridBlocks(n2, 256), 256, 0, ctx->stream>>>(n2, R, psi1at2, psi2, ldpsi, g2.w, scale, coul);
+        kCoulombSource<<<gridBlocks(n2, 256), 256, 0, ctx->stream>>>(n2, R, sym ? psi1 : psi1at2, p2side, ldpsi, g2.w, scale, coul);
         TCSCF_LAUNCH(ctx);
         c.coul = coul;
         c.VH = VH + size_t(s) * n1;
@@ -1093,8 +1108,18 @@ int fockBuildDevice(tcscf_ctx * ctx, Grid & g1, Grid & g2, int nspin, const doub
     TCSCF_LAUNCH(ctx);
   }
   double const cJ = nspin == 1 ? 2.0 : 1.0;
+  double * GRhalf = nullptr;
+  if (symSpin[0] || symSpin[1]) TCSCF_TRY(scratch(ctx, "fock_sym_half", sizeof(double) * size_t(nb) * nb, reinterpret_cast<void **>(&GRhalf)));
   for (int s = 0; s < nspin; ++s) {
     TCSCF_TRY(reduceFockReal(ctx, n1, nb, g1.phiR, g1.w, VHtot, cJ, Tre + size_t(s) * n1 * ldt, ldt, 1.0, GRre + size_t(s) * nb * nb));
+    if (symSpin[s]) {
+      // the exchange of the pairs below the diagonal tiles: the transpose of T's own contribution
+      // (reduceFockReal adds into its output)
+      TCSCF_CUDA(ctx, cudaMemsetAsync(GRhalf, 0, sizeof(double) * size_t(nb) * nb, ctx->stream));
+      TCSCF_TRY(reduceFockReal(ctx, n1, nb, g1.phiR, g1.w, nullptr, 0.0, Tre + size_t(s) * n1 * ldt, ldt, 1.0, GRhalf));
+      kAddTransposed<<<gridBlocks(int64_t(nb) * nb, 256), 256, 0, ctx->stream>>>(nb, GRhalf, GRre + size_t(s) * nb * nb);
+      TCSCF_LAUNCH(ctx);
+    }
     if (anyComplex)
       TCSCF_TRY(reduceFockReal(ctx, n1, nb, g1.phiR, g1.w, nullptr, 0.0, Tim + size_t(s) * n1 * ldt, ldt, 1.0, GRim + size_t(s) * nb * nb));
   }
@@ -1194,9 +1219,12 @@ int fockBuildBatch(tcscf_ctx * ctx, int count, Grid * const * g1s, Grid * const 
     Factor f;
     TCSCF_TRY(factorFinish(ctx, g1, fbufs[k], hStatus[k], f));
     Contraction & c = cs[k];
+    // one grid on both sides and X1 = X2: the symmetric split-BF16 contraction (psi2 = psi1)
+    bool const sym = precision == TCSCF_PREC_BF16X3 && &g1 == &g2 && f.same;
     c.R = f.R;
     c.T = T; c.VH = VH; c.V = V; c.ldv = nb;
-    c.psi1 = psi1; c.psi2 = psi2; c.coul = coul;
+    c.psi1 = psi1; c.psi2 = sym ? psi1 : psi2; c.coul = coul;
+    c.sym = sym ? 1 : 0;
     std::string why;
     bool eligible = (precision == TCSCF_PREC_BF16X3 || precision == TCSCF_PREC_TF32) && f.R > 0 && !f.complex &&
                     tensorPathAvailable(c, precision, &why) && tensorArenaBytes(c, precision) <= arenaBytes[k];
@@ -1215,11 +1243,13 @@ int fockBuildBatch(tcscf_ctx * ctx, int count, Grid * const * g1s, Grid * const 
     size_t const sm = sizeof(double) * size_t(nb) * f.R;
     kOrbitals<<<gridBlocks(n1 * f.R, 256), 256, sm, ctx->stream>>>(n1, nb, f.R, g1.phiR, f.X1, f.ldx, psi1, nb);
     TCSCF_LAUNCH(ctx);
-    kOrbitals<<<gridBlocks(n2 * f.R, 256), 256, sm, ctx->stream>>>(n2, nb, f.R, g2.phiR, f.X2, f.ldx, psi2, nb);
-    TCSCF_LAUNCH(ctx);
-    kOrbitals<<<gridBlocks(n2 * f.R, 256), 256, sm, ctx->stream>>>(n2, nb, f.R, g2.phiR, f.X1, f.ldx, psi1at2, nb);
-    TCSCF_LAUNCH(ctx);
-    kCoulombSource<<<gridBlocks(n2, 256), 256, 0, ctx->stream>>>(n2, f.R, psi1at2, psi2, nb, g2.w, scale, coul);
+    if (!sym) {
+      kOrbitals<<<gridBlocks(n2 * f.R, 256), 256, sm, ctx->stream>>>(n2, nb, f.R, g2.phiR, f.X2, f.ldx, psi2, nb);
+      TCSCF_LAUNCH(ctx);
+      kOrbitals<<<gridBlocks(n2 * f.R, 256), 256, sm, ctx->stream>>>(n2, nb, f.R, g2.phiR, f.X1, f.ldx, psi1at2, nb);
+      TCSCF_LAUNCH(ctx);
+    }
+    kCoulombSource<<<gridBlocks(n2, 256), 256, 0, ctx->stream>>>(n2, f.R, sym ? psi1 : psi1at2, c.psi2, nb, g2.w, scale, coul);
     TCSCF_LAUNCH(ctx);
     TCSCF_TRY(tensorPrepare(ctx, c, precision, arena, arenaBytes[k], preps[k]));
     tensorOk[k] = 1;
@@ -1231,6 +1261,8 @@ int fockBuildBatch(tcscf_ctx * ctx, int count, Grid * const * g1s, Grid * const 
     TCSCF_CUDA(ctx, cudaEventSynchronize(ctx->ev[3]));
     cudaEventElapsedTime(&contractionMs, ctx->ev[2], ctx->ev[3]);
   }
+  double * GRhalf = nullptr;
+  TCSCF_TRY(scratch(ctx, "batch_sym_half", sizeof(double) * size_t(maxNb) * maxNb, reinterpret_cast<void **>(&GRhalf)));
   for (int k = 0; k < count; ++k) {
     Grid & g1 = *g1s[k];
     int const nb = g1.nb;
@@ -1242,6 +1274,12 @@ int fockBuildBatch(tcscf_ctx * ctx, int count, Grid * const * g1s, Grid * const 
     double * GR = c.VH + g1.n;
     TCSCF_CUDA(ctx, cudaMemsetAsync(GR, 0, sizeof(double) * nb * nb, ctx->stream));
     TCSCF_TRY(reduceFockReal(ctx, g1.n, nb, g1.phiR, g1.w, c.VH, 2.0, c.T, nb, 1.0, GR));
+    if (c.sym) {
+      TCSCF_CUDA(ctx, cudaMemsetAsync(GRhalf, 0, sizeof(double) * nb * nb, ctx->stream));
+      TCSCF_TRY(reduceFockReal(ctx, g1.n, nb, g1.phiR, g1.w, nullptr, 0.0, c.T, nb, 1.0, GRhalf));
+      kAddTransposed<<<gridBlocks(int64_t(nb) * nb, 256), 256, 0, ctx->stream>>>(nb, GRhalf, GR);
+      TCSCF_LAUNCH(ctx);
+    }
     kRealToReference<<<gridBlocks(int64_t(nb) * nb, 256), 256, 0, ctx->stream>>>(1, nb, g1.dsto, GR, nullptr, dGs[k]);
     TCSCF_LAUNCH(ctx);
     kFinalize<<<1, 512, 0, ctx->stream>>>(1, nb, dHs[k], dGs[k], nullptr, dDs[k], respectSym, 2.0, dFs[k], dEs[k]);
@@ -1645,11 +1683,17 @@ int scfGraph(tcscf_ctx * ctx, Grid & g1, Grid & g2, int nocc, const double * S, 
   TCSCF_CUDA(ctx, cudaMemcpyAsync(st, &st0, sizeof(st0), cudaMemcpyHostToDevice, ctx->stream));
   kWeightedBasis<<<gridBlocks(n2 * nb, 256), 256, 0, ctx->stream>>>(n2, nb, g2.phiR, g2.w, scale, Vw);
   TCSCF_LAUNCH(ctx);
+  bool const tensor = precision != TCSCF_PREC_FP64;
+  // one grid on both sides: psi1 = psi2 (both C on the same points), the symmetric split-BF16 or FP64
+  // contraction (pairs on and above each r1 tile's diagonal; the exchange plus its transpose)
+  bool const sym = (precision == TCSCF_PREC_BF16X3 || precision == TCSCF_PREC_FP64) && &g1 == &g2;
   Contraction c;
   c.n1 = n1; c.n2 = n2; c.R = nocc; c.ncol = nb;
-  c.p1 = g1.pts; c.p2 = g2.pts; c.psi1 = psi1; c.psi2 = psi2; c.ldpsi = ldpsi;
+  c.p1 = g1.pts; c.p2 = g2.pts; c.psi1 = psi1; c.psi2 = sym ? psi1 : psi2; c.ldpsi = ldpsi;
   c.V = Vw; c.ldv = nb; c.T = Tb; c.ldt = nb; c.coul = coul; c.VH = VH;
-  bool const tensor = precision != TCSCF_PREC_FP64;
+  c.sym = sym ? 1 : 0;
+  double * FRhalf = nullptr;
+  if (sym) TCSCF_TRY(scratch(ctx, "scf_graph_sym_half", sizeof(double) * nn, reinterpret_cast<void **>(&FRhalf)));
   TensorPrep tp;
   TensorPlan plan;
   void * arena = nullptr;
@@ -1677,9 +1721,11 @@ int scfGraph(tcscf_ctx * ctx, Grid & g1, Grid & g2, int nocc, const double * S, 
     } else {
     kOrbitals<<<gridBlocks(n1 * nocc, 256), 256, sm, ctx->stream>>>(n1, nb, nocc, g1.phiR, C, nocc, psi1, ldpsi);
     TCSCF_LAUNCH(ctx);
-    kOrbitals<<<gridBlocks(n2 * nocc, 256), 256, sm, ctx->stream>>>(n2, nb, nocc, g2.phiR, C, nocc, psi2, ldpsi);
-    TCSCF_LAUNCH(ctx);
-    kCoulombSource<<<gridBlocks(n2, 256), 256, 0, ctx->stream>>>(n2, nocc, psi2, psi2, ldpsi, g2.w, scale, coul);
+    if (!sym) {
+      kOrbitals<<<gridBlocks(n2 * nocc, 256), 256, sm, ctx->stream>>>(n2, nb, nocc, g2.phiR, C, nocc, psi2, ldpsi);
+      TCSCF_LAUNCH(ctx);
+    }
+    kCoulombSource<<<gridBlocks(n2, 256), 256, 0, ctx->stream>>>(n2, nocc, c.psi2, c.psi2, ldpsi, g2.w, scale, coul);
     TCSCF_LAUNCH(ctx);
     if (tensor) {
       TCSCF_TRY(tensorPrepare(ctx, c, precision, arena, arenaBytes, tp));
@@ -1691,6 +1737,12 @@ int scfGraph(tcscf_ctx * ctx, Grid & g1, Grid & g2, int nocc, const double * S, 
     }
     TCSCF_CUDA(ctx, cudaMemsetAsync(FR, 0, sizeof(double) * nn, ctx->stream));
     TCSCF_TRY(reduceFockReal(ctx, n1, nb, g1.phiR, g1.w, VH, 2.0, Tb, nb, 1.0, FR));
+    if (sym && !zeroDensity) {
+      TCSCF_CUDA(ctx, cudaMemsetAsync(FRhalf, 0, sizeof(double) * nn, ctx->stream));
+      TCSCF_TRY(reduceFockReal(ctx, n1, nb, g1.phiR, g1.w, nullptr, 0.0, Tb, nb, 1.0, FRhalf));
+      kAddTransposed<<<gridBlocks(int64_t(nn), 256), 256, 0, ctx->stream>>>(nb, FRhalf, FR);
+      TCSCF_LAUNCH(ctx);
+    }
     kRealToReference<<<gridBlocks(int64_t(nn), 256), 256, 0, ctx->stream>>>(1, nb, g1.dsto, FR, nullptr, dG);
     TCSCF_LAUNCH(ctx);
     kFinalize<<<1, 512, 0, ctx->stream>>>(1, nb, dH, dG, nullptr, dD, respectSym, 2.0, dF, dE);

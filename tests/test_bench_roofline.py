@@ -50,3 +50,23 @@ def test_measured_peaks_take_precedence(tmp_path, monkeypatch):
     (tmp_path / "MEASURED_PEAKS.json").write_text('{"hbm_gbs": 6555.8, "bf16_tflops": 1651.8, "bf16_tflops_sustained": 1395.3}')
     peaks, kind = bench.load_peaks()
     assert kind == "measured" and peaks["bf16_tflops"] == 1651.8
+
+
+def test_symmetric_pair_counts_and_roofline():
+    # one grid as r1 and r2: each 128-point r1 tile from its own diagonal on (the diagonal tile in full)
+    n = KR["n"]
+    tiles, blocks = -(-n // 128), -(-n // 64)
+    assert bench.symmetric_pairs(n) == sum(128 * 64 * (blocks - 2 * p) for p in range(tiles)) == 82_450_481_152
+    assert bench.symmetric_pairs(n, fp64=True) == sum(128 * (n - 128 * p) for p in range(tiles))
+    assert abs(bench.symmetric_pairs(n) / n ** 2 - 0.5) < 1e-3
+    r = bench.roofline(ffi.PREC_BF16X3, n, KR["nb"], KR["nocc"], 233.6, bench.PEAKS_FALLBACK, "fallback", 2.889e10, sym=True)
+    assert r["symmetric"] and r["pairs"] == 82_450_481_152
+    assert r["achieved"] == pytest.approx(2 * 82_450_481_152 * 2161 / 0.2336 / 1e12)
+    assert r["full_pairs_tflops"] == pytest.approx(2 * n ** 2 * 2161 / 0.2336 / 1e12)
+    # traffic given for a full launch scales with the units computed
+    assert r["traffic"] == pytest.approx(2.889e10 * 82_450_481_152 / (tiles * 128 * blocks * 64))
+    f = bench.roofline(ffi.PREC_FP64, n, KR["nb"], KR["nocc"], 1610.0, bench.PEAKS_FALLBACK, "fallback", None, sym=True)
+    assert f["symmetric"] and f["achieved"] == pytest.approx(2 * bench.symmetric_pairs(n, fp64=True) * 139 / 1.61 / 1e12)
+    # TF32 keeps the full contraction
+    t = bench.roofline(ffi.PREC_TF32, n, KR["nb"], KR["nocc"], 312.0, bench.PEAKS_FALLBACK, "fallback", None, sym=True)
+    assert not t["symmetric"] and t["pairs"] == float(n) ** 2

@@ -194,12 +194,15 @@ def test_rcs_scf_matches_oracle_he(ctx, he_setup):
     S, h = api.overlap_core(w.basis, w.Z)
     vals1 = oracle.basis_values(g.points, w.basis)
     F = oracle.compute_F(g.points, g.points, g.weights, vals1, w.nb)
-    st, Er, itr, Dr, eig = oracle.scf(1, 1, 1, F, vals1, g.weights, S, h, tol=1e-8, max_iter=50)
+    # converged to 1e-10 Eh so that the two energies agree to E_TOL wherever each loop stops: the GPU
+    # build's rounding differs from the oracle's (it contracts each pair once when r1 = r2), which can
+    # move the iteration that first meets the threshold by one
+    st, Er, itr, Dr, eig = oracle.scf(1, 1, 1, F, vals1, g.weights, S, h, tol=1e-10, max_iter=50)
     assert st == 0
     hf = api.RCSHartreeFock(1, 1, w.nb)
-    Eg = hf.compute(S, h, G, G, tol=1e-8)
+    Eg = hf.compute(S, h, G, G, tol=1e-10)
     assert abs(Eg - Er) < E_TOL, (Eg, Er, itr, hf.numberOfConvergenceLoops())
-    assert hf.numberOfConvergenceLoops() == itr
+    assert abs(hf.numberOfConvergenceLoops() - itr) <= 1
     # physically sensible: within the 50 x 50 product grid's quadrature error of the He Hartree-Fock
     # limit -2.8617 Eh (src/unitTests/HartreeFockTest.cpp:591-602)
     assert -2.95 < Eg < -2.75

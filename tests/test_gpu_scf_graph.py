@@ -40,9 +40,10 @@ def _graph(w, G, S, h, precision, capture, tol=1e-10, max_iter=60):
 
 def test_captured_and_uncaptured_device_loops_are_bit_identical(ctx, ne_case):
     w, g, G, S, h = ne_case
-    for prec in (ffi.PREC_FP64, ffi.PREC_BF16X3):
-        Ec, hc = _graph(w, G, S, h, prec, True)
-        Eu, hu = _graph(w, G, S, h, prec, False)
+    # the split-BF16 energies move by their own ~1e-9 Eh between builds: stop that loop at 1e-8 Eh
+    for prec, tol in ((ffi.PREC_FP64, 1e-10), (ffi.PREC_BF16X3, 1e-8)):
+        Ec, hc = _graph(w, G, S, h, prec, True, tol=tol)
+        Eu, hu = _graph(w, G, S, h, prec, False, tol=tol)
         assert hc.graphLaunches == 1 and hu.graphLaunches == 0
         assert Ec == Eu, (prec, Ec, Eu)
         assert hc.numberOfConvergenceLoops() == hu.numberOfConvergenceLoops()
