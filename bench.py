@@ -553,6 +553,8 @@ def run_batch(args, rank: int) -> None:
 
     with ClockSampler(int(os.environ.get("LOCAL_RANK", 0))) as clk:
         tb, Eb = timed(batched, args.steps, args.warmup)
+    # device times of the last batched call: the persistent tensor launches alone, and the whole call
+    batch_contraction_ms, batch_total_ms, batch_launches = ctx.last_timing()
     t1, E1 = timed(one_by_one, max(1, min(args.steps, 2)), 1)
     E64 = np.array([api.fock_build(G, G, D, h, precision=ffi.PREC_FP64)[2] for G, D, h in zip(Gs, Ds, hs)])
     err = np.abs(Eb - E64)
@@ -563,6 +565,7 @@ def run_batch(args, rank: int) -> None:
                                    "Lebedev 110-1202 points (seed 20261203), core-Hamiltonian guess densities",
                        "points_total": int(sum(npts)), "points_max": int(max(npts)), "timing": "host wall clock around the "
                        "public batched call, inputs resident on the device except the densities"},
+            "contraction_ms": batch_contraction_ms, "device_total_ms": batch_total_ms, "launches": batch_launches,
             "one_at_a_time_s": t1, "batch_speedup": t1 / tb, "batched_equals_one_at_a_time": bool(np.array_equal(Eb, E1)),
             "dE_vs_fp64_max": float(err.max()), "dE_vs_fp64_median": float(np.median(err)),
             "dE_rel_vs_fp64_max": float((err / np.abs(E64)).max()), "clocks": clk.summary(),

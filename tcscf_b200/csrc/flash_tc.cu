@@ -662,43 +662,66 @@ __global__ void kPackCoordPairs(int64_t n, int64_t npad, const double * pts, con
 // r1 tile's diagonal, which the tensor kernel skips, added to the potential:
 //   VH[r] += sum_{j < BM tile(r)} g(r, j) c(j)
 // with the tensor kernel's FP32 arithmetic on the same packed points (its drop rule and its
-// Newton-refined rsqrt), FP32 sums per 64-point block added in FP64.  One thread per r1 point, one
-// block per r1 tile, the tiles with the most pairs first.
-__global__ void __launch_bounds__(BM) kCoulombLower(int nTiles, int64_t n1, const float4 * __restrict__ r1xyz,
-                                                   const float4 * __restrict__ r2pairs, double * VH)
+// Newton-refined rsqrt), FP32 sums per 64-point block added in FP64.  One block of 64 threads per r1
+// tile, the tiles with the most pairs first; each thread takes two rows of the tile (r and r + 64), so
+// that every r2 point it loads serves both.
+__device__ __forceinline__ uint64_t coulombPair(uint64_t px, uint64_t py, uint64_t pz, float thr, float4 qa, float4 qb)
 {
-  int const tile = nTiles - 1 - int(blockIdx.x);
-  int64_t const r = int64_t(tile) * BM + threadIdx.x;
-  float4 const p1 = r1xyz[r];
-  uint64_t const p1x = f2pack(p1.x, p1.x), p1y = f2pack(p1.y, p1.y), p1z = f2pack(p1.z, p1.z);
   uint64_t const mOne = f2pack(-1.0f, -1.0f), mHalf = f2pack(-0.5f, -0.5f);
-  double vh = 0.0;
-  int64_t const nPairs = int64_t(tile) * (BM / 2);   // the points [0, BM tile) in pairs
-  for (int64_t b = 0; b < nPairs; b += BK / 2) {
-    uint64_t vs = 0;
-#pragma unroll 8
+  uint64_t const dx = f2sub(px, f2pack(qa.x, qa.y));
+  uint64_t const dy = f2sub(py, f2pack(qa.z, qa.w));
+  uint64_t const dz = f2sub(pz, f2pack(qb.x, qb.y));
+  uint64_t const r2 = f2fma(dx, dx, f2fma(dy, dy, f2mul(dz, dz)));
+  float r2a, r2b;
+  f2unpack(r2, r2a, r2b);
+  uint64_t y = f2pack(rsqrtApprox(r2a), rsqrtApprox(r2b));
+  uint64_t const em = f2fma(f2mul(r2, y), y, mOne);
+  y = f2fma(f2mul(y, mHalf), em, y);
+  float ya, yb;
+  f2unpack(y, ya, yb);
+  ya = r2a >= thr ? ya : 0.0f;
+  yb = r2b >= thr ? yb : 0.0f;
+  return f2pack(ya, yb);
+}
+
+__global__ void __launch_bounds__(BM / 2) kCoulombLower(int nTiles, int64_t n1, const float4 * __restrict__ r1xyz,
+                                                       const float4 * __restrict__ r2pairs, double * VH)
+{
+  // the r2 points pass through shared memory in 64-point blocks (64 float4 in pair layout, one per
+  // thread), the next block's load in flight while the current one is summed
+  __shared__ float4 sq[2][BK];
+  int const tile = nTiles - 1 - int(blockIdx.x);
+  int const t = threadIdx.x;
+  int64_t const r0 = int64_t(tile) * BM + t, r1 = r0 + BM / 2;
+  float4 const pa = r1xyz[r0], pb = r1xyz[r1];
+  uint64_t const ax = f2pack(pa.x, pa.x), ay = f2pack(pa.y, pa.y), az = f2pack(pa.z, pa.z);
+  uint64_t const bx = f2pack(pb.x, pb.x), by = f2pack(pb.y, pb.y), bz = f2pack(pb.z, pb.z);
+  double vha = 0.0, vhb = 0.0;
+  int const nBlk = tile * (BM / BK);   // the points [0, BM tile) in 64-point blocks
+  if (nBlk > 0) sq[0][t] = r2pairs[t];
+  __syncthreads();
+  for (int j = 0; j < nBlk; ++j) {
+    int const buf = j & 1;
+    bool const more = j + 1 < nBlk;
+    float4 const nxt = more ? r2pairs[int64_t(j + 1) * BK + t] : make_float4(0, 0, 0, 0);
+    uint64_t va = 0, vb = 0;
+#pragma unroll 4
     for (int e = 0; e < BK / 2; ++e) {
-      float4 const qa = r2pairs[2 * (b + e)], qb = r2pairs[2 * (b + e) + 1];
-      uint64_t const dx = f2sub(p1x, f2pack(qa.x, qa.y));
-      uint64_t const dy = f2sub(p1y, f2pack(qa.z, qa.w));
-      uint64_t const dz = f2sub(p1z, f2pack(qb.x, qb.y));
-      uint64_t const r2 = f2fma(dx, dx, f2fma(dy, dy, f2mul(dz, dz)));
-      float r2a, r2b;
-      f2unpack(r2, r2a, r2b);
-      uint64_t y = f2pack(rsqrtApprox(r2a), rsqrtApprox(r2b));
-      uint64_t const em = f2fma(f2mul(r2, y), y, mOne);
-      y = f2fma(f2mul(y, mHalf), em, y);
-      float ya, yb;
-      f2unpack(y, ya, yb);
-      ya = r2a >= p1.w ? ya : 0.0f;
-      yb = r2b >= p1.w ? yb : 0.0f;
-      vs = f2fma(f2pack(ya, yb), f2pack(qb.z, qb.w), vs);
+      float4 const qa = sq[buf][2 * e], qb = sq[buf][2 * e + 1];
+      uint64_t const c = f2pack(qb.z, qb.w);
+      va = f2fma(coulombPair(ax, ay, az, pa.w, qa, qb), c, va);
+      vb = f2fma(coulombPair(bx, by, bz, pb.w, qa, qb), c, vb);
     }
-    float v0, v1;
-    f2unpack(vs, v0, v1);
-    vh += double(v0 + v1);
+    float u0, u1;
+    f2unpack(va, u0, u1);
+    vha += double(u0 + u1);
+    f2unpack(vb, u0, u1);
+    vhb += double(u0 + u1);
+    if (more) sq[buf ^ 1][t] = nxt;   // block j - 1's buffer: every thread finished it before the last barrier
+    __syncthreads();
   }
-  if (r < n1) VH[r] += vh;
+  if (r0 < n1) VH[r0] += vha;
+  if (r1 < n1) VH[r1] += vhb;
 }
 
 }  // namespace tc
@@ -1022,7 +1045,7 @@ namespace {
 int coulombLower(tcscf_ctx * ctx, tc::Instance const & I, Contraction const & c)
 {
   if (!I.sym || !c.VH || I.nTiles < 2) return TCSCF_OK;
-  tc::kCoulombLower<<<unsigned(I.nTiles), tc::BM, 0, ctx->stream>>>(I.nTiles, c.n1, I.r1xyz, I.r2pairs, c.VH);
+  tc::kCoulombLower<<<unsigned(I.nTiles), tc::BM / 2, 0, ctx->stream>>>(I.nTiles, c.n1, I.r1xyz, I.r2pairs, c.VH);
   TCSCF_LAUNCH(ctx);
   return TCSCF_OK;
 }
