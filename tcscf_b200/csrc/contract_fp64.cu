@@ -256,26 +256,52 @@ __global__ void __launch_bounds__(NT, RPT == 8 ? 1 : 2) kContractFp64(KArgs a)
 
 // Symmetric contractions: the Coulomb row sums over the r2 points before each block's first row (the
 // pairs kContractFp64 skips), added to the potential: VH[r] += sum_{j < bm floor(r / bm)} g(r, j) c(j),
-// FP64 with the exact-coincidence rule.  One thread per r1 point; the r2 points are read by all threads
-// of a block at once (broadcast).
-__global__ void __launch_bounds__(128) kCoulombLowerFp64(int64_t n, int bm, const double * __restrict__ p, const double * __restrict__ coul,
-                                                        double * VH)
+// FP64 with the exact-coincidence rule and 64-term partial sums.  One block of 64 threads per 128 rows;
+// each thread takes rows r and r + 64 (the same bm tile, or consecutive 64-row tiles when bm = 64, so
+// every condition below is uniform over the block), and the r2 points pass through shared memory in
+// 64-point chunks, the next chunk's load in flight while the current one is summed.
+__global__ void __launch_bounds__(64) kCoulombLowerFp64(int64_t n, int bm, const double * __restrict__ p, const double * __restrict__ coul,
+                                                       double * VH)
 {
-  int64_t const r = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  int64_t const rr = r < n ? r : n - 1;   // rows past n repeat the last one (nothing is written for them)
-  double const x = p[rr], y = p[n + rr], z = p[2 * n + rr];
-  int64_t const jend = (rr / bm) * bm;   // a multiple of 64
-  double vh = 0.0;
-  for (int64_t j0 = 0; j0 < jend; j0 += 64) {
-    double part = 0.0;   // sums of 64 terms added into the total (shorter rounding chains)
-    for (int64_t j = j0; j < j0 + 64; ++j) {
-      double const dx = x - p[j], dy = y - p[n + j], dz = z - p[2 * n + j];
-      double const q = fma(dx, dx, fma(dy, dy, dz * dz));
-      if (q != 0.0) part = fma(rsqrt_fp64(q), coul[j], part);
+  __shared__ double4 sq[2][64];   // x, y, z, c
+  int const t = threadIdx.x;
+  int64_t const r0 = int64_t(blockIdx.x) * 128 + t, r1 = r0 + 64;
+  int64_t const a0 = r0 < n ? r0 : n - 1, a1 = r1 < n ? r1 : n - 1;   // rows past n repeat the last one (not written)
+  double const x0 = p[a0], y0 = p[n + a0], z0 = p[2 * n + a0];
+  double const x1 = p[a1], y1 = p[n + a1], z1 = p[2 * n + a1];
+  int64_t const end0 = (int64_t(blockIdx.x) * 128 / bm) * bm;   // the points before row r0's tile (a multiple of 64)
+  int64_t const end1 = ((int64_t(blockIdx.x) * 128 + 64) / bm) * bm;
+  // when row r1's tile starts past n, every r1 row is past n (not written): only row r0's points are read
+  int64_t const nChunks = (end1 <= n ? end1 : end0) / 64;
+  auto load = [&](int64_t k) { int64_t const j = k * 64 + t; return make_double4(p[j], p[n + j], p[2 * n + j], coul[j]); };
+  if (nChunks > 0) sq[0][t] = load(0);
+  __syncthreads();
+  double vh0 = 0.0, vh1 = 0.0;
+  for (int64_t k = 0; k < nChunks; ++k) {
+    int const buf = int(k & 1);
+    bool const more = k + 1 < nChunks;
+    double4 const nxt = more ? load(k + 1) : make_double4(0, 0, 0, 0);
+    bool const row0 = (k + 1) * 64 <= end0;
+    double part0 = 0.0, part1 = 0.0;
+#pragma unroll 4
+    for (int e = 0; e < 64; ++e) {
+      double4 const q = sq[buf][e];
+      double dx = x1 - q.x, dy = y1 - q.y, dz = z1 - q.z;
+      double d = fma(dx, dx, fma(dy, dy, dz * dz));
+      if (d != 0.0) part1 = fma(rsqrt_fp64(d), q.w, part1);
+      if (row0) {
+        dx = x0 - q.x; dy = y0 - q.y; dz = z0 - q.z;
+        d = fma(dx, dx, fma(dy, dy, dz * dz));
+        if (d != 0.0) part0 = fma(rsqrt_fp64(d), q.w, part0);
+      }
     }
-    vh += part;
+    vh0 += part0;
+    vh1 += part1;
+    if (more) sq[buf ^ 1][t] = nxt;   // chunk k - 1's buffer: every thread finished it before the last barrier
+    __syncthreads();
   }
-  if (r < n) VH[r] += vh;
+  if (r0 < n) VH[r0] += vh0;
+  if (r1 < n) VH[r1] += vh1;
 }
 
 // deterministic sum of split partials: out[i] = sum_s part[s*stride + i]
@@ -521,7 +547,7 @@ int contractFp64(tcscf_ctx * ctx, Contraction const & c)
     }
   }
   if (c.sym && c.coul && tiles > 1) {
-    kCoulombLowerFp64<<<unsigned((c.n1 + 127) / 128), 128, 0, ctx->stream>>>(c.n1, bm, c.p1, c.coul, c.VH);
+    kCoulombLowerFp64<<<unsigned((c.n1 + 127) / 128), 64, 0, ctx->stream>>>(c.n1, bm, c.p1, c.coul, c.VH);
     TCSCF_LAUNCH(ctx);
   }
   return TCSCF_OK;

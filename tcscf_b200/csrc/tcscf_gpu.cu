@@ -738,6 +738,16 @@ __global__ void kRealDensity(int nb, int nocc, const double * C, double * DR)
   }
 }
 
+// the occupied eigenvectors of a real-harmonic eigen-solve (columns of the column-major C) as the
+// density factor X [nb][ldx] (X[k][a] = C[a][k]): D_R = X X^T, the density kRealDensity forms
+__global__ void kFactorFromOrbitals(int nb, int nocc, const double * C, int ldx, double * X)
+{
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < nb * nocc; idx += gridDim.x * blockDim.x) {
+    int const k = idx / nocc, a = idx % nocc;
+    X[int64_t(k) * ldx + a] = C[a * nb + k];
+  }
+}
+
 // ---- Pulay DIIS (optional SCF acceleration; the reference iterates plain Roothaan steps) ---------
 // dots[j] = Re <E[slot], E[j]> (Frobenius product of the commutator error matrices of both spins)
 // for the used history slots j < count, one block per j
@@ -1012,7 +1022,7 @@ int checkBasisPair(tcscf_ctx * ctx, Grid * g1, Grid * g2)
 // Direct-form Fock build with device-resident densities dD [nspin][nb][nb] complex.
 // Leaves G (masked), Fock (row-major) and the energy on the device.
 int fockBuildDevice(tcscf_ctx * ctx, Grid & g1, Grid & g2, int nspin, const double2 * dD, const double * dH, int respectSym,
-                    int precision, double2 * dG, double2 * dFock, double * dE)
+                    int precision, double2 * dG, double2 * dFock, double * dE, Factor const * given)
 {
   int const nb = g1.nb;
   int64_t const n1 = g1.n, n2 = g2.n;
@@ -1053,7 +1063,8 @@ int fockBuildDevice(tcscf_ctx * ctx, Grid & g1, Grid & g2, int nspin, const doub
   if (precision == TCSCF_PREC_BF16X3) TCSCF_TRY(tensorPackedV(ctx, g2, V, scale, &vtPacked));
   for (int s = 0; s < nspin; ++s) {
     Factor f;
-    TCSCF_TRY(factorDensity(ctx, g1, dD + size_t(s) * nb * nb, s, f));
+    if (given && given[s].X1) f = given[s];   // the caller's factor of this spin's density (its occupied orbitals)
+    else TCSCF_TRY(factorDensity(ctx, g1, dD + size_t(s) * nb * nb, s, f));
     double * Ts = Tre + size_t(s) * n1 * ldt;
     double * Ti = Tim + size_t(s) * n1 * ldt;
     if (f.R == 0) {
@@ -1267,7 +1278,7 @@ int fockBuildBatch(tcscf_ctx * ctx, int count, Grid * const * g1s, Grid * const 
     Grid & g1 = *g1s[k];
     int const nb = g1.nb;
     if (!tensorOk[k]) {
-      TCSCF_TRY(fockBuildDevice(ctx, g1, *g2s[k], 1, dDs[k], dHs[k], respectSym, precision, dGs[k], dFs[k], dEs[k]));
+      TCSCF_TRY(fockBuildDevice(ctx, g1, *g2s[k], 1, dDs[k], dHs[k], respectSym, precision, dGs[k], dFs[k], dEs[k], nullptr));
       continue;
     }
     Contraction const & c = cs[k];
@@ -2181,7 +2192,7 @@ int tcscf_fock_build(tcscf_ctx * ctx, int r1, int r2, int nspin, const double * 
   double * dE = dH + nn;
   TCSCF_CUDA(ctx, cudaMemcpyAsync(dD, density, sizeof(double2) * nn * nspin, cudaMemcpyHostToDevice, ctx->stream));
   TCSCF_CUDA(ctx, cudaMemcpyAsync(dH, h, sizeof(double) * nn, cudaMemcpyHostToDevice, ctx->stream));
-  TCSCF_TRY(fockBuildDevice(ctx, *g1, *g2, nspin, dD, dH, respect_symmetry, precision, dG, dF, dE));
+  TCSCF_TRY(fockBuildDevice(ctx, *g1, *g2, nspin, dD, dH, respect_symmetry, precision, dG, dF, dE, nullptr));
   if (G) TCSCF_CUDA(ctx, cudaMemcpyAsync(G, dG, sizeof(double2) * nn * nspin, cudaMemcpyDeviceToHost, ctx->stream));
   if (fock) TCSCF_CUDA(ctx, cudaMemcpyAsync(fock, dF, sizeof(double2) * nn * nspin, cudaMemcpyDeviceToHost, ctx->stream));
   double e = 0;
@@ -2209,7 +2220,8 @@ int tcscf_fock_build_device(tcscf_ctx * ctx, int r1, int r2, int nspin, const do
   TCSCF_TRY(scratch(ctx, "fock_dev_io", sizeof(double2) * nn * nspin * 2, &p));
   double2 * dG = G ? reinterpret_cast<double2 *>(G) : static_cast<double2 *>(p);
   double2 * dF = fock ? reinterpret_cast<double2 *>(fock) : static_cast<double2 *>(p) + nn * nspin;
-  TCSCF_TRY(fockBuildDevice(ctx, *g1, *g2, nspin, reinterpret_cast<const double2 *>(density), h, respect_symmetry, precision, dG, dF, energy));
+  TCSCF_TRY(fockBuildDevice(ctx, *g1, *g2, nspin, reinterpret_cast<const double2 *>(density), h, respect_symmetry, precision, dG, dF, energy,
+                            nullptr));
   TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return TCSCF_OK;
 }
@@ -2498,8 +2510,13 @@ int tcscf_scf(tcscf_ctx * ctx, int r1, int r2, int nspin, int n_up, int n_down, 
   }
   double2 const one = make_double2(1, 0), zero = make_double2(0, 0), mone = make_double2(-1, 0);
   double e = std::numeric_limits<double>::max();
+  // density factors from the previous iteration's real-harmonic eigen-solve (every spin solved real)
+  Factor given[2];
+  bool givenOk = false;
+  double * Xocc = nullptr;
+  if (realPath) TCSCF_TRY(scratch(ctx, "scf_occ_factor", sizeof(double) * 2 * nn + 64, reinterpret_cast<void **>(&Xocc)));
   for (int it = 0; it < max_iter; ++it) {
-    TCSCF_TRY(fockBuildDevice(ctx, *g1, *g2, nspin, dD, dH, respect_symmetry, precision, dG, dF, dE));
+    TCSCF_TRY(fockBuildDevice(ctx, *g1, *g2, nspin, dD, dH, respect_symmetry, precision, dG, dF, dE, givenOk ? given : nullptr));
     double ne = 0;
     TCSCF_CUDA(ctx, cudaMemcpyAsync(&ne, dE, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
@@ -2547,6 +2564,8 @@ int tcscf_scf(tcscf_ctx * ctx, int r1, int r2, int nspin, int n_up, int n_down, 
         }
       }
     }
+    int solvedReal = 0;
+    given[0] = given[1] = Factor{};
     for (int s = 0; s < nspin; ++s) {
       if (realPath) {
         kDensityToReal<<<gridBlocks(nn, 256), 256, 0, ctx->stream>>>(1, nb, g1->dsto, Fuse + s * nn, FR);
@@ -2570,6 +2589,18 @@ int tcscf_scf(tcscf_ctx * ctx, int r1, int r2, int nspin, int n_up, int n_down, 
           TCSCF_LAUNCH(ctx);
           kRealToReference<<<gridBlocks(nn, 256), 256, 0, ctx->stream>>>(1, nb, g1->dsto, DRre, nullptr, dD + s * nn);
           TCSCF_LAUNCH(ctx);
+          // the next build factors this density as its occupied orbitals themselves (D_R = C C^T):
+          // smooth from one iteration to the next, unlike a pivoted factorisation of D
+          if (nocc[s] > 0) {
+            kFactorFromOrbitals<<<gridBlocks(int64_t(nb) * nocc[s], 256), 256, 0, ctx->stream>>>(nb, nocc[s], Ar, nb, Xocc + size_t(s) * nn);
+            TCSCF_LAUNCH(ctx);
+            given[s].R = nocc[s];
+            given[s].X1 = given[s].X2 = Xocc + size_t(s) * nn;
+            given[s].ldx = nb;
+            given[s].complex = false;
+            given[s].same = true;
+          }
+          ++solvedReal;
           continue;
         }
       }
@@ -2586,6 +2617,7 @@ int tcscf_scf(tcscf_ctx * ctx, int r1, int r2, int nspin, int n_up, int n_down, 
       kDensityFromOrbitals<<<gridBlocks(nn, 256), 256, 0, ctx->stream>>>(nb, nocc[s], A, dD + s * nn);
       TCSCF_LAUNCH(ctx);
     }
+    givenOk = solvedReal == nspin;
   }
   if (energy) *energy = e;
   if (density) TCSCF_CUDA(ctx, cudaMemcpy(density, dD, sizeof(double2) * nn * nspin, cudaMemcpyDeviceToHost));
