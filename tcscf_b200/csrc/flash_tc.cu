@@ -684,13 +684,13 @@ __device__ __forceinline__ uint64_t coulombPair(uint64_t px, uint64_t py, uint64
   return f2pack(ya, yb);
 }
 
-__global__ void __launch_bounds__(BM / 2) kCoulombLower(int nTiles, int64_t n1, const float4 * __restrict__ r1xyz,
-                                                       const float4 * __restrict__ r2pairs, double * VH)
+// the lower rows of one r1 tile (tile >= 1) of one contraction
+__device__ __forceinline__ void coulombLowerTile(int tile, int64_t n1, const float4 * __restrict__ r1xyz, const float4 * __restrict__ r2pairs,
+                                                 double * VH)
 {
   // the r2 points pass through shared memory in 64-point blocks (64 float4 in pair layout, one per
   // thread), the next block's load in flight while the current one is summed
   __shared__ float4 sq[2][BK];
-  int const tile = nTiles - 1 - int(blockIdx.x);
   int const t = threadIdx.x;
   int64_t const r0 = int64_t(tile) * BM + t, r1 = r0 + BM / 2;
   float4 const pa = r1xyz[r0], pb = r1xyz[r1];
@@ -722,6 +722,27 @@ __global__ void __launch_bounds__(BM / 2) kCoulombLower(int nTiles, int64_t n1, 
   }
   if (r0 < n1) VH[r0] += vha;
   if (r1 < n1) VH[r1] += vhb;
+}
+
+__global__ void __launch_bounds__(BM / 2) kCoulombLower(int nTiles, int64_t n1, const float4 * __restrict__ r1xyz,
+                                                       const float4 * __restrict__ r2pairs, double * VH)
+{
+  coulombLowerTile(nTiles - 1 - int(blockIdx.x), n1, r1xyz, r2pairs, VH);
+}
+
+// the lower rows of several contractions in one launch: block b takes tile tiles[b].y of job tiles[b].x
+// (the list holds every (job, tile >= 1) once, the tiles with the most pairs first)
+struct CoulombLowerJob {
+  const float4 * r1xyz;
+  const float4 * r2pairs;
+  double * VH;
+  int64_t n1;
+};
+__global__ void __launch_bounds__(BM / 2) kCoulombLowerBatch(const CoulombLowerJob * __restrict__ jobs, const int2 * __restrict__ tiles)
+{
+  int2 const jt = tiles[blockIdx.x];
+  CoulombLowerJob const j = jobs[jt.x];
+  coulombLowerTile(jt.y, j.n1, j.r1xyz, j.r2pairs, j.VH);
 }
 
 }  // namespace tc
@@ -1145,6 +1166,8 @@ int tensorRun(tcscf_ctx * ctx, TensorPrep * const * preps, int count, bool recor
   TCSCF_CUDA(ctx, cudaMemcpyAsync(&st, dStatus, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   if (st != 0) return fail(ctx, TCSCF_ERR_TIMEOUT, "tensor-core contraction: bounded wait expired (code " + std::to_string(st) + ")");
+  std::vector<tc::CoulombLowerJob> jobs;
+  std::vector<int2> lowerTiles;
   for (int k = 0; k < count; ++k) {
     tc::Instance const & I = preps[k]->inst;
     Contraction const & c = preps[k]->c;
@@ -1153,7 +1176,25 @@ int tensorRun(tcscf_ctx * ctx, TensorPrep * const * preps, int count, bool recor
       TCSCF_TRY(sumSplitsLaunch(ctx, n, I.nSplit, int64_t(c.n1) * c.ldt, I.T, c.T, c.n1, c.ncol, c.ldt, c.ldt));
       if (c.VH) TCSCF_TRY(sumSplitsLaunch(ctx, c.n1, I.nSplit, c.n1, I.VH, c.VH, c.n1, 1, 1, 1));
     }
-    TCSCF_TRY(coulombLower(ctx, I, c));
+    if (count == 1) {
+      TCSCF_TRY(coulombLower(ctx, I, c));
+    } else if (I.sym && c.VH && I.nTiles >= 2) {
+      for (int t = 1; t < I.nTiles; ++t) lowerTiles.push_back(make_int2(int(jobs.size()), t));
+      jobs.push_back({I.r1xyz, I.r2pairs, c.VH, c.n1});
+    }
+  }
+  if (!lowerTiles.empty()) {
+    // the lower Coulomb rows of all symmetric instances in one launch, the tiles with the most pairs first
+    std::stable_sort(lowerTiles.begin(), lowerTiles.end(), [](int2 const & a, int2 const & b) { return a.y > b.y; });
+    void * q = nullptr;
+    TCSCF_TRY(scratch(ctx, "coulomb_lower_jobs", align256(sizeof(tc::CoulombLowerJob) * jobs.size()) + sizeof(int2) * lowerTiles.size() + 256, &q));
+    auto * dJobs = static_cast<tc::CoulombLowerJob *>(q);
+    auto * dTiles = reinterpret_cast<int2 *>(static_cast<char *>(q) + align256(sizeof(tc::CoulombLowerJob) * jobs.size()));
+    TCSCF_CUDA(ctx, cudaMemcpyAsync(dJobs, jobs.data(), sizeof(tc::CoulombLowerJob) * jobs.size(), cudaMemcpyHostToDevice, ctx->stream));
+    TCSCF_CUDA(ctx, cudaMemcpyAsync(dTiles, lowerTiles.data(), sizeof(int2) * lowerTiles.size(), cudaMemcpyHostToDevice, ctx->stream));
+    tc::kCoulombLowerBatch<<<unsigned(lowerTiles.size()), tc::BM / 2, 0, ctx->stream>>>(dJobs, dTiles);
+    TCSCF_LAUNCH(ctx);
+    TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));   // the host lists are consumed before they go out of scope
   }
   return TCSCF_OK;
 }
