@@ -106,6 +106,9 @@ __global__ void __launch_bounds__(NT, RPT == 8 ? 1 : 2) kContractFp64(KArgs a)
 {
   constexpr int CPT = BN / 16;            // columns per thread
   constexpr int BMT = 16 * RPT;           // r1 rows per block
+  // the 128 x 128 tile's GEMM on the FP64 tensor cores (mma.m8n8k4): its operands come from registers,
+  // so shared memory stops limiting the FP64 rate as it does the 8 x 8 register tile on the CUDA cores
+  constexpr bool kDmma = BN == 128 && RPT == 8;
   constexpr int VPT = BMT * BK / NT;      // phase-B values per thread
   constexpr int TPR = BK / VPT;           // phase-B threads per row
   extern __shared__ __align__(16) double sm[];
@@ -212,6 +215,29 @@ __global__ void __launch_bounds__(NT, RPT == 8 ? 1 : 2) kContractFp64(KArgs a)
       sX[c * BMT + rB] = (k0 + c < r2half ? 0.5 * g : g) * rho[j];
     }
     __syncthreads();
+    if constexpr (kDmma) {
+      // FP64 tensor cores: warp w owns rows 64 (w & 1) .. + 64 and columns 32 (w >> 1) .. + 32 of the
+      // block as 8 x 4 tiles of 8 x 8; mma.m8n8k4 fragments: A[r][k] at lane 4 r + k, B[k][n] at lane
+      // 4 n + k, C[r][2 q + e] at lane 4 r + q (element e)
+      int const lane = tid & 31, wr = ((tid >> 5) & 1) * 64, wc = (tid >> 6) * 32;
+      int const fr = lane >> 2, fk = lane & 3;
+#pragma unroll 2
+      for (int k = 0; k < BK; k += 4) {
+        double av[8], bv[4];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) av[i] = sX[(k + fk) * BMT + wr + 8 * i + fr];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) bv[j] = sV[(k + fk) * BN + wc + 8 * j + fr];
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j)
+            asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                         : "+d"(acc[i][2 * j]), "+d"(acc[i][2 * j + 1])
+                         : "d"(av[i]), "d"(bv[j]));
+      }
+      continue;
+    }
 #pragma unroll 4
     for (int k = 0; k < BK; ++k) {
       double av[RPT];
@@ -236,14 +262,30 @@ __global__ void __launch_bounds__(NT, RPT == 8 ? 1 : 2) kContractFp64(KArgs a)
   }
 
   double * T = a.T + blockIdx.y * a.tStrideSplit;
+  if constexpr (kDmma) {
+    int const lane = tid & 31, wr = ((tid >> 5) & 1) * 64, wc = (tid >> 6) * 32;
 #pragma unroll
-  for (int i = 0; i < RPT; ++i) {
-    int64_t const g = r1base + tr * RPT + i;
-    if (g >= a.n1) continue;
+    for (int i = 0; i < 8; ++i) {
+      int64_t const g = r1base + wr + 8 * i + (lane >> 2);
+      if (g >= a.n1) continue;
 #pragma unroll
-    for (int j = 0; j < CPT; ++j) {
-      int const col = cg * BN + 32 * (j / 2) + 2 * tc + (j & 1);
-      if (col < a.ncol) T[g * a.ldt + col] = acc[i][j];
+      for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          int const col = cg * BN + wc + 8 * j + 2 * (lane & 3) + e;
+          if (col < a.ncol) T[g * a.ldt + col] = acc[i][2 * j + e];
+        }
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < RPT; ++i) {
+      int64_t const g = r1base + tr * RPT + i;
+      if (g >= a.n1) continue;
+#pragma unroll
+      for (int j = 0; j < CPT; ++j) {
+        int const col = cg * BN + 32 * (j / 2) + 2 * tc + (j & 1);
+        if (col < a.ncol) T[g * a.ldt + col] = acc[i][j];
+      }
     }
   }
   if (doCoul) {
