@@ -321,7 +321,7 @@ def roofline(prec: int, n: int, nb: int, nocc: int, c_ms: float, peaks: dict, pe
     # the build needs: N^2, or with the symmetric contraction each unordered pair once (the diagonal
     # tiles in full); the kernels contract the same sum in factored form, 2 P (nocc + nb + 1) flops
     # (rho GEMM, exchange GEMM, Coulomb), reported beside it as kernel_algorithm_tflops
-    sym = sym and prec in (ffi.PREC_BF16X3, ffi.PREC_FP64)
+    sym = sym and prec in (ffi.PREC_BF16X3, ffi.PREC_FP64)   # TF32 keeps the full contraction
     pairs = float(symmetric_pairs(n, fp64=prec == ffi.PREC_FP64)) if sym else float(n) * n
     flops = 2.0 * pairs * (nb * nocc + 1)
     kernel_flops = 2.0 * pairs * (nocc + nb + 1)
@@ -333,7 +333,7 @@ def roofline(prec: int, n: int, nb: int, nocc: int, c_ms: float, peaks: dict, pe
                  "kernel_algorithm_tflops": kernel_achieved,
                  "frac_note": "frac counts F_alg, the pair-density work the factored form avoids; issued_frac (the "
                               "slice products the tensor pipe executes) and ncu's tensor-pipe activity measure the hardware"}
-    if traffic is not None and sym and prec == ffi.PREC_BF16X3:   # the full-launch figure, scaled by the units
+    if traffic is not None and sym and prec != ffi.PREC_FP64:   # the full-launch figure, scaled by the units
         traffic = traffic * pairs / (float(-(-n // 128) * 128) * (-(-n // 64) * 64))
     if prec == ffi.PREC_FP64:
         # the FP64 kernel runs on the FP64 pipe: its roofline counts the flops it performs
@@ -352,7 +352,7 @@ def roofline(prec: int, n: int, nb: int, nocc: int, c_ms: float, peaks: dict, pe
         RP = 32                            # TF32 launches hold rank 32 (larger ranks run in chunks)
         NB = 64 if nb <= 64 else 128
         chunks = -(-nocc // RP)
-        issued = n * n * chunks * (2.0 * RP + 2.0 * NB) / (c_ms / 1e3) / 1e12
+        issued = pairs * chunks * (2.0 * RP + 2.0 * NB) / (c_ms / 1e3) / 1e12
         roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                 "traffic": None, "peak_source": src,
                 "issued_tensor_tflops": issued, "issued_frac": issued / peak, **numerator}
@@ -475,10 +475,11 @@ def run_ours(args, rank: int, world: int) -> None:
     dropped, near = grids.coincident_pairs(g, g)   # r1 = r2 grid: the diagonal pairs contribute 0
     c_ms = statistics.median(cms)
     allpeaks = dict(peaks, **mm_peaks)
-    # one grid object serves as r1 and r2, so the split-BF16 build takes the symmetric contraction
+    # one grid object serves as r1 and r2 and the guess density is real and positive semi-definite, so
+    # the split-BF16 and FP64 builds take the symmetric contraction
     roof = roofline(prec, n, w.nb, w.n_up, c_ms, allpeaks, peak_kind,
                     TRAFFIC_BYTES_PER_LAUNCH.get(w.name) if prec == ffi.PREC_BF16X3 and args.nrad == 0 else None,
-                    sym=prec == ffi.PREC_BF16X3)
+                    sym=True)
     if fp64 is not None:
         fp64["roofline"] = roofline(ffi.PREC_FP64, n, w.nb, w.n_up, fp64["contraction_ms"], allpeaks, peak_kind, None, sym=True)
     cpu = None

@@ -1028,6 +1028,8 @@ int tensorPrepare(tcscf_ctx * ctx, Contraction const & c, int precision, void * 
   tc::Instance & I = tp.inst;
   I = tc::Instance{};
   I.nTiles = sh.nTiles; I.nSplit = sh.nSplit; I.blocksPerSplit = sh.perSplit; I.nBlocks = sh.nBlocks;
+  // TF32 keeps the full contraction: with 11-bit operands its mirrored half would carry the r2-side
+  // rounding of V twice (Ne: |dE| 2.1e-5 against 7.5e-7 Eh for the full form)
   I.sym = c.sym && !tf32 ? 1 : 0;
   I.n1 = int(c.n1); I.nb = c.ncol; I.ldt = c.ldt;
   I.r1xyz = r1c; I.r2pairs = r2c;

@@ -1074,8 +1074,8 @@ int fockBuildDevice(tcscf_ctx * ctx, Grid & g1, Grid & g2, int nspin, const doub
     int const R = f.R;
     // one grid on both sides and X1 = X2: psi1 = psi2 and X = g rho is symmetric, so the split-BF16 and
     // FP64 contractions compute only the pairs on and above each r1 tile's diagonal (T'), and the
-    // exchange matrix is sum W T' plus its transpose
-    bool const sym = (precision == TCSCF_PREC_BF16X3 || precision == TCSCF_PREC_FP64) && &g1 == &g2 && f.same;
+    // exchange matrix is sum W T' plus its transpose (TF32 keeps the full form: tensorPrepare)
+    bool const sym = precision != TCSCF_PREC_TF32 && &g1 == &g2 && f.same;
     symSpin[s] = sym;
     for (int part = 0; part < (f.complex ? 2 : 1); ++part) {
       double const * X1 = part == 0 ? f.X1 : f.X1im;
@@ -1697,7 +1697,7 @@ int scfGraph(tcscf_ctx * ctx, Grid & g1, Grid & g2, int nocc, const double * S, 
   bool const tensor = precision != TCSCF_PREC_FP64;
   // one grid on both sides: psi1 = psi2 (both C on the same points), the symmetric split-BF16 or FP64
   // contraction (pairs on and above each r1 tile's diagonal; the exchange plus its transpose)
-  bool const sym = (precision == TCSCF_PREC_BF16X3 || precision == TCSCF_PREC_FP64) && &g1 == &g2;
+  bool const sym = precision != TCSCF_PREC_TF32 && &g1 == &g2;
   Contraction c;
   c.n1 = n1; c.n2 = n2; c.R = nocc; c.ncol = nb;
   c.p1 = g1.pts; c.p2 = g2.pts; c.psi1 = psi1; c.psi2 = sym ? psi1 : psi2; c.ldpsi = ldpsi;

@@ -58,6 +58,11 @@ def test_symmetric_matches_full_and_fp64_ne(ctx, nrad, order):
     G64f, _, E64f = api.fock_build(G, Gb, D, h, precision=ffi.PREC_FP64)
     assert np.abs(G64 - G64f).max() <= 1e-12 * scale, np.abs(G64 - G64f).max() / scale
     assert abs(E64 - E64f) <= 1e-10, (E64, E64f)
+    # TF32 keeps the full contraction on one grid: the same bits as on the twin grid objects
+    Gt, _, Et = api.fock_build(G, G, D, h, precision=ffi.PREC_TF32)
+    Gtf, _, Etf = api.fock_build(G, Gb, D, h, precision=ffi.PREC_TF32)
+    assert Et == Etf
+    np.testing.assert_array_equal(Gt, Gtf)
     G.close()
     Gb.close()
 
