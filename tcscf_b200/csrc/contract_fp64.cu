@@ -109,15 +109,19 @@ __global__ void __launch_bounds__(NT, RPT == 8 ? 1 : 2) kContractFp64(KArgs a)
   // the 128 x 128 tile's GEMM on the FP64 tensor cores (mma.m8n8k4): its operands come from registers,
   // so shared memory stops limiting the FP64 rate as it does the 8 x 8 register tile on the CUDA cores
   constexpr bool kDmma = BN == 128 && RPT == 8;
+  // row strides of the X and V tiles: the DMMA fragments read 4 rows (k) x 8 consecutive doubles per
+  // warp, which a stride of 8 (mod 16) doubles spreads over all 32 banks (two wavefronts, the minimum)
+  constexpr int XLD = kDmma ? BMT + 8 : BMT;
+  constexpr int VLD = kDmma ? BN + 8 : BN;
   constexpr int VPT = BMT * BK / NT;      // phase-B values per thread
   constexpr int TPR = BK / VPT;           // phase-B threads per row
   extern __shared__ __align__(16) double sm[];
   int const R = a.R;
   double * sP1 = sm;                              // [R][BMT]
   double * sC1 = sP1 + R * BMT;                   // [3][BMT]
-  double * sX = sC1 + 3 * BMT;                    // [BK][BMT]
-  double * stage0 = sX + BK * BMT;                // per stage: sV [BK][BN], sC2 [4][BK], sP2 [R][BK]
-  int const stageSize = BK * BN + 4 * BK + R * BK;
+  double * sX = sC1 + 3 * BMT;                    // [BK][XLD]
+  double * stage0 = sX + BK * XLD;                // per stage: sV [BK][VLD], sC2 [4][BK], sP2 [R][BK]
+  int const stageSize = BK * VLD + 4 * BK + R * BK;
 
   int const tid = threadIdx.x;
   int64_t const r1base = int64_t(blockIdx.x) * BMT;
@@ -132,14 +136,14 @@ __global__ void __launch_bounds__(NT, RPT == 8 ? 1 : 2) kContractFp64(KArgs a)
 
   auto issue = [&](int64_t k0, int st) {
     double * sV = stage0 + st * stageSize;
-    double * sC2 = sV + BK * BN;
+    double * sC2 = sV + BK * VLD;
     double * sP2 = sC2 + 4 * BK;
     int const kn = int(min(int64_t(BK), r2end - k0));
     for (int idx = tid; idx < BK * BN; idx += NT) {
       int const k = idx / BN, c = idx % BN;
       int const col = cg * BN + c;
       bool const ok = k < kn && col < a.ncol;
-      cpAsync8(&sV[idx], ok ? &a.V[(k0 + k) * a.ldv + col] : a.V, ok);
+      cpAsync8(&sV[k * VLD + c], ok ? &a.V[(k0 + k) * a.ldv + col] : a.V, ok);
     }
     for (int idx = tid; idx < R * BK; idx += NT) {
       int const k = idx / R, b = idx % R;
@@ -190,7 +194,7 @@ __global__ void __launch_bounds__(NT, RPT == 8 ? 1 : 2) kContractFp64(KArgs a)
     cpAsyncWait1();
     __syncthreads();
     double const * sV = stage0 + st * stageSize;
-    double const * sC2 = sV + BK * BN;
+    double const * sC2 = sV + BK * VLD;
     double const * sP2 = sC2 + 4 * BK;
     int const kn = int(min(int64_t(BK), r2end - k0));
     double rho[VPT];
@@ -212,7 +216,7 @@ __global__ void __launch_bounds__(NT, RPT == 8 ? 1 : 2) kContractFp64(KArgs a)
       double g = r12Kernel<KIND>(a, x1, y1, z1, sC2[c], sC2[BK + c], sC2[2 * BK + c]);
       g = c < kn ? g : 0.0;
       vh = fma(g, sC2[3 * BK + c], vh);
-      sX[c * BMT + rB] = (k0 + c < r2half ? 0.5 * g : g) * rho[j];
+      sX[c * XLD + rB] = (k0 + c < r2half ? 0.5 * g : g) * rho[j];
     }
     __syncthreads();
     if constexpr (kDmma) {
@@ -225,9 +229,9 @@ __global__ void __launch_bounds__(NT, RPT == 8 ? 1 : 2) kContractFp64(KArgs a)
       for (int k = 0; k < BK; k += 4) {
         double av[8], bv[4];
 #pragma unroll
-        for (int i = 0; i < 8; ++i) av[i] = sX[(k + fk) * BMT + wr + 8 * i + fr];
+        for (int i = 0; i < 8; ++i) av[i] = sX[(k + fk) * XLD + wr + 8 * i + fr];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) bv[j] = sV[(k + fk) * BN + wc + 8 * j + fr];
+        for (int j = 0; j < 4; ++j) bv[j] = sV[(k + fk) * VLD + wc + 8 * j + fr];
 #pragma unroll
         for (int i = 0; i < 8; ++i)
 #pragma unroll
@@ -243,14 +247,14 @@ __global__ void __launch_bounds__(NT, RPT == 8 ? 1 : 2) kContractFp64(KArgs a)
       double av[RPT];
 #pragma unroll
       for (int q = 0; q < RPT / 2; ++q) {
-        double2 const aa = *reinterpret_cast<double2 const *>(&sX[k * BMT + tr * RPT + 2 * q]);
+        double2 const aa = *reinterpret_cast<double2 const *>(&sX[k * XLD + tr * RPT + 2 * q]);
         av[2 * q] = aa.x;
         av[2 * q + 1] = aa.y;
       }
       double bv[CPT];
 #pragma unroll
       for (int q = 0; q < CPT / 2; ++q) {
-        double2 const bb = *reinterpret_cast<double2 const *>(&sV[k * BN + 32 * q + 2 * tc]);
+        double2 const bb = *reinterpret_cast<double2 const *>(&sV[k * VLD + 32 * q + 2 * tc]);
         bv[2 * q] = bb.x;
         bv[2 * q + 1] = bb.y;
       }
@@ -574,7 +578,8 @@ int contractFp64(tcscf_ctx * ctx, Contraction const & c)
   TCSCF_CHECK(ctx, !c.sym || (c.p1 == c.p2 && c.n1 == c.n2 && c.psi1 == c.psi2 && c.R > 0 && (c.VH != nullptr) == (c.coul != nullptr)),
               TCSCF_ERR_INVALID_ARGUMENT, "internal: a symmetric contraction needs r1 = r2 and psi1 = psi2");
   a.sym = c.sym ? 1 : 0;
-  size_t const smem = sizeof(double) * (size_t(c.R) * bm + 3 * bm + BK * bm + 2 * (size_t(BK) * bn + 4 * BK + size_t(c.R) * BK));
+  int const pad = bn == 128 && rpt == 8 ? 8 : 0;   // the DMMA tile's padded X and V row strides
+  size_t const smem = sizeof(double) * (size_t(c.R) * bm + 3 * bm + BK * (bm + pad) + 2 * (size_t(BK) * (bn + pad) + 4 * BK + size_t(c.R) * BK));
   // the contraction kernel alone is bracketed by the context's timing events (tcscf_last_timing)
   if (!ctx->capturing) cudaEventRecord(ctx->ev[2], ctx->stream);
   TCSCF_TRY(launchContract(ctx, kind, bn, rpt, a, unsigned(tiles), unsigned(nsplit), smem));
