@@ -393,15 +393,40 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         uint32_t const g = blockCount + jj;
         int const s = g % NSTAGE, b = g & 1;
         if (!(ok = waitBar(&S.full[s], (g / NSTAGE) & 1, abortFlag, P.status, 32))) break;
-        if (!(ok = waitBar(&S.sfull[b], (g >> 1) & 1, abortFlag, P.status, 33))) break;
-        fenceAfterSync();
         // this warp's Vt column scales, kept for the flush of block g after the stage is released
         for (int c = lane; c < NB / 2; c += 32) S.cinvT[cw][b][c] = S.cinv[s][half * (NB / 2) + c];
-        // X' = g * a2inv * (256 rho_hh + rho_cross) for this warp's 32 r2 points (16 pairs)
+        // g * a2inv for this warp's 32 r2 points (16 pairs) from the stage alone, while GEMM1 of the
+        // block may still run; then X' = g * a2inv * (256 rho_hh + rho_cross)
         float4 const * cc = S.coords[s] + half * 32;
         float2 const * sa = reinterpret_cast<float2 const *>(S.a2inv[s] + half * 32);
         uint64_t xv[16];
         uint64_t vsum2 = 0;
+#pragma unroll
+        for (int pr = 0; pr < 16; ++pr) {
+          float4 const qa = cc[2 * pr], qb = cc[2 * pr + 1];
+          uint64_t const dx = f2sub(p1x, f2pack(qa.x, qa.y));
+          uint64_t const dy = f2sub(p1y, f2pack(qa.z, qa.w));
+          uint64_t const dz = f2sub(p1z, f2pack(qb.x, qb.y));
+          uint64_t const r2 = f2fma(dx, dx, f2fma(dy, dy, f2mul(dz, dz)));
+          float r2a, r2b;
+          f2unpack(r2, r2a, r2b);
+          uint64_t y = f2pack(rsqrtApprox(r2a), rsqrtApprox(r2b));
+          // one Newton step on the hardware estimate: y += (-y/2) (r2 y^2 - 1)
+          uint64_t const em = f2fma(f2mul(r2, y), y, mOne);
+          y = f2fma(f2mul(y, mHalf), em, y);
+          float ya, yb;
+          f2unpack(y, ya, yb);
+          // pairs below the FP32 resolution of r1 (nearThreshold, packed as r1's w) are dropped here;
+          // the near-pair correction adds those that are not exactly coincident in FP64
+          ya = r2a >= p1.w ? ya : 0.0f;
+          yb = r2b >= p1.w ? yb : 0.0f;
+          y = f2pack(ya, yb);
+          vsum2 = f2fma(y, f2pack(qb.z, qb.w), vsum2);
+          float2 const a2 = sa[pr];
+          xv[pr] = f2mul(y, f2pack(a2.x, a2.y));
+        }
+        if (!(ok = waitBar(&S.sfull[b], (g >> 1) & 1, abortFlag, P.status, 33))) break;
+        fenceAfterSync();
         uint32_t const rhoAddr = tmem + laneBase + uint32_t(b * 2 * BK + half * 32);
 #pragma unroll
         for (int hh = 0; hh < 2; ++hh) {
@@ -417,29 +442,9 @@ __global__ void __launch_bounds__(NTHREADS, 1)
           }
 #pragma unroll
           for (int e = 0; e < 8; ++e) {
-            int const pr = hh * 8 + e;                  // pair index within the warp's 16 pairs
-            float4 const qa = cc[2 * pr], qb = cc[2 * pr + 1];
-            uint64_t const dx = f2sub(p1x, f2pack(qa.x, qa.y));
-            uint64_t const dy = f2sub(p1y, f2pack(qa.z, qa.w));
-            uint64_t const dz = f2sub(p1z, f2pack(qb.x, qb.y));
-            uint64_t const r2 = f2fma(dx, dx, f2fma(dy, dy, f2mul(dz, dz)));
-            float r2a, r2b;
-            f2unpack(r2, r2a, r2b);
-            uint64_t y = f2pack(rsqrtApprox(r2a), rsqrtApprox(r2b));
-            // one Newton step on the hardware estimate: y += (-y/2) (r2 y^2 - 1)
-            uint64_t const em = f2fma(f2mul(r2, y), y, mOne);
-            y = f2fma(f2mul(y, mHalf), em, y);
-            float ya, yb;
-            f2unpack(y, ya, yb);
-            // pairs below the FP32 resolution of r1 (nearThreshold, packed as r1's w) are dropped here;
-            // the near-pair correction adds those that are not exactly coincident in FP64
-            ya = r2a >= p1.w ? ya : 0.0f;
-            yb = r2b >= p1.w ? yb : 0.0f;
-            y = f2pack(ya, yb);
-            vsum2 = f2fma(y, f2pack(qb.z, qb.w), vsum2);
-            float2 const a2 = sa[pr];
+            int const pr = hh * 8 + e;
             uint64_t const rho = f2fma(f2pack(rh[2 * e], rh[2 * e + 1]), k256, f2pack(rx[2 * e], rx[2 * e + 1]));
-            xv[pr] = f2mul(f2mul(y, f2pack(a2.x, a2.y)), rho);
+            xv[pr] = f2mul(xv[pr], rho);
           }
         }
         // row maximum of |X'| over the block's 64 r2 points: this warp's 32 and the other half's
@@ -794,7 +799,6 @@ int launchFlash(tcscf_ctx * ctx, tc::Params const & P, int grid)
   return TCSCF_OK;
 }
 
-// tile classes: (NB, RP, XS); XS = 0 is the TF32 kernel
 // tile classes: (NB, RP, XS, TMA stages); XS = 0 is the TF32 kernel (its stage count is its own)
 constexpr int kClasses[8][4] = {{64, 32, 2, 3}, {64, 32, 3, 3}, {64, 32, 3, 2}, {64, 64, 2, 2},
                                 {128, 32, 2, 2}, {128, 32, 3, 2}, {64, 32, 0, 0}, {128, 32, 0, 0}};
