@@ -192,14 +192,12 @@ struct OchiDev {
 
 __device__ __forceinline__ double rsqrt_fp64(double x)
 {
-  // 1/sqrt(x) by two Newton-Raphson steps y <- y (3 - x y^2) / 2 from the FP32 hardware estimate
-  // (quadratic convergence: ~2^-22 -> 2^-44 -> below FP64 rounding).
+  // 1/sqrt(x) by two Newton-Raphson steps from the FP32 hardware estimate (quadratic convergence:
+  // ~2^-22 -> 2^-44 -> below FP64 rounding): y <- y (3 - x y^2) / 2, then the same step in the
+  // residual form y + y (1 - x y^2) / 2 with the residual by FMA, which rounds faithfully
   double y = double(rsqrtf(float(x)));
-  double h = x * y;
+  double const h = x * y;
   y = y * fma(-0.5 * h, y, 1.5);
-  h = x * y;
-  y = y * fma(-0.5 * h, y, 1.5);
-  // final correction step
   double const r = fma(-x * y, y, 1.0);
   return fma(0.5 * y, r, y);
 }

@@ -108,7 +108,7 @@ __global__ void __launch_bounds__(NT, RPT == 8 ? 1 : 2) kContractFp64(KArgs a)
   constexpr int BMT = 16 * RPT;           // r1 rows per block
   // the 128 x 128 tile's GEMM on the FP64 tensor cores (mma.m8n8k4): its operands come from registers,
   // so shared memory stops limiting the FP64 rate as it does the 8 x 8 register tile on the CUDA cores
-  constexpr bool kDmma = BN == 128 && RPT == 8;
+  constexpr bool kDmma = BN == 128;
   // row strides of the X and V tiles: the DMMA fragments read 4 rows (k) x 8 consecutive doubles per
   // warp, which a stride of 8 (mod 16) doubles spreads over all 32 banks (two wavefronts, the minimum)
   constexpr int XLD = kDmma ? BMT + 8 : BMT;
@@ -220,20 +220,20 @@ __global__ void __launch_bounds__(NT, RPT == 8 ? 1 : 2) kContractFp64(KArgs a)
     }
     __syncthreads();
     if constexpr (kDmma) {
-      // FP64 tensor cores: warp w owns rows 64 (w & 1) .. + 64 and columns 32 (w >> 1) .. + 32 of the
-      // block as 8 x 4 tiles of 8 x 8; mma.m8n8k4 fragments: A[r][k] at lane 4 r + k, B[k][n] at lane
-      // 4 n + k, C[r][2 q + e] at lane 4 r + q (element e)
-      int const lane = tid & 31, wr = ((tid >> 5) & 1) * 64, wc = (tid >> 6) * 32;
+      // FP64 tensor cores: warp w owns rows BMT/2 (w & 1) .. + BMT/2 and columns 32 (w >> 1) .. + 32 of
+      // the block as RPT x 4 tiles of 8 x 8; mma.m8n8k4 fragments: A[r][k] at lane 4 r + k, B[k][n] at
+      // lane 4 n + k, C[r][2 q + e] at lane 4 r + q (element e)
+      int const lane = tid & 31, wr = ((tid >> 5) & 1) * (BMT / 2), wc = (tid >> 6) * 32;
       int const fr = lane >> 2, fk = lane & 3;
 #pragma unroll 2
       for (int k = 0; k < BK; k += 4) {
-        double av[8], bv[4];
+        double av[RPT], bv[4];
 #pragma unroll
-        for (int i = 0; i < 8; ++i) av[i] = sX[(k + fk) * XLD + wr + 8 * i + fr];
+        for (int i = 0; i < RPT; ++i) av[i] = sX[(k + fk) * XLD + wr + 8 * i + fr];
 #pragma unroll
         for (int j = 0; j < 4; ++j) bv[j] = sV[(k + fk) * VLD + wc + 8 * j + fr];
 #pragma unroll
-        for (int i = 0; i < 8; ++i)
+        for (int i = 0; i < RPT; ++i)
 #pragma unroll
           for (int j = 0; j < 4; ++j)
             asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
@@ -267,9 +267,9 @@ __global__ void __launch_bounds__(NT, RPT == 8 ? 1 : 2) kContractFp64(KArgs a)
 
   double * T = a.T + blockIdx.y * a.tStrideSplit;
   if constexpr (kDmma) {
-    int const lane = tid & 31, wr = ((tid >> 5) & 1) * 64, wc = (tid >> 6) * 32;
+    int const lane = tid & 31, wr = ((tid >> 5) & 1) * (BMT / 2), wc = (tid >> 6) * 32;
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
+    for (int i = 0; i < RPT; ++i) {
       int64_t const g = r1base + wr + 8 * i + (lane >> 2);
       if (g >= a.n1) continue;
 #pragma unroll
@@ -578,7 +578,7 @@ int contractFp64(tcscf_ctx * ctx, Contraction const & c)
   TCSCF_CHECK(ctx, !c.sym || (c.p1 == c.p2 && c.n1 == c.n2 && c.psi1 == c.psi2 && c.R > 0 && (c.VH != nullptr) == (c.coul != nullptr)),
               TCSCF_ERR_INVALID_ARGUMENT, "internal: a symmetric contraction needs r1 = r2 and psi1 = psi2");
   a.sym = c.sym ? 1 : 0;
-  int const pad = bn == 128 && rpt == 8 ? 8 : 0;   // the DMMA tile's padded X and V row strides
+  int const pad = bn == 128 ? 8 : 0;   // the DMMA tiles' padded X and V row strides
   size_t const smem = sizeof(double) * (size_t(c.R) * bm + 3 * bm + BK * (bm + pad) + 2 * (size_t(BK) * (bn + pad) + 4 * BK + size_t(c.R) * BK));
   // the contraction kernel alone is bracketed by the context's timing events (tcscf_last_timing)
   if (!ctx->capturing) cudaEventRecord(ctx->ev[2], ctx->stream);
