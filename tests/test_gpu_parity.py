@@ -155,6 +155,30 @@ def test_rcs_fock_build_direct_ne_subset(ctx):
     np.testing.assert_allclose(Gg, Gr, rtol=0, atol=1e-11)
 
 
+@pytest.mark.parametrize("n1", [96, 160])
+def test_rcs_fock_build_direct_kr_basis_subset(ctx, n1):
+    # nb = 120 takes the 128-column FP64 tile (the warp-specialised FP64 tensor-core contraction for
+    # this rank): 18 occupied orbitals, one partial or two r1 tiles of sampled points against a
+    # 12 x Lebedev-77 r2 grid (24,360 points), split over r2 into blocks of a few steps
+    w = wl.kr()
+    g = grids.product_grid(12, w.order)
+    rng = np.random.default_rng(n1)
+    g1 = grids.subset(g, rng.choice(g.n, n1, replace=False))
+    G1 = api.QMCGrid(ctx, g1)
+    G1.setBasisFunctions(w.basis)
+    G2 = api.QMCGrid(ctx, g)
+    G2.setBasisFunctions(w.basis)
+    D = real_density(w.basis, 18, rng)
+    S, h = api.overlap_core(w.basis, w.Z)
+    (Gr, Fr, Er), _, _ = _oracle_fock(g1, g, w.basis, D, h)
+    Gg, Fg, Eg = api.fock_build(G1, G2, D, h, precision=ffi.PREC_FP64)
+    scale = np.abs(Gr).max()
+    assert abs(Eg - Er) < E_TOL * max(1.0, abs(Er)), (Eg, Er)
+    assert np.abs(Gg - Gr).max() <= 1e-12 * scale, np.abs(Gg - Gr).max() / scale
+    G1.close()
+    G2.close()
+
+
 def test_uos_fock_build_and_2d_r2_grid(ctx, he_setup):
     w, g, G = he_setup
     rng = np.random.default_rng(5)

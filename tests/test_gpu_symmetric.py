@@ -67,6 +67,24 @@ def test_symmetric_matches_full_and_fp64_ne(ctx, nrad, order):
     Gb.close()
 
 
+def test_symmetric_fp64_kr_basis(ctx):
+    # nb = 120, rank 18: the 128 x 128 FP64 tensor-core tile (warp-specialised), symmetric against the
+    # full contraction on a grid with a partial last tile
+    w = wl.kr()
+    g = grids.product_grid(12, 77)
+    assert g.n % 128 != 0
+    G, Gb = _twins(ctx, g, w.basis)
+    _, h = api.overlap_core(w.basis, w.Z)
+    D = _real_density(w.basis, 18, np.random.default_rng(3))
+    Gs, _, Es = api.fock_build(G, G, D, h, precision=ffi.PREC_FP64)
+    Gf, _, Ef = api.fock_build(G, Gb, D, h, precision=ffi.PREC_FP64)
+    scale = np.abs(Gf).max()
+    assert np.abs(Gs - Gf).max() <= 1e-12 * scale, np.abs(Gs - Gf).max() / scale
+    assert abs(Es - Ef) <= 1e-10 * abs(Ef), (Es, Ef)
+    G.close()
+    Gb.close()
+
+
 def test_symmetric_uos(ctx):
     w = wl.ne()
     g = grids.product_grid(30, 17)
