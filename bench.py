@@ -308,12 +308,14 @@ def symmetric_pairs(n: int, fp64: bool = False) -> int:
     return sum(128 * 64 * (blocks - 2 * p) for p in range(tiles))
 
 
-def roofline(prec: int, n: int, nb: int, nocc: int, c_ms: float, peaks: dict, peak_kind: str, traffic, sym: bool = False) -> dict:
+def roofline(prec: int, n: int, nb: int, nocc: int, c_ms: float, peaks: dict, peak_kind: str, traffic, sym: bool = False,
+             traffic_per_pair_sym=None) -> dict:
     """The line's roofline object for one Fock build of n points (r1 = r2 grid) whose contraction
     kernel took c_ms milliseconds.  peaks: the BF16 peak (bf16_tflops) and the FP64 / TF32 matmul rates
     (fp64_tflops, tf32_tflops) when measured.  sym: the split-BF16 kernel computed only the pairs on and
     above the diagonal tiles (X = g rho is symmetric when r1 = r2 and psi1 = psi2); its work counts those
-    pairs, and traffic (given for a full launch) scales with them."""
+    pairs, and traffic is traffic_per_pair_sym times them when that figure (measured on a symmetric
+    launch) is given, else the full-launch figure scaled by them."""
     from tcscf_b200 import ffi
 
     # algorithmic work per Fock build: F_alg = 2 P (nb nocc + 1), the pair-density count of the direct
@@ -333,7 +335,9 @@ def roofline(prec: int, n: int, nb: int, nocc: int, c_ms: float, peaks: dict, pe
                  "kernel_algorithm_tflops": kernel_achieved,
                  "frac_note": "frac counts F_alg, the pair-density work the factored form avoids; issued_frac (the "
                               "slice products the tensor pipe executes) and ncu's tensor-pipe activity measure the hardware"}
-    if traffic is not None and sym and prec != ffi.PREC_FP64:   # the full-launch figure, scaled by the units
+    if sym and prec != ffi.PREC_FP64 and traffic_per_pair_sym is not None:
+        traffic = traffic_per_pair_sym * pairs
+    elif traffic is not None and sym and prec != ffi.PREC_FP64:   # the full-launch figure, scaled by the units
         traffic = traffic * pairs / (float(-(-n // 128) * 128) * (-(-n // 64) * 64))
     if prec == ffi.PREC_FP64:
         # the FP64 kernel runs on the FP64 pipe: its roofline counts the flops it performs
@@ -378,6 +382,11 @@ METRIC = "Fock-build s/iter, mixed vs FP64 GPU at |dE|<=1 uEh; % of roofline"
 # once per (r1 tile, r2 block) unit where L2 misses, so the figure scales with the unit count,
 # 3172 x 6344 at 406,000 points against 2062 x 4124 (x 2.366), to 2.889e10 B
 TRAFFIC_BYTES_PER_LAUNCH = {"Kr": 2.889e10}
+# The symmetric launch (r1 = r2 grid, psi1 = psi2) of the same kernel moves more DRAM bytes per pair: its
+# r1 tiles start their r2 streams at different blocks, so they share less in L2.  One symmetric launch on
+# the 263,900-point grid read 13.57 GB and wrote 0.244 GB for its 3.4848e10 computed pairs:
+# 0.3964 B per pair (3.27e10 B for the 8.245e10 pairs at 406,000 points)
+TRAFFIC_BYTES_PER_PAIR_SYM = {"Kr": 13.814e9 / 3.4848e10}
 
 
 def run_ours(args, rank: int, world: int) -> None:
@@ -479,7 +488,7 @@ def run_ours(args, rank: int, world: int) -> None:
     # the split-BF16 and FP64 builds take the symmetric contraction
     roof = roofline(prec, n, w.nb, w.n_up, c_ms, allpeaks, peak_kind,
                     TRAFFIC_BYTES_PER_LAUNCH.get(w.name) if prec == ffi.PREC_BF16X3 and args.nrad == 0 else None,
-                    sym=True)
+                    sym=True, traffic_per_pair_sym=TRAFFIC_BYTES_PER_PAIR_SYM.get(w.name) if prec == ffi.PREC_BF16X3 else None)
     if fp64 is not None:
         fp64["roofline"] = roofline(ffi.PREC_FP64, n, w.nb, w.n_up, fp64["contraction_ms"], allpeaks, peak_kind, None, sym=True)
     cpu = None
