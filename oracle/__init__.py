@@ -278,3 +278,106 @@ def assemble_g(Qss, Qso, Qoo, D):
     lib().oracle_assemble_g(nb, _p(np.ascontiguousarray(Qss)), _p(np.ascontiguousarray(Qso)), _p(np.ascontiguousarray(Qoo)),
                             _p(np.ascontiguousarray(D, dtype=np.complex128)), _p(G3))
     return G3
+
+
+# ---- the reference's own hot-path code (oracle/_ref, built by `make -C oracle ref`) ----------------
+# oracle/ref_hot_path.cpp compiles the reference's HartreeFock.cpp / HartreeFock.hpp, integration
+# headers, SlaterTypeOrbital.hpp and jastrowFunctions.hpp where they lie, over the LvArray / RAJA /
+# Caliper / qmc stand-ins in oracle/ref_shim/.  The tests pin the restatement above to it.
+REF_LIB = HERE / "_ref" / "libtcscf_ref.so"
+_ref = None
+
+
+def build_ref() -> Path | None:
+    """Builds oracle/_ref/libtcscf_ref.so when the reference sources are present; returns its path,
+    or None when it is neither built nor buildable here."""
+    sources = [HERE / "ref_hot_path.cpp", *HERE.glob("ref_shim/**/*.hpp")]
+    stale = not REF_LIB.exists() or any(s.stat().st_mtime > REF_LIB.stat().st_mtime for s in sources)
+    if stale:
+        res = subprocess.run(["make", "-s", "-C", str(HERE), "ref"], capture_output=True, text=True)
+        if res.returncode != 0 and not REF_LIB.exists():
+            return None
+    return REF_LIB if REF_LIB.exists() else None
+
+
+def ref_lib() -> C.CDLL | None:
+    global _ref
+    if _ref is None:
+        if build_ref() is None:
+            return None
+        _ref = C.CDLL(str(REF_LIB))
+        paths = sorted(glob.glob(os.path.join(os.path.dirname(np.__file__), "..", "scipy.libs", "libscipy_openblas*.so")))
+        if not paths or _ref.tcscf_ref_set_lapack(paths[0].encode()) != 0:
+            raise RuntimeError("no LAPACK (scipy's bundled OpenBLAS) for the reference build")
+    return _ref
+
+
+def _c(a):
+    return _p(np.ascontiguousarray(a))
+
+
+def ref_compute_F(p1, w1, vals1, p2, w2, vals2, nb: int, kernel: int = 0, u: Ochi | None = None):
+    """precomputeIntegrand + computeF of the reference (HartreeFock.hpp:23-180)."""
+    N1, N2, ndim2 = p1.shape[1], p2.shape[1], p2.shape[0]
+    F = np.empty((N1, nb, nb), dtype=np.complex128 if ndim2 == 3 else np.float64)
+    st = ref_lib().tcscf_ref_compute_F(_c(p1), _c(w1), C.c_int64(N1), _c(vals1), _c(p2), _c(w2), C.c_int64(N2), ndim2, _c(vals2), nb,
+                                       kernel, C.byref(u) if u else None, _p(F))
+    assert st == 0, st
+    return F
+
+
+def ref_compute_V(p1, w1, vals1, p2, w2, vals2, nb: int, kernel: int, u: Ochi):
+    """precomputeIntegrand + computeV of the reference (HartreeFock.hpp:185-229)."""
+    N1, N2 = p1.shape[1], p2.shape[1]
+    V = np.empty((N1, nb, nb, 3), dtype=np.complex128)
+    st = ref_lib().tcscf_ref_compute_V(_c(p1), _c(w1), C.c_int64(N1), _c(vals1), _c(p2), _c(w2), C.c_int64(N2), _c(vals2), nb, kernel,
+                                       C.byref(u), _p(V))
+    assert st == 0, st
+    return V
+
+
+def ref_scf(nspin: int, n_up: int, n_down: int, F, p1, w1, vals1, S, h, respect_symmetry=True):
+    """RCSHartreeFock (nspin 1) / UOSHartreeFock (nspin 2) ::compute of the reference on a real F:
+    (convergence loops or -1, energy, density)."""
+    nb = vals1.shape[1]
+    e = C.c_double()
+    D = np.empty((nspin, nb, nb), dtype=np.complex128)
+    loops = ref_lib().tcscf_ref_scf(nspin, n_up, n_down, _c(F), _c(p1), _c(w1), C.c_int64(vals1.shape[0]), nb, _c(vals1), _c(S), _c(h),
+                                    int(respect_symmetry), C.byref(e), _p(D))
+    return loops, e.value, D
+
+
+def ref_tc_scf(Fs, Fo, Vs, Vo, p1, w1, vals1, grads1, S, h, n_up, n_down, respect_symmetry=True):
+    """TCHartreeFock::compute of the reference: (convergence loops or -1, energy, density)."""
+    nb = vals1.shape[1]
+    e = C.c_double()
+    D = np.empty((2, nb, nb), dtype=np.complex128)
+    loops = ref_lib().tcscf_ref_tc_scf(_c(Fs), _c(Fo), _c(Vs), _c(Vo), _c(p1), _c(w1), C.c_int64(vals1.shape[0]), nb, _c(vals1), _c(grads1),
+                                       _c(S), _c(h), n_up, n_down, int(respect_symmetry), C.byref(e), _p(D))
+    return loops, e.value, D
+
+
+def ref_qmc_grid(u: np.ndarray):
+    """Points and weights of the reference's QMCGrid built on the unit-cube points u [ndim][N]."""
+    ndim, N = u.shape
+    pts, w = np.empty((ndim, N)), np.empty(N)
+    assert ref_lib().tcscf_ref_qmc_grid(ndim, C.c_int64(N), _c(u), _p(pts), _p(w)) == 0
+    return pts, w
+
+
+def ref_sto_values(points: np.ndarray, basis, gradients: bool = False):
+    """QMCGrid::setBasisFunctions of the reference with SlaterTypeOrbital functions."""
+    ndim, N = points.shape
+    nb = len(basis)
+    vals = np.empty((N, nb), dtype=np.complex128 if ndim == 3 else np.float64)
+    grads = np.empty((N, nb, 3), dtype=np.complex128) if gradients else None
+    assert ref_lib().tcscf_ref_sto_values(ndim, C.c_int64(N), _c(points), _sto(basis), nb, _p(vals), _p(grads)) == 0
+    return (vals, grads) if gradients else vals
+
+
+def ref_overlap_core(basis, Z: int):
+    """The reference's analytic STO overlap and core-Hamiltonian matrices."""
+    nb = len(basis)
+    S, H = np.empty((nb, nb)), np.empty((nb, nb))
+    assert ref_lib().tcscf_ref_overlap_core(_sto(basis), nb, Z, _p(S), _p(H)) == 0
+    return S, H

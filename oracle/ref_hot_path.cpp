@@ -1,0 +1,364 @@
+// The reference's own hot-path code, compiled from its sources where they lie (src/HartreeFock.cpp,
+// which includes src/HartreeFock.hpp and the src/integration headers) over the LvArray / RAJA /
+// Caliper / qmc stand-ins in oracle/ref_shim/, with C entry points that take the oracle's array
+// layouts.  Test infrastructure only: the tests pin the oracle's restatement (tcscf_oracle.cpp) to
+// these functions.  Built by `make ref` into oracle/_ref/ where the reference sources are present.
+//
+// Each entry point builds the reference's QMCGrid objects and then replaces their points, weights,
+// basis values and gradients with the caller's, so the reference's templates run on exactly the
+// oracle's inputs:
+//   tcscf_ref_compute_F  precomputeIntegrand + computeF (HartreeFock.hpp:23-180) with the kernels of
+//                        the reference's tests (1/r12: HartreeFockTest.cpp:248-253; the TC scalar
+//                        kernels: :274-295), 2-D real or 3-D complex r2 grids
+//   tcscf_ref_compute_V  precomputeIntegrand + computeV (HartreeFock.hpp:185-229) with grad u
+//                        (HartreeFockTest.cpp:299-317)
+//   tcscf_ref_scf        RCSHartreeFock / UOSHartreeFock::compute (HartreeFock.cpp:785-1003): the SCF
+//                        loop with calculateIaa / calculateFai, the Fock assembly, constructSCFOperator
+//                        and zhegvd
+//   tcscf_ref_tc_scf     TCHartreeFock::compute (HartreeFock.cpp:1007-1362) with zggev
+//   tcscf_ref_qmc_grid   the QMCGrid constructor (integrateAll.hpp:21-63: createGrid with the
+//                        TreutlerAhlrichsM4 / azimuthal / linear maps, then the r^2 sin(theta) jacobian)
+//                        on the caller's unit-cube points
+//   tcscf_ref_sto_values QMCGrid::setBasisFunctions (integrateAll.hpp:88-137) with SlaterTypeOrbital
+//                        values and gradients (SlaterTypeOrbital.hpp:16-112) on the caller's points
+//   tcscf_ref_overlap_core  the analytic STO overlap and core-Hamiltonian elements
+//                        (SlaterTypeOrbital.hpp:118-176)
+// Array layouts (row-major, complex as interleaved doubles): points [ndim][N]; weights [N]; basis
+// values [N][nb] (complex for 3-D grids, real for 2-D); gradients [N][nb][3] complex; F [N1][nb][nb]
+// (real for 2-D r2, complex for 3-D); V [N1][nb][nb][3] complex; S, h [nb][nb] real; density
+// [nspin][nb][nb] complex.
+#include <dlfcn.h>
+
+#include "HartreeFock.cpp"
+#include "SlaterTypeOrbital.hpp"
+#include "jastrowFunctions.hpp"
+
+namespace {
+
+using namespace tcscf;
+using cplx = std::complex<double>;
+
+// the oracle's basis-function record (tcscf_oracle.cpp; family 0 = STO)
+struct StoParams {
+  double alpha;
+  int32_t n, l, m, family;
+};
+
+std::vector<SlaterTypeOrbital<double>> makeStos(StoParams const * b, int nb)
+{
+  std::vector<SlaterTypeOrbital<double>> out;
+  for (int i = 0; i < nb; ++i) out.emplace_back(b[i].alpha, b[i].n, b[i].l, b[i].m);
+  return out;
+}
+
+// the oracle's Ochi parameter block (tcscf_oracle.cpp)
+struct OchiParams {
+  double a, a12;
+  int32_t nterms, pad;
+  int32_t S[8][3];
+  double c[8][2];   // [term][0 = opposite spin, 1 = same spin]
+};
+
+jastrowFunctions::Ochi<double> makeOchi(OchiParams const & p)
+{
+  Array2d<double> c(p.nterms, 2);
+  Array2d<int> S(p.nterms, 3);
+  for (int t = 0; t < p.nterms; ++t) {
+    c(t, 0) = p.c[t][0];
+    c(t, 1) = p.c[t][1];
+    for (int d = 0; d < 3; ++d) S(t, d) = p.S[t][d];
+  }
+  return jastrowFunctions::Ochi<double> {p.a, p.a12, c, S};
+}
+
+template <int NDIM>
+integration::QMCGrid<double, NDIM> makeGrid(double const * pts, double const * w, int64_t n, double const * vals, double const * grads, int nb)
+{
+  integration::QMCGrid<double, NDIM> g(1);
+  g.quadratureGrid = integration::QuadratureGrid<double>(NDIM, int(n));
+  for (int d = 0; d < NDIM; ++d)
+    for (int64_t i = 0; i < n; ++i) g.quadratureGrid.points(d, i) = pts[d * n + i];
+  for (int64_t i = 0; i < n; ++i) g.quadratureGrid.weights(i) = w[i];
+  g.basisValues.resize(n, nb);
+  for (int64_t i = 0; i < n; ++i)
+    for (int b = 0; b < nb; ++b) {
+      if constexpr (NDIM == 3)
+        g.basisValues(i, b) = cplx(vals[2 * (i * nb + b)], vals[2 * (i * nb + b) + 1]);
+      else
+        g.basisValues(i, b) = vals[i * nb + b];
+    }
+  if (grads) {
+    g.basisGradients.resize(n, nb);
+    for (int64_t i = 0; i < n; ++i)
+      for (int b = 0; b < nb; ++b) {
+        double const * q = grads + 6 * (i * nb + b);
+        g.basisGradients(i, b) = Cartesian<cplx> {cplx(q[0], q[1]), cplx(q[2], q[3]), cplx(q[4], q[5])};
+      }
+  }
+  return g;
+}
+
+// The kernels of the reference's tests: 1/r12 (kernel 0) and the TC scalar kernels 2/r12 - |grad_12 u|^2
+// - |grad_21 u|^2 for same (1) and opposite (2) spins.
+template <typename GRID2>
+Array2d<double> scalarIntegrand(integration::QMCGrid<double, 3> const & g1, GRID2 const & g2, int kernel, OchiParams const * up)
+{
+  Array2d<double> values(g1.nGrid(), g2.nGrid());
+  if (kernel == 0) {
+    precomputeIntegrand(values.toView(), g1, g2, [](Cartesian<double> const & r1, Cartesian<double> const & r2) { return 1 / (r1 - r2).r(); });
+  } else {
+    jastrowFunctions::Ochi<double> const u = makeOchi(*up);
+    bool const same = kernel == 1;
+    precomputeIntegrand(values.toView(), g1, g2, [&u, same](Cartesian<double> const & r1, Cartesian<double> const & r2) {
+      Cartesian<double> const grad12 = u.gradient(r1, r2, same);
+      Cartesian<double> const grad21 = u.gradient(r2, r1, same);
+      return 2 / (r1 - r2).r() - dot(grad12, grad12) - dot(grad21, grad21);
+    });
+  }
+  return values;
+}
+
+template <typename F>
+int guarded(F && f)
+{
+  try {
+    return f();
+  } catch (std::exception const & e) {
+    std::fprintf(stderr, "tcscf_ref: %s\n", e.what());
+    return -1;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+// LAPACK (zhegvd, zggev) from a shared library, e.g. scipy's bundled OpenBLAS; 0 on success
+int tcscf_ref_set_lapack(char const * path)
+{
+  void * h = dlopen(path, RTLD_NOW | RTLD_LOCAL);
+  if (!h) return -1;
+  using namespace LvArray::dense::lapack;
+  zhegvd() = reinterpret_cast<zhegvd_t>(dlsym(h, "scipy_zhegvd_"));
+  if (!zhegvd()) zhegvd() = reinterpret_cast<zhegvd_t>(dlsym(h, "zhegvd_"));
+  zggev() = reinterpret_cast<zggev_t>(dlsym(h, "scipy_zggev_"));
+  if (!zggev()) zggev() = reinterpret_cast<zggev_t>(dlsym(h, "zggev_"));
+  return (zhegvd() && zggev()) ? 0 : -2;
+}
+
+int tcscf_ref_compute_F(double const * p1, double const * w1, int64_t N1, double const * vals1, double const * p2, double const * w2,
+                        int64_t N2, int ndim2, double const * vals2, int nb, int kernel, OchiParams const * u, double * F)
+{
+  return guarded([&] {
+    auto const g1 = makeGrid<3>(p1, w1, N1, vals1, nullptr, nb);
+    if (ndim2 == 2) {
+      auto const g2 = makeGrid<2>(p2, w2, N2, vals2, nullptr, nb);
+      Array2d<double> const values = scalarIntegrand(g1, g2, kernel, u);
+      Array3d<double> const out = computeF(g1, g2, values.toViewConst());
+      for (int64_t a = 0; a < N1; ++a)
+        for (int j = 0; j < nb; ++j)
+          for (int i = 0; i < nb; ++i) F[(a * nb + j) * nb + i] = out(a, j, i);
+    } else {
+      auto const g2 = makeGrid<3>(p2, w2, N2, vals2, nullptr, nb);
+      Array2d<double> const values = scalarIntegrand(g1, g2, kernel, u);
+      Array3d<cplx> const out = computeF(g1, g2, values.toViewConst());
+      for (int64_t a = 0; a < N1; ++a)
+        for (int j = 0; j < nb; ++j)
+          for (int i = 0; i < nb; ++i) {
+            cplx const v = out(a, j, i);
+            F[2 * ((a * nb + j) * nb + i)] = v.real();
+            F[2 * ((a * nb + j) * nb + i) + 1] = v.imag();
+          }
+    }
+    return 0;
+  });
+}
+
+// kernel 3: grad u same spin, 4: opposite spin
+int tcscf_ref_compute_V(double const * p1, double const * w1, int64_t N1, double const * vals1, double const * p2, double const * w2,
+                        int64_t N2, double const * vals2, int nb, int kernel, OchiParams const * up, double * V)
+{
+  return guarded([&] {
+    auto const g1 = makeGrid<3>(p1, w1, N1, vals1, nullptr, nb);
+    auto const g2 = makeGrid<3>(p2, w2, N2, vals2, nullptr, nb);
+    jastrowFunctions::Ochi<double> const u = makeOchi(*up);
+    bool const same = kernel == 3;
+    Array2d<Cartesian<double>> values(N1, N2);
+    precomputeIntegrand(values.toView(), g1, g2,
+                        [&u, same](Cartesian<double> const & r1, Cartesian<double> const & r2) { return u.gradient(r1, r2, same); });
+    Array3d<Cartesian<cplx>> const out = computeV(g1, g2, values.toViewConst());
+    for (int64_t a = 0; a < N1; ++a)
+      for (int j = 0; j < nb; ++j)
+        for (int i = 0; i < nb; ++i) {
+          Cartesian<cplx> const v = out(a, j, i);
+          double * o = V + 6 * ((a * nb + j) * nb + i);
+          cplx const c[3] = {v.x(), v.y(), v.z()};
+          for (int d = 0; d < 3; ++d) {
+            o[2 * d] = c[d].real();
+            o[2 * d + 1] = c[d].imag();
+          }
+        }
+    return 0;
+  });
+}
+
+// RCS (nspin 1) or UOS (nspin 2) SCF on a real F [N1][nb][nb]; returns the driver's convergence-loop
+// count, or -1 when it threw (non-convergence included)
+int tcscf_ref_scf(int nspin, int nup, int ndown, double const * F, double const * p1, double const * w1, int64_t N1, int nb,
+                  double const * vals1, double const * S, double const * h, int respectSym, double * energy, double * density)
+{
+  return guarded([&] {
+    auto const g1 = makeGrid<3>(p1, w1, N1, vals1, nullptr, nb);
+    Array3d<double> Fji(N1, nb, nb);
+    for (int64_t a = 0; a < N1; ++a)
+      for (int j = 0; j < nb; ++j)
+        for (int i = 0; i < nb; ++i) Fji(a, j, i) = F[(a * nb + j) * nb + i];
+    Array2d<cplx, RAJA::PERM_JI> overlap(nb, nb);
+    Array2d<double> H(nb, nb);
+    for (int j = 0; j < nb; ++j)
+      for (int i = 0; i < nb; ++i) {
+        overlap(j, i) = S[j * nb + i];
+        H(j, i) = h[j * nb + i];
+      }
+    auto copyDensity = [&](auto const & D) {
+      for (int s = 0; s < nspin; ++s)
+        for (int j = 0; j < nb; ++j)
+          for (int i = 0; i < nb; ++i) {
+            cplx const v = D(s, j, i);
+            density[2 * ((s * nb + j) * nb + i)] = v.real();
+            density[2 * ((s * nb + j) * nb + i) + 1] = v.imag();
+          }
+    };
+    if (nspin == 1) {
+      RCSHartreeFock<cplx> hf(nup + ndown, nb);
+      *energy = hf.compute(overlap.toViewConst(), H.toViewConst(), g1, Fji.toViewConst(), respectSym != 0);
+      copyDensity(hf.density);
+      return hf.numberOfConvergenceLoops();
+    }
+    UOSHartreeFock<cplx> hf(nup, ndown, nb);
+    *energy = hf.compute(overlap.toViewConst(), H.toViewConst(), g1, Fji.toViewConst(), respectSym != 0);
+    copyDensity(hf.density);
+    return hf.numberOfConvergenceLoops();
+  });
+}
+
+// TC SCF on real FjiSame / FjiOppo [N1][nb][nb] and complex VjiSame / VjiOppo [N1][nb][nb][3]
+int tcscf_ref_tc_scf(double const * FjiSame, double const * FjiOppo, double const * VjiSame, double const * VjiOppo, double const * p1,
+                     double const * w1, int64_t N1, int nb, double const * vals1, double const * grads1, double const * S,
+                     double const * h, int nup, int ndown, int respectSym, double * energy, double * density)
+{
+  return guarded([&] {
+    auto const g1 = makeGrid<3>(p1, w1, N1, vals1, grads1, nb);
+    Array3d<double> Fs(N1, nb, nb), Fo(N1, nb, nb);
+    Array3d<Cartesian<cplx>> Vs(N1, nb, nb), Vo(N1, nb, nb);
+    for (int64_t a = 0; a < N1; ++a)
+      for (int j = 0; j < nb; ++j)
+        for (int i = 0; i < nb; ++i) {
+          int64_t const k = (a * nb + j) * nb + i;
+          Fs(a, j, i) = FjiSame[k];
+          Fo(a, j, i) = FjiOppo[k];
+          double const * s = VjiSame + 6 * k;
+          double const * o = VjiOppo + 6 * k;
+          Vs(a, j, i) = Cartesian<cplx> {cplx(s[0], s[1]), cplx(s[2], s[3]), cplx(s[4], s[5])};
+          Vo(a, j, i) = Cartesian<cplx> {cplx(o[0], o[1]), cplx(o[2], o[3]), cplx(o[4], o[5])};
+        }
+    Array2d<cplx, RAJA::PERM_JI> overlap(nb, nb);
+    Array2d<double> H(nb, nb);
+    for (int j = 0; j < nb; ++j)
+      for (int i = 0; i < nb; ++i) {
+        overlap(j, i) = S[j * nb + i];
+        H(j, i) = h[j * nb + i];
+      }
+    TCHartreeFock<cplx> hf(nup, ndown, nb);
+    *energy = hf.compute(overlap.toViewConst(), H.toViewConst(), g1, Fs.toViewConst(), Fo.toViewConst(), Vs.toViewConst(), Vo.toViewConst(),
+                         respectSym != 0);
+    for (int s = 0; s < 2; ++s)
+      for (int j = 0; j < nb; ++j)
+        for (int i = 0; i < nb; ++i) {
+          cplx const v = hf.density(s, j, i);
+          density[2 * ((s * nb + j) * nb + i)] = v.real();
+          density[2 * ((s * nb + j) * nb + i) + 1] = v.imag();
+        }
+    return hf.numberOfConvergenceLoops();
+  });
+}
+
+// points [ndim][N] and weights [N] of the reference's QMC grid built from the unit-cube points u [ndim][N]
+int tcscf_ref_qmc_grid(int ndim, int64_t N, double const * u, double * pts, double * w)
+{
+  return guarded([&] {
+    auto & given = integrators::providedPoints();
+    given.assign(size_t(N), std::vector<double>(size_t(ndim)));
+    for (int64_t i = 0; i < N; ++i)
+      for (int d = 0; d < ndim; ++d) given[size_t(i)][size_t(d)] = u[d * N + i];
+    auto readBack = [&](auto const & g) {
+      LVARRAY_ERROR_IF_NE(g.quadratureGrid.weights.size(), N);
+      for (int d = 0; d < ndim; ++d)
+        for (int64_t i = 0; i < N; ++i) pts[d * N + i] = g.quadratureGrid.points(d, i);
+      for (int64_t i = 0; i < N; ++i) w[i] = g.quadratureGrid.weights(i);
+    };
+    if (ndim == 2)
+      readBack(integration::QMCGrid<double, 2>(N));
+    else
+      readBack(integration::QMCGrid<double, 3>(N));
+    given.clear();
+    return 0;
+  });
+}
+
+// STO values [N][nb] (complex for ndim 3, real for ndim 2) and, when grads is not null, gradients
+// [N][nb][3] complex on the points [ndim][N]
+int tcscf_ref_sto_values(int ndim, int64_t N, double const * pts, StoParams const * basis, int nb, double * vals, double * grads)
+{
+  return guarded([&] {
+    std::vector<SlaterTypeOrbital<double>> const stos = makeStos(basis, nb);
+    std::vector<double> const zeros(size_t(N), 0.0);
+    auto run = [&](auto & g) {
+      for (int d = 0; d < ndim; ++d)
+        for (int64_t i = 0; i < N; ++i) g.quadratureGrid.points(d, i) = pts[d * N + i];
+      g.setBasisFunctions(stos, grads != nullptr);
+      for (int64_t i = 0; i < N; ++i)
+        for (int b = 0; b < nb; ++b) {
+          auto const v = g.basisValues(i, b);
+          if constexpr (std::is_same_v<std::decay_t<decltype(v)>, cplx>) {
+            vals[2 * (i * nb + b)] = v.real();
+            vals[2 * (i * nb + b) + 1] = v.imag();
+          } else {
+            vals[i * nb + b] = v;
+          }
+          if (grads) {
+            Cartesian<cplx> const q = g.basisGradients(i, b);
+            cplx const c[3] = {q.x(), q.y(), q.z()};
+            for (int d = 0; d < 3; ++d) {
+              grads[6 * (i * nb + b) + 2 * d] = c[d].real();
+              grads[6 * (i * nb + b) + 2 * d + 1] = c[d].imag();
+            }
+          }
+        }
+    };
+    if (ndim == 2) {
+      auto g = makeGrid<2>(pts, zeros.data(), N, nullptr, nullptr, 0);
+      run(g);
+    } else {
+      auto g = makeGrid<3>(pts, zeros.data(), N, nullptr, nullptr, 0);
+      run(g);
+    }
+    return 0;
+  });
+}
+
+// analytic S and core H [nb][nb] (row j, column i) for nuclear charge Z
+int tcscf_ref_overlap_core(StoParams const * basis, int nb, int Z, double * S, double * H)
+{
+  return guarded([&] {
+    std::vector<SlaterTypeOrbital<double>> const stos = makeStos(basis, nb);
+    for (int j = 0; j < nb; ++j)
+      for (int i = 0; i < nb; ++i) {
+        S[j * nb + i] = overlap(stos[size_t(j)], stos[size_t(i)]);
+        H[j * nb + i] = coreMatrixElement(Z, stos[size_t(j)], stos[size_t(i)]);
+      }
+    return 0;
+  });
+}
+
+}  // extern "C"
