@@ -381,3 +381,78 @@ def ref_overlap_core(basis, Z: int):
     S, H = np.empty((nb, nb)), np.empty((nb, nb))
     assert ref_lib().tcscf_ref_overlap_core(_sto(basis), nb, Z, _p(S), _p(H)) == 0
     return S, H
+
+
+def ref_family_values(points: np.ndarray, basis, gradients: bool = False):
+    """QMCGrid::setBasisFunctions of the reference with Ochi (family 1) or hydrogen-like (family 2) functions."""
+    ndim, N = points.shape
+    nb = len(basis)
+    vals = np.empty((N, nb), dtype=np.complex128 if ndim == 3 else np.float64)
+    grads = np.empty((N, nb, 3), dtype=np.complex128) if gradients else None
+    assert ref_lib().tcscf_ref_family_values(ndim, C.c_int64(N), _c(points), _sto(basis), nb, _p(vals), _p(grads)) == 0
+    return (vals, grads) if gradients else vals
+
+
+def ref_family_overlap_core(basis, Z: int):
+    """S and core H of an Ochi / hydrogen-like basis as the reference's driver fills them (S NaN for
+    the hydrogen-like family, whose overlap the reference integrates numerically)."""
+    nb = len(basis)
+    S, H = np.empty((nb, nb)), np.empty((nb, nb))
+    assert ref_lib().tcscf_ref_family_overlap_core(_sto(basis), nb, Z, _p(S), _p(H)) == 0
+    return S, H
+
+
+def ref_integrate_all_r1r2(use_gradient: bool, p1, w1, vals1, p2, w2, vals2, grads2, nb: int, kernel: int, u: Ochi | None):
+    """integrateAllR1R2 of the reference: [nb]^4 complex."""
+    out = np.empty((nb,) * 4, dtype=np.complex128)
+    st = ref_lib().tcscf_ref_integrate_all_r1r2(int(use_gradient), _c(p1), _c(w1), C.c_int64(p1.shape[1]), _c(vals1), _c(p2), _c(w2),
+                                                C.c_int64(p2.shape[1]), _c(vals2), _p(None if grads2 is None else np.ascontiguousarray(grads2)),
+                                                nb, kernel, C.byref(u) if u else None, _p(out))
+    assert st == 0, st
+    return out
+
+
+def ref_three_electron_integrals(p1, w1, vals1, p2, w2, vals2, nb: int, u: Ochi):
+    """threeElectronIntegrals of the reference: [nb]^6 complex."""
+    out = np.empty((nb,) * 6, dtype=np.complex128)
+    st = ref_lib().tcscf_ref_three_electron_integrals(_c(p1), _c(w1), C.c_int64(p1.shape[1]), _c(vals1), _c(p2), _c(w2), C.c_int64(p2.shape[1]),
+                                                      _c(vals2), nb, C.byref(u), _p(out))
+    assert st == 0, st
+    return out
+
+
+def ref_compute_q(w1, vals1, Vs, Vo):
+    """internal::computeQ of the reference: (Qss, Qso, Qoo), each complex [nb]^6."""
+    N1, nb = vals1.shape
+    out = [np.empty((nb,) * 6, dtype=np.complex128) for _ in range(3)]
+    st = ref_lib().tcscf_ref_compute_q(C.c_int64(N1), nb, _c(w1), _c(np.asarray(vals1, dtype=np.complex128)), _c(Vs), _c(Vo), _p(out[0]),
+                                       _p(out[1]), _p(out[2]))
+    assert st == 0, st
+    return tuple(out)
+
+
+def ref_assemble_g(Qss, Qso, Qoo, D):
+    """internal::assembleG of the reference: G3 [2][nb][nb]."""
+    nb = Qss.shape[0]
+    G3 = np.empty((2, nb, nb), dtype=np.complex128)
+    st = ref_lib().tcscf_ref_assemble_g(nb, _c(Qss), _c(Qso), _c(Qoo), _c(np.asarray(D, dtype=np.complex128)), _p(G3))
+    assert st == 0, st
+    return G3
+
+
+def ref_load_sto(directory, basis_set: str, element: str, max_l: int):
+    """loadSTO of the reference: [(alpha, n, l, m)], or None when the reference's loader rejects the arguments."""
+    out = (Sto * 4096)()
+    n = ref_lib().tcscf_ref_load_sto(str(directory).encode(), basis_set.encode(), element.encode(), max_l, out, 4096)
+    if n < 0:
+        return None
+    assert n <= 4096
+    return [(out[i].alpha, out[i].n, out[i].l, out[i].m) for i in range(n)]
+
+
+def ref_basis_library() -> Path | None:
+    """The reference's basis-set library directory the reference build was given (None if absent)."""
+    f = ref_lib().tcscf_ref_basis_library
+    f.restype = C.c_char_p
+    p = Path(f().decode())
+    return p if str(p) and p.is_dir() else None

@@ -23,6 +23,15 @@
 //                        values and gradients (SlaterTypeOrbital.hpp:16-112) on the caller's points
 //   tcscf_ref_overlap_core  the analytic STO overlap and core-Hamiltonian elements
 //                        (SlaterTypeOrbital.hpp:118-176)
+//   tcscf_ref_family_values / tcscf_ref_family_overlap_core  the same for the Ochi and hydrogen-like
+//                        families (OchiBasis.hpp, HydrogenLikeBasis.hpp), the core elements on the
+//                        grid of the reference's driver (ChebyshevGauss(1000) with TreutlerAhlrichsM4(1,
+//                        0.9), HartreeFockTest.cpp:363-365)
+//   tcscf_ref_integrate_all_r1r2, tcscf_ref_three_electron_integrals  the 4- and 6-index tensors
+//                        (integrateAll.hpp:152-442)
+//   tcscf_ref_compute_q, tcscf_ref_assemble_g  the 3-body verification route (HartreeFock.cpp:613-752)
+//   tcscf_ref_load_sto   loadSTO (SlaterTypeOrbital.cpp:24-75), and tcscf_ref_basis_library the
+//                        reference's basis-set library directory the build was given
 // Array layouts (row-major, complex as interleaved doubles): points [ndim][N]; weights [N]; basis
 // values [N][nb] (complex for 3-D grids, real for 2-D); gradients [N][nb][3] complex; F [N1][nb][nb]
 // (real for 2-D r2, complex for 3-D); V [N1][nb][nb][3] complex; S, h [nb][nb] real; density
@@ -30,7 +39,11 @@
 #include <dlfcn.h>
 
 #include "HartreeFock.cpp"
+#include "SlaterTypeOrbital.cpp"
 #include "SlaterTypeOrbital.hpp"
+#include "OchiBasis.hpp"
+#include "HydrogenLikeBasis.hpp"
+#include "integration/ChebyshevGauss.hpp"
 #include "jastrowFunctions.hpp"
 
 namespace {
@@ -116,6 +129,39 @@ Array2d<double> scalarIntegrand(integration::QMCGrid<double, 3> const & g1, GRID
     });
   }
   return values;
+}
+
+// Calls body with the reference test's kernel as a lambda of (r1, r2): 1/r12 (0), the TC scalar kernels
+// (1 same spin, 2 opposite) or grad u (3 same, 4 opposite)
+template <typename BODY>
+void withKernel(int kernel, OchiParams const * up, BODY && body)
+{
+  if (kernel == 0) {
+    body([](Cartesian<double> const & r1, Cartesian<double> const & r2) { return 1 / (r1 - r2).r(); });
+    return;
+  }
+  jastrowFunctions::Ochi<double> const u = makeOchi(*up);
+  if (kernel <= 2) {
+    bool const same = kernel == 1;
+    body([&u, same](Cartesian<double> const & r1, Cartesian<double> const & r2) {
+      Cartesian<double> const grad12 = u.gradient(r1, r2, same);
+      Cartesian<double> const grad21 = u.gradient(r2, r1, same);
+      return 2 / (r1 - r2).r() - dot(grad12, grad12) - dot(grad21, grad21);
+    });
+  } else {
+    bool const same = kernel == 3;
+    body([&u, same](Cartesian<double> const & r1, Cartesian<double> const & r2) { return u.gradient(r1, r2, same); });
+  }
+}
+
+template <typename T, int N, typename A>
+void copyOut(A const & a, int64_t count, double * out)
+{
+  T const * d = a.data();
+  for (int64_t k = 0; k < count; ++k) {
+    out[2 * k] = d[k].real();
+    out[2 * k + 1] = d[k].imag();
+  }
 }
 
 template <typename F>
@@ -359,6 +405,202 @@ int tcscf_ref_overlap_core(StoParams const * basis, int nb, int Z, double * S, d
       }
     return 0;
   });
+}
+
+// values [N][nb] (complex for ndim 3, real for ndim 2) and, for the Ochi family when grads is not null,
+// gradients [N][nb][3] of Ochi (family 1, alpha the exponent) or hydrogen-like (family 2, alpha the
+// nuclear charge) functions
+int tcscf_ref_family_values(int ndim, int64_t N, double const * pts, StoParams const * basis, int nb, double * vals, double * grads)
+{
+  return guarded([&] {
+    std::vector<double> const zeros(size_t(N), 0.0);
+    auto run = [&](auto & g, auto const & fns) {
+      for (int d = 0; d < ndim; ++d)
+        for (int64_t i = 0; i < N; ++i) g.quadratureGrid.points(d, i) = pts[d * N + i];
+      g.setBasisFunctions(fns, grads != nullptr);
+      for (int64_t i = 0; i < N; ++i)
+        for (int b = 0; b < nb; ++b) {
+          auto const v = g.basisValues(i, b);
+          if constexpr (std::is_same_v<std::decay_t<decltype(v)>, cplx>) {
+            vals[2 * (i * nb + b)] = v.real();
+            vals[2 * (i * nb + b) + 1] = v.imag();
+          } else {
+            vals[i * nb + b] = v;
+          }
+          if (grads) {
+            Cartesian<cplx> const q = g.basisGradients(i, b);
+            cplx const c[3] = {q.x(), q.y(), q.z()};
+            for (int d = 0; d < 3; ++d) {
+              grads[6 * (i * nb + b) + 2 * d] = c[d].real();
+              grads[6 * (i * nb + b) + 2 * d + 1] = c[d].imag();
+            }
+          }
+        }
+    };
+    auto byFamily = [&](auto & g) {
+      if (basis[0].family == 1) {
+        std::vector<OchiBasisFunction<double>> fns;
+        for (int i = 0; i < nb; ++i) fns.emplace_back(basis[i].alpha, basis[i].n, basis[i].l, basis[i].m);
+        run(g, fns);
+      } else {
+        std::vector<HydrogenLikeBasisFunction<double>> fns;
+        for (int i = 0; i < nb; ++i) fns.emplace_back(int(basis[i].alpha), basis[i].n, basis[i].l, basis[i].m);
+        run(g, fns);
+      }
+    };
+    if (ndim == 2) {
+      auto g = makeGrid<2>(pts, zeros.data(), N, nullptr, nullptr, 0);
+      byFamily(g);
+    } else {
+      auto g = makeGrid<3>(pts, zeros.data(), N, nullptr, nullptr, 0);
+      byFamily(g);
+    }
+    return 0;
+  });
+}
+
+// S and core H [nb][nb] of an Ochi (family 1) or hydrogen-like (family 2) basis as the reference's driver
+// fills them; S of the hydrogen-like family is the generic numerical overlap and is not computed (NaN)
+int tcscf_ref_family_overlap_core(StoParams const * basis, int nb, int Z, double * S, double * H)
+{
+  return guarded([&] {
+    integration::QuadratureGrid<double> const coreGrid =
+        integration::createGrid(integration::ChebyshevGauss<double>(1000), integration::changeOfVariables::TreutlerAhlrichsM4<double>(1, 0.9));
+    if (basis[0].family == 1) {
+      std::vector<OchiBasisFunction<double>> fns;
+      for (int i = 0; i < nb; ++i) fns.emplace_back(basis[i].alpha, basis[i].n, basis[i].l, basis[i].m);
+      for (int i = 0; i < nb; ++i)
+        for (int j = 0; j < nb; ++j) {
+          S[i * nb + j] = overlap(fns[size_t(i)], fns[size_t(j)]);
+          H[i * nb + j] = coreMatrixElement(coreGrid, Z, fns[size_t(i)], fns[size_t(j)]);
+        }
+    } else {
+      std::vector<HydrogenLikeBasisFunction<double>> fns;
+      for (int i = 0; i < nb; ++i) fns.emplace_back(int(basis[i].alpha), basis[i].n, basis[i].l, basis[i].m);
+      for (int i = 0; i < nb; ++i)
+        for (int j = 0; j < nb; ++j) {
+          S[i * nb + j] = std::numeric_limits<double>::quiet_NaN();
+          H[i * nb + j] = coreMatrixElement(coreGrid, Z, fns[size_t(i)], fns[size_t(j)]);
+        }
+    }
+    return 0;
+  });
+}
+
+// integrateAllR1R2<use_gradient>: r1 3-D (complex values), r2 2-D (real values; complex gradients
+// [N2][nb][3] for use_gradient), the kernel of withKernel (scalar kernels 0-2 without, grad u 3-4 with
+// gradients); answer [nb]^4 complex
+int tcscf_ref_integrate_all_r1r2(int useGradient, double const * p1, double const * w1, int64_t N1, double const * vals1, double const * p2,
+                                 double const * w2, int64_t N2, double const * vals2, double const * grads2, int nb, int kernel,
+                                 OchiParams const * u, double * out)
+{
+  return guarded([&] {
+    auto const g1 = makeGrid<3>(p1, w1, N1, vals1, nullptr, nb);
+    auto const g2 = makeGrid<2>(p2, w2, N2, vals2, useGradient ? grads2 : nullptr, nb);
+    int64_t const n4 = int64_t(nb) * nb * nb * nb;
+    withKernel(kernel, u, [&](auto && f) {
+      using R = decltype(f(Cartesian<double> {}, Cartesian<double> {}));
+      if constexpr (std::is_same_v<R, double>) {
+        LVARRAY_ERROR_IF(useGradient, "integrateAllR1R2: a scalar kernel takes the value form");
+        Array4d<cplx> const a = integration::integrateAllR1R2<false>(g1, g2, f);
+        copyOut<cplx, 4>(a, n4, out);
+      } else {
+        LVARRAY_ERROR_IF(!useGradient, "integrateAllR1R2: a vector kernel takes the gradient form");
+        Array4d<cplx> const a = integration::integrateAllR1R2<true>(g1, g2, f);
+        copyOut<cplx, 4>(a, n4, out);
+      }
+    });
+    return 0;
+  });
+}
+
+// threeElectronIntegrals with the Ochi Jastrow factor: r1, r2 3-D grids; answer [nb]^6 complex
+int tcscf_ref_three_electron_integrals(double const * p1, double const * w1, int64_t N1, double const * vals1, double const * p2,
+                                       double const * w2, int64_t N2, double const * vals2, int nb, OchiParams const * up, double * out)
+{
+  return guarded([&] {
+    auto const g1 = makeGrid<3>(p1, w1, N1, vals1, nullptr, nb);
+    auto const g2 = makeGrid<3>(p2, w2, N2, vals2, nullptr, nb);
+    jastrowFunctions::Ochi<double> const u = makeOchi(*up);
+    Array6d<cplx> const a = integration::threeElectronIntegrals(g1, g2, u);
+    int64_t const n6 = int64_t(nb) * nb * nb * nb * nb * nb;
+    copyOut<cplx, 6>(a, n6, out);
+    return 0;
+  });
+}
+
+// internal::computeQ: Q same-same, same-opposite, opposite-opposite [nb]^6 complex from the grad-u
+// tensors Vs, Vo [N1][nb][nb][3] complex, the r1 weights and basis values [N1][nb] complex
+int tcscf_ref_compute_q(int64_t N1, int nb, double const * w1, double const * vals1, double const * Vs, double const * Vo, double * Qss,
+                        double * Qso, double * Qoo)
+{
+  return guarded([&] {
+    Array1d<double> W(N1);
+    Array2d<cplx> B(N1, nb);
+    Array3d<Cartesian<cplx>> S3(N1, nb, nb), O3(N1, nb, nb);
+    for (int64_t a = 0; a < N1; ++a) {
+      W(a) = w1[a];
+      for (int b = 0; b < nb; ++b) B(a, b) = cplx(vals1[2 * (a * nb + b)], vals1[2 * (a * nb + b) + 1]);
+      for (int j = 0; j < nb; ++j)
+        for (int i = 0; i < nb; ++i) {
+          int64_t const k = (a * nb + j) * nb + i;
+          double const * s = Vs + 6 * k;
+          double const * o = Vo + 6 * k;
+          S3(a, j, i) = Cartesian<cplx> {cplx(s[0], s[1]), cplx(s[2], s[3]), cplx(s[4], s[5])};
+          O3(a, j, i) = Cartesian<cplx> {cplx(o[0], o[1]), cplx(o[2], o[3]), cplx(o[4], o[5])};
+        }
+    }
+    Array6d<cplx> qss(nb, nb, nb, nb, nb, nb), qso(nb, nb, nb, nb, nb, nb), qoo(nb, nb, nb, nb, nb, nb);
+    internal::computeQ(qss.toView(), qso.toView(), qoo.toView(), S3.toViewConst(), O3.toViewConst(), W.toViewConst(), B.toViewConst());
+    int64_t const n6 = int64_t(nb) * nb * nb * nb * nb * nb;
+    copyOut<cplx, 6>(qss, n6, Qss);
+    copyOut<cplx, 6>(qso, n6, Qso);
+    copyOut<cplx, 6>(qoo, n6, Qoo);
+    return 0;
+  });
+}
+
+// internal::assembleG: G3 [2][nb][nb] complex from the Q tensors and the spin densities [2][nb][nb]
+int tcscf_ref_assemble_g(int nb, double const * Qss, double const * Qso, double const * Qoo, double const * density, double * G3)
+{
+  return guarded([&] {
+    int64_t const n6 = int64_t(nb) * nb * nb * nb * nb * nb;
+    Array6d<cplx> qss(nb, nb, nb, nb, nb, nb), qso(nb, nb, nb, nb, nb, nb), qoo(nb, nb, nb, nb, nb, nb);
+    for (int64_t k = 0; k < n6; ++k) {
+      qss.data()[k] = cplx(Qss[2 * k], Qss[2 * k + 1]);
+      qso.data()[k] = cplx(Qso[2 * k], Qso[2 * k + 1]);
+      qoo.data()[k] = cplx(Qoo[2 * k], Qoo[2 * k + 1]);
+    }
+    Array3d<cplx> D(2, nb, nb), G(2, nb, nb);
+    for (int64_t k = 0; k < 2 * int64_t(nb) * nb; ++k) D.data()[k] = cplx(density[2 * k], density[2 * k + 1]);
+    internal::assembleG(G.toView(), qss.toViewConst(), qso.toViewConst(), qoo.toViewConst(), D.toViewConst());
+    copyOut<cplx, 3>(G, 2 * int64_t(nb) * nb, G3);
+    return 0;
+  });
+}
+
+// loadSTO(directory, basisSet, element, maxL): the number of functions (at most maxOut written to out,
+// family 0), or -1 when the reference's loader rejected the arguments
+int tcscf_ref_load_sto(char const * directory, char const * basisSet, char const * element, int maxL, StoParams * out, int maxOut)
+{
+  try {
+    std::vector<SlaterTypeOrbital<double>> const b = loadSTO(directory, basisSet, element, maxL);
+    for (size_t i = 0; i < b.size() && int(i) < maxOut; ++i) out[i] = StoParams {b[i].alpha, b[i].n, b[i].l, b[i].m, 0};
+    return int(b.size());
+  } catch (std::exception const &) {
+    return -1;
+  }
+}
+
+// the reference's basis-set library directory (basisFunctions/ beside its src/), or "" when the build was
+// not told
+char const * tcscf_ref_basis_library()
+{
+#ifdef TCSCF_REF_BASIS_DIR
+  return TCSCF_REF_BASIS_DIR;
+#else
+  return "";
+#endif
 }
 
 }  // extern "C"

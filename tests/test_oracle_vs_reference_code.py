@@ -13,7 +13,12 @@ against which every GPU path is checked, computes what the reference computes:
   * precomputeIntegrand + computeF (HartreeFock.hpp:23-180) with 1/r12 on 2-D real and 3-D complex r2
     grids and with the TC scalar kernels, and computeV with grad u (HartreeFock.hpp:185-229), the
     kernels being those of the reference's tests (HartreeFockTest.cpp:248-317);
-  * the RCS, UOS and TC SCF drivers (HartreeFock.cpp:785-1362): iteration count, energy and density.
+  * the RCS, UOS and TC SCF drivers (HartreeFock.cpp:785-1362): iteration count, energy and density;
+  * the Ochi and hydrogen-like families (OchiBasis.hpp, HydrogenLikeBasis.hpp): values, Ochi
+    gradients, S and core H on the reference driver's core grid;
+  * the 4- and 6-index tensors integrateAllR1R2 (value and gradient forms) and threeElectronIntegrals
+    (integrateAll.hpp:152-442), and the 3-body verification route computeQ / assembleG
+    (HartreeFock.cpp:613-752).
 The reference's drivers call LAPACK through LvArray; the build gives them the LAPACK the oracle uses.
 """
 from __future__ import annotations
@@ -22,6 +27,7 @@ import numpy as np
 import pytest
 
 import oracle
+from tcscf_b200 import basis as wl
 from tcscf_b200 import ffi, grids
 
 if oracle.ref_lib() is None:
@@ -143,3 +149,112 @@ def test_tc_scf_matches_reference(setting):
     assert st == 0 and loops == it
     assert abs(E - Er) < 1e-12 * abs(Er), (E, Er)
     assert np.abs(D - Dr).max() < 1e-12
+
+
+@pytest.mark.parametrize("family", ["ochi", "hydrogen"])
+def test_basis_families_match_reference(family):
+    """Values on 2-D and 3-D points (Ochi gradients too: the reference has no hydrogen-like gradient),
+    and S / core H as the reference's driver fills them (HartreeFockTest.cpp:363-378); the
+    hydrogen-like overlap, which the reference integrates numerically in 3-D, is compared in the
+    GPU tests against the analytic orthonormality instead."""
+    basis, Z = (wl.ochi_functions(3, 2, 1.7), 2) if family == "ochi" else (wl.hydrogen_functions(3, 2, 2), 2)
+    rng = np.random.default_rng(RNG_SEED + 20)
+    for ndim in (2, 3):
+        pts, _ = oracle.qmc_grid(np.ascontiguousarray(rng.random((ndim, 400))))
+        grads = family == "ochi" and ndim == 3
+        if grads:
+            vo, go = oracle.basis_values(pts, basis, gradients=True)
+            vr, gr = oracle.ref_family_values(pts, basis, gradients=True)
+            assert _rel(go, gr) < 1e-13
+        else:
+            vo = oracle.basis_values(pts, basis)
+            vr = oracle.ref_family_values(pts, basis)
+        assert _rel(vo, vr) < 1e-13
+    S, H = oracle.overlap_core(basis, Z)
+    Sr, Hr = oracle.ref_family_overlap_core(basis, Z)
+    assert _rel(H, Hr) < 1e-13
+    if family == "ochi":
+        assert np.array_equal(S, Sr)
+
+
+@pytest.fixture(scope="module")
+def tensor_grids():
+    """r1: 96 QMC points in 3-D; r2: 400 in (r, theta) with gradients; the basis of the GPU tensor tests."""
+    rng = np.random.default_rng(RNG_SEED + 30)
+    basis = wl.expand(0, [0.8, 1.9]) + wl.expand(1, [1.3])
+    p1, w1 = oracle.qmc_grid(np.ascontiguousarray(rng.random((3, 96))))
+    p2, w2 = oracle.qmc_grid(np.ascontiguousarray(rng.random((2, 400))))
+    v1 = oracle.basis_values(p1, basis)
+    v2, g2 = oracle.basis_values(p2, basis, gradients=True)
+    return basis, p1, w1, v1, p2, w2, v2, g2
+
+
+@pytest.mark.parametrize("kernel", [ffi.K_INV_R12, ffi.K_TC_SCALAR_SAME, ffi.K_GRAD_U_SAME, ffi.K_GRAD_U_OPPO])
+def test_integrate_all_r1r2_matches_reference(tensor_grids, kernel):
+    basis, p1, w1, v1, p2, w2, v2, g2 = tensor_grids
+    grad = kernel >= ffi.K_GRAD_U_SAME
+    u = JASTROW if kernel != ffi.K_INV_R12 else None
+    ours = oracle.integrate_all_r1r2(grad, p1, w1, v1, p2, w2, v2, g2 if grad else None, len(basis), kernel, u)
+    ref = oracle.ref_integrate_all_r1r2(grad, p1, w1, v1, p2, w2, v2, g2 if grad else None, len(basis), kernel, u)
+    assert _rel(ours, ref) < 1e-13
+
+
+def test_three_electron_integrals_match_reference():
+    rng = np.random.default_rng(RNG_SEED + 40)
+    basis = wl.expand(0, [0.9]) + wl.expand(1, [1.4])
+    p1, w1 = oracle.qmc_grid(np.ascontiguousarray(rng.random((3, 60))))
+    p2, w2 = oracle.qmc_grid(np.ascontiguousarray(rng.random((3, 200))))
+    v1, v2 = oracle.basis_values(p1, basis), oracle.basis_values(p2, basis)
+    ours = oracle.three_electron_integrals(p1, w1, v1, p2, w2, v2, len(basis), JASTROW)
+    ref = oracle.ref_three_electron_integrals(p1, w1, v1, p2, w2, v2, len(basis), JASTROW)
+    assert _rel(ours, ref) < 1e-13
+
+
+def test_compute_q_and_assemble_g_match_reference():
+    """computeQ / assembleG on grad-u tensors of a Jastrow factor with c_same = c_opposite / 2 in every
+    term, the convention assembleG itself asserts (Q_so = 2 Q_ss, HartreeFock.cpp:722)."""
+    jastrow = oracle.ochi(1.0, 1.0, [((1, 0, 0), 0.5, 0.25), ((0, 1, 1), 0.1, 0.05), ((2, 0, 0), -0.2, -0.1)])
+    rng = np.random.default_rng(RNG_SEED + 50)
+    basis = wl.expand(0, [0.9, 2.0]) + wl.expand(1, [1.4])
+    nb = len(basis)
+    p1, w1 = oracle.qmc_grid(np.ascontiguousarray(rng.random((3, 50))))
+    p3, w3 = oracle.qmc_grid(np.ascontiguousarray(rng.random((3, 300))))
+    v1, v3 = oracle.basis_values(p1, basis), oracle.basis_values(p3, basis)
+    Vs = oracle.compute_V(p1, p3, w3, v3, nb, ffi.K_GRAD_U_SAME, jastrow)
+    Vo = oracle.compute_V(p1, p3, w3, v3, nb, ffi.K_GRAD_U_OPPO, jastrow)
+    Q = oracle.compute_q(w1, v1, Vs, Vo)
+    Qr = oracle.ref_compute_q(w1, v1, Vs, Vo)
+    for a, b in zip(Q, Qr):
+        assert _rel(a, b) < 1e-13
+    C = [rng.normal(size=(n, nb)) + 1j * rng.normal(size=(n, nb)) for n in (2, 1)]
+    D = np.stack([c.T @ c.conj() for c in C])
+    assert _rel(oracle.assemble_g(*Q, D), oracle.ref_assemble_g(*Q, D)) < 1e-13
+
+
+def test_load_sto_matches_reference_on_its_library():
+    """The product's loadSTO (host code, no GPU) against the reference's (SlaterTypeOrbital.cpp:24-75)
+    on every file of the reference's basis-set library, for each basis set and several l cut-offs:
+    identical function lists (exponents parsed to the same doubles, m expanded -l..l in file order).
+    Files the reference's loader rejects (a shell type beyond f, as in Gd, Th and Ra) and an unknown
+    basis set are rejected by both."""
+    from tcscf_b200 import api
+
+    lib = oracle.ref_basis_library()
+    if lib is None:
+        pytest.skip("the reference build was not given its basis-set library")
+    checked = rejected = 0
+    for basis_set in ("TZ3P", "QZ6P", "ATZ3P", "AQZ6P"):
+        for element in sorted(p.name for p in (lib / basis_set).iterdir() if p.is_file()):
+            for max_l in (0, 1, 3, 99):
+                ref = oracle.ref_load_sto(lib, basis_set, element, max_l)
+                if ref is None:
+                    with pytest.raises(ffi.TcscfError):
+                        api.loadSTO(lib, basis_set, element, max_l)
+                    rejected += 1
+                else:
+                    assert [tuple(f) for f in api.loadSTO(lib, basis_set, element, max_l)] == ref, (basis_set, element, max_l)
+                checked += 1
+    assert checked > 1000 and rejected < checked // 10
+    assert oracle.ref_load_sto(lib, "XZ9P", "He", 3) is None
+    with pytest.raises(ffi.TcscfError):
+        api.loadSTO(lib, "XZ9P", "He", 3)
