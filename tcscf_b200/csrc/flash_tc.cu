@@ -667,9 +667,10 @@ __global__ void kPackCoordPairs(int64_t n, int64_t npad, const double * pts, con
 // r1 tile's diagonal, which the tensor kernel skips, added to the potential:
 //   VH[r] += sum_{j < BM tile(r)} g(r, j) c(j)
 // with the tensor kernel's FP32 arithmetic on the same packed points (its drop rule and its
-// Newton-refined rsqrt), FP32 sums per 64-point block added in FP64.  One block of 64 threads per r1
-// tile, the tiles with the most pairs first; each thread takes two rows of the tile (r and r + 64), so
-// that every r2 point it loads serves both.
+// Newton-refined rsqrt), FP32 sums per 64-point block added in FP64.  One block of 64 threads per
+// (r1 tile, chunk of its lower r2 blocks), the tiles with the most pairs first; each thread takes two
+// rows of the tile (r and r + 64), so that every r2 point it loads serves both.  Each chunk's row sums
+// go to an FP64 partial, and the partials of a row are added in chunk order (deterministic).
 __device__ __forceinline__ uint64_t coulombPair(uint64_t px, uint64_t py, uint64_t pz, float thr, float4 qa, float4 qb)
 {
   uint64_t const mOne = f2pack(-1.0f, -1.0f), mHalf = f2pack(-0.5f, -0.5f);
@@ -689,9 +690,10 @@ __device__ __forceinline__ uint64_t coulombPair(uint64_t px, uint64_t py, uint64
   return f2pack(ya, yb);
 }
 
-// the lower rows of one r1 tile (tile >= 1) of one contraction
-__device__ __forceinline__ void coulombLowerTile(int tile, int64_t n1, const float4 * __restrict__ r1xyz, const float4 * __restrict__ r2pairs,
-                                                 double * VH)
+// The lower rows of one r1 tile of one contraction over the r2 blocks [jb, je) (a chunk of the blocks
+// before the tile): out[t] and out[t + 64] receive the two rows' sums (rows r = BM tile + t, r + 64)
+__device__ __forceinline__ void coulombLowerChunk(int tile, int jb, int je, const float4 * __restrict__ r1xyz, const float4 * __restrict__ r2pairs,
+                                                  double * out)
 {
   // the r2 points pass through shared memory in 64-point blocks (64 float4 in pair layout, one per
   // thread), the next block's load in flight while the current one is summed
@@ -702,12 +704,11 @@ __device__ __forceinline__ void coulombLowerTile(int tile, int64_t n1, const flo
   uint64_t const ax = f2pack(pa.x, pa.x), ay = f2pack(pa.y, pa.y), az = f2pack(pa.z, pa.z);
   uint64_t const bx = f2pack(pb.x, pb.x), by = f2pack(pb.y, pb.y), bz = f2pack(pb.z, pb.z);
   double vha = 0.0, vhb = 0.0;
-  int const nBlk = tile * (BM / BK);   // the points [0, BM tile) in 64-point blocks
-  if (nBlk > 0) sq[0][t] = r2pairs[t];
+  if (je > jb) sq[0][t] = r2pairs[int64_t(jb) * BK + t];
   __syncthreads();
-  for (int j = 0; j < nBlk; ++j) {
-    int const buf = j & 1;
-    bool const more = j + 1 < nBlk;
+  for (int j = jb; j < je; ++j) {
+    int const buf = (j - jb) & 1;
+    bool const more = j + 1 < je;
     float4 const nxt = more ? r2pairs[int64_t(j + 1) * BK + t] : make_float4(0, 0, 0, 0);
     uint64_t va = 0, vb = 0;
 #pragma unroll 4
@@ -725,14 +726,43 @@ __device__ __forceinline__ void coulombLowerTile(int tile, int64_t n1, const flo
     if (more) sq[buf ^ 1][t] = nxt;   // block j - 1's buffer: every thread finished it before the last barrier
     __syncthreads();
   }
-  if (r0 < n1) VH[r0] += vha;
-  if (r1 < n1) VH[r1] += vhb;
+  out[t] = vha;
+  out[t + BM / 2] = vhb;
 }
 
-__global__ void __launch_bounds__(BM / 2) kCoulombLower(int nTiles, int64_t n1, const float4 * __restrict__ r1xyz,
-                                                       const float4 * __restrict__ r2pairs, double * VH)
+// The lower blocks of tile p (its 2 p r2 blocks before the diagonal) in kLowerChunks chunks, chunk c the
+// blocks [c 2p / S, (c + 1) 2p / S): heavy tiles in short pieces, so that no single block's work sets
+// the kernel's tail
+constexpr int kLowerChunks = 8;
+__device__ __forceinline__ void lowerChunkRange(int tile, int c, int & jb, int & je)
 {
-  coulombLowerTile(nTiles - 1 - int(blockIdx.x), n1, r1xyz, r2pairs, VH);
+  int const n = tile * (BM / BK);
+  jb = int(int64_t(n) * c / kLowerChunks);
+  je = int(int64_t(n) * (c + 1) / kLowerChunks);
+}
+
+// one block per (tile >= 1, chunk), the tiles with the most pairs first: the chunk's row sums into
+// part[((tile - 1) kLowerChunks + chunk) BM + row]
+__global__ void __launch_bounds__(BM / 2) kCoulombLower(int nTiles, const float4 * __restrict__ r1xyz, const float4 * __restrict__ r2pairs,
+                                                       double * part)
+{
+  int const tile = nTiles - 1 - int(blockIdx.x) / kLowerChunks, c = int(blockIdx.x) % kLowerChunks;
+  int jb, je;
+  lowerChunkRange(tile, c, jb, je);
+  coulombLowerChunk(tile, jb, je, r1xyz, r2pairs, part + (int64_t(tile - 1) * kLowerChunks + c) * BM);
+}
+
+// VH[r] += the chunk sums of row r in chunk order, for the rows of tiles >= 1
+__global__ void kCoulombLowerSum(int64_t n1, const double * __restrict__ part, double * VH)
+{
+  for (int64_t r = BM + blockIdx.x * int64_t(blockDim.x) + threadIdx.x; r < n1; r += int64_t(gridDim.x) * blockDim.x) {
+    int64_t const tile = r / BM;
+    double const * q = part + (tile - 1) * kLowerChunks * BM + r % BM;
+    double s = 0.0;
+#pragma unroll
+    for (int c = 0; c < kLowerChunks; ++c) s += q[c * BM];
+    VH[r] += s;
+  }
 }
 
 // the lower rows of several contractions in one launch: block b takes tile tiles[b].y of job tiles[b].x
@@ -743,11 +773,32 @@ struct CoulombLowerJob {
   double * VH;
   int64_t n1;
 };
-__global__ void __launch_bounds__(BM / 2) kCoulombLowerBatch(const CoulombLowerJob * __restrict__ jobs, const int2 * __restrict__ tiles)
+// one block per (listed (job, tile), chunk): the chunk's row sums into part[(entry kLowerChunks + chunk) BM + row]
+__global__ void __launch_bounds__(BM / 2) kCoulombLowerBatch(const CoulombLowerJob * __restrict__ jobs, const int2 * __restrict__ tiles,
+                                                            double * part)
+{
+  int const entry = int(blockIdx.x) / kLowerChunks, c = int(blockIdx.x) % kLowerChunks;
+  int2 const jt = tiles[entry];
+  CoulombLowerJob const j = jobs[jt.x];
+  int jb, je;
+  lowerChunkRange(jt.y, c, jb, je);
+  coulombLowerChunk(jt.y, jb, je, j.r1xyz, j.r2pairs, part + (int64_t(entry) * kLowerChunks + c) * BM);
+}
+
+// VH[r] += the chunk sums of the listed (job, tile)'s rows in chunk order; one block of BM threads per entry
+__global__ void __launch_bounds__(BM) kCoulombLowerBatchSum(const CoulombLowerJob * __restrict__ jobs, const int2 * __restrict__ tiles,
+                                                           const double * __restrict__ part)
 {
   int2 const jt = tiles[blockIdx.x];
   CoulombLowerJob const j = jobs[jt.x];
-  coulombLowerTile(jt.y, j.n1, j.r1xyz, j.r2pairs, j.VH);
+  int const t = threadIdx.x;
+  int64_t const r = int64_t(jt.y) * BM + t;
+  if (r >= j.n1) return;
+  double const * q = part + int64_t(blockIdx.x) * kLowerChunks * BM + t;
+  double s = 0.0;
+#pragma unroll
+  for (int c = 0; c < kLowerChunks; ++c) s += q[c * BM];
+  j.VH[r] += s;
 }
 
 }  // namespace tc
@@ -1068,11 +1119,20 @@ int tensorPrepare(tcscf_ctx * ctx, Contraction const & c, int precision, void * 
 }
 
 namespace {
-// the Coulomb row sums a symmetric instance skipped (kCoulombLower), once c.VH holds the rest
-int coulombLower(tcscf_ctx * ctx, tc::Instance const & I, Contraction const & c)
+// whether a contraction has Coulomb rows below its diagonal tiles to add (symmetric, with a potential)
+bool hasLowerRows(tc::Instance const & I, Contraction const & c) { return I.sym && c.VH && I.nTiles >= 2; }
+// bytes of the chunk partials of kCoulombLower for nTiles r1 tiles (or of kCoulombLowerBatch for that
+// many listed tiles)
+size_t lowerPartBytes(int64_t nTiles) { return size_t(std::max<int64_t>(nTiles, 1)) * tc::kLowerChunks * tc::BM * sizeof(double); }
+
+// the Coulomb row sums a symmetric instance skipped, once c.VH holds the rest: the chunks of every tile
+// (kCoulombLower) into part (lowerPartBytes(nTiles - 1)), then their sums in chunk order
+int coulombLower(tcscf_ctx * ctx, tc::Instance const & I, Contraction const & c, double * part)
 {
-  if (!I.sym || !c.VH || I.nTiles < 2) return TCSCF_OK;
-  tc::kCoulombLower<<<unsigned(I.nTiles), tc::BM / 2, 0, ctx->stream>>>(I.nTiles, c.n1, I.r1xyz, I.r2pairs, c.VH);
+  if (!hasLowerRows(I, c)) return TCSCF_OK;
+  tc::kCoulombLower<<<unsigned((I.nTiles - 1) * tc::kLowerChunks), tc::BM / 2, 0, ctx->stream>>>(I.nTiles, I.r1xyz, I.r2pairs, part);
+  TCSCF_LAUNCH(ctx);
+  tc::kCoulombLowerSum<<<gridBlocks(c.n1, 256), 256, 0, ctx->stream>>>(c.n1, part, c.VH);
   TCSCF_LAUNCH(ctx);
   return TCSCF_OK;
 }
@@ -1183,8 +1243,12 @@ int tensorRun(tcscf_ctx * ctx, TensorPrep * const * preps, int count, bool recor
       if (c.VH) TCSCF_TRY(sumSplitsLaunch(ctx, c.n1, I.nSplit, c.n1, I.VH, c.VH, c.n1, 1, 1, 1));
     }
     if (count == 1) {
-      TCSCF_TRY(coulombLower(ctx, I, c));
-    } else if (I.sym && c.VH && I.nTiles >= 2) {
+      if (hasLowerRows(I, c)) {
+        void * q = nullptr;
+        TCSCF_TRY(scratch(ctx, "coulomb_lower_partials", lowerPartBytes(I.nTiles - 1), &q));
+        TCSCF_TRY(coulombLower(ctx, I, c, static_cast<double *>(q)));
+      }
+    } else if (hasLowerRows(I, c)) {
       for (int t = 1; t < I.nTiles; ++t) lowerTiles.push_back(make_int2(int(jobs.size()), t));
       jobs.push_back({I.r1xyz, I.r2pairs, c.VH, c.n1});
     }
@@ -1193,12 +1257,16 @@ int tensorRun(tcscf_ctx * ctx, TensorPrep * const * preps, int count, bool recor
     // the lower Coulomb rows of all symmetric instances in one launch, the tiles with the most pairs first
     std::stable_sort(lowerTiles.begin(), lowerTiles.end(), [](int2 const & a, int2 const & b) { return a.y > b.y; });
     void * q = nullptr;
-    TCSCF_TRY(scratch(ctx, "coulomb_lower_jobs", align256(sizeof(tc::CoulombLowerJob) * jobs.size()) + sizeof(int2) * lowerTiles.size() + 256, &q));
+    size_t const jobBytes = align256(sizeof(tc::CoulombLowerJob) * jobs.size()), tileBytes = align256(sizeof(int2) * lowerTiles.size());
+    TCSCF_TRY(scratch(ctx, "coulomb_lower_jobs", jobBytes + tileBytes + lowerPartBytes(int64_t(lowerTiles.size())) + 256, &q));
     auto * dJobs = static_cast<tc::CoulombLowerJob *>(q);
-    auto * dTiles = reinterpret_cast<int2 *>(static_cast<char *>(q) + align256(sizeof(tc::CoulombLowerJob) * jobs.size()));
+    auto * dTiles = reinterpret_cast<int2 *>(static_cast<char *>(q) + jobBytes);
+    auto * dPart = reinterpret_cast<double *>(static_cast<char *>(q) + jobBytes + tileBytes);
     TCSCF_CUDA(ctx, cudaMemcpyAsync(dJobs, jobs.data(), sizeof(tc::CoulombLowerJob) * jobs.size(), cudaMemcpyHostToDevice, ctx->stream));
     TCSCF_CUDA(ctx, cudaMemcpyAsync(dTiles, lowerTiles.data(), sizeof(int2) * lowerTiles.size(), cudaMemcpyHostToDevice, ctx->stream));
-    tc::kCoulombLowerBatch<<<unsigned(lowerTiles.size()), tc::BM / 2, 0, ctx->stream>>>(dJobs, dTiles);
+    tc::kCoulombLowerBatch<<<unsigned(lowerTiles.size() * tc::kLowerChunks), tc::BM / 2, 0, ctx->stream>>>(dJobs, dTiles, dPart);
+    TCSCF_LAUNCH(ctx);
+    tc::kCoulombLowerBatchSum<<<unsigned(lowerTiles.size()), tc::BM, 0, ctx->stream>>>(dJobs, dTiles, dPart);
     TCSCF_LAUNCH(ctx);
     TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));   // the host lists are consumed before they go out of scope
   }
@@ -1226,6 +1294,13 @@ int tensorPlanUpload(tcscf_ctx * ctx, TensorPrep & tp, char const * scratchName,
   plan.inst = dInst;
   plan.status = dStatus;
   plan.prep = &tp;
+  plan.lowerPart = nullptr;
+  if (hasLowerRows(tp.inst, tp.c)) {
+    // the lower rows' chunk partials, allocated here because the launches may be captured in a graph
+    void * q = nullptr;
+    TCSCF_TRY(scratch(ctx, (std::string(scratchName) + "_lower").c_str(), lowerPartBytes(tp.inst.nTiles - 1), &q));
+    plan.lowerPart = static_cast<double *>(q);
+  }
   return TCSCF_OK;
 }
 
@@ -1244,7 +1319,7 @@ int tensorPlanLaunch(tcscf_ctx * ctx, TensorPlan const & plan)
     TCSCF_TRY(sumSplitsLaunch(ctx, n, I.nSplit, int64_t(c.n1) * c.ldt, I.T, c.T, c.n1, c.ncol, c.ldt, c.ldt));
     if (c.VH) TCSCF_TRY(sumSplitsLaunch(ctx, c.n1, I.nSplit, c.n1, I.VH, c.VH, c.n1, 1, 1, 1));
   }
-  return coulombLower(ctx, I, c);
+  return coulombLower(ctx, I, c, plan.lowerPart);
 }
 
 namespace {

@@ -136,6 +136,7 @@ struct TensorPlan {
   int NB = 0, RP = 0, XS = 0, NS = 0, grid = 0, nItems = 0;
   const void * inst = nullptr;
   int * status = nullptr;
+  double * lowerPart = nullptr;   // chunk partials of the Coulomb rows below the diagonal tiles (symmetric instances)
   TensorPrep * prep = nullptr;
 };
 int tensorPlanUpload(tcscf_ctx * ctx, TensorPrep & tp, char const * scratchName, TensorPlan & plan);
