@@ -1138,6 +1138,31 @@ int coulombLower(tcscf_ctx * ctx, tc::Instance const & I, Contraction const & c,
 }
 }  // namespace
 
+// Work items of one persistent launch, weighed by their r2 blocks (a symmetric instance's tiles start at
+// their diagonal, so their items shrink with the tile index), sorted with the most blocks first and put
+// in snake order over rounds of `grid` items: the kernel deals item i to CTA i % grid, so round r goes to
+// CTAs 0, 1, ... when r is even and in reverse when r is odd, and every CTA gets about the same number
+// of blocks (Kr symmetric build: the busiest CTA 0.2 % above the mean, against 4.7 % for tiles in order).
+// The order changes no result: every item writes its own rows of its own split.
+void dealItems(std::vector<int4> & items, int grid)
+{
+  std::stable_sort(items.begin(), items.end(), [](int4 const & a, int4 const & b) { return a.w > b.w; });
+  size_t const g = size_t(std::max(grid, 1));
+  for (size_t r0 = 0; r0 < items.size(); r0 += g)
+    if ((r0 / g) % 2 == 1) std::reverse(items.begin() + int64_t(r0), items.begin() + int64_t(std::min(items.size(), r0 + g)));
+}
+
+// the work items (instance k, tile, split, r2 blocks) of one prepared contraction
+void appendItems(std::vector<int4> & items, int k, tc::Instance const & I)
+{
+  for (int t = 0; t < I.nTiles; ++t)
+    for (int sp = 0; sp < I.nSplit; ++sp) {
+      int jb, je;
+      tc::itemBlocks(I, t, sp, jb, je);
+      items.push_back(make_int4(k, t, sp, je - jb));
+    }
+}
+
 int tensorRun(tcscf_ctx * ctx, TensorPrep * const * preps, int count, bool recordStart)
 {
   int const sms = smCount();
@@ -1163,7 +1188,7 @@ int tensorRun(tcscf_ctx * ctx, TensorPrep * const * preps, int count, bool recor
   TCSCF_CUDA(ctx, cudaMemcpyAsync(dMaps, hMaps.data(), sizeof(CUtensorMap) * hMaps.size(), cudaMemcpyHostToDevice, ctx->stream));
   TCSCF_CUDA(ctx, cudaMemsetAsync(dStatus, 0, sizeof(int), ctx->stream));
 
-  // one persistent launch per tile class; within it, work items longest first, dealt round-robin
+  // one persistent launch per tile class; within it, the work items dealt by dealItems
   struct Launch {
     int NB, RP, XS, NS, grid;
     tc::Params P;
@@ -1176,19 +1201,18 @@ int tensorRun(tcscf_ctx * ctx, TensorPrep * const * preps, int count, bool recor
     std::vector<int4> items;
     for (int k = 0; k < count; ++k) {
       if (preps[k]->NB != NB || preps[k]->RP != RP || preps[k]->XS != XS || preps[k]->NS != NS) continue;
-      tc::Instance const & I = preps[k]->inst;
-      for (int t = 0; t < I.nTiles; ++t)
-        for (int sp = 0; sp < I.nSplit; ++sp) items.push_back(make_int4(k, t, sp, std::min(I.nBlocks - sp * I.blocksPerSplit, I.blocksPerSplit)));
+      appendItems(items, k, preps[k]->inst);
     }
     if (items.empty()) continue;
-    std::stable_sort(items.begin(), items.end(), [](int4 const & a, int4 const & b) { return a.w > b.w; });
+    int const grid = std::min(int(items.size()), sms);
+    dealItems(items, grid);
     TCSCF_CUDA(ctx, cudaMemcpyAsync(dItems + offset, items.data(), sizeof(int4) * items.size(), cudaMemcpyHostToDevice, ctx->stream));
     tc::Params P{};
     P.nItems = int(items.size());
-    P.items = count == 1 ? nullptr : dItems + offset;
+    P.items = dItems + offset;
     P.inst = dInst;
     P.status = dStatus;
-    launches.push_back({NB, RP, XS, NS, std::min(int(items.size()), sms), P});
+    launches.push_back({NB, RP, XS, NS, grid, P});
     offset += items.size();
   }
   if (count == 1) {
@@ -1275,22 +1299,30 @@ int tensorRun(tcscf_ctx * ctx, TensorPrep * const * preps, int count, bool recor
 
 int tensorPlanUpload(tcscf_ctx * ctx, TensorPrep & tp, char const * scratchName, TensorPlan & plan)
 {
+  std::vector<int4> items;
+  appendItems(items, 0, tp.inst);
+  int const grid = std::min(int(items.size()), smCount());
+  dealItems(items, grid);
   size_t const instBytes = align256(sizeof(tc::Instance));
   size_t const mapBytes = align256(sizeof(CUtensorMap) * tc::kMapsPerInstance);
+  size_t const itemBytes = align256(sizeof(int4) * items.size());
   void * p = nullptr;
-  TCSCF_TRY(scratch(ctx, scratchName, instBytes + mapBytes + 256, &p));
+  TCSCF_TRY(scratch(ctx, scratchName, instBytes + mapBytes + itemBytes + 256, &p));
   auto * dInst = static_cast<tc::Instance *>(p);
   auto * dMaps = reinterpret_cast<CUtensorMap *>(static_cast<char *>(p) + instBytes);
-  int * dStatus = reinterpret_cast<int *>(static_cast<char *>(p) + instBytes + mapBytes);
+  auto * dItems = reinterpret_cast<int4 *>(static_cast<char *>(p) + instBytes + mapBytes);
+  int * dStatus = reinterpret_cast<int *>(static_cast<char *>(p) + instBytes + mapBytes + itemBytes);
   tc::Instance hInst = tp.inst;
   hInst.maps = dMaps;
   TCSCF_CUDA(ctx, cudaMemcpyAsync(dInst, &hInst, sizeof(tc::Instance), cudaMemcpyHostToDevice, ctx->stream));
   TCSCF_CUDA(ctx, cudaMemcpyAsync(dMaps, tp.maps, sizeof(CUtensorMap) * tc::kMapsPerInstance, cudaMemcpyHostToDevice, ctx->stream));
+  TCSCF_CUDA(ctx, cudaMemcpyAsync(dItems, items.data(), sizeof(int4) * items.size(), cudaMemcpyHostToDevice, ctx->stream));
   TCSCF_CUDA(ctx, cudaMemsetAsync(dStatus, 0, sizeof(int), ctx->stream));
   TCSCF_CUDA(ctx, cudaStreamSynchronize(ctx->stream));   // the host copies are consumed before they go out of scope
   plan.NB = tp.NB; plan.RP = tp.RP; plan.XS = tp.XS; plan.NS = tp.NS;
-  plan.nItems = tp.inst.nTiles * tp.inst.nSplit;
-  plan.grid = std::min(plan.nItems, smCount());
+  plan.nItems = int(items.size());
+  plan.grid = grid;
+  plan.items = dItems;
   plan.inst = dInst;
   plan.status = dStatus;
   plan.prep = &tp;
@@ -1308,7 +1340,7 @@ int tensorPlanLaunch(tcscf_ctx * ctx, TensorPlan const & plan)
 {
   tc::Params P{};
   P.nItems = plan.nItems;
-  P.items = nullptr;   // one instance: item = tile * nSplit + split
+  P.items = static_cast<int4 const *>(plan.items);
   P.inst = static_cast<tc::Instance const *>(plan.inst);
   P.status = plan.status;
   TCSCF_TRY(launchClass(ctx, plan.NB, plan.RP, plan.XS, plan.NS, P, plan.grid));

@@ -136,6 +136,7 @@ struct TensorPlan {
   int NB = 0, RP = 0, XS = 0, NS = 0, grid = 0, nItems = 0;
   const void * inst = nullptr;
   int * status = nullptr;
+  const void * items = nullptr;   // the work items (int4) in the order the persistent CTAs take them
   double * lowerPart = nullptr;   // chunk partials of the Coulomb rows below the diagonal tiles (symmetric instances)
   TensorPrep * prep = nullptr;
 };
