@@ -611,8 +611,10 @@ int sumSplitsLaunch(tcscf_ctx * ctx, int64_t n, int nsplit, int64_t stride, cons
 int reduceFockReal(tcscf_ctx * ctx, int64_t n1, int nb, const double * phi, const double * w1, const double * VH, double cJ,
                    const double * T, int ldt, double sgnT, double * out)
 {
-  // output tile 64 wide when nb <= 64; row chunks sized for about two blocks per SM (16 to 1024 rows)
-  int const W = nb <= 64 ? 64 : 128;
+  // output tiles 64 wide (70 registers a thread: three blocks per SM, where the 128-wide tile's 168
+  // allowed one, whose global-to-shared staging then stalled its FP64 FMAs); row chunks sized for about
+  // two blocks per SM per output tile (16 to 1024 rows)
+  int const W = 64;
   int const g = (nb + W - 1) / W;
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
