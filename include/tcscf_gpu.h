@@ -267,6 +267,13 @@ int tcscf_autotune_stats(tcscf_ctx * ctx, int * shapes, int * batches, int * mea
  * the default rule's first, then 1, 2, 3, 4, 6, 8 while every split keeps at least 16 r2 blocks of 64
  * points (effective counts, no repeats); writes at most capacity of them and their number to count */
 int tcscf_autotune_split_candidates(int64_t n1, int64_t n2, int sms, int * splits, int capacity, int * count);
+/* host only: the order in which the persistent tensor-core launch over one instance of n1 x n2 points
+ * (sym != 0: one grid as r1 and r2, each r1 tile from its diagonal r2 block on) with nsplit r2 splits
+ * hands out its work items to grid CTAs, CTA b taking items b, b + grid, ...: the items weighed by their
+ * r2 blocks, the most first, in snake order over rounds of grid items.  Writes tile, split and r2 block
+ * count (3 ints) of at most capacity items, in that order, and the item count to count.  No reference
+ * counterpart (launch scheduling). */
+int tcscf_schedule_items(int64_t n1, int64_t n2, int sym, int nsplit, int grid, int * items, int capacity, int * count);
 
 /* ---- SCF drivers (RCSHartreeFock/UOSHartreeFock::compute, HartreeFock.cpp:785-1003) ---------- */
 /* Options of tcscf_scf on this context (no reference counterpart; the defaults, 0 and 0, reproduce

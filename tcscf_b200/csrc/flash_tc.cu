@@ -1163,6 +1163,29 @@ void appendItems(std::vector<int4> & items, int k, tc::Instance const & I)
     }
 }
 
+extern "C" int tcscf_schedule_items(int64_t n1, int64_t n2, int sym, int nsplit, int grid, int * items, int capacity, int * count)
+{
+  if (n1 <= 0 || n2 <= 0 || nsplit <= 0 || grid <= 0 || !count || capacity < 0 || (capacity > 0 && !items)) return TCSCF_ERR_INVALID_ARGUMENT;
+  if (n1 > (int64_t(1) << 36) || n2 > (int64_t(1) << 36)) return TCSCF_ERR_INVALID_ARGUMENT;   // tile and block counts stay int
+  tc::Instance I{};
+  I.nTiles = int((n1 + tc::BM - 1) / tc::BM);
+  I.nBlocks = int((n2 + tc::BK - 1) / tc::BK);
+  I.blocksPerSplit = (I.nBlocks + nsplit - 1) / nsplit;
+  I.nSplit = (I.nBlocks + I.blocksPerSplit - 1) / I.blocksPerSplit;
+  I.sym = sym != 0;
+  std::vector<int4> v;
+  appendItems(v, 0, I);
+  dealItems(v, std::min(grid, int(v.size())));
+  int const n = std::min<int>(capacity, int(v.size()));
+  for (int i = 0; i < n; ++i) {
+    items[3 * i] = v[size_t(i)].y;
+    items[3 * i + 1] = v[size_t(i)].z;
+    items[3 * i + 2] = v[size_t(i)].w;
+  }
+  *count = int(v.size());
+  return TCSCF_OK;
+}
+
 int tensorRun(tcscf_ctx * ctx, TensorPrep * const * preps, int count, bool recordStart)
 {
   int const sms = smCount();

@@ -75,6 +75,7 @@ SIGNATURES: dict[str, tuple] = {
     "tcscf_set_autotune": (_I, [_P, _I]),
     "tcscf_autotune_stats": (_I, [_P, C.POINTER(_I), C.POINTER(_I), C.POINTER(_I)]),
     "tcscf_autotune_split_candidates": (_I, [C.c_int64, C.c_int64, _I, C.POINTER(_I), _I, C.POINTER(_I)]),
+    "tcscf_schedule_items": (_I, [C.c_int64, C.c_int64, _I, _I, _I, C.POINTER(_I), _I, C.POINTER(_I)]),
     "tcscf_tc_compute_q": (_I, [_P, _I, _I, _I, _D, _D, _D]),
     "tcscf_tc_assemble_g": (_I, [_P, _I, _D, _D, _D, _D, _D]),
     "tcscf_tc_scf": (_I, [_P, _I, _I, _I, _I, _I, _D, _D, _I, _I, _I, C.c_double, _I, _D, C.POINTER(_I), _D, _D]),
