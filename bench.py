@@ -382,11 +382,12 @@ METRIC = "Fock-build s/iter, mixed vs FP64 GPU at |dE|<=1 uEh; % of roofline"
 # once per (r1 tile, r2 block) unit where L2 misses, so the figure scales with the unit count,
 # 3172 x 6344 at 406,000 points against 2062 x 4124 (x 2.366), to 2.889e10 B
 TRAFFIC_BYTES_PER_LAUNCH = {"Kr": 2.889e10}
-# The symmetric launch (r1 = r2 grid, psi1 = psi2) of the same kernel moves more DRAM bytes per pair: its
-# r1 tiles start their r2 streams at different blocks, so they share less in L2.  One symmetric launch on
-# the 263,900-point grid read 13.57 GB and wrote 0.244 GB for its 3.4848e10 computed pairs:
-# 0.3964 B per pair (3.27e10 B for the 8.245e10 pairs at 406,000 points)
-TRAFFIC_BYTES_PER_PAIR_SYM = {"Kr": 13.814e9 / 3.4848e10}
+# The symmetric launch (r1 = r2 grid, psi1 = psi2) of the same kernel, its work items dealt by weight in
+# snake order (so the CTAs running at a time hold tiles of similar index, whose r2 streams overlap in L2):
+# one launch on the 263,900-point grid read 2.457 GB and wrote 0.237 GB for its 3.4848e10 computed pairs,
+# 0.0773 B per pair (6.37e9 B for the 8.245e10 pairs at 406,000 points).  With the tiles in index order
+# it was 13.81 GB, 0.3964 B per pair.
+TRAFFIC_BYTES_PER_PAIR_SYM = {"Kr": (2.4566e9 + 0.2366e9) / 3.4848e10}
 
 
 def run_ours(args, rank: int, world: int) -> None:

@@ -68,7 +68,7 @@ def test_symmetric_pair_counts_and_roofline():
     # ... and a per-pair figure measured on a symmetric launch takes precedence
     rs = bench.roofline(ffi.PREC_BF16X3, n, KR["nb"], KR["nocc"], 233.6, bench.PEAKS_FALLBACK, "fallback", 2.889e10, sym=True,
                         traffic_per_pair_sym=bench.TRAFFIC_BYTES_PER_PAIR_SYM["Kr"])
-    assert rs["traffic"] == pytest.approx(13.814e9 / 3.4848e10 * 82_450_481_152)
+    assert rs["traffic"] == pytest.approx((2.4566e9 + 0.2366e9) / 3.4848e10 * 82_450_481_152)
     f = bench.roofline(ffi.PREC_FP64, n, KR["nb"], KR["nocc"], 1610.0, bench.PEAKS_FALLBACK, "fallback", None, sym=True)
     assert f["symmetric"] and f["achieved"] == pytest.approx(2 * bench.symmetric_pairs(n, fp64=True) * 139 / 1.61 / 1e12)
     # TF32 keeps the full contraction
