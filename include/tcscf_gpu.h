@@ -328,10 +328,13 @@ int tcscf_tc_fock_build(tcscf_ctx * ctx, int r1, int fji_same, int fji_oppo, int
  * tcscf_tc_fock_build, commented out in TCHartreeFock::compute): the 6-index tensors
  * Q[j][p][r][i][q][s] = sum_r1 w (conj(b_j) (V_pq . V_rs) b_i + conj(b_p) (V_ji . V_rs) b_q
  * + conj(b_r) (V_ji . V_pq) b_s) for the same-same, same-opposite and opposite-opposite pairs of the
- * computeV handles vji_same / vji_oppo on the r1 grid.  Outputs complex [nb]^6 row-major (nb <= 16). */
+ * computeV handles vji_same / vji_oppo on the r1 grid.  Outputs complex [nb]^6 row-major.  Limited by
+ * device memory: UNSUPPORTED when its four nb^6 complex buffers (12 GiB at nb = 24) would take more than
+ * 3/4 of the device (and for nb > 46). */
 int tcscf_tc_compute_q(tcscf_ctx * ctx, int r1, int vji_same, int vji_oppo, double * Qss, double * Qso, double * Qoo);
 /* assembleG (HartreeFock.cpp:687-752, without its debugging checks): G3 [2][nb][nb] complex from the
- * three Q tensors and the spin densities [2][nb][nb] complex (element (q, p) at [q][p]). */
+ * three Q tensors and the spin densities [2][nb][nb] complex (element (q, p) at [q][p]).  Limited by
+ * device memory like tcscf_tc_compute_q (three nb^6 complex buffers). */
 int tcscf_tc_assemble_g(tcscf_ctx * ctx, int nb, const double * Qss, const double * Qso, const double * Qoo, const double * density,
                         double * G3);
 

@@ -342,6 +342,18 @@ int tcscf_three_electron_integrals(tcscf_ctx * ctx, int r1, int r2, const tcscf_
   return TCSCF_OK;
 }
 
+// The 6-index tensors are limited by device memory, not by a basis size: UNSUPPORTED when their buffers
+// (bytes) would take more than 3/4 of the device, so that the grids and tensors already resident keep room
+int sixIndexFits(tcscf_ctx * ctx, size_t bytes, char const * what)
+{
+  size_t freeB = 0, totalB = 0;
+  TCSCF_CUDA(ctx, cudaMemGetInfo(&freeB, &totalB));
+  TCSCF_CHECK(ctx, bytes <= totalB / 4 * 3, TCSCF_ERR_UNSUPPORTED,
+              std::string(what) + ": the nb^6 tensors need " + std::to_string(bytes >> 20) + " MiB of device memory, beyond 3/4 of the " +
+                  std::to_string(totalB >> 20) + " MiB on the device");
+  return TCSCF_OK;
+}
+
 int tcscf_tc_compute_q(tcscf_ctx * ctx, int r1, int vsame, int voppo, double * Qss, double * Qso, double * Qoo)
 {
   TCSCF_NVTX();
@@ -356,7 +368,7 @@ int tcscf_tc_compute_q(tcscf_ctx * ctx, int r1, int vsame, int voppo, double * Q
   int const nb = g1->nb;
   TCSCF_CHECK(ctx, itS->second.nb == nb && itO->second.nb == nb && itS->second.n1 == g1->n && itO->second.n1 == g1->n,
               TCSCF_ERR_INVALID_ARGUMENT, "computeQ: the tensors do not match the r1 grid");
-  TCSCF_CHECK(ctx, nb <= 16, TCSCF_ERR_UNSUPPORTED, "computeQ: nb <= 16 (three nb^6 complex tensors)");
+  TCSCF_CHECK(ctx, nb <= 46, TCSCF_ERR_UNSUPPORTED, "computeQ: nb <= 46 (nb^4 stays an int GEMM dimension)");
   int64_t const nn = int64_t(nb) * nb, n4 = nn * nn, n6 = n4 * nn, n1 = g1->n;
   const double2 * Vs = reinterpret_cast<const double2 *>(itS->second.d);
   const double2 * Vo = reinterpret_cast<const double2 *>(itO->second.d);
@@ -364,6 +376,7 @@ int tcscf_tc_compute_q(tcscf_ctx * ctx, int r1, int vsame, int voppo, double * Q
   TCSCF_TRY(blasHandle(ctx, &h));
   int64_t const chunk = std::max<int64_t>(1, std::min<int64_t>(n1, (int64_t(1) << 26) / n4));
   size_t const bytes = sizeof(double2) * (size_t(chunk) * nn + size_t(chunk) * n4 + 4 * size_t(n6));
+  TCSCF_TRY(sixIndexFits(ctx, bytes, "computeQ"));
   void * p = nullptr;
   TCSCF_TRY(scratch(ctx, "compute_q", bytes, &p));
   double2 * X = static_cast<double2 *>(p);
@@ -401,9 +414,10 @@ int tcscf_tc_assemble_g(tcscf_ctx * ctx, int nb, const double * Qss, const doubl
   TCSCF_NVTX();
   if (!ctx) return TCSCF_ERR_INVALID_ARGUMENT;
   cudaSetDevice(ctx->device);
-  TCSCF_CHECK(ctx, nb >= 1 && nb <= 16 && Qss && Qso && Qoo && density && G3, TCSCF_ERR_INVALID_ARGUMENT,
-              "assembleG: nb in 1..16 and all arrays are required");
+  TCSCF_CHECK(ctx, nb >= 1 && Qss && Qso && Qoo && density && G3, TCSCF_ERR_INVALID_ARGUMENT, "assembleG: nb >= 1 and all arrays are required");
+  TCSCF_CHECK(ctx, nb <= 46, TCSCF_ERR_UNSUPPORTED, "assembleG: nb <= 46");
   int64_t const nn = int64_t(nb) * nb, n6 = nn * nn * nn;
+  TCSCF_TRY(sixIndexFits(ctx, sizeof(double2) * (3 * size_t(n6) + 4 * size_t(nn)), "assembleG"));
   void * p = nullptr;
   TCSCF_TRY(scratch(ctx, "assemble_g", sizeof(double2) * (3 * size_t(n6) + 4 * size_t(nn)), &p));
   double2 * Q = static_cast<double2 *>(p);

@@ -166,3 +166,38 @@ def test_tc_fock_build_shapes(ctx, case):
     finally:
         for d in t.values():
             d.close()
+
+
+def test_compute_q_and_assemble_g_beyond_sixteen_functions(ctx):
+    # the 6-index route is limited by device memory rather than a basis size: 18 functions (the old
+    # fixed limit was 16; 3 x 18^6 complex = 1.6 GB per set of Q tensors), against the oracle
+    basis = wl.expand(0, [0.5, 1.1, 2.4, 5.2, 11.0, 23.0]) + wl.expand(1, [0.9, 2.0, 4.4, 9.5])   # 6 + 12 = 18
+    nb = len(basis)
+    g1 = grids.qmc_grid(3, 16, 71)
+    g2 = grids.qmc_grid(3, 256, 72)
+    G1 = api.QMCGrid(ctx, g1)
+    G1.setBasisFunctions(basis)
+    G2 = api.QMCGrid(ctx, g2)
+    G2.setBasisFunctions(basis)
+    u = ffi.ochi_struct(U["a"], U["a12"], U["terms"])
+    uo = oracle.ochi(U["a"], U["a12"], U["terms"])
+    Vs = api.computeV(G1, G2, ffi.K_GRAD_U_SAME, u, keep=True, copy=False)[1]
+    Vo = api.computeV(G1, G2, ffi.K_GRAD_U_OPPO, u, keep=True, copy=False)[1]
+    try:
+        Q = api.tc_compute_q(G1, Vs, Vo)
+    finally:
+        Vs.close()
+        Vo.close()
+    vals2 = oracle.basis_values(g2.points, basis)
+    Vso = oracle.compute_V(g1.points, g2.points, g2.weights, vals2, nb, ffi.K_GRAD_U_SAME, uo)
+    Voo = oracle.compute_V(g1.points, g2.points, g2.weights, vals2, nb, ffi.K_GRAD_U_OPPO, uo)
+    Qr = oracle.compute_q(g1.weights, oracle.basis_values(g1.points, basis), Vso, Voo)
+    for a, b in zip(Q, Qr):
+        np.testing.assert_allclose(a, b, rtol=0, atol=1e-10 * np.abs(b).max())
+    del Q
+    rng = np.random.default_rng(11)
+    occ = [_random_orbitals(nb, n, rng) for n in (NUP, NDOWN)]
+    D = np.stack([c.T @ c.conj() for c in occ])
+    G3 = api.tc_assemble_g(ctx, *Qr, D)
+    G3r = oracle.assemble_g(*Qr, D)
+    np.testing.assert_allclose(G3, G3r, rtol=0, atol=1e-12 * np.abs(G3r).max())
