@@ -456,3 +456,10 @@ def ref_basis_library() -> Path | None:
     f.restype = C.c_char_p
     p = Path(f().decode())
     return p if str(p) and p.is_dir() else None
+
+
+def ref_radial_grid(n: int, map_: int, p0: float = 0.0, p1: float = 0.0):
+    """createGrid(ChebyshevGauss(n), map) of the reference (maps 0-3: None, Linear, XOver1mX, TreutlerAhlrichsM4)."""
+    u, w = np.empty(n), np.empty(n)
+    assert ref_lib().tcscf_ref_radial_grid(n, map_, C.c_double(p0), C.c_double(p1), _p(u), _p(w)) == 0
+    return u, w

@@ -30,6 +30,8 @@
 //   tcscf_ref_integrate_all_r1r2, tcscf_ref_three_electron_integrals  the 4- and 6-index tensors
 //                        (integrateAll.hpp:152-442)
 //   tcscf_ref_compute_q, tcscf_ref_assemble_g  the 3-body verification route (HartreeFock.cpp:613-752)
+//   tcscf_ref_radial_grid  createGrid(ChebyshevGauss(n), map) (quadrature.hpp:75-104, ChebyshevGauss.hpp)
+//                        with the None, Linear, XOver1mX or TreutlerAhlrichsM4 change of variables
 //   tcscf_ref_load_sto   loadSTO (SlaterTypeOrbital.cpp:24-75), and tcscf_ref_basis_library the
 //                        reference's basis-set library directory the build was given
 // Array layouts (row-major, complex as interleaved doubles): points [ndim][N]; weights [N]; basis
@@ -575,6 +577,29 @@ int tcscf_ref_assemble_g(int nb, double const * Qss, double const * Qso, double 
     for (int64_t k = 0; k < 2 * int64_t(nb) * nb; ++k) D.data()[k] = cplx(density[2 * k], density[2 * k + 1]);
     internal::assembleG(G.toView(), qss.toViewConst(), qso.toViewConst(), qoo.toViewConst(), D.toViewConst());
     copyOut<cplx, 3>(G, 2 * int64_t(nb) * nb, G3);
+    return 0;
+  });
+}
+
+// points u [n] and weights w [n] of createGrid(ChebyshevGauss(n), map), map 0 None, 1 Linear(p0),
+// 2 XOver1mX, 3 TreutlerAhlrichsM4(p0, p1)
+int tcscf_ref_radial_grid(int n, int map, double p0, double p1, double * u, double * w)
+{
+  return guarded([&] {
+    using namespace integration;
+    auto store = [&](QuadratureGrid<double> const & g) {
+      LVARRAY_ERROR_IF_NE(g.weights.size(), n);
+      for (int i = 0; i < n; ++i) {
+        u[i] = g.points(0, i);
+        w[i] = g.weights(i);
+      }
+    };
+    ChebyshevGauss<double> const cg(n);
+    if (map == 0) store(createGrid(cg, changeOfVariables::None<double, 1> {}));
+    else if (map == 1) store(createGrid(cg, changeOfVariables::Linear<double> {p0}));
+    else if (map == 2) store(createGrid(cg, changeOfVariables::XOver1mX<double> {}));
+    else if (map == 3) store(createGrid(cg, changeOfVariables::TreutlerAhlrichsM4<double>(p0, p1)));
+    else throw std::runtime_error("radial map not in the reference");
     return 0;
   });
 }

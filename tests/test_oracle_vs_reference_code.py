@@ -258,3 +258,43 @@ def test_load_sto_matches_reference_on_its_library():
     assert oracle.ref_load_sto(lib, "XZ9P", "He", 3) is None
     with pytest.raises(ffi.TcscfError):
         api.loadSTO(lib, "XZ9P", "He", 3)
+
+
+# ---- the product's host code against the reference's, directly ---------------------------------------
+
+@pytest.mark.parametrize("map_,p0,p1", [(ffi.MAP_NONE, 0.0, 0.0), (ffi.MAP_LINEAR, 2.5, 0.0), (ffi.MAP_X_OVER_1MX, 0.0, 0.0),
+                                        (ffi.MAP_TREUTLER_AHLRICHS_M4, 1.0, 0.9)])
+def test_product_radial_grids_match_reference(map_, p0, p1):
+    """tcscf_grid_radial against createGrid(ChebyshevGauss(n), map) of the reference: identical doubles
+    (r = (1+x)/(1-x), the fifth map, is not in the reference)."""
+    for n in (7, 50, 200):
+        u, w = grids.radial_grid(n, map_, p0, p1)
+        ur, wr = oracle.ref_radial_grid(n, map_, p0, p1)
+        assert np.array_equal(u, ur) and np.array_equal(w, wr)
+
+
+@pytest.mark.parametrize("ndim", [2, 3])
+def test_product_qmc_map_matches_reference(ndim):
+    """tcscf_grid_qmc (the map under grids.qmc_grid) against the reference's QMCGrid on the same points."""
+    u = np.ascontiguousarray(np.random.default_rng(RNG_SEED + 60 + ndim).random((ndim, 3000)))
+    pts, w = np.empty_like(u), np.empty(u.shape[1])
+    ffi.check(ffi.lib().tcscf_grid_qmc(ndim, u.shape[1], ffi.dptr(u), ffi.dptr(pts), ffi.dptr(w)))
+    pr, wr = oracle.ref_qmc_grid(u)
+    assert _rel(pts, pr) < 1e-15 and _rel(w, wr) < 1e-14
+
+
+def test_product_analytic_overlap_core_matches_reference():
+    """The product's analytic S and core H (tcscf_overlap_core_analytic) for the STO family, and for the
+    Ochi and hydrogen-like families on the reference driver's core grid (S of the hydrogen-like family
+    is the reference's numerical 3-D overlap, not compared)."""
+    from tcscf_b200 import api
+
+    S, H = api.overlap_core(BASIS_LM, 5)
+    Sr, Hr = oracle.ref_overlap_core(BASIS_LM, 5)
+    assert _rel(S, Sr) < 1e-14 and _rel(H, Hr) < 1e-14
+    for basis in (wl.ochi_functions(3, 2, 1.7), wl.hydrogen_functions(3, 2, 2)):
+        S, H = api.overlap_core(basis, 2)
+        Sr, Hr = oracle.ref_family_overlap_core(basis, 2)
+        assert _rel(H, Hr) < 1e-13
+        if basis[0][4] == 1:
+            assert np.array_equal(S, Sr)
