@@ -1,11 +1,13 @@
-// Minimal stand-in for RAJA as the reference's hot-path sources use it: execution-policy tags, a serial
-// forall over a typed range, atomics and sum reductions that copies of the reducer share (as RAJA's
-// reducers captured by value in a loop body do), and the permutation tags of LvArray arrays.
-// Every loop runs serially in index order, so the oracle's reference build is deterministic.
+// Minimal stand-in for RAJA as the reference's hot-path sources use it: execution-policy tags, forall
+// over a typed range (OpenMP parallel for the omp_parallel_for_exec policy, as RAJA runs it, and in
+// index order otherwise), atomics, and reducers that the copies captured by value in a loop body share
+// (thread-safe), and the permutation tags of LvArray arrays.
 #pragma once
 
 #include <cstddef>
 #include <memory>
+#include <mutex>
+#include <type_traits>
 #include <utility>
 
 namespace camp {
@@ -65,60 +67,81 @@ struct TypedRangeSegment {
 template <typename POLICY, typename INDEX, typename BODY>
 void forall(TypedRangeSegment<INDEX> const & seg, BODY && body)
 {
-  for (INDEX i = seg.begin; i < seg.end; ++i) body(i);
+  if constexpr (std::is_same_v<POLICY, omp_parallel_for_exec>) {
+#pragma omp parallel for schedule(dynamic, 1)
+    for (INDEX i = seg.begin; i < seg.end; ++i) body(i);
+  } else {
+    for (INDEX i = seg.begin; i < seg.end; ++i) body(i);
+  }
 }
 
 template <typename POLICY, typename T, typename U>
 T atomicAdd(T * ptr, U const & value)
 {
-  T const old = *ptr;
-  *ptr += value;
+  T old;
+#pragma omp atomic capture
+  {
+    old = *ptr;
+    *ptr += value;
+  }
   return old;
 }
+
+namespace detail {
+template <typename T>
+struct Shared {
+  explicit Shared(T v) : value(v) {}
+  T value;
+  std::mutex lock;
+};
+}  // namespace detail
 
 template <typename REDUCE, typename T>
 class ReduceSum {
  public:
-  explicit ReduceSum(T init) : m_value(std::make_shared<T>(init)) {}
+  explicit ReduceSum(T init) : m_s(std::make_shared<detail::Shared<T>>(init)) {}
   ReduceSum const & operator+=(T const & v) const
   {
-    *m_value += v;
+    std::lock_guard<std::mutex> g(m_s->lock);
+    m_s->value += v;
     return *this;
   }
-  T get() const { return *m_value; }
-  operator T() const { return *m_value; }
+  T get() const { return m_s->value; }
+  operator T() const { return m_s->value; }
 
  private:
-  std::shared_ptr<T> m_value;
+  std::shared_ptr<detail::Shared<T>> m_s;
 };
 
 template <typename REDUCE, typename T>
 class ReduceMax {
  public:
-  explicit ReduceMax(T init) : m_value(std::make_shared<T>(init)) {}
+  explicit ReduceMax(T init) : m_s(std::make_shared<detail::Shared<T>>(init)) {}
   ReduceMax const & max(T const & v) const
   {
-    if (v > *m_value) *m_value = v;
+    std::lock_guard<std::mutex> g(m_s->lock);
+    if (v > m_s->value) m_s->value = v;
     return *this;
   }
-  T get() const { return *m_value; }
+  T get() const { return m_s->value; }
 
  private:
-  std::shared_ptr<T> m_value;
+  std::shared_ptr<detail::Shared<T>> m_s;
 };
 
 template <typename REDUCE, typename T>
 class ReduceMin {
  public:
-  explicit ReduceMin(T init) : m_value(std::make_shared<T>(init)) {}
+  explicit ReduceMin(T init) : m_s(std::make_shared<detail::Shared<T>>(init)) {}
   ReduceMin const & min(T const & v) const
   {
-    if (v < *m_value) *m_value = v;
+    std::lock_guard<std::mutex> g(m_s->lock);
+    if (v < m_s->value) m_s->value = v;
     return *this;
   }
-  T get() const { return *m_value; }
+  T get() const { return m_s->value; }
 
  private:
-  std::shared_ptr<T> m_value;
+  std::shared_ptr<detail::Shared<T>> m_s;
 };
 }  // namespace RAJA
