@@ -115,25 +115,29 @@ def test_tc_kernels_match_reference(setting):
         assert _rel(oracle.compute_V(p1, p3, w3, v3, nb, k, JASTROW), oracle.ref_compute_V(p1, w1, v1, p3, w3, v3, nb, k, JASTROW)) < 1e-14
 
 
-@pytest.mark.parametrize("nspin,n_up,n_down,Z", [(1, 1, 1, 2), (2, 1, 1, 2), (2, 2, 1, 3)])
-def test_rcs_uos_scf_match_reference(setting, nspin, n_up, n_down, Z):
+@pytest.mark.parametrize("nspin,n_up,n_down,Z,sym", [(1, 1, 1, 2, True), (2, 1, 1, 2, True), (2, 2, 1, 3, True), (1, 1, 1, 2, False),
+                                                     (2, 2, 1, 3, False)])
+def test_rcs_uos_scf_match_reference(setting, nspin, n_up, n_down, Z, sym):
     """RCS He, UOS He and UOS Li (two spin-up electrons, one spin-down) through the reference's
-    drivers (their own 1e-5 stopping rule) and the oracle's restatement of them."""
+    drivers (their own 1e-5 stopping rule) and the oracle's restatement of them, with and without the
+    one-electron symmetry mask of the two-electron terms."""
     p1, w1, p2, w2, _, _ = setting
     nb = len(BASIS_SP)
     v1 = oracle.basis_values(p1, BASIS_SP)
     F = oracle.compute_F(p1, p2, w2, oracle.basis_values(p2, BASIS_SP), nb)
     S, h = oracle.overlap_core(BASIS_SP, Z)
-    st, E, it, D, _ = oracle.scf(nspin, n_up, n_down, F, v1, w1, S, h)
-    loops, Er, Dr = oracle.ref_scf(nspin, n_up, n_down, F, p1, w1, v1, S, h)
+    st, E, it, D, _ = oracle.scf(nspin, n_up, n_down, F, v1, w1, S, h, respect_symmetry=sym)
+    loops, Er, Dr = oracle.ref_scf(nspin, n_up, n_down, F, p1, w1, v1, S, h, respect_symmetry=sym)
     assert st == 0 and loops == it
     assert abs(E - Er) < 1e-12 * abs(Er), (E, Er)
     assert np.abs(D - Dr).max() < 1e-12
 
 
-def test_tc_scf_matches_reference(setting):
+@pytest.mark.parametrize("n_up,n_down,Z", [(1, 1, 2), (2, 1, 3)])
+def test_tc_scf_matches_reference(setting, n_up, n_down, Z):
     """TCHartreeFock::compute (zggev, the sort by real part, the S-metric MGS with its quirk) on the
-    TC tensors of a nonzero Jastrow factor, He with one electron of each spin."""
+    TC tensors of a nonzero Jastrow factor: He with one electron of each spin, and Li with two
+    spin-up electrons and one spin-down."""
     p1, w1, p2, w2, p3, w3 = setting
     nb = len(BASIS_SP)
     v1, g1 = oracle.basis_values(p1, BASIS_SP, gradients=True)
@@ -143,9 +147,9 @@ def test_tc_scf_matches_reference(setting):
     Fo = oracle.compute_F(p1, p2, w2, v2, nb, ffi.K_TC_SCALAR_OPPO, JASTROW)
     Vs = oracle.compute_V(p1, p3, w3, v3, nb, ffi.K_GRAD_U_SAME, JASTROW)
     Vo = oracle.compute_V(p1, p3, w3, v3, nb, ffi.K_GRAD_U_OPPO, JASTROW)
-    S, h = oracle.overlap_core(BASIS_SP, 2)
-    st, E, it, D, _ = oracle.tc_scf(Fs, Fo, Vs, Vo, v1, g1, w1, S, h, 1, 1)
-    loops, Er, Dr = oracle.ref_tc_scf(Fs, Fo, Vs, Vo, p1, w1, v1, g1, S, h, 1, 1)
+    S, h = oracle.overlap_core(BASIS_SP, Z)
+    st, E, it, D, _ = oracle.tc_scf(Fs, Fo, Vs, Vo, v1, g1, w1, S, h, n_up, n_down)
+    loops, Er, Dr = oracle.ref_tc_scf(Fs, Fo, Vs, Vo, p1, w1, v1, g1, S, h, n_up, n_down)
     assert st == 0 and loops == it
     assert abs(E - Er) < 1e-12 * abs(Er), (E, Er)
     assert np.abs(D - Dr).max() < 1e-12
