@@ -333,6 +333,7 @@ def roofline(prec: int, n: int, nb: int, nocc: int, c_ms: float, peaks: dict, pe
                  "pairs": pairs, "symmetric": bool(sym),
                  "full_pairs_tflops": 2.0 * n * n * (nb * nocc + 1) / (c_ms / 1e3) / 1e12,
                  "kernel_algorithm_tflops": kernel_achieved,
+                 "frac_kind": "effective",
                  "frac_note": "frac counts F_alg, the pair-density work the factored form avoids; issued_frac (the "
                               "slice products the tensor pipe executes) and ncu's tensor-pipe activity measure the hardware"}
     if sym and prec != ffi.PREC_FP64 and traffic_per_pair_sym is not None:
